@@ -1,0 +1,200 @@
+/*
+ * wavecore_c.h — C ABI of the B200 implementation of wavecore's time step.
+ *
+ * The reference (mlaegn/wavesim, crate `wavecore`) is a Rust library with no FFI. Each entry
+ * point below replaces one method or builder of its `Solver` / `State` API, cited as
+ * `crates/wavecore/src/<file>.rs:<line>`; a Rust `extern "C"` block can bind this header as is
+ * (INTEGRATION.md shows the binding).
+ *
+ * Conventions shared with the reference:
+ *   - every array is "padded": (nx + 2*WC_GHOST) * (ny + 2*WC_GHOST) values, row-major with y
+ *     outer, interior cells at [WC_GHOST, WC_GHOST+nx) x [WC_GHOST, WC_GHOST+ny)
+ *     (crates/wavecore/src/grid.rs:4-57);
+ *   - host arrays are FP64, owned by the caller (crates/wavecore/src/state.rs:7-17);
+ *   - the bed `b` is metres relative to still water, negative under water
+ *     (crates/wavecore/src/bathymetry.rs:3-9).
+ *
+ * Differences a caller can observe, all deliberate:
+ *   - the device computes in FP32 with a compensated (hi+lo) depth, FP64 reductions and FP64
+ *     mass accumulation; results agree with the FP64 reference to the tolerances documented in
+ *     DESIGN.md, and still water stays exactly still;
+ *   - ghost cells of the bed are taken from the boundary rule (mirrored at walls, wrapped when
+ *     periodic in y), which is what every `Bathymetry` constructor and `with_periodic_y` produce;
+ *     the ghost values the caller passes are not read;
+ *   - on return from wc_step the ghost cells of h/hu/hv hold the boundary fill of the new state
+ *     (the reference leaves a blend that its next step overwrites);
+ *   - setup errors that the reference raises with `assert!`/`panic!` return a status instead.
+ */
+#ifndef WAVECORE_C_H
+#define WAVECORE_C_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Ghost layers on every side: crates/wavecore/src/grid.rs:4. */
+#define WC_GHOST 3
+
+typedef enum wc_status {
+    WC_OK = 0,
+    WC_EINVAL = 1,        /* invalid argument; the reference panics on these (grid.rs:87-91,
+                             forcing.rs:63-66,89-90, solver.rs:377-383) */
+    WC_EPERIODIC = 2,     /* oblique wave-maker does not fit the periodic domain (solver.rs:421-429) */
+    WC_ENAN = 3,          /* the state holds a NaN (stable_dt is NaN, solver.rs:431-450) */
+    WC_EUNCONVERGED = 4,  /* a dispersive solve stopped at max_iterations: reported, not fatal,
+                             as the reference only counts it (dispersion.rs:541-545) */
+    WC_ETIMEOUT = 5,      /* a bounded device wait ran out; the context stays usable */
+    WC_ECUDA = 6,         /* a CUDA runtime call failed */
+    WC_ENOMEM = 7,        /* device allocation failed */
+    WC_EUNSUPPORTED = 8   /* a configuration this build does not implement */
+} wc_status;
+
+/* crates/wavecore/src/grid.rs:12-18 (`Grid { nx, ny, dx, dy }`). */
+typedef struct wc_grid {
+    uint64_t nx, ny;
+    double dx, dy;
+} wc_grid;
+
+/* crates/wavecore/src/solver.rs:34-50 (`Order`). */
+typedef enum wc_order { WC_ORDER_FIRST = 0, WC_ORDER_SECOND = 1, WC_ORDER_FIFTH = 2 } wc_order;
+
+/* crates/wavecore/src/forcing.rs:146-178 (`Sponge`, built by `Sponge::new(width, strength)
+ * .edges(west, east, south, north)`; `level` defaults to 0). */
+typedef struct wc_sponge {
+    uint64_t width;
+    double strength;
+    double level;
+    int32_t west, east, south, north;
+} wc_sponge;
+
+/* crates/wavecore/src/forcing.rs:18-33 (`WaveMaker`). */
+typedef struct wc_wavemaker {
+    double x, amplitude, period, angle, sigma, ramp_periods;
+} wc_wavemaker;
+
+/* crates/wavecore/src/dispersion.rs:44-74 (`Breaking`). The reference's `viscosity`
+ * (followed fronts, crates/wavecore/src/eddy.rs) is not part of this build: it is `None` here. */
+typedef struct wc_breaking {
+    double eta_ratio_lo, eta_ratio_hi;
+    double slope_lo, slope_hi;
+} wc_breaking;
+
+/* Preconditioner of the dispersive solve. JACOBI is the reference's
+ * (dispersion.rs:493-545); LEARNED is this build's network preconditioner (no counterpart in
+ * the reference), run inside flexible CG with the same stopping rule. */
+typedef enum wc_preconditioner { WC_PC_JACOBI = 0, WC_PC_LEARNED = 1 } wc_preconditioner;
+
+/* crates/wavecore/src/dispersion.rs:76-97 (`Dispersion`). */
+typedef struct wc_dispersion {
+    wc_breaking breaking;
+    int32_t nonlinear;
+    double tolerance;
+    uint64_t max_iterations;
+    int32_t preconditioner; /* wc_preconditioner */
+} wc_dispersion;
+
+/* Every builder of `Solver` (crates/wavecore/src/solver.rs:283-419) as one struct. */
+typedef struct wc_config {
+    double cfl;                       /* `Solver::cfl`, default 0.4 (solver.rs:287) */
+    int32_t order;                    /* wc_order, default Second (solver.rs:288, :302-305) */
+    double manning;                   /* `with_manning` (solver.rs:307-311) */
+    int32_t periodic_y;               /* `with_periodic_y` (solver.rs:411-419) */
+    const wc_sponge* sponges;         /* `with_sponge`, repeatable (solver.rs:313-317) */
+    uint64_t n_sponges;
+    const wc_wavemaker* wavemaker;    /* `with_wavemaker` or NULL (solver.rs:319-325) */
+    const wc_dispersion* dispersion;  /* `with_dispersion` or NULL = shallow water (:327-334) */
+    const uint8_t* shallow_cells;     /* `with_shallow_cells` or NULL; nx*ny, y outer (:367-384) */
+} wc_config;
+
+/* crates/wavecore/src/dispersion.rs:99-106 (`DispersionStats`). */
+typedef struct wc_stats {
+    uint64_t solves, iterations, unconverged;
+} wc_stats;
+
+/* crates/wavecore/src/solver.rs:248-258 (`Limiting`): i, j count interior cells from 0. */
+typedef struct wc_limiting {
+    uint64_t i, j;
+    double depth, speed;
+} wc_limiting;
+
+/* crates/wavecore/src/state.rs:78-102 (`volume`, `max_abs_momentum`, `min_depth`). */
+typedef struct wc_diagnostics {
+    double volume, max_abs_momentum, min_depth;
+} wc_diagnostics;
+
+typedef struct wc_solver wc_solver;
+
+/* Defaults of `Solver::new` (solver.rs:283-299): cfl 0.4, Second order, no friction, walls. */
+void wc_config_default(wc_config* cfg);
+/* `Dispersion::default()` (dispersion.rs:88-97) with `Breaking::default()` (:56-74). */
+void wc_dispersion_default(wc_dispersion* d);
+
+/* `Solver::new(grid, bed)` followed by the builders in `cfg` (solver.rs:283-429).
+ * `bed_padded` holds (nx+6)*(ny+6) values; only its interior is read. Returns WC_EINVAL where
+ * the reference panics on setup, WC_EPERIODIC for an oblique wave-maker that does not fit a
+ * periodic domain, WC_EUNSUPPORTED for configurations this build does not run. */
+wc_status wc_solver_create(const wc_grid* grid, const double* bed_padded, const wc_config* cfg,
+                           wc_solver** out);
+void wc_solver_destroy(wc_solver* s);
+
+/* `Solver::step(&mut State, dt)` (solver.rs:479-507) on host FP64 arrays, in place: uploads the
+ * state, runs one SSP-RK2 step on the device, downloads it and advances `*time` by dt.
+ * `breaking` is carried unchanged (it only changes with followed fronts, not in this build). */
+wc_status wc_step(wc_solver* s, double* h, double* hu, double* hv, double* breaking,
+                  double* time, double dt);
+
+/* `Solver::stable_dt(&State)` (solver.rs:431-450): *dt_out is NaN when a cell is not a number
+ * (status WC_ENAN), 0 when a speed is infinite, +inf when nothing can move (status WC_OK). */
+wc_status wc_stable_dt(wc_solver* s, const double* h, const double* hu, const double* hv,
+                       double* dt_out);
+
+/* `Solver::limiting_cell(&State)` (solver.rs:452-477): *found = 0 where the reference returns
+ * None. */
+wc_status wc_limiting_cell(wc_solver* s, const double* h, const double* hu, const double* hv,
+                           wc_limiting* out, int32_t* found);
+
+/* `Solver::breaking_indicator(&State)` (solver.rs:336-349): nx*ny values, y outer. */
+wc_status wc_breaking_indicator(wc_solver* s, const double* h, const double* hu,
+                                const double* hv, double* out_interior);
+
+/* `Solver::dispersion_stats()` (solver.rs:391-396): *has = 0 for shallow water. */
+wc_status wc_dispersion_stats(wc_solver* s, wc_stats* out, int32_t* has);
+
+/* ---- Device-resident throughput path (no counterpart in the reference) ----------------- */
+
+/* Copy a padded FP64 host state onto the device (interior only) and set the device clock. */
+wc_status wc_state_upload(wc_solver* s, const double* h, const double* hu, const double* hv,
+                          double time);
+/* Copy the device state back into padded FP64 host arrays (ghosts filled by the boundary
+ * rule); `time` may be NULL. */
+wc_status wc_state_download(wc_solver* s, double* h, double* hu, double* hv, double* time);
+/* One step of size dt on the device-resident state. Asynchronous: errors of the step itself
+ * surface at the next synchronising call. */
+wc_status wc_step_device(wc_solver* s, double dt);
+/* n_steps steps on the device-resident state, each of size min(stable_dt, t_end - time) read
+ * on the device, as the reference's test loop does (crates/wavecore/tests/common/mod.rs:53-60).
+ * Stops early (on the device) once time >= t_end. Asynchronous. */
+wc_status wc_step_n(wc_solver* s, uint64_t n_steps, double t_end);
+/* stable_dt of the device-resident state, synchronising. */
+wc_status wc_stable_dt_device(wc_solver* s, double* dt_out);
+/* FP64 reductions over the device-resident state (state.rs:78-102), synchronising. */
+wc_status wc_diagnostics_device(wc_solver* s, wc_diagnostics* out);
+/* Device time of the device-resident state, synchronising. */
+wc_status wc_time_device(wc_solver* s, double* time_out);
+/* Wait for all queued device work of this solver and report its status: WC_ETIMEOUT if a
+ * bounded device wait ran out, WC_ENAN if a step met a NaN. */
+wc_status wc_synchronize(wc_solver* s);
+
+/* Kernel launches this solver has queued since it was created (for accounting). */
+uint64_t wc_launch_count(const wc_solver* s);
+/* Human-readable text of the last error on this thread ("" if none). */
+const char* wc_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WAVECORE_C_H */
