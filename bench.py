@@ -1,0 +1,353 @@
+"""Benchmark of wavecore's time step on B200: cell-steps/s with SGN on.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload config2|config3|config1]
+    python bench.py --impl reference ...   # the reference algorithm on the host cores
+
+A step is one SSP-RK2 step of the whole grid (both stages, both dispersive solves); one
+cell-step is one interior cell advanced one step. The default workload is a 1024x512 grid at
+2 m: fifth order + SGN by Jacobi PCG to a relative residual of 1e-8, periodic in y, a seeded
+rough 1:30 beach, H = 2 m, T = 14 s (see wavesim_b200/workloads.py). The state starts as a
+linear wave train over the shelf, so every timed step carries the swell.
+
+`value` is device-timed (CUDA events on the solver's stream, one step at a time, L2 flushed
+between steps by writing a 256 MiB buffer outside the timed events). `e2e` is the same metric
+through the reference-facing call (`wc_step` on pinned host FP64 arrays, the copies in and out
+inside the timed region). With N > 1 (torchrun) every rank advances its own replica (the runs
+share nothing) and rank 0 reports the sum of cell-steps over the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from wavesim_b200 import workloads as W  # noqa: E402
+from wavesim_b200.model import State  # noqa: E402
+
+METRIC = "cell-steps/s (SGN on), learned-PC vs plain PCG on 1 B200 at equal residual"
+UNIT = "cell-steps/s"
+L2_FLUSH_BYTES = 256 << 20
+
+# Algorithmic bytes per interior cell (FP32 state with a compensated depth).
+STAGE_BYTES_SGN = 16 + 4 + 8 + 8 + 4 + 4 + 8   # read q, b; write hn, pred, c, heff, b-vector
+SOLVE_INIT_BYTES = 8 + 4 + 4 + 8 + 8 + 8 + 8 + 8  # read w, c, heff, b; write w, r, p, diag
+SOLVE_ITER_BYTES = 24 + 56 + 32                 # sweeps A, B, C
+SOLVE_FINISH_BYTES = (44 + 60) / 2              # stage 1 / stage 2 epilogue, averaged
+STAGE_BYTES_SWE = (36 + 52) / 2                 # stage 1 / stage 2 (RK average + damping)
+
+
+def workload(name: str):
+    return {"config1": W.config1, "config2": W.config2, "config3": W.config3}[name]()
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True,
+            )
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 8:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax = float(p[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, p[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_baseline(w, steps: int):
+    """The FP64 oracle (the reference's algorithm restated) on all host cores, on a bounded sample
+    of the same workload: `steps` steps from the same start."""
+    from oracle.oracle import OracleSolver, set_threads
+
+    threads = set_threads(0)
+    sol = w.solver(OracleSolver)
+    s = W.wave_train_state(w)
+    sol.step(s, sol.stable_dt(s))  # untimed warm-up of caches and thread pool
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        sol.step(s, sol.stable_dt(s))
+    el = time.perf_counter() - t0
+    st = sol.dispersion_stats()
+    return {
+        "value": w.interior_cells() * steps / el,
+        "unit": UNIT,
+        "cores": threads,
+        "kind": "port",
+        "sample": f"{steps} steps of {w.name} from the wave-train start on {threads} threads "
+                  f"({el:.1f} s; {st.iterations / max(1, st.solves):.1f} PCG iterations/solve)" if st else
+                  f"{steps} steps of {w.name} on {threads} threads ({el:.1f} s)",
+    }
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    from oracle.oracle import OracleSolver, set_threads
+
+    w = workload(args.workload)
+    threads = set_threads(0)
+    sol = w.solver(OracleSolver)
+    s = W.wave_train_state(w)
+    for _ in range(args.warmup):
+        sol.step(s, sol.stable_dt(s))
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        sol.step(s, sol.stable_dt(s))
+        times.append(time.perf_counter() - t0)
+    el = sum(times)
+    value = w.interior_cells() * args.steps / el
+    st = sol.dispersion_stats()
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 * el / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": w.name, "nx": w.grid.nx, "ny": w.grid.ny, "dx_m": w.grid.dx,
+                   "tolerance": w.dispersion.tolerance if w.dispersion else None, **{k: v for k, v in w.meta.items() if k != "bed"}},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} timed steps of {w.name} after {args.warmup} warm-up steps, "
+                                   f"{threads} threads; {st.iterations / max(1, st.solves):.1f} PCG iterations/solve" if st else ""},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_b200(args, world, rank, local):
+    import torch
+
+    from wavesim_b200 import Solver
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    w = workload(args.workload)
+    stream = torch.cuda.Stream()  # a real stream handle: the solver and the events share it
+    torch.cuda.set_stream(stream)
+    sol = w.solver(Solver)
+    sol.set_stream(stream.cuda_stream)
+    s0 = W.wave_train_state(w)
+    sol.upload(s0)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    # warm-up: adaptive steps on the device
+    sol.step_n(args.warmup)
+    sol.synchronize()
+    st0 = sol.dispersion_stats()
+    l0 = sol.launch_count()
+    sol.profile(True)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        for k in range(args.steps):
+            flush.zero_()
+            ev[k][0].record(stream)
+            sol.step_n(1)
+            ev[k][1].record(stream)
+        torch.cuda.synchronize()
+    sol.synchronize()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    prof = sol.profile_read()
+    sol.profile(False)
+    launches = sol.launch_count() - l0
+    st1 = sol.dispersion_stats()
+    total_ms = sum(step_ms)
+    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    total_ms_max = float(t.item())
+    cells = w.interior_cells()
+    value = cells * args.steps * world / (total_ms_max / 1e3)
+
+    # end to end through the reference-facing call, pinned host FP64 arrays
+    pin = lambda a: torch.from_numpy(a).pin_memory().numpy()  # noqa: E731
+    hs = State(pin(s0.h), pin(s0.hu), pin(s0.hv), pin(s0.breaking), s0.time)
+    e2e_sol = w.solver(Solver)
+    e2e_sol.set_stream(stream.cuda_stream)
+    dt = 0.5 * sol.stable_dt_device()
+    for _ in range(2):
+        e2e_sol.step(hs, dt)
+    n_e2e = max(3, min(args.steps, 50))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(n_e2e):
+        e2e_sol.step(hs, dt)
+    e2e_s = time.perf_counter() - t0
+    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = cells * n_e2e * world / float(te.item())
+    npad = w.grid.cells()
+
+    line = None
+    if rank == 0:
+        iters = (st1.iterations - st0.iterations) / max(1, st1.solves - st0.solves) if st1 else 0.0
+        solve_n, solve_ms = prof["solve"]
+        stage_n, stage_ms = prof["stage"]
+        peak, peak_kind = measured_peaks()
+        if solve_n and solve_ms >= stage_ms:
+            per_cell = SOLVE_INIT_BYTES + SOLVE_ITER_BYTES * iters + SOLVE_FINISH_BYTES
+            dom = {"kernel": "pcg_kernel (persistent dispersive solve)", "launches": solve_n, "avg_ms": solve_ms / solve_n,
+                   "bytes_per_cell": per_cell}
+        else:
+            per_cell = STAGE_BYTES_SGN if w.dispersion else STAGE_BYTES_SWE
+            dom = {"kernel": "stage_kernel (fused RK stage)", "launches": stage_n, "avg_ms": stage_ms / max(1, stage_n),
+                   "bytes_per_cell": per_cell}
+        achieved = per_cell * cells / (dom["avg_ms"] / 1e3) / 1e9
+        ck = clocks.summary()
+        line = {
+            "metric": METRIC,
+            "value": value,
+            "unit": UNIT,
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": total_ms_max / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic",
+            "config": {
+                "workload": w.name, "nx": w.grid.nx, "ny": w.grid.ny, "dx_m": w.grid.dx,
+                "scheme": "fifth order + SGN" if w.dispersion else "second order SWE",
+                "preconditioner": "jacobi (plain PCG)" if w.dispersion else None,
+                "tolerance": w.dispersion.tolerance if w.dispersion else None,
+                "pcg_iterations_per_solve": iters,
+                "l2": "flushed between timed steps (256 MiB write outside the timed events)",
+                "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                **{k: v for k, v in w.meta.items() if k != "bed"},
+            },
+            "roofline": {
+                "bound": "hbm",
+                "kernel": dom["kernel"],
+                "achieved": achieved,
+                "peak": peak,
+                "unit": "GB/s",
+                "frac": achieved / peak,
+                "peak_source": peak_kind,
+                "algorithmic_bytes_per_cell": dom["bytes_per_cell"],
+                "traffic": None,
+            },
+            "kernel_ms_per_step": {"stage": stage_ms / args.steps, "solve": solve_ms / args.steps,
+                                   "other": prof["other"][1] / args.steps},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 3 * npad * 8,
+                    "d2h_bytes_per_step": 3 * npad * 8, "steps": n_e2e,
+                    "path": "wc_step on pinned host FP64 arrays (upload, step, download per call)"},
+            "gpu_launches": int(launches),
+            "clocks": ck,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(w, args.cpu_steps)
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="config2", choices=["config1", "config2", "config3"])
+    ap.add_argument("--cpu-steps", type=int, default=40)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be at least 3")
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+    run_b200(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -188,6 +188,22 @@ wc_status wc_time_device(wc_solver* s, double* time_out);
  * bounded device wait ran out, WC_ENAN if a step met a NaN. */
 wc_status wc_synchronize(wc_solver* s);
 
+/* Run this solver's work on the caller's CUDA stream (a cudaStream_t; NULL restores the solver's
+ * own stream), so that a caller can order and time it with its own events, as cublasSetStream
+ * does. The caller keeps the stream alive while the solver uses it. */
+wc_status wc_set_stream(wc_solver* s, void* stream);
+
+/* Per-kernel device timing (no counterpart in the reference). While enabled, every launch of
+ * the step is bracketed by CUDA events on the solver's stream; wc_profile_read synchronises and
+ * returns, per kernel kind, the launch count and the summed device milliseconds since the last
+ * enable. Kinds: 0 = RK-stage stencil kernel, 1 = dispersive solve kernel, 2 = other. */
+typedef struct wc_kernel_time {
+    uint64_t launches;
+    double total_ms;
+} wc_kernel_time;
+wc_status wc_profile_enable(wc_solver* s, int32_t on);
+wc_status wc_profile_read(wc_solver* s, wc_kernel_time out[3]);
+
 /* Kernel launches this solver has queued since it was created (for accounting). */
 uint64_t wc_launch_count(const wc_solver* s);
 /* Human-readable text of the last error on this thread ("" if none). */

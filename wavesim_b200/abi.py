@@ -111,6 +111,12 @@ class wc_diagnostics(C.Structure):
     ]
 
 
+class wc_kernel_time(C.Structure):
+    _fields_ = [("launches", C.c_uint64), ("total_ms", C.c_double)]
+
+
+KERNEL_KINDS = ("stage", "solve", "other")
+
 DPTR = C.POINTER(C.c_double)
 
 

@@ -1,0 +1,804 @@
+// wavecore.cu — the C ABI of include/wavecore_c.h on sm_100a.
+//
+// Host side of the B200 build: owns the device buffers of one solver, its stream and its launch
+// sequence. The reference's `Solver` (crates/wavecore/src/solver.rs) is a host object whose
+// `step` runs the whole update on the CPU; here `wc_step` moves the caller's FP64 arrays to the
+// device, runs the step there and moves them back, and the device-resident entry points keep
+// the state in HBM across steps with the clock and the adaptive time step on the device.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/wavecore_c.h"
+#include "aux.cuh"
+#include "common.cuh"
+#include "pcg.cuh"
+#include "stage.cuh"
+
+using namespace wcb;
+
+namespace {
+
+thread_local std::string g_err;
+
+wc_status set_err(wc_status st, const std::string& msg) {
+    g_err = msg;
+    return st;
+}
+
+#define CK(call)                                                                                \
+    do {                                                                                        \
+        cudaError_t e_ = (call);                                                                \
+        if (e_ != cudaSuccess)                                                                  \
+            return set_err(WC_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_));       \
+    } while (0)
+
+constexpr double TAU = 6.283185307179586;
+constexpr unsigned long long BARRIER_TIMEOUT_NS = 2000000000ull;  // 2 s per grid barrier
+
+struct Drive {
+    double omega = 0, ky = 0, strength = 0;
+};
+
+// forcing.rs:46-75
+wc_status linear_wave(double omega, double h, bool dispersive, double* k, double* cg) {
+    if (!dispersive) {
+        const double c = std::sqrt(9.81 * h);
+        *k = omega / c;
+        *cg = c;
+        return WC_OK;
+    }
+    const double nu = omega * omega * h / 9.81;
+    if (!(nu < 3.0))
+        return set_err(WC_EINVAL, "a wave of this angular frequency is too short for the dispersive "
+                                  "model at the wave-maker's depth");
+    const double kh = std::sqrt(nu / (1.0 - nu / 3.0));
+    *k = kh / h;
+    const double ps = omega / *k;
+    *cg = ps / (1.0 + kh * kh / 3.0);
+    return WC_OK;
+}
+
+}  // namespace
+
+struct wc_solver {
+    wc_grid grid{};
+    DevGrid g{};
+    int W = 0, R = 0;      // padded width and rows (host layout)
+    size_t npad = 0;       // padded cells
+    size_t ncell = 0;      // device cells: ny * pitch
+    int order = WC_ORDER_SECOND;
+    double cfl = 0.4;
+    int sgn = 0;
+    wc_dispersion disp{};
+    BreakingDev br{};
+    DampParams damp{};
+    int has_maker = 0;
+    wc_wavemaker maker{};
+    Drive drive{};
+
+    cudaStream_t stream = nullptr;      // the stream work is queued on
+    cudaStream_t own_stream = nullptr;  // the solver's own stream
+    float4 *q0 = nullptr, *q1 = nullptr;
+    float* bed = nullptr;
+    float* prof = nullptr;
+    float2* ycs = nullptr;
+    uint8_t* shallow = nullptr;
+    float2 *hn = nullptr, *pred = nullptr, *bv = nullptr, *w = nullptr, *r = nullptr, *p = nullptr,
+           *ap = nullptr, *diag = nullptr;
+    float *cc = nullptr, *heff = nullptr;
+    double* part = nullptr;
+    unsigned* bar = nullptr;
+    Ctl* ctl = nullptr;
+    Ctl* ctl_host = nullptr;  // pinned mirror
+    double *st_h = nullptr, *st_hu = nullptr, *st_hv = nullptr;  // padded FP64 staging
+    Rate64Out* r64 = nullptr;
+    double* diag_bands = nullptr;
+    unsigned* diag_done = nullptr;
+    double* diag_out = nullptr;
+    int pcg_blocks = 0, pcg_tiles_x = 0, pcg_tiles_y = 0;
+    unsigned long long launches = 0;
+    unsigned long long seen_unconverged = 0;
+    // Opt-in per-kernel timing: event pairs per launch, read back by wc_profile_read.
+    bool prof_on = false;
+    struct ProfEv {
+        int kind;
+        cudaEvent_t a, b;
+    };
+    std::vector<ProfEv> prof_live;
+    std::vector<cudaEvent_t> prof_pool;
+
+    ~wc_solver() {
+        void* bufs[] = {q0, q1, bed, prof, ycs, shallow, hn, pred, bv, w, r, p, ap, diag, cc, heff,
+                        part, bar, ctl, st_h, st_hu, st_hv, r64, diag_bands, diag_done, diag_out};
+        for (void* b : bufs)
+            if (b) cudaFree(b);
+        if (ctl_host) cudaFreeHost(ctl_host);
+        for (auto& e : prof_live) {
+            cudaEventDestroy(e.a);
+            cudaEventDestroy(e.b);
+        }
+        for (auto e : prof_pool) cudaEventDestroy(e);
+        if (own_stream) cudaStreamDestroy(own_stream);
+    }
+};
+
+namespace {
+
+template <typename T>
+wc_status dalloc(T** p, size_t n) {
+    cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
+    if (e != cudaSuccess) return set_err(WC_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    e = cudaMemset(*p, 0, n * sizeof(T));
+    if (e != cudaSuccess) return set_err(WC_ECUDA, std::string("cudaMemset: ") + cudaGetErrorString(e));
+    return WC_OK;
+}
+
+#define TRY(x)                          \
+    do {                                \
+        wc_status st_ = (x);            \
+        if (st_ != WC_OK) return st_;   \
+    } while (0)
+
+cudaEvent_t prof_event(wc_solver* s) {
+    if (!s->prof_pool.empty()) {
+        cudaEvent_t e = s->prof_pool.back();
+        s->prof_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+// Brackets one launch with events when profiling is on.
+struct ProfScope {
+    wc_solver* s;
+    int kind;
+    cudaEvent_t a = nullptr;
+    ProfScope(wc_solver* s_, int kind_) : s(s_), kind(kind_) {
+        if (s->prof_on) {
+            a = prof_event(s);
+            cudaEventRecord(a, s->stream);
+        }
+    }
+    ~ProfScope() {
+        if (a) {
+            cudaEvent_t b = prof_event(s);
+            cudaEventRecord(b, s->stream);
+            s->prof_live.push_back({kind, a, b});
+        }
+    }
+};
+
+dim3 aux_grid(size_t n) {
+    size_t b = (n + AUX_NT - 1) / AUX_NT;
+    return dim3((unsigned)std::min<size_t>(std::max<size_t>(b, 1), 148 * 16));
+}
+
+// Configure every stage-kernel instantiation for its dynamic shared memory once per process.
+wc_status configure_kernels() {
+    static bool done = false;
+    static wc_status st = WC_OK;
+    if (done) return st;
+    done = true;
+#define ATTR(K, B) CK(cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, B))
+    ATTR((stage_kernel<MODE_STAGE1, 1, false>), SMEM_SWE);
+    ATTR((stage_kernel<MODE_STAGE1, 2, false>), SMEM_SWE);
+    ATTR((stage_kernel<MODE_STAGE2, 1, false>), SMEM_SWE);
+    ATTR((stage_kernel<MODE_STAGE2, 2, false>), SMEM_SWE);
+    ATTR((stage_kernel<MODE_FIRST, 0, false>), SMEM_SWE);
+    ATTR((stage_kernel<MODE_STAGE1, 0, true>), SMEM_SGN);
+    ATTR((stage_kernel<MODE_STAGE1, 1, true>), SMEM_SGN);
+    ATTR((stage_kernel<MODE_STAGE1, 2, true>), SMEM_SGN);
+#undef ATTR
+    return WC_OK;
+}
+
+wc_status launch_stage(wc_solver* s, int mode, const float4* qin, const float4* qold, float4* qout,
+                       bool plus_dt) {
+    StageArgs a{};
+    a.g = s->g;
+    a.qin = qin;
+    a.qold = qold;
+    a.qout = qout;
+    a.bed = s->bed;
+    a.shallow = s->shallow;
+    a.br = s->br;
+    a.maker.on = s->has_maker;
+    a.maker.omega = s->drive.omega;
+    a.maker.ramp_time = s->maker.ramp_periods * s->maker.period;
+    a.maker.prof = s->prof;
+    a.maker.ycs = s->ycs;
+    a.damp = s->damp;
+    a.ctl = s->ctl;
+    a.stage_time_plus_dt = plus_dt ? 1 : 0;
+    a.nonlinear = s->disp.nonlinear;
+    a.hn = s->hn;
+    a.pred = s->pred;
+    a.cc = s->cc;
+    a.heff = s->heff;
+    a.bv = s->bv;
+    dim3 grid((s->g.nx + ST_TX - 1) / ST_TX, (s->g.ny + ST_TY - 1) / ST_TY);
+    dim3 block(ST_NT);
+    cudaStream_t st = s->stream;
+    ProfScope ps(s, 0);
+    const int o = s->order;
+    if (s->sgn) {
+        if (o == 0) stage_kernel<MODE_STAGE1, 0, true><<<grid, block, SMEM_SGN, st>>>(a);
+        else if (o == 1) stage_kernel<MODE_STAGE1, 1, true><<<grid, block, SMEM_SGN, st>>>(a);
+        else stage_kernel<MODE_STAGE1, 2, true><<<grid, block, SMEM_SGN, st>>>(a);
+    } else if (mode == MODE_FIRST) {
+        stage_kernel<MODE_FIRST, 0, false><<<grid, block, SMEM_SWE, st>>>(a);
+    } else if (mode == MODE_STAGE1) {
+        if (o == 1) stage_kernel<MODE_STAGE1, 1, false><<<grid, block, SMEM_SWE, st>>>(a);
+        else stage_kernel<MODE_STAGE1, 2, false><<<grid, block, SMEM_SWE, st>>>(a);
+    } else {
+        if (o == 1) stage_kernel<MODE_STAGE2, 1, false><<<grid, block, SMEM_SWE, st>>>(a);
+        else stage_kernel<MODE_STAGE2, 2, false><<<grid, block, SMEM_SWE, st>>>(a);
+    }
+    s->launches++;
+    CK(cudaGetLastError());
+    return WC_OK;
+}
+
+wc_status launch_pcg(wc_solver* s, int mode, const float4* qold, float4* qout) {
+    PcgArgs a{};
+    a.g = s->g;
+    a.cc = s->cc;
+    a.heff = s->heff;
+    a.bv = s->bv;
+    a.w = s->w;
+    a.r = s->r;
+    a.p = s->p;
+    a.ap = s->ap;
+    a.diag = s->diag;
+    a.part = s->part;
+    a.bar = s->bar;
+    a.hn = s->hn;
+    a.pred = s->pred;
+    a.qold = qold;
+    a.qout = qout;
+    a.bed = s->bed;
+    a.ctl = s->ctl;
+    a.tol = s->disp.tolerance;
+    a.max_iter = (long long)s->disp.max_iterations;
+    a.mode = mode;
+    a.tiles_x = s->pcg_tiles_x;
+    a.tiles_y = s->pcg_tiles_y;
+    a.damp = s->damp;
+    a.timeout_ns = BARRIER_TIMEOUT_NS;
+    CK(cudaMemsetAsync(s->bar, 0, 2 * sizeof(unsigned), s->stream));
+    ProfScope ps(s, 1);
+    void* args[] = {&a};
+    CK(cudaLaunchCooperativeKernel((void*)pcg_kernel, dim3(s->pcg_blocks), dim3(PG_NT), args, 0,
+                                   s->stream));
+    s->launches++;
+    return WC_OK;
+}
+
+// One SSP-RK2 step (solver.rs:479-507) of size ctl->dt on the device-resident state q0.
+wc_status enqueue_step(wc_solver* s) {
+    if (s->order == WC_ORDER_FIRST) {
+        TRY(launch_stage(s, MODE_FIRST, s->q0, s->q0, s->q1, false));
+        if (s->sgn) TRY(launch_pcg(s, MODE_FIRST, s->q0, s->q1));
+        CK(cudaMemcpyAsync(s->q0, s->q1, s->ncell * sizeof(float4), cudaMemcpyDeviceToDevice, s->stream));
+        return WC_OK;
+    }
+    if (!s->sgn) {
+        TRY(launch_stage(s, MODE_STAGE1, s->q0, s->q0, s->q1, false));
+        TRY(launch_stage(s, MODE_STAGE2, s->q1, s->q0, s->q0, true));
+        return WC_OK;
+    }
+    TRY(launch_stage(s, MODE_STAGE1, s->q0, s->q0, s->q1, false));
+    TRY(launch_pcg(s, MODE_STAGE1, s->q0, s->q1));
+    TRY(launch_stage(s, MODE_STAGE1, s->q1, s->q0, s->q1, true));
+    TRY(launch_pcg(s, MODE_STAGE2, s->q0, s->q0));
+    return WC_OK;
+}
+
+wc_status read_ctl(wc_solver* s) {
+    CK(cudaMemcpyAsync(s->ctl_host, s->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return WC_OK;
+}
+
+wc_status status_of(wc_solver* s) {
+    TRY(read_ctl(s));
+    if (s->ctl_host->error & ERR_TIMEOUT)
+        return set_err(WC_ETIMEOUT, "a grid barrier of the dispersive solve timed out");
+    if (s->ctl_host->error & ERR_NAN) return set_err(WC_ENAN, "the state holds a NaN");
+    return WC_OK;
+}
+
+wc_status stage_host(wc_solver* s, const double* h, const double* hu, const double* hv) {
+    const size_t bytes = s->npad * sizeof(double);
+    CK(cudaMemcpyAsync(s->st_h, h, bytes, cudaMemcpyHostToDevice, s->stream));
+    CK(cudaMemcpyAsync(s->st_hu, hu, bytes, cudaMemcpyHostToDevice, s->stream));
+    CK(cudaMemcpyAsync(s->st_hv, hv, bytes, cudaMemcpyHostToDevice, s->stream));
+    return WC_OK;
+}
+
+// Ghost cells of a padded host array by the boundary rule, without sign changes
+// (grid.rs:60-87): the carried `breaking` memory.
+void fill_scalar_ghosts(const wc_grid& gr, bool periodic, double* a) {
+    const size_t nx = gr.nx, ny = gr.ny, w = nx + 6;
+    auto at = [&](size_t i, size_t j) -> double& { return a[j * w + i]; };
+    for (size_t j = 3; j < 3 + ny; j++)
+        for (size_t k = 0; k < 3; k++) {
+            at(2 - k, j) = at(3 + k, j);
+            at(3 + nx + k, j) = at(2 + nx - k, j);
+        }
+    for (size_t i = 0; i < w; i++)
+        for (size_t k = 0; k < 3; k++) {
+            at(i, 2 - k) = at(i, 3 + k);
+            at(i, 3 + ny + k) = at(i, 2 + ny - k);
+        }
+    if (periodic)
+        for (size_t i = 0; i < w; i++)
+            for (size_t k = 0; k < 3; k++) {
+                at(i, 2 - k) = at(i, 2 + ny - k);
+                at(i, 3 + ny + k) = at(i, 3 + k);
+            }
+}
+
+}  // namespace
+
+extern "C" {
+
+void wc_config_default(wc_config* cfg) {
+    std::memset(cfg, 0, sizeof *cfg);
+    cfg->cfl = 0.4;
+    cfg->order = WC_ORDER_SECOND;
+}
+
+void wc_dispersion_default(wc_dispersion* d) {
+    std::memset(d, 0, sizeof *d);
+    d->breaking.eta_ratio_lo = 0.30;
+    d->breaking.eta_ratio_hi = 0.55;
+    d->breaking.slope_lo = 0.40;
+    d->breaking.slope_hi = 0.65;
+    d->nonlinear = 1;
+    d->tolerance = 1e-4;
+    d->max_iterations = 200;
+    d->preconditioner = WC_PC_JACOBI;
+}
+
+const char* wc_last_error(void) { return g_err.c_str(); }
+
+uint64_t wc_launch_count(const wc_solver* s) { return s ? s->launches : 0; }
+
+wc_status wc_solver_create(const wc_grid* grid, const double* bed_padded, const wc_config* cfg,
+                           wc_solver** out) {
+    if (!out) return set_err(WC_EINVAL, "out is null");
+    *out = nullptr;
+    if (!grid || !bed_padded || !cfg) return set_err(WC_EINVAL, "null argument");
+    if (!(grid->nx > 0 && grid->ny > 0)) return set_err(WC_EINVAL, "grid must have at least one interior cell");
+    if (!(grid->dx > 0.0 && grid->dy > 0.0)) return set_err(WC_EINVAL, "cell size must be positive");
+    if ((double)grid->nx * (double)grid->ny > 1.5e9 || grid->nx > (1u << 30) || grid->ny > (1u << 30))
+        return set_err(WC_EINVAL, "grid too large for 32-bit cell indexing");
+    if (cfg->order < WC_ORDER_FIRST || cfg->order > WC_ORDER_FIFTH) return set_err(WC_EINVAL, "unknown order");
+    if (cfg->n_sponges > (uint64_t)MAX_SPONGES)
+        return set_err(WC_EUNSUPPORTED, "at most 8 sponges are supported");
+    if (cfg->n_sponges && !cfg->sponges) return set_err(WC_EINVAL, "sponges is null");
+    if (cfg->dispersion) {
+        if (cfg->dispersion->preconditioner != WC_PC_JACOBI)
+            return set_err(WC_EUNSUPPORTED, "this build's solver takes the Jacobi preconditioner");
+        if (!(cfg->dispersion->tolerance >= 0.0)) return set_err(WC_EINVAL, "tolerance must be >= 0");
+    }
+    TRY(configure_kernels());
+
+    wc_solver* s = new wc_solver();
+    auto fail = [&](wc_status st) {
+        delete s;
+        return st;
+    };
+    s->grid = *grid;
+    const int nx = (int)grid->nx, ny = (int)grid->ny;
+    s->W = nx + 6;
+    s->R = ny + 6;
+    s->npad = (size_t)s->W * s->R;
+    const int pitch = (nx + 31) / 32 * 32;
+    s->ncell = (size_t)ny * pitch;
+    DevGrid& g = s->g;
+    g.nx = nx;
+    g.ny = ny;
+    g.pitch = pitch;
+    g.periodic = cfg->periodic_y ? 1 : 0;
+    g.dx = (float)grid->dx;
+    g.dy = (float)grid->dy;
+    g.ix = (float)(0.5 / grid->dx);
+    g.iy = (float)(0.5 / grid->dy);
+    g.inv_dx = (float)(1.0 / grid->dx);
+    g.inv_dy = (float)(1.0 / grid->dy);
+    g.dxd = grid->dx;
+    g.dyd = grid->dy;
+    s->order = cfg->order;
+    s->cfl = cfg->cfl;
+    s->sgn = cfg->dispersion ? 1 : 0;
+    if (cfg->dispersion) s->disp = *cfg->dispersion;
+    else wc_dispersion_default(&s->disp);
+    const wc_breaking& b = s->disp.breaking;  // Breaking::default() for shallow water (solver.rs:618-623)
+    s->br.er_lo = (float)b.eta_ratio_lo;
+    s->br.er_inv = (float)(1.0 / (b.eta_ratio_hi - b.eta_ratio_lo));
+    s->br.sl_lo = (float)b.slope_lo;
+    s->br.sl_inv = (float)(1.0 / (b.slope_hi - b.slope_lo));
+    s->damp.nsp = (int)cfg->n_sponges;
+    s->damp.manning = (float)cfg->manning;
+    for (int m = 0; m < s->damp.nsp; m++) {
+        const wc_sponge& sp = cfg->sponges[m];
+        SpongeDev& d = s->damp.sp[m];
+        d.width = (int)std::min<uint64_t>(sp.width, (uint64_t)1 << 30);
+        d.strength = (float)sp.strength;
+        d.inv_w = (float)(1.0 / (double)sp.width);
+        d.level = sp.level;
+        d.west = sp.west;
+        d.east = sp.east;
+        d.south = sp.south;
+        d.north = sp.north;
+    }
+
+    // The bed as the reference's solver holds it: with_periodic_y wraps its ghost rows; the
+    // wave-maker's depth is read at the source column, mid-row (solver.rs:400-409).
+    if (cfg->wavemaker) {
+        const wc_wavemaker& spec = *cfg->wavemaker;
+        double rr = std::round(spec.x / grid->dx - 0.5);
+        if (rr < 0.0) rr = 0.0;
+        size_t i = (size_t)rr;
+        if (i > (size_t)nx - 1) i = nx - 1;
+        i += 3;
+        const double depth = -bed_padded[(size_t)(3 + ny / 2) * s->W + i];
+        // Drive::new (forcing.rs:87-117)
+        if (!(depth > 0.0)) return fail(set_err(WC_EINVAL, "wave-maker must sit in water"));
+        if (!(spec.period > 0.0 && spec.sigma > 0.0 && spec.amplitude >= 0.0))
+            return fail(set_err(WC_EINVAL, "wave-maker period and sigma must be positive, amplitude >= 0"));
+        const double omega = TAU / spec.period;
+        double k, cg;
+        wc_status st = linear_wave(omega, depth, s->sgn != 0, &k, &cg);
+        if (st != WC_OK) return fail(st);
+        const double ky = k * std::sin(spec.angle), kx = k * std::cos(spec.angle);
+        const double rolloff = std::exp(0.5 * kx * kx * spec.sigma * spec.sigma);
+        const double flux = 2.0 * cg * spec.amplitude * std::cos(spec.angle) * rolloff;
+        double norm = 0.0;
+        for (int ii = 0; ii < nx; ii++) {
+            const double x = ((double)ii + 0.5) * grid->dx, d = x - spec.x;
+            norm += std::exp(-(d * d) / (2.0 * spec.sigma * spec.sigma)) * grid->dx;
+        }
+        s->drive.omega = omega;
+        s->drive.ky = ky;
+        s->drive.strength = flux / norm;
+        s->maker = spec;
+        s->has_maker = 1;
+        // check_periodic (solver.rs:421-429)
+        if (cfg->periodic_y) {
+            const double turns = ky * (double)ny * grid->dy / TAU;
+            if (!(std::fabs(turns - std::round(turns)) < 1e-6))
+                return fail(set_err(WC_EPERIODIC, "wave-maker does not fit the periodic domain: "
+                                                  "k_y * Ly / 2pi must be a whole number"));
+        }
+    }
+
+    if (cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking) != cudaSuccess)
+        return fail(set_err(WC_ECUDA, "cudaStreamCreate failed"));
+    s->stream = s->own_stream;
+    wc_status st;
+#define ALLOC(p, n)                       \
+    if ((st = dalloc(&(p), (n))) != WC_OK) \
+        return fail(st);
+    ALLOC(s->q0, s->ncell);
+    ALLOC(s->q1, s->ncell);
+    ALLOC(s->bed, s->ncell);
+    ALLOC(s->ctl, 1);
+    ALLOC(s->st_h, s->npad);
+    ALLOC(s->st_hu, s->npad);
+    ALLOC(s->st_hv, s->npad);
+    ALLOC(s->r64, 1);
+    const int bands = std::max(1, std::min(ny, 1024));
+    ALLOC(s->diag_bands, 3 * (size_t)bands);
+    ALLOC(s->diag_done, 1);
+    ALLOC(s->diag_out, 3);
+    if (s->has_maker) {
+        ALLOC(s->prof, (size_t)pitch);
+        ALLOC(s->ycs, (size_t)ny);
+        std::vector<float> prof(pitch, 0.f);
+        for (int ii = 0; ii < nx; ii++) {
+            const double x = ((double)ii + 0.5) * grid->dx, d = x - s->maker.x;
+            const double pr = std::exp(-(d * d) / (2.0 * s->maker.sigma * s->maker.sigma));
+            prof[ii] = pr < 1e-12 ? 0.f : (float)(s->drive.strength * pr);
+        }
+        std::vector<float2> ycs(ny);
+        for (int jj = 0; jj < ny; jj++) {
+            const double y = ((double)jj + 0.5) * grid->dy;
+            ycs[jj] = make_float2((float)std::cos(s->drive.ky * y), (float)std::sin(s->drive.ky * y));
+        }
+        if (cudaMemcpy(s->prof, prof.data(), pitch * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(s->ycs, ycs.data(), ny * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess)
+            return fail(set_err(WC_ECUDA, "maker tables upload failed"));
+    }
+    if (cfg->shallow_cells) {
+        ALLOC(s->shallow, s->ncell);
+        std::vector<uint8_t> m(s->ncell, 0);
+        for (int jj = 0; jj < ny; jj++)
+            for (int ii = 0; ii < nx; ii++) m[(size_t)jj * pitch + ii] = cfg->shallow_cells[(size_t)jj * nx + ii] ? 1 : 0;
+        if (cudaMemcpy(s->shallow, m.data(), s->ncell, cudaMemcpyHostToDevice) != cudaSuccess)
+            return fail(set_err(WC_ECUDA, "shallow-cell mask upload failed"));
+    }
+    if (s->sgn) {
+        ALLOC(s->hn, s->ncell);
+        ALLOC(s->pred, s->ncell);
+        ALLOC(s->bv, s->ncell);
+        ALLOC(s->w, s->ncell);
+        ALLOC(s->r, s->ncell);
+        ALLOC(s->p, s->ncell);
+        ALLOC(s->ap, s->ncell);
+        ALLOC(s->diag, s->ncell);
+        ALLOC(s->cc, s->ncell);
+        ALLOC(s->heff, s->ncell);
+        ALLOC(s->bar, 2);
+        int dev = 0, sms = 0, occ = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, pcg_kernel, PG_NT, 0) != cudaSuccess || occ < 1)
+            return fail(set_err(WC_ECUDA, "occupancy query for the solve kernel failed"));
+        s->pcg_tiles_x = (nx + PG_TX - 1) / PG_TX;
+        s->pcg_tiles_y = (ny + PG_TY - 1) / PG_TY;
+        const int tiles = s->pcg_tiles_x * s->pcg_tiles_y;
+        s->pcg_blocks = std::max(1, std::min(tiles, sms * std::min(occ, 2)));
+        ALLOC(s->part, 2 * 4 * (size_t)s->pcg_blocks);
+    }
+#undef ALLOC
+    if (cudaMallocHost(&s->ctl_host, sizeof(Ctl)) != cudaSuccess)
+        return fail(set_err(WC_ENOMEM, "cudaMallocHost failed"));
+
+    // The bed, interior only, FP32.
+    if (cudaMemcpy(s->st_h, bed_padded, s->npad * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail(set_err(WC_ECUDA, "bed upload failed"));
+    pack_f32_kernel<<<aux_grid(s->ncell), AUX_NT, 0, s->stream>>>(s->g, s->st_h, s->bed);
+    s->launches++;
+    Ctl c{};
+    c.cfl = s->cfl;
+    c.active = 1;
+    c.stable_dt = std::nan("");
+    std::memcpy(s->ctl_host, &c, sizeof c);
+    if (cudaMemcpyAsync(s->ctl, s->ctl_host, sizeof(Ctl), cudaMemcpyHostToDevice, s->stream) != cudaSuccess ||
+        cudaStreamSynchronize(s->stream) != cudaSuccess)
+        return fail(set_err(WC_ECUDA, std::string("solver setup failed: ") + cudaGetErrorString(cudaGetLastError())));
+    *out = s;
+    return WC_OK;
+}
+
+void wc_solver_destroy(wc_solver* s) {
+    if (s) cudaStreamSynchronize(s->stream);
+    delete s;
+}
+
+wc_status wc_profile_enable(wc_solver* s, int32_t on) {
+    if (!s) return set_err(WC_EINVAL, "null solver");
+    CK(cudaStreamSynchronize(s->stream));
+    for (auto& e : s->prof_live) {
+        s->prof_pool.push_back(e.a);
+        s->prof_pool.push_back(e.b);
+    }
+    s->prof_live.clear();
+    s->prof_on = on != 0;
+    return WC_OK;
+}
+
+wc_status wc_profile_read(wc_solver* s, wc_kernel_time out[3]) {
+    if (!s || !out) return set_err(WC_EINVAL, "null argument");
+    CK(cudaStreamSynchronize(s->stream));
+    for (int k = 0; k < 3; k++) out[k] = wc_kernel_time{0, 0.0};
+    for (auto& e : s->prof_live) {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, e.a, e.b));
+        out[e.kind].launches += 1;
+        out[e.kind].total_ms += ms;
+    }
+    return WC_OK;
+}
+
+wc_status wc_set_stream(wc_solver* s, void* stream) {
+    if (!s) return set_err(WC_EINVAL, "null solver");
+    CK(cudaStreamSynchronize(s->stream));
+    s->stream = stream ? (cudaStream_t)stream : s->own_stream;
+    return WC_OK;
+}
+
+wc_status wc_state_upload(wc_solver* s, const double* h, const double* hu, const double* hv, double time) {
+    if (!s || !h || !hu || !hv) return set_err(WC_EINVAL, "null argument");
+    TRY(stage_host(s, h, hu, hv));
+    upload_kernel<<<aux_grid(s->ncell), AUX_NT, 0, s->stream>>>(s->g, s->st_h, s->st_hu, s->st_hv, s->q0);
+    s->launches++;
+    CK(cudaGetLastError());
+    // The clock; a new state clears the error bits.
+    TRY(read_ctl(s));
+    s->ctl_host->t = time;
+    s->ctl_host->error = 0;
+    s->ctl_host->active = 1;
+    s->ctl_host->adaptive = 0;
+    CK(cudaMemcpyAsync(s->ctl, s->ctl_host, sizeof(Ctl), cudaMemcpyHostToDevice, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return WC_OK;
+}
+
+wc_status wc_state_download(wc_solver* s, double* h, double* hu, double* hv, double* time) {
+    if (!s || !h || !hu || !hv) return set_err(WC_EINVAL, "null argument");
+    download_kernel<<<aux_grid(s->npad), AUX_NT, 0, s->stream>>>(s->g, s->q0, s->st_h, s->st_hu, s->st_hv);
+    s->launches++;
+    CK(cudaGetLastError());
+    const size_t bytes = s->npad * sizeof(double);
+    CK(cudaMemcpyAsync(h, s->st_h, bytes, cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaMemcpyAsync(hu, s->st_hu, bytes, cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaMemcpyAsync(hv, s->st_hv, bytes, cudaMemcpyDeviceToHost, s->stream));
+    TRY(read_ctl(s));
+    if (time) *time = s->ctl_host->t;
+    return WC_OK;
+}
+
+wc_status wc_step_device(wc_solver* s, double dt) {
+    if (!s) return set_err(WC_EINVAL, "null solver");
+    clear_adaptive_kernel<<<1, 1, 0, s->stream>>>(s->ctl);
+    set_dt_kernel<<<1, 1, 0, s->stream>>>(s->ctl, dt);
+    s->launches += 2;
+    TRY(enqueue_step(s));
+    return WC_OK;
+}
+
+wc_status wc_step_n(wc_solver* s, uint64_t n_steps, double t_end) {
+    if (!s) return set_err(WC_EINVAL, "null solver");
+    state_rate_kernel<<<aux_grid(s->ncell), AUX_NT, 0, s->stream>>>(s->g, s->q0, s->ctl);
+    set_adaptive_kernel<<<1, 1, 0, s->stream>>>(s->ctl, t_end);
+    s->launches += 2;
+    for (uint64_t n = 0; n < n_steps; n++) TRY(enqueue_step(s));
+    clear_adaptive_kernel<<<1, 1, 0, s->stream>>>(s->ctl);
+    s->launches++;
+    CK(cudaGetLastError());
+    return WC_OK;
+}
+
+wc_status wc_synchronize(wc_solver* s) {
+    if (!s) return set_err(WC_EINVAL, "null solver");
+    CK(cudaStreamSynchronize(s->stream));
+    return status_of(s);
+}
+
+wc_status wc_step(wc_solver* s, double* h, double* hu, double* hv, double* breaking, double* time,
+                  double dt) {
+    if (!s || !h || !hu || !hv || !time) return set_err(WC_EINVAL, "null argument");
+    TRY(wc_state_upload(s, h, hu, hv, *time));
+    TRY(wc_step_device(s, dt));
+    TRY(status_of(s));
+    TRY(wc_state_download(s, h, hu, hv, nullptr));
+    if (breaking) fill_scalar_ghosts(s->grid, s->g.periodic != 0, breaking);
+    // `s.time = t + dt` (solver.rs:506)
+    *time = *time + dt;
+    if (s->ctl_host->unconverged != s->seen_unconverged) {
+        s->seen_unconverged = s->ctl_host->unconverged;
+        return set_err(WC_EUNCONVERGED, "a dispersive solve stopped at max_iterations (counted, "
+                                        "as the reference does; the step is complete)");
+    }
+    return WC_OK;
+}
+
+wc_status wc_stable_dt(wc_solver* s, const double* h, const double* hu, const double* hv, double* dt_out) {
+    if (!s || !h || !hu || !hv || !dt_out) return set_err(WC_EINVAL, "null argument");
+    TRY(stage_host(s, h, hu, hv));
+    Rate64Out init{0ull, ~0ull, ~0ull};
+    CK(cudaMemcpyAsync(s->r64, &init, sizeof init, cudaMemcpyHostToDevice, s->stream));
+    rate64_kernel<<<aux_grid(s->ncell), AUX_NT, 0, s->stream>>>(s->g.nx, s->g.ny, s->g.dxd, s->g.dyd,
+                                                                s->st_h, s->st_hu, s->st_hv, s->r64);
+    s->launches++;
+    Rate64Out res;
+    CK(cudaMemcpyAsync(&res, s->r64, sizeof res, cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    if (res.first_nan != ~0ull) {
+        *dt_out = std::nan("");
+        return set_err(WC_ENAN, "a cell's water is not a number");
+    }
+    double rate;
+    std::memcpy(&rate, &res.max_bits, sizeof rate);
+    *dt_out = rate > 0.0 ? s->cfl / rate : INFINITY;
+    return WC_OK;
+}
+
+wc_status wc_limiting_cell(wc_solver* s, const double* h, const double* hu, const double* hv,
+                           wc_limiting* out, int32_t* found) {
+    if (!s || !h || !hu || !hv || !out || !found) return set_err(WC_EINVAL, "null argument");
+    TRY(stage_host(s, h, hu, hv));
+    Rate64Out init{0ull, ~0ull, ~0ull};
+    CK(cudaMemcpyAsync(s->r64, &init, sizeof init, cudaMemcpyHostToDevice, s->stream));
+    rate64_kernel<<<aux_grid(s->ncell), AUX_NT, 0, s->stream>>>(s->g.nx, s->g.ny, s->g.dxd, s->g.dyd,
+                                                                s->st_h, s->st_hu, s->st_hv, s->r64);
+    argmax64_kernel<<<aux_grid(s->ncell), AUX_NT, 0, s->stream>>>(s->g.nx, s->g.ny, s->g.dxd, s->g.dyd,
+                                                                  s->st_h, s->st_hu, s->st_hv, s->r64);
+    s->launches += 2;
+    Rate64Out res;
+    CK(cudaMemcpyAsync(&res, s->r64, sizeof res, cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    unsigned long long c;
+    double rate;
+    std::memcpy(&rate, &res.max_bits, sizeof rate);
+    if (res.first_nan != ~0ull) c = res.first_nan;
+    else if (rate > 0.0) c = res.first_max;
+    else {
+        *found = 0;
+        return WC_OK;
+    }
+    const size_t nx = s->grid.nx;
+    const size_t i = c % nx, j = c / nx;
+    const size_t k = (j + 3) * (size_t)s->W + (i + 3);
+    const double hh = h[k];
+    const double u = hh > 1e-8 ? hu[k] / hh : 0.0, v = hh > 1e-8 ? hv[k] / hh : 0.0;
+    out->i = i;
+    out->j = j;
+    out->depth = hh;
+    out->speed = std::hypot(u, v);
+    *found = 1;
+    return WC_OK;
+}
+
+wc_status wc_breaking_indicator(wc_solver* s, const double* h, const double* hu, const double* hv,
+                                double* out_interior) {
+    if (!s || !h || !hu || !hv || !out_interior) return set_err(WC_EINVAL, "null argument");
+    TRY(stage_host(s, h, hu, hv));
+    upload_kernel<<<aux_grid(s->ncell), AUX_NT, 0, s->stream>>>(s->g, s->st_h, s->st_hu, s->st_hv, s->q1);
+    breaking_kernel<<<aux_grid(s->ncell), AUX_NT, 0, s->stream>>>(s->g, s->q1, s->bed, s->br, s->st_h);
+    s->launches += 2;
+    CK(cudaMemcpyAsync(out_interior, s->st_h, s->grid.nx * s->grid.ny * sizeof(double),
+                       cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return WC_OK;
+}
+
+wc_status wc_dispersion_stats(wc_solver* s, wc_stats* out, int32_t* has) {
+    if (!s || !out || !has) return set_err(WC_EINVAL, "null argument");
+    if (!s->sgn) {
+        *has = 0;
+        return WC_OK;
+    }
+    TRY(read_ctl(s));
+    out->solves = s->ctl_host->solves;
+    out->iterations = s->ctl_host->iterations;
+    out->unconverged = s->ctl_host->unconverged;
+    *has = 1;
+    return WC_OK;
+}
+
+wc_status wc_stable_dt_device(wc_solver* s, double* dt_out) {
+    if (!s || !dt_out) return set_err(WC_EINVAL, "null argument");
+    state_rate_kernel<<<aux_grid(s->ncell), AUX_NT, 0, s->stream>>>(s->g, s->q0, s->ctl);
+    s->launches++;
+    TRY(read_ctl(s));
+    *dt_out = s->ctl_host->stable_dt;
+    if (std::isnan(*dt_out)) return set_err(WC_ENAN, "a cell's water is not a number");
+    return WC_OK;
+}
+
+wc_status wc_diagnostics_device(wc_solver* s, wc_diagnostics* out) {
+    if (!s || !out) return set_err(WC_EINVAL, "null argument");
+    const int bands = std::max(1, std::min(s->g.ny, 1024));
+    diagnostics_kernel<<<bands, AUX_NT, 0, s->stream>>>(s->g, s->q0, s->diag_bands, s->diag_bands + bands,
+                                                        s->diag_bands + 2 * bands, s->diag_done, s->diag_out);
+    s->launches++;
+    double v[3];
+    CK(cudaMemcpyAsync(v, s->diag_out, sizeof v, cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    out->volume = v[0];
+    out->max_abs_momentum = v[1];
+    out->min_depth = v[2];
+    return WC_OK;
+}
+
+wc_status wc_time_device(wc_solver* s, double* time_out) {
+    if (!s || !time_out) return set_err(WC_EINVAL, "null argument");
+    TRY(read_ctl(s));
+    *time_out = s->ctl_host->t;
+    return WC_OK;
+}
+
+}  // extern "C"

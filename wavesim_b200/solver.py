@@ -1,0 +1,237 @@
+"""`Solver`: wavecore's solver API over the device library (include/wavecore_c.h).
+
+The step runs only on the GPU, in `libwavecore_b200.so`; there is no CPU path. If the library or
+a CUDA device is missing, creating a solver raises.
+
+Builders follow the reference (`Solver::new(grid, bed).with_order(..).with_dispersion(..)`,
+crates/wavecore/src/solver.rs:283-419); `step`, `stable_dt`, `limiting_cell`,
+`breaking_indicator` and `dispersion_stats` take and return host FP64 arrays like the reference.
+The device-resident methods (`upload`, `step_device`, `step_n`, `download`, ...) are the
+throughput path and have no counterpart in the reference.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+import warnings
+
+import numpy as np
+
+from . import abi
+from .model import DispersionStats, Limiting, SolverConfig, State
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libwavecore_b200.so")
+_lib = None
+
+EXPORTS = [
+    "wc_config_default",
+    "wc_dispersion_default",
+    "wc_solver_create",
+    "wc_solver_destroy",
+    "wc_step",
+    "wc_stable_dt",
+    "wc_limiting_cell",
+    "wc_breaking_indicator",
+    "wc_dispersion_stats",
+    "wc_state_upload",
+    "wc_state_download",
+    "wc_step_device",
+    "wc_step_n",
+    "wc_stable_dt_device",
+    "wc_diagnostics_device",
+    "wc_time_device",
+    "wc_synchronize",
+    "wc_set_stream",
+    "wc_profile_enable",
+    "wc_profile_read",
+    "wc_launch_count",
+    "wc_last_error",
+]
+
+
+class WavecoreError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{abi.STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+def load(path: str = LIB_PATH):
+    """Load the device library (it must have been built: `python -m wavesim_b200.build`)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(
+            f"{path} is missing: build it with `python -m wavesim_b200.build` (there is no CPU fallback)"
+        )
+    L = C.CDLL(path)
+    D = abi.DPTR
+    V = C.c_void_p
+    L.wc_config_default.argtypes = [C.POINTER(abi.wc_config)]
+    L.wc_dispersion_default.argtypes = [C.POINTER(abi.wc_dispersion)]
+    L.wc_solver_create.argtypes = [C.POINTER(abi.wc_grid), D, C.POINTER(abi.wc_config), C.POINTER(V)]
+    L.wc_solver_destroy.argtypes = [V]
+    L.wc_step.argtypes = [V, D, D, D, D, D, C.c_double]
+    L.wc_stable_dt.argtypes = [V, D, D, D, D]
+    L.wc_limiting_cell.argtypes = [V, D, D, D, C.POINTER(abi.wc_limiting), C.POINTER(C.c_int32)]
+    L.wc_breaking_indicator.argtypes = [V, D, D, D, D]
+    L.wc_dispersion_stats.argtypes = [V, C.POINTER(abi.wc_stats), C.POINTER(C.c_int32)]
+    L.wc_state_upload.argtypes = [V, D, D, D, C.c_double]
+    L.wc_state_download.argtypes = [V, D, D, D, D]
+    L.wc_step_device.argtypes = [V, C.c_double]
+    L.wc_step_n.argtypes = [V, C.c_uint64, C.c_double]
+    L.wc_stable_dt_device.argtypes = [V, D]
+    L.wc_diagnostics_device.argtypes = [V, C.POINTER(abi.wc_diagnostics)]
+    L.wc_time_device.argtypes = [V, D]
+    L.wc_synchronize.argtypes = [V]
+    L.wc_set_stream.argtypes = [V, V]
+    L.wc_profile_enable.argtypes = [V, C.c_int32]
+    L.wc_profile_read.argtypes = [V, C.POINTER(abi.wc_kernel_time)]
+    L.wc_launch_count.argtypes = [V]
+    L.wc_launch_count.restype = C.c_uint64
+    L.wc_last_error.restype = C.c_char_p
+    for name in (
+        "wc_solver_create", "wc_step", "wc_stable_dt", "wc_limiting_cell", "wc_breaking_indicator",
+        "wc_dispersion_stats", "wc_state_upload", "wc_state_download", "wc_step_device", "wc_step_n",
+        "wc_stable_dt_device", "wc_diagnostics_device", "wc_time_device", "wc_synchronize",
+        "wc_set_stream", "wc_profile_enable", "wc_profile_read",
+    ):
+        getattr(L, name).restype = C.c_int
+    L.wc_config_default.restype = None
+    L.wc_dispersion_default.restype = None
+    L.wc_solver_destroy.restype = None
+    _lib = L
+    return L
+
+
+def _check(status: int, allow=(abi.WC_OK,)):
+    if status in allow:
+        return status
+    if status == abi.WC_EUNCONVERGED:
+        warnings.warn(load().wc_last_error().decode(), RuntimeWarning, stacklevel=3)
+        return status
+    raise WavecoreError(status, load().wc_last_error().decode())
+
+
+class Solver(SolverConfig):
+    """wavecore's `Solver` (solver.rs:260-733) on a B200."""
+
+    def _release(self):
+        if getattr(self, "_handle", None):
+            load().wc_solver_destroy(self._handle)
+        self._handle = None
+
+    def __del__(self):
+        try:
+            self._release()
+        except Exception:
+            pass
+
+    def _h(self):
+        if self._handle is None:
+            L = load()
+            cfg, keep = self._c_config()
+            g = self.grid.to_c()
+            out = C.c_void_p()
+            _check(L.wc_solver_create(C.byref(g), abi.dptr(self.bed.b), C.byref(cfg), C.byref(out)))
+            self._handle = out
+        return self._handle
+
+    def check(self):
+        """Create the device solver now, raising where the reference's builders would panic."""
+        self._h()
+        return self
+
+    # ---- the reference's host-array API -------------------------------------------------
+
+    def step(self, s: State, dt: float) -> None:
+        """solver.rs:479-507: one step of size dt, in place on the host state."""
+        t = C.c_double(s.time)
+        _check(
+            load().wc_step(self._h(), abi.dptr(s.h), abi.dptr(s.hu), abi.dptr(s.hv), abi.dptr(s.breaking), C.byref(t), float(dt))
+        )
+        s.time = t.value
+
+    def stable_dt(self, s: State) -> float:
+        """solver.rs:431-450 (NaN when a cell is not a number, inf when nothing moves)."""
+        out = C.c_double()
+        _check(load().wc_stable_dt(self._h(), abi.dptr(s.h), abi.dptr(s.hu), abi.dptr(s.hv), C.byref(out)),
+               allow=(abi.WC_OK, abi.WC_ENAN))
+        return out.value
+
+    def limiting_cell(self, s: State):
+        """solver.rs:452-477."""
+        out = abi.wc_limiting()
+        found = C.c_int32()
+        _check(load().wc_limiting_cell(self._h(), abi.dptr(s.h), abi.dptr(s.hu), abi.dptr(s.hv), C.byref(out), C.byref(found)))
+        if not found.value:
+            return None
+        return Limiting(out.i, out.j, out.depth, out.speed)
+
+    def breaking_indicator(self, s: State) -> np.ndarray:
+        """solver.rs:336-349: nx*ny values, y outer."""
+        out = np.zeros(self.grid.nx * self.grid.ny)
+        _check(load().wc_breaking_indicator(self._h(), abi.dptr(s.h), abi.dptr(s.hu), abi.dptr(s.hv), abi.dptr(out)))
+        return out
+
+    def dispersion_stats(self):
+        """solver.rs:391-396."""
+        st = abi.wc_stats()
+        has = C.c_int32()
+        _check(load().wc_dispersion_stats(self._h(), C.byref(st), C.byref(has)))
+        if not has.value:
+            return None
+        return DispersionStats(st.solves, st.iterations, st.unconverged)
+
+    # ---- the device-resident throughput path --------------------------------------------
+
+    def upload(self, s: State) -> None:
+        _check(load().wc_state_upload(self._h(), abi.dptr(s.h), abi.dptr(s.hu), abi.dptr(s.hv), float(s.time)))
+
+    def download(self, s: State) -> None:
+        t = C.c_double()
+        _check(load().wc_state_download(self._h(), abi.dptr(s.h), abi.dptr(s.hu), abi.dptr(s.hv), C.byref(t)))
+        s.time = t.value
+
+    def step_device(self, dt: float) -> None:
+        _check(load().wc_step_device(self._h(), float(dt)))
+
+    def step_n(self, n: int, t_end: float = math.inf) -> None:
+        _check(load().wc_step_n(self._h(), int(n), float(t_end)))
+
+    def set_stream(self, stream_handle: int) -> None:
+        """Queue work on the caller's CUDA stream (an integer cudaStream_t; 0 = own stream)."""
+        _check(load().wc_set_stream(self._h(), C.c_void_p(int(stream_handle) or None)))
+
+    def profile(self, on: bool) -> None:
+        """Start (clearing earlier records) or stop per-kernel device timing."""
+        _check(load().wc_profile_enable(self._h(), int(bool(on))))
+
+    def profile_read(self) -> dict:
+        """{kind: (launches, total device ms)} since profiling was enabled."""
+        out = (abi.wc_kernel_time * 3)()
+        _check(load().wc_profile_read(self._h(), out))
+        return {abi.KERNEL_KINDS[k]: (int(out[k].launches), float(out[k].total_ms)) for k in range(3)}
+
+    def synchronize(self) -> None:
+        _check(load().wc_synchronize(self._h()))
+
+    def stable_dt_device(self) -> float:
+        out = C.c_double()
+        _check(load().wc_stable_dt_device(self._h(), C.byref(out)), allow=(abi.WC_OK, abi.WC_ENAN))
+        return out.value
+
+    def diagnostics_device(self):
+        d = abi.wc_diagnostics()
+        _check(load().wc_diagnostics_device(self._h(), C.byref(d)))
+        return d.volume, d.max_abs_momentum, d.min_depth
+
+    def time_device(self) -> float:
+        t = C.c_double()
+        _check(load().wc_time_device(self._h(), C.byref(t)))
+        return t.value
+
+    def launch_count(self) -> int:
+        return int(load().wc_launch_count(self._h()))
