@@ -69,8 +69,9 @@ def test_swe_plane_beach_config1_matches_the_oracle():
     s0 = State.lake_at_rest(w.grid, w.bed, 0.0)
     m, _, _ = compare(w, s0, 1000)
     record("swe_plane_beach_256x64_1000steps", m)
-    assert m["eta_max_abs_diff_m"] < 2e-4
-    assert m["eta_rms_diff_m"] < 2e-5
+    # FP32 against FP64 after 1000 steps of a 1 m wave: measured 2.6e-6 m max, 6.5e-7 m rms.
+    assert m["eta_max_abs_diff_m"] < 2e-5
+    assert m["eta_rms_diff_m"] < 3e-6
     assert m["wet_mask_agreement"] > 0.999
     assert m["breaking_mask_agreement"] > 0.999
     assert m["volume_rel_diff"] < 1e-6
@@ -82,8 +83,9 @@ def test_fifth_order_sgn_periodic_beach_matches_the_oracle():
     s0 = W.wave_train_state(w)
     m, sg, _ = compare(w, s0, 150)
     record("sgn_beach_192x96_150steps", m)
-    assert m["eta_max_abs_diff_m"] < 2e-3
-    assert m["eta_rms_diff_m"] < 2e-4
+    # Measured 4.1e-6 m max, 4.5e-7 m rms on a 3.4 m surface range.
+    assert m["eta_max_abs_diff_m"] < 3e-5
+    assert m["eta_rms_diff_m"] < 3e-6
     assert m["wet_mask_agreement"] > 0.995
     assert m["breaking_mask_agreement"] > 0.995
     assert m["volume_rel_diff"] < 1e-5
@@ -105,7 +107,7 @@ def test_dam_break_wet_dry_front_matches_the_oracle():
         gpu.step(sg, dt)
     d = np.abs(grid.inner(sg.h) - grid.inner(so.h))
     record("dam_break_dry_200steps", {"h_max_abs_diff_m": float(d.max())})
-    assert d.max() < 1e-3
+    assert d.max() < 1e-5  # measured 3.0e-7 m on a 2 m column
     assert abs(sg.volume(grid) - so.volume(grid)) < 1e-12 * so.volume(grid)
 
 

@@ -2,11 +2,20 @@
 //
 // The reference solves  h w - grad(c div w) = r  by Jacobi-preconditioned conjugate gradients
 // from the previous solution, stopping when ||r|| <= tol ||b|| + 1e-10 or after max_iterations
-// (crates/wavecore/src/dispersion.rs:493-545). Here every CTA owns a fixed set of 32x8 tiles for
-// the whole solve; the sweeps are separated by grid barriers whose waits are bounded in time
-// (on expiry the kernel sets an error bit and returns, never traps), and the dot products are
-// FP64, reduced per CTA with a fixed tree and then over CTAs in a fixed order by every CTA, so
-// all CTAs take the same convergence decision and results are reproducible run to run.
+// (crates/wavecore/src/dispersion.rs:493-545). The recurrences here are the same; the sweeps
+// are arranged for the GPU:
+//   init   r = b - A w, diag, <b,b>, <r,z>, <r,r>           (z = r / diag, recomputed)
+//   A'     p = z + beta p (on the tile and a 2-cell halo), Ap, <p,Ap>
+//   B      w += alpha p, r -= alpha Ap, <r,r>, <r,z>
+// two grid-wide reductions per iteration. p is double-buffered: sweep A' reads the previous p
+// around its tile while other CTAs write the new one.
+//
+// Every CTA owns a fixed set of 32x16 tiles for the whole solve, and every sweep is software-
+// pipelined: the next tile's halo box is loaded into registers while the current tile computes.
+// A reduction is also the grid barrier: CTAs publish FP64 partials and arrive; after the release
+// every CTA adds all partials in CTA order with the same tree, so every CTA holds the same bits
+// and takes the same convergence decision (reproducible runs). Waits are bounded in time; on
+// expiry the kernel sets ERR_TIMEOUT and every CTA returns.
 //
 // After the loop the same kernel finishes the stage: hu = pred + dt * h * w (the reference's
 // lhu = h w + u lh, dispersion.rs:547-562), clean_dry, and on the last stage the RK2 average,
@@ -18,10 +27,9 @@
 
 namespace wcb {
 
-constexpr int PG_TX = 32, PG_TY = 8, PG_NT = 256;
+constexpr int PG_TX = 32, PG_TY = 16, PG_NT = PG_TX * PG_TY;
 constexpr int PB_W = PG_TX + 4, PB_H = PG_TY + 4, PB_N = PB_W * PB_H;  // vector box, halo 2
 constexpr int PC_W = PG_TX + 2, PC_H = PG_TY + 2, PC_N = PC_W * PC_H;  // c and c div p, halo 1
-
 struct PcgArgs {
     DevGrid g;
     const float* cc;
@@ -29,12 +37,12 @@ struct PcgArgs {
     const float2* bv;
     float2* w;
     float2* r;
-    float2* p;
+    float2* p0;       // p, double-buffered
+    float2* p1;
     float2* ap;
     float2* diag;
-    double* part;     // [2][gridDim.x][4]: double-buffered so that a CTA publishing the next
-                      // sums never overwrites values a slower CTA is still reading
-    unsigned* bar;    // [2]: arrivals, released epoch; zeroed before each launch
+    double* part;     // [gridDim.x][4] CTA partials
+    unsigned* cnt;    // [0] arrivals, [1] released epoch; zeroed before each launch
     const float2* hn;
     const float2* pred;
     const float4* qold;
@@ -49,22 +57,27 @@ struct PcgArgs {
     unsigned long long timeout_ns;
 };
 
-// Bounded grid barrier: a monotonic arrival counter and a released-epoch word. Every CTA is
-// co-resident (cooperative launch), so the wait ends unless a CTA has failed; it gives up after
-// timeout_ns, sets ERR_TIMEOUT and makes every CTA leave.
-__device__ __forceinline__ bool grid_barrier(const PcgArgs& a, unsigned& epoch) {
+// Grid-wide sum of up to three values that is also a barrier. Each CTA publishes its partials
+// and arrives; the last to arrive releases; every CTA then adds all partials in CTA order with
+// the same reduction tree, so all CTAs hold identical totals. Returns false if the wait timed out.
+__device__ bool reduce_barrier(const PcgArgs& a, unsigned& epoch, double v0, double v1, double v2,
+                               double* out, double* red) {
     __shared__ int s_ok;
-    __syncthreads();
+    block_sum3<PG_NT>(v0, v1, v2, red);
     if (threadIdx.x == 0) {
         epoch += 1;
-        int ok = 1;
+        double* pp = a.part + 4 * (size_t)blockIdx.x;
+        pp[0] = v0;
+        pp[1] = v1;
+        pp[2] = v2;
         __threadfence();
-        const unsigned arrived = atomicAdd(&a.bar[0], 1u) + 1u;
+        int ok = 1;
+        const unsigned arrived = atomicAdd(a.cnt, 1u) + 1u;
         if (arrived == epoch * gridDim.x) {
-            st_release_u32(&a.bar[1], epoch);
+            st_release_u32(a.cnt + 1, epoch);
         } else {
             const unsigned long long t0 = globaltimer_ns();
-            while (ld_acquire_u32(&a.bar[1]) < epoch) {
+            while (ld_acquire_u32(a.cnt + 1) < epoch) {
                 if (ld_volatile_int(&a.ctl->error) & ERR_TIMEOUT) {
                     ok = 0;
                     break;
@@ -74,97 +87,139 @@ __device__ __forceinline__ bool grid_barrier(const PcgArgs& a, unsigned& epoch) 
                     ok = 0;
                     break;
                 }
-                __nanosleep(40);
             }
         }
         __threadfence();
         s_ok = ok;
     }
     __syncthreads();
-    return s_ok != 0;
-}
-
-// The CTAs' partial sums of one slot, summed in CTA order by every CTA.
-__device__ __forceinline__ void grid_totals(const PcgArgs& a, int buf, int nslots, double* out,
-                                            double* red) {
-    double v[3] = {0.0, 0.0, 0.0};
-    const double* part = a.part + (size_t)buf * gridDim.x * 4;
-    for (int b = threadIdx.x; b < (int)gridDim.x; b += PG_NT)
-        for (int s = 0; s < nslots; s++) v[s] += __ldcg(part + 4 * b + s);
-    block_sum3<PG_NT>(v[0], v[1], v[2], red);
-    for (int s = 0; s < nslots; s++) out[s] = v[s];
-}
-
-__device__ __forceinline__ void publish(const PcgArgs& a, int buf, double x, double y, double z,
-                                        double* red) {
+    if (!s_ok) return false;
+    double x = 0.0, y = 0.0, z = 0.0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += PG_NT) {
+        const double* pp = a.part + 4 * (size_t)b;
+        x += __ldcg(pp);
+        y += __ldcg(pp + 1);
+        z += __ldcg(pp + 2);
+    }
     block_sum3<PG_NT>(x, y, z, red);
-    if (threadIdx.x == 0) {
-        double* part = a.part + ((size_t)buf * gridDim.x + blockIdx.x) * 4;
-        part[0] = x;
-        part[1] = y;
-        part[2] = z;
-    }
+    out[0] = x;
+    out[1] = y;
+    out[2] = z;
+    return true;
 }
 
-// A v on one tile (dispersion.rs:269-317): v is staged with a 2-cell halo of ghost-synthesised
-// values (vector ghosts: the wall-normal component flips), c with a 1-cell halo, c div v on
-// the tile plus one ring, then mask (heff v - grad(c div v)). With INIT the source is the warm
-// start, masked on the fly (dispersion.rs:480-490), and the tile also writes the Jacobi diagonal.
+struct TileSmem {
+    float2 sv[PB_N];
+    float scc[PC_N];
+    float sf[PC_N];
+};
+
+constexpr int PB_PER = (PB_N + PG_NT - 1) / PG_NT;  // box positions per thread
+constexpr int PC_PER = (PC_N + PG_NT - 1) / PG_NT;
+
+// A tile's box of vector data, c box and own-cell heff, held in registers between the loads
+// and the moment the tile's shared memory is free: the next tile's loads overlap this tile's
+// arithmetic.
+struct BoxPrefetch {
+    float2 v0[PB_PER], v1[PB_PER], v2[PB_PER];
+    float sx[PB_PER], sy[PB_PER];
+    float c[PC_PER];
+    float he;
+};
+
+__device__ __forceinline__ void tile_origin(const PcgArgs& a, int tl, int& i0, int& j0) {
+    i0 = (tl % a.tiles_x) * PG_TX;
+    j0 = (tl / a.tiles_x) * PG_TY;
+}
+
+// INIT: v0 = warm start w, v1.x = heff at the box position. Otherwise: v0 = r, v1 = diag,
+// v2 = previous p.
 template <bool INIT>
-__device__ __forceinline__ float2 tile_matvec(const PcgArgs& a, int i0, int j0, const float2* src,
-                                              float2* sv, float* scc, float* sf, bool& own_valid,
-                                              int& k_own, float& heff_own) {
+__device__ __forceinline__ void box_prefetch(const PcgArgs& a, int tl, const float2* p_old, bool first,
+                                             BoxPrefetch& f) {
+    int i0, j0;
+    tile_origin(a, tl, i0, j0);
     const DevGrid& g = a.g;
-    const int tid = threadIdx.x;
-    for (int q = tid; q < PB_N; q += PG_NT) {
-        const int bx = q % PB_W, by = q / PB_W;
-        const Mapped m = map_cell(g, i0 - 2 + bx, j0 - 2 + by);
-        float2 v = INIT ? src[m.k] : __ldcg(src + m.k);
-        if (INIT && !(__ldg(a.heff + m.k) >= H_DISP_MIN)) v = make_float2(0.f, 0.f);
-        sv[q] = make_float2(v.x * m.sx, v.y * m.sy);
-    }
-    for (int q = tid; q < PC_N; q += PG_NT) {
-        const int bx = q % PC_W, by = q / PC_W;
-        const Mapped m = map_cell(g, i0 - 1 + bx, j0 - 1 + by);
-        scc[q] = __ldg(a.cc + m.k);
-    }
-    __syncthreads();
-    for (int q = tid; q < PC_N; q += PG_NT) {
-        const int bx = q % PC_W, by = q / PC_W;
-        const int pv = (by + 1) * PB_W + (bx + 1);
-        sf[q] = scc[q] * ((sv[pv + 1].x - sv[pv - 1].x) * g.ix + (sv[pv + PB_W].y - sv[pv - PB_W].y) * g.iy);
-    }
-    __syncthreads();
-    const int cx = tid % PG_TX, cy = tid / PG_TX;
-    const int i = i0 + cx, j = j0 + cy;
-    own_valid = i < g.nx && j < g.ny;
-    float2 av = make_float2(0.f, 0.f);
-    if (own_valid) {
-        k_own = j * g.pitch + i;
-        heff_own = __ldg(a.heff + k_own);
-        const float mask = heff_own >= H_DISP_MIN ? 1.f : 0.f;
-        const int pc = (cy + 1) * PC_W + (cx + 1);
-        const float2 v = sv[(cy + 2) * PB_W + (cx + 2)];
-        av.x = mask * (heff_own * v.x - (sf[pc + 1] - sf[pc - 1]) * g.ix);
-        av.y = mask * (heff_own * v.y - (sf[pc + PC_W] - sf[pc - PC_W]) * g.iy);
-        if (INIT) {
-            float2 d = make_float2(1.f, 1.f);
-            if (mask != 0.f) {
-                d.x = heff_own + (scc[pc + 1] + scc[pc - 1]) * 0.25f / (g.dx * g.dx);
-                d.y = heff_own + (scc[pc + PC_W] + scc[pc - PC_W]) * 0.25f / (g.dy * g.dy);
+#pragma unroll
+    for (int n = 0; n < PB_PER; n++) {
+        const int q = threadIdx.x + n * PG_NT;
+        if (q < PB_N) {
+            const Mapped m = map_cell(g, i0 - 2 + q % PB_W, j0 - 2 + q / PB_W);
+            f.sx[n] = m.sx;
+            f.sy[n] = m.sy;
+            if (INIT) {
+                f.v0[n] = a.w[m.k];
+                f.v1[n].x = __ldg(a.heff + m.k);
+            } else {
+                f.v0[n] = __ldcg(a.r + m.k);
+                f.v1[n] = __ldcg(a.diag + m.k);
+                if (!first) f.v2[n] = __ldcg(p_old + m.k);
             }
-            a.diag[k_own] = d;
-            a.w[k_own] = v;  // the warm start, masked
         }
     }
-    __syncthreads();  // the boxes are reused by the next tile
+#pragma unroll
+    for (int n = 0; n < PC_PER; n++) {
+        const int q = threadIdx.x + n * PG_NT;
+        if (q < PC_N) {
+            const Mapped m = map_cell(g, i0 - 1 + q % PC_W, j0 - 1 + q / PC_W);
+            f.c[n] = __ldg(a.cc + m.k);
+        }
+    }
+    const int i = i0 + threadIdx.x % PG_TX, j = j0 + threadIdx.x / PG_TX;
+    f.he = (i < g.nx && j < g.ny) ? __ldg(a.heff + j * g.pitch + i) : 0.f;
+}
+
+template <bool INIT>
+__device__ __forceinline__ void box_commit(const BoxPrefetch& f, TileSmem& t, float beta, bool first) {
+#pragma unroll
+    for (int n = 0; n < PB_PER; n++) {
+        const int q = threadIdx.x + n * PG_NT;
+        if (q < PB_N) {
+            float2 v;
+            if (INIT) {
+                v = f.v1[n].x >= H_DISP_MIN ? f.v0[n] : make_float2(0.f, 0.f);  // dispersion.rs:480-490
+            } else {
+                v = make_float2(f.v0[n].x / f.v1[n].x, f.v0[n].y / f.v1[n].y);  // z = r / diag
+                if (!first) {
+                    v.x += beta * f.v2[n].x;
+                    v.y += beta * f.v2[n].y;
+                }
+            }
+            t.sv[q] = make_float2(v.x * f.sx[n], v.y * f.sy[n]);
+        }
+    }
+#pragma unroll
+    for (int n = 0; n < PC_PER; n++) {
+        const int q = threadIdx.x + n * PG_NT;
+        if (q < PC_N) t.scc[q] = f.c[n];
+    }
+}
+
+// f = c div v on the tile plus one ring, then A v = mask (heff v - grad f) for the own cell
+// (dispersion.rs:269-317). sv holds v on the tile plus a 2-cell halo.
+__device__ __forceinline__ float2 apply_a(const DevGrid& g, TileSmem& t, int cx, int cy, float heff_own) {
+    for (int q = threadIdx.x; q < PC_N; q += PG_NT) {
+        const int bx = q % PC_W, by = q / PC_W;
+        const int pv = (by + 1) * PB_W + (bx + 1);
+        t.sf[q] = t.scc[q] * ((t.sv[pv + 1].x - t.sv[pv - 1].x) * g.ix + (t.sv[pv + PB_W].y - t.sv[pv - PB_W].y) * g.iy);
+    }
+    __syncthreads();
+    const float mask = heff_own >= H_DISP_MIN ? 1.f : 0.f;
+    const int pc = (cy + 1) * PC_W + (cx + 1);
+    const float2 v = t.sv[(cy + 2) * PB_W + (cx + 2)];
+    float2 av;
+    av.x = mask * (heff_own * v.x - (t.sf[pc + 1] - t.sf[pc - 1]) * g.ix);
+    av.y = mask * (heff_own * v.y - (t.sf[pc + PC_W] - t.sf[pc - PC_W]) * g.iy);
     return av;
 }
 
-__global__ void __launch_bounds__(PG_NT) pcg_kernel(PcgArgs a) {
-    __shared__ float2 sv[PB_N];
-    __shared__ float scc[PC_N];
-    __shared__ float sf[PC_N];
+// Own-cell vectors of sweep B, prefetched one tile ahead.
+struct CellPrefetch {
+    float2 p, ap, w, r, d;
+};
+
+__global__ void __launch_bounds__(PG_NT, 2) pcg_kernel(PcgArgs a) {
+    __shared__ TileSmem t;
     __shared__ double red[100];
     __shared__ float s_rate[PG_NT / 32];
     __shared__ int s_nan;
@@ -173,108 +228,123 @@ __global__ void __launch_bounds__(PG_NT) pcg_kernel(PcgArgs a) {
     if (!ctl->active) return;
     const DevGrid& g = a.g;
     const int tid = threadIdx.x;
+    const int cx = tid % PG_TX, cy = tid / PG_TX;
     const int ntiles = a.tiles_x * a.tiles_y;
     const double dt = ctl->dt;
     const float dt_f = (float)dt;
     unsigned epoch = 0;
-    int buf = 0;  // partial-sum buffer of the next reduction
+    double tot[3];
     if (tid == 0) s_nan = 0;
+    BoxPrefetch f;
 
-    // ---- initial residual: r = b - A w, z = r / diag, p = z (dispersion.rs:493-515) ----------
+    // ---- initial residual: r = b - A w (dispersion.rs:493-515) ---------------------------
     double bb = 0.0, rz_p = 0.0, rr_p = 0.0;
-    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        const int i0 = (t % a.tiles_x) * PG_TX, j0 = (t / a.tiles_x) * PG_TY;
-        bool ok;
-        int k;
-        float he;
-        const float2 aw = tile_matvec<true>(a, i0, j0, a.w, sv, scc, sf, ok, k, he);
-        if (ok) {
+    if ((int)blockIdx.x < ntiles) box_prefetch<true>(a, blockIdx.x, nullptr, true, f);
+    for (int tl = blockIdx.x; tl < ntiles; tl += gridDim.x) {
+        int i0, j0;
+        tile_origin(a, tl, i0, j0);
+        box_commit<true>(f, t, 0.f, true);
+        const float he = f.he;
+        __syncthreads();
+        if (tl + (int)gridDim.x < ntiles) box_prefetch<true>(a, tl + gridDim.x, nullptr, true, f);
+        const float2 aw = apply_a(g, t, cx, cy, he);
+        const int i = i0 + cx, j = j0 + cy;
+        if (i < g.nx && j < g.ny) {
+            const int k = j * g.pitch + i;
+            const int pc = (cy + 1) * PC_W + (cx + 1);
+            float2 d = make_float2(1.f, 1.f);
+            if (he >= H_DISP_MIN) {
+                d.x = he + (t.scc[pc + 1] + t.scc[pc - 1]) * 0.25f / (g.dx * g.dx);
+                d.y = he + (t.scc[pc + PC_W] + t.scc[pc - PC_W]) * 0.25f / (g.dy * g.dy);
+            }
             const float2 b = __ldg(a.bv + k);
-            const float2 d = a.diag[k];
             const float2 r = make_float2(b.x - aw.x, b.y - aw.y);
-            const float2 z = make_float2(r.x / d.x, r.y / d.y);
+            a.w[k] = t.sv[(cy + 2) * PB_W + (cx + 2)];  // the warm start, masked
+            a.diag[k] = d;
             a.r[k] = r;
-            a.p[k] = z;
             bb += (double)b.x * b.x + (double)b.y * b.y;
-            rz_p += (double)r.x * z.x + (double)r.y * z.y;
+            rz_p += (double)r.x * (r.x / d.x) + (double)r.y * (r.y / d.y);
             rr_p += (double)r.x * r.x + (double)r.y * r.y;
         }
+        __syncthreads();
     }
-    publish(a, buf, bb, rz_p, rr_p, red);
-    if (!grid_barrier(a, epoch)) return;
-    double tot[3];
-    grid_totals(a, buf, 3, tot, red);
-    buf ^= 1;
+    if (!reduce_barrier(a, epoch, bb, rz_p, rr_p, tot, red)) return;
     const double target = a.tol * sqrt(tot[0]) + 1e-10;
     double rz = tot[1];
     bool converged = sqrt(tot[2]) <= target;
     long long it = 0;
+    float beta_f = 0.f;
 
     while (!converged && it < a.max_iter) {
-        // sweep A: Ap and <p, Ap>
+        const float2* p_old = (it & 1) ? a.p1 : a.p0;
+        float2* p_new = (it & 1) ? a.p0 : a.p1;
+        const bool first = it == 0;
+        // sweep A': p = z + beta p on the tile and its halo, then A p and <p, Ap>
         double pap = 0.0;
-        for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-            const int i0 = (t % a.tiles_x) * PG_TX, j0 = (t / a.tiles_x) * PG_TY;
-            bool ok;
-            int k;
-            float he;
-            const float2 av = tile_matvec<false>(a, i0, j0, a.p, sv, scc, sf, ok, k, he);
-            if (ok) {
-                a.ap[k] = av;
-                const float2 p = __ldcg(a.p + k);
-                pap += (double)p.x * av.x + (double)p.y * av.y;
-            }
-        }
-        publish(a, buf, pap, 0.0, 0.0, red);
-        if (!grid_barrier(a, epoch)) return;
-        grid_totals(a, buf, 1, tot, red);
-        buf ^= 1;
-        const double alpha = rz / tot[0];
-        const float alpha_f = (float)alpha;
-        // sweep B: w += alpha p, r -= alpha Ap, z = r / diag; <r, r> and <r, z>
-        double rr = 0.0, rzn = 0.0;
-        for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-            const int i = (t % a.tiles_x) * PG_TX + tid % PG_TX;
-            const int j = (t / a.tiles_x) * PG_TY + tid / PG_TX;
+        if ((int)blockIdx.x < ntiles) box_prefetch<false>(a, blockIdx.x, p_old, first, f);
+        for (int tl = blockIdx.x; tl < ntiles; tl += gridDim.x) {
+            int i0, j0;
+            tile_origin(a, tl, i0, j0);
+            box_commit<false>(f, t, beta_f, first);
+            const float he = f.he;
+            __syncthreads();
+            if (tl + (int)gridDim.x < ntiles) box_prefetch<false>(a, tl + gridDim.x, p_old, first, f);
+            const float2 av = apply_a(g, t, cx, cy, he);
+            const int i = i0 + cx, j = j0 + cy;
             if (i < g.nx && j < g.ny) {
                 const int k = j * g.pitch + i;
-                const float2 p = __ldcg(a.p + k), ap = __ldcg(a.ap + k);
-                float2 w = __ldcg(a.w + k), r = __ldcg(a.r + k);
-                const float2 d = __ldcg(a.diag + k);
-                w.x += alpha_f * p.x;
-                w.y += alpha_f * p.y;
-                r.x -= alpha_f * ap.x;
-                r.y -= alpha_f * ap.y;
+                const float2 p = t.sv[(cy + 2) * PB_W + (cx + 2)];
+                p_new[k] = p;
+                a.ap[k] = av;
+                pap += (double)p.x * av.x + (double)p.y * av.y;
+            }
+            __syncthreads();
+        }
+        if (!reduce_barrier(a, epoch, pap, 0.0, 0.0, tot, red)) return;
+        const double alpha = rz / tot[0];
+        const float alpha_f = (float)alpha;
+        // sweep B: w += alpha p, r -= alpha Ap, <r, r> and <r, z>
+        double rr = 0.0, rzn = 0.0;
+        CellPrefetch c{};
+        auto cell_load = [&](int tl, CellPrefetch& o) {
+            int i0, j0;
+            tile_origin(a, tl, i0, j0);
+            const int i = i0 + cx, j = j0 + cy;
+            if (i < g.nx && j < g.ny) {
+                const int k = j * g.pitch + i;
+                o.p = __ldcg(p_new + k);
+                o.ap = __ldcg(a.ap + k);
+                o.w = __ldcg(a.w + k);
+                o.r = __ldcg(a.r + k);
+                o.d = __ldcg(a.diag + k);
+            }
+        };
+        if ((int)blockIdx.x < ntiles) cell_load(blockIdx.x, c);
+        for (int tl = blockIdx.x; tl < ntiles; tl += gridDim.x) {
+            const CellPrefetch cur = c;
+            if (tl + (int)gridDim.x < ntiles) cell_load(tl + gridDim.x, c);
+            int i0, j0;
+            tile_origin(a, tl, i0, j0);
+            const int i = i0 + cx, j = j0 + cy;
+            if (i < g.nx && j < g.ny) {
+                const int k = j * g.pitch + i;
+                float2 w = cur.w, r = cur.r;
+                w.x += alpha_f * cur.p.x;
+                w.y += alpha_f * cur.p.y;
+                r.x -= alpha_f * cur.ap.x;
+                r.y -= alpha_f * cur.ap.y;
                 a.w[k] = w;
                 a.r[k] = r;
                 rr += (double)r.x * r.x + (double)r.y * r.y;
-                rzn += (double)r.x * (r.x / d.x) + (double)r.y * (r.y / d.y);
+                rzn += (double)r.x * (r.x / cur.d.x) + (double)r.y * (r.y / cur.d.y);
             }
         }
-        publish(a, buf, rr, rzn, 0.0, red);
-        if (!grid_barrier(a, epoch)) return;
-        grid_totals(a, buf, 2, tot, red);
-        buf ^= 1;
+        if (!reduce_barrier(a, epoch, rr, rzn, 0.0, tot, red)) return;
         it += 1;
         converged = sqrt(tot[0]) <= target;
         const double beta = tot[1] / rz;
         rz = tot[1];
-        if (converged || it >= a.max_iter) break;
-        // sweep C: p = z + beta p
-        const float beta_f = (float)beta;
-        for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-            const int i = (t % a.tiles_x) * PG_TX + tid % PG_TX;
-            const int j = (t / a.tiles_x) * PG_TY + tid / PG_TX;
-            if (i < g.nx && j < g.ny) {
-                const int k = j * g.pitch + i;
-                const float2 r = __ldcg(a.r + k), d = __ldcg(a.diag + k);
-                float2 p = __ldcg(a.p + k);
-                p.x = r.x / d.x + beta_f * p.x;
-                p.y = r.y / d.y + beta_f * p.y;
-                a.p[k] = p;
-            }
-        }
-        if (!grid_barrier(a, epoch)) return;
+        beta_f = (float)beta;
     }
     if (blockIdx.x == 0 && tid == 0) {
         ctl->solves += 1;
@@ -282,21 +352,22 @@ __global__ void __launch_bounds__(PG_NT) pcg_kernel(PcgArgs a) {
         if (!converged) ctl->unconverged += 1;
         ctl->last_iterations = (int)it;
     }
-    // The solution of every cell must be final before any CTA finishes the stage.
-    if (!grid_barrier(a, epoch)) return;
 
-    // ---- finish the stage: the state from the solve --------------------------------------------
+    // ---- finish the stage from the solution (every w is final: the last reduction was a barrier)
     float rmax = 0.f;
     int nan_here = 0;
-    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        const int i = (t % a.tiles_x) * PG_TX + tid % PG_TX;
-        const int j = (t / a.tiles_x) * PG_TY + tid / PG_TX;
+    for (int tl = blockIdx.x; tl < ntiles; tl += gridDim.x) {
+        int i0, j0;
+        tile_origin(a, tl, i0, j0);
+        const int i = i0 + cx, j = j0 + cy;
         if (i >= g.nx || j >= g.ny) continue;
         const int k = j * g.pitch + i;
         const float2 hn = __ldg(a.hn + k);
         const float2 pr = __ldg(a.pred + k);
         const float2 w = __ldcg(a.w + k);
         const float he = __ldg(a.heff + k);
+        float4 q0 = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (a.mode == MODE_STAGE2) q0 = __ldg(a.qold + k);
         double h = (double)hn.x + (double)hn.y;
         float hu = pr.x + dt_f * (he * w.x);
         float hv = pr.y + dt_f * (he * w.y);
@@ -306,7 +377,6 @@ __global__ void __launch_bounds__(PG_NT) pcg_kernel(PcgArgs a) {
             continue;
         }
         if (a.mode == MODE_STAGE2) {
-            const float4 q0 = __ldg(a.qold + k);
             h = 0.5 * (depth64(q0) + h);
             hu = 0.5f * (q0.z + hu);
             hv = 0.5f * (q0.w + hv);

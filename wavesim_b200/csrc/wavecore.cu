@@ -89,11 +89,11 @@ struct wc_solver {
     float* prof = nullptr;
     float2* ycs = nullptr;
     uint8_t* shallow = nullptr;
-    float2 *hn = nullptr, *pred = nullptr, *bv = nullptr, *w = nullptr, *r = nullptr, *p = nullptr,
-           *ap = nullptr, *diag = nullptr;
+    float2 *hn = nullptr, *pred = nullptr, *bv = nullptr, *w = nullptr, *r = nullptr, *p0 = nullptr,
+           *p1 = nullptr, *ap = nullptr, *diag = nullptr;
     float *cc = nullptr, *heff = nullptr;
-    double* part = nullptr;
-    unsigned* bar = nullptr;
+    double* part = nullptr;   // CTA partials of the solve's reductions
+    unsigned* bar = nullptr;  // grid-barrier counters: arrivals, released epoch
     Ctl* ctl = nullptr;
     Ctl* ctl_host = nullptr;  // pinned mirror
     double *st_h = nullptr, *st_hu = nullptr, *st_hv = nullptr;  // padded FP64 staging
@@ -114,7 +114,7 @@ struct wc_solver {
     std::vector<cudaEvent_t> prof_pool;
 
     ~wc_solver() {
-        void* bufs[] = {q0, q1, bed, prof, ycs, shallow, hn, pred, bv, w, r, p, ap, diag, cc, heff,
+        void* bufs[] = {q0, q1, bed, prof, ycs, shallow, hn, pred, bv, w, r, p0, p1, ap, diag, cc, heff,
                         part, bar, ctl, st_h, st_hu, st_hv, r64, diag_bands, diag_done, diag_out};
         for (void* b : bufs)
             if (b) cudaFree(b);
@@ -255,11 +255,12 @@ wc_status launch_pcg(wc_solver* s, int mode, const float4* qold, float4* qout) {
     a.bv = s->bv;
     a.w = s->w;
     a.r = s->r;
-    a.p = s->p;
+    a.p0 = s->p0;
+    a.p1 = s->p1;
     a.ap = s->ap;
     a.diag = s->diag;
     a.part = s->part;
-    a.bar = s->bar;
+    a.cnt = s->bar;
     a.hn = s->hn;
     a.pred = s->pred;
     a.qold = qold;
@@ -534,12 +535,12 @@ wc_status wc_solver_create(const wc_grid* grid, const double* bed_padded, const 
         ALLOC(s->bv, s->ncell);
         ALLOC(s->w, s->ncell);
         ALLOC(s->r, s->ncell);
-        ALLOC(s->p, s->ncell);
+        ALLOC(s->p0, s->ncell);
+        ALLOC(s->p1, s->ncell);
         ALLOC(s->ap, s->ncell);
         ALLOC(s->diag, s->ncell);
         ALLOC(s->cc, s->ncell);
         ALLOC(s->heff, s->ncell);
-        ALLOC(s->bar, 2);
         int dev = 0, sms = 0, occ = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -548,8 +549,9 @@ wc_status wc_solver_create(const wc_grid* grid, const double* bed_padded, const 
         s->pcg_tiles_x = (nx + PG_TX - 1) / PG_TX;
         s->pcg_tiles_y = (ny + PG_TY - 1) / PG_TY;
         const int tiles = s->pcg_tiles_x * s->pcg_tiles_y;
-        s->pcg_blocks = std::max(1, std::min(tiles, sms * std::min(occ, 2)));
-        ALLOC(s->part, 2 * 4 * (size_t)s->pcg_blocks);
+        s->pcg_blocks = std::max(1, std::min(tiles, sms * std::min(occ, 4)));
+        ALLOC(s->part, 4 * (size_t)s->pcg_blocks);
+        ALLOC(s->bar, 2);
     }
 #undef ALLOC
     if (cudaMallocHost(&s->ctl_host, sizeof(Ctl)) != cudaSuccess)

@@ -120,7 +120,8 @@ def sgn_beach(nx: int, ny: int, dx: float, seed: int, tolerance: float = 1e-8, h
               period: float = 14.0, angle_deg: float = 15.0, sigma_bed: float = 0.5, corr: float = 20.0,
               name: str | None = None, steps: int = 5000, preconditioner: int = 0) -> Workload:
     """Fifth order + SGN by PCG, periodic in y: a 20 m shelf, then a 1:30 beach whose still-water
-    shoreline is at 0.85 Lx, plus a Gaussian random field; maker H, T at x = 160 m in ~20 m,
+    shoreline is at 0.85 Lx, plus a Gaussian random field; maker H, T at x = 160 m (0.15 Lx on
+    small grids) in ~20 m,
     oblique at the angle nearest `angle_deg` that fits the periodic width; a 100 m sponge at the
     offshore edge; Manning 0.02; CFL 0.4."""
     grid = Grid(nx, ny, dx, dx)
@@ -128,7 +129,7 @@ def sgn_beach(nx: int, ny: int, dx: float, seed: int, tolerance: float = 1e-8, h
     base = shelf_and_beach(grid, 20.0, 1.0 / 30.0, 0.85 * lx)
     b = base + gaussian_field(nx, ny, dx, dx, sigma_bed, corr, seed)
     bed = Bathymetry.from_interior(grid, b)
-    maker_x = 160.0
+    maker_x = min(160.0, 0.15 * lx)
     i_m = min(max(int(round(maker_x / dx - 0.5)), 0), nx - 1)
     depth = -b[ny // 2, i_m]
     omega = 2.0 * math.pi / period
