@@ -204,6 +204,22 @@ typedef struct wc_kernel_time {
 wc_status wc_profile_enable(wc_solver* s, int32_t on);
 wc_status wc_profile_read(wc_solver* s, wc_kernel_time out[3]);
 
+/* No counterpart in the reference: wc_stable_dt for callers that cannot allocate device memory
+ * when they need the time step, such as code running while a CUDA stream capture is open (where
+ * cudaMalloc is not allowed) or an application that hands all device memory to its own pool
+ * allocator and runs under a fixed budget. The state belongs to the caller: padded FP64 device
+ * arrays h, hu, hv of (nx+6)*(ny+6) values each, read on `stream` (a cudaStream_t; NULL is the
+ * legacy default stream). The call allocates nothing: its scratch is a fixed 64 KiB array inside
+ * the library, which every GPU that loads the library holds until the process exits, and grids
+ * of more than 16,777,216 interior cells (4096 x 4096) are refused with WC_EINVAL. The first call
+ * on a device looks up that array's device address, so make it before any stream capture begins.
+ * All calls share the one array, which keeps the last call's contents (each call rewrites every
+ * slot it reads): calls that overlap on the GPU race, so do not run two at once. Returns in
+ * *dt_out, with the same status, what wc_stable_dt returns for the same state. */
+wc_status wc_stable_dt_noalloc(const wc_grid* grid, double cfl, const double* d_h,
+                               const double* d_hu, const double* d_hv, void* stream,
+                               double* dt_out);
+
 /* Kernel launches this solver has queued since it was created (for accounting). */
 uint64_t wc_launch_count(const wc_solver* s);
 /* Human-readable text of the last error on this thread ("" if none). */

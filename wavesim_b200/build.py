@@ -11,7 +11,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libwavecore_b200.so")
-SOURCES = [os.path.join(HERE, "csrc", "wavecore.cu")]
+SOURCES = [os.path.join(HERE, "csrc", "wavecore.cu"), os.path.join(HERE, "csrc", "noalloc.cu")]
 DEPENDS = [os.path.join(HERE, "csrc", f) for f in os.listdir(os.path.join(HERE, "csrc"))] + [
     os.path.join(ROOT, "include", "wavecore_c.h")
 ]

@@ -66,6 +66,10 @@ wc_status linear_wave(double omega, double h, bool dispersive, double* k, double
 
 }  // namespace
 
+namespace wcb_host {
+void set_last_error(const std::string& msg) { g_err = msg; }
+}  // namespace wcb_host
+
 struct wc_solver {
     wc_grid grid{};
     DevGrid g{};

@@ -48,6 +48,7 @@ EXPORTS = [
     "wc_profile_read",
     "wc_launch_count",
     "wc_last_error",
+    "wc_stable_dt_noalloc",
 ]
 
 
@@ -89,6 +90,8 @@ def load(path: str = LIB_PATH):
     L.wc_set_stream.argtypes = [V, V]
     L.wc_profile_enable.argtypes = [V, C.c_int32]
     L.wc_profile_read.argtypes = [V, C.POINTER(abi.wc_kernel_time)]
+    L.wc_stable_dt_noalloc.argtypes = [C.POINTER(abi.wc_grid), C.c_double, V, V, V, V, D]
+    L.wc_stable_dt_noalloc.restype = C.c_int
     L.wc_launch_count.argtypes = [V]
     L.wc_launch_count.restype = C.c_uint64
     L.wc_last_error.restype = C.c_char_p
@@ -113,6 +116,20 @@ def _check(status: int, allow=(abi.WC_OK,)):
         warnings.warn(load().wc_last_error().decode(), RuntimeWarning, stacklevel=3)
         return status
     raise WavecoreError(status, load().wc_last_error().decode())
+
+
+def stable_dt_noalloc(grid, cfl: float, d_h: int, d_hu: int, d_hv: int, stream: int = 0) -> float:
+    """`wc_stable_dt_noalloc`: the time-step limit of a state held in the caller's device memory
+    (padded FP64 arrays given as device addresses), computed without allocating anything. For
+    callers that cannot allocate device memory at that point, e.g. inside a stream capture."""
+    g = grid.to_c()
+    out = C.c_double()
+    _check(
+        load().wc_stable_dt_noalloc(C.byref(g), float(cfl), C.c_void_p(d_h), C.c_void_p(d_hu), C.c_void_p(d_hv),
+                                    C.c_void_p(stream or None), C.byref(out)),
+        allow=(abi.WC_OK, abi.WC_ENAN),
+    )
+    return out.value
 
 
 class Solver(SolverConfig):
