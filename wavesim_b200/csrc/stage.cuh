@@ -27,31 +27,38 @@
 
 namespace wcb {
 
-constexpr int ST_TX = 32, ST_TY = 16, ST_HALO = 4;
-constexpr int ST_BX = ST_TX + 2 * ST_HALO, ST_BY = ST_TY + 2 * ST_HALO, ST_NB = ST_BX * ST_BY;
-constexpr int ST_NT = 256;
-constexpr int SX_W = ST_TX + 2, SX_N = SX_W * ST_TY;   // x reconstructions: cx in [-1, TX]
-constexpr int SY_H = ST_TY + 2, SY_N = ST_TX * SY_H;   // y reconstructions: cy in [-1, TY]
-constexpr int FX_W = ST_TX + 1, FX_N = FX_W * ST_TY;   // x faces
-constexpr int FY_H = ST_TY + 1, FY_N = ST_TX * FY_H;   // y faces
-constexpr int DV_W = ST_TX + 4, DV_H = ST_TY + 4, DV_N = DV_W * DV_H;  // div on [-2, T+2)
-constexpr int CF_W = ST_TX + 2, CF_H = ST_TY + 2, CF_N = CF_W * CF_H;  // c, cN on [-1, T+1)
-constexpr int OWN = ST_TX * ST_TY;
+constexpr int ST_TX = 32, ST_HALO = 4, ST_BX = ST_TX + 2 * ST_HALO;
+constexpr int ST_TY = 16;  // tile height of the standalone stage kernel
+constexpr int ST_NT = 256; // its block size
 
-// Shared-memory layout, in floats.
-constexpr int OFF_ETA = 0, OFF_H = ST_NB, OFF_U = 2 * ST_NB, OFF_V = 3 * ST_NB, OFF_B = 4 * ST_NB;
-constexpr int OFF_PHI = 5 * ST_NB;
-constexpr int OFF_SX = 6 * ST_NB;             // 8 arrays of SX_N
-constexpr int OFF_SY = OFF_SX + 8 * SX_N;     // 8 arrays of SY_N
-constexpr int OFF_P = OFF_SY + 8 * SY_N;      // Px, Py: 2 * OWN
-constexpr int OFF_DIV = OFF_P + 2 * OWN;      // dispersive runs only
-constexpr int OFF_C = OFF_DIV + DV_N;
-constexpr int OFF_F = OFF_C + CF_N;
-constexpr int SMEM_SWE = OFF_DIV * 4;
-constexpr int SMEM_SGN = (OFF_F + CF_N) * 4;
-// Face fluxes reuse the box (dead after P3): 4 arrays of FX_N, then 4 of FY_N.
-constexpr int OFF_FX = 0, OFF_FY = 4 * FX_N;
-static_assert(4 * FX_N + 4 * FY_N <= 5 * ST_NB, "face arrays must fit in the box");
+// Tile geometry for a TX x TY tile (TX = 32) and the shared-memory layout of one tile, in floats.
+template <int TY>
+struct StageGeom {
+    static constexpr int BY = TY + 2 * ST_HALO, NB = ST_BX * BY;
+    static constexpr int SX_W = ST_TX + 2, SX_N = SX_W * TY;   // x reconstructions: cx in [-1, TX]
+    static constexpr int SY_H = TY + 2, SY_N = ST_TX * SY_H;   // y reconstructions: cy in [-1, TY]
+    static constexpr int FX_W = ST_TX + 1, FX_N = FX_W * TY;   // x faces
+    static constexpr int FY_H = TY + 1, FY_N = ST_TX * FY_H;   // y faces
+    static constexpr int DV_W = ST_TX + 4, DV_H = TY + 4, DV_N = DV_W * DV_H;  // div on [-2, T+2)
+    static constexpr int CF_W = ST_TX + 2, CF_H = TY + 2, CF_N = CF_W * CF_H;  // c, cN on [-1, T+1)
+    static constexpr int OWN = ST_TX * TY;
+    static constexpr int OFF_ETA = 0, OFF_H = NB, OFF_U = 2 * NB, OFF_V = 3 * NB, OFF_B = 4 * NB;
+    static constexpr int OFF_PHI = 5 * NB;
+    static constexpr int OFF_SX = 6 * NB;             // 8 arrays of SX_N
+    static constexpr int OFF_SY = OFF_SX + 8 * SX_N;  // 8 arrays of SY_N
+    static constexpr int OFF_P = OFF_SY + 8 * SY_N;   // Px, Py: 2 * OWN
+    static constexpr int OFF_DIV = OFF_P + 2 * OWN;   // dispersive runs only
+    static constexpr int OFF_C = OFF_DIV + DV_N;
+    static constexpr int OFF_F = OFF_C + CF_N;
+    static constexpr int SMEM_SWE = OFF_DIV * 4;
+    static constexpr int SMEM_SGN = (OFF_F + CF_N) * 4;
+    // Face fluxes reuse the box (dead after P3): 4 arrays of FX_N, then 4 of FY_N.
+    static constexpr int OFF_FX = 0, OFF_FY = 4 * FX_N;
+    static_assert(4 * FX_N + 4 * FY_N <= 5 * NB, "face arrays must fit in the box");
+};
+
+constexpr int SMEM_SWE = StageGeom<ST_TY>::SMEM_SWE;
+constexpr int SMEM_SGN = StageGeom<ST_TY>::SMEM_SGN;
 
 enum StageMode { MODE_STAGE1 = 0, MODE_STAGE2 = 1, MODE_FIRST = 2 };
 
@@ -115,15 +122,15 @@ __device__ __forceinline__ void face_values(float v0, float v1, float c, float v
 
 // solver.rs:140-183 for the cell at shared index p, stencil stride s. Writes both face sides and
 // the cell's combined pressure + bed-source term P = g/2 (h_hi + h_lo)(eta_hi - eta_lo).
-template <int ORDER>
+template <int ORDER, typename Gm>
 __device__ __forceinline__ void reconstruct(const float* __restrict__ sm, int p, int s,
                                             bool x_axis, Side& lo, Side& hi, float& P) {
-    const float* eta = sm + OFF_ETA;
-    const float* hh = sm + OFF_H;
-    const float* un = sm + (x_axis ? OFF_U : OFF_V);
-    const float* ut = sm + (x_axis ? OFF_V : OFF_U);
-    const float* bb = sm + OFF_B;
-    const float* phi = sm + OFF_PHI;
+    const float* eta = sm + Gm::OFF_ETA;
+    const float* hh = sm + Gm::OFF_H;
+    const float* un = sm + (x_axis ? Gm::OFF_U : Gm::OFF_V);
+    const float* ut = sm + (x_axis ? Gm::OFF_V : Gm::OFF_U);
+    const float* bb = sm + Gm::OFF_B;
+    const float* phi = sm + Gm::OFF_PHI;
     const float hc = hh[p];
     Side first;
     first.eta = eta[p];
@@ -202,25 +209,36 @@ __device__ __forceinline__ void hll_face(const Side& l, const Side& r, float& F0
     }
 }
 
-template <int MODE, int ORDER, bool SGN>
-__global__ void __launch_bounds__(ST_NT) stage_kernel(StageArgs a) {
-    extern __shared__ float4 smem4[];
-    float* sm = reinterpret_cast<float*>(smem4);
-    __shared__ float s_maker[2];
-    __shared__ float s_red[ST_NT / 32];
-    __shared__ int s_nan;
+// Shared scalars of one tile's work.
+struct StageShared {
+    float maker[2];
+};
 
+// One RK stage on the TX x TY tile at (i0, j0), by a block of NT threads, in the dynamic shared
+// memory `sm`. Finishing shallow-water stages fold the tile's CFL rate into rmax / nan_here.
+template <int MODE, int ORDER, bool SGN, int TY, int NT>
+__device__ __forceinline__ void stage_tile(const StageArgs& a, int i0, int j0, float* sm,
+                                           StageShared& ss, float& rmax, int& nan_here) {
+    using Gm = StageGeom<TY>;
+    constexpr int ST_BY = Gm::BY, ST_NB = Gm::NB;
+    constexpr int SX_W = Gm::SX_W, SX_N = Gm::SX_N, SY_N = Gm::SY_N, FX_W = Gm::FX_W;
+    constexpr int FX_N = Gm::FX_N, FY_N = Gm::FY_N, DV_W = Gm::DV_W, DV_N = Gm::DV_N;
+    constexpr int CF_W = Gm::CF_W, CF_N = Gm::CF_N, OWN = Gm::OWN;
+    constexpr int OFF_ETA = Gm::OFF_ETA, OFF_H = Gm::OFF_H, OFF_U = Gm::OFF_U, OFF_V = Gm::OFF_V;
+    constexpr int OFF_B = Gm::OFF_B, OFF_PHI = Gm::OFF_PHI, OFF_SX = Gm::OFF_SX, OFF_SY = Gm::OFF_SY;
+    constexpr int OFF_P = Gm::OFF_P, OFF_DIV = Gm::OFF_DIV, OFF_C = Gm::OFF_C, OFF_F = Gm::OFF_F;
+    constexpr int OFF_FX = Gm::OFF_FX, OFF_FY = Gm::OFF_FY;
+    constexpr int ST_TY_ = TY;
     const Ctl* ctl = a.ctl;
-    if (!ctl->active) return;
     const DevGrid& g = a.g;
     const int tid = threadIdx.x;
-    const int i0 = blockIdx.x * ST_TX, j0 = blockIdx.y * ST_TY;
+    float* s_maker = ss.maker;
     const double dt = ctl->dt;
     const float dt_f = (float)dt;
     const float dtdx = (float)(dt / g.dxd), dtdy = (float)(dt / g.dyd);
 
+    __syncthreads();  // the previous tile's shared memory is free
     if (tid == 0) {
-        s_nan = 0;
         if (a.maker.on) {
             // forcing.rs:124-138 split as profile(x) * ramp(t) * (sin wt cos k_y y - cos wt sin k_y y)
             const double t = ctl->t + (a.stage_time_plus_dt ? dt : 0.0);
@@ -233,7 +251,7 @@ __global__ void __launch_bounds__(ST_NT) stage_kernel(StageArgs a) {
     }
 
     // ---- P1: the box with ghost cells synthesised ------------------------------------------
-    for (int p = tid; p < ST_NB; p += ST_NT) {
+    for (int p = tid; p < ST_NB; p += NT) {
         const int bx = p % ST_BX, by = p / ST_BX;
         const Mapped m = map_cell(g, i0 - ST_HALO + bx, j0 - ST_HALO + by);
         const float4 q = __ldg(a.qin + m.k);
@@ -250,7 +268,7 @@ __global__ void __launch_bounds__(ST_NT) stage_kernel(StageArgs a) {
     // ---- P2: breaking switch on [-3, T+3) ----------------------------------------------------
     if (ORDER == 2 || SGN) {
         constexpr int W = ST_BX - 2, H = ST_BY - 2;
-        for (int w = tid; w < W * H; w += ST_NT) {
+        for (int w = tid; w < W * H; w += NT) {
             const int bx = 1 + w % W, by = 1 + w / W;
             const int p = by * ST_BX + bx;
             const float h = sm[OFF_H + p];
@@ -274,7 +292,7 @@ __global__ void __launch_bounds__(ST_NT) stage_kernel(StageArgs a) {
     if (SGN) {
         __syncthreads();
         // div of the masked velocities on [-2, T+2)
-        for (int w = tid; w < DV_N; w += ST_NT) {
+        for (int w = tid; w < DV_N; w += NT) {
             const int bx = 2 + w % DV_W, by = 2 + w / DV_W;
             const int p = by * ST_BX + bx;
             auto um = [&](int q) { return sm[OFF_H + q] >= H_DISP_MIN ? sm[OFF_U + q] : 0.f; };
@@ -283,7 +301,7 @@ __global__ void __launch_bounds__(ST_NT) stage_kernel(StageArgs a) {
         }
         __syncthreads();
         // c and c N on [-1, T+1)
-        for (int w = tid; w < CF_N; w += ST_NT) {
+        for (int w = tid; w < CF_N; w += NT) {
             const int cx = w % CF_W, cy = w / CF_W;
             const int p = (cy + 3) * ST_BX + (cx + 3);
             const int d = (cy + 1) * DV_W + (cx + 1);
@@ -305,7 +323,7 @@ __global__ void __launch_bounds__(ST_NT) stage_kernel(StageArgs a) {
     __syncthreads();
 
     // ---- P3: reconstructions, one per cell and axis -------------------------------------------
-    for (int w = tid; w < SX_N + SY_N; w += ST_NT) {
+    for (int w = tid; w < SX_N + SY_N; w += NT) {
         Side lo, hi;
         float P;
         float* side;
@@ -313,7 +331,7 @@ __global__ void __launch_bounds__(ST_NT) stage_kernel(StageArgs a) {
         if (w < SX_N) {
             const int cx = w % SX_W - 1, cy = w / SX_W;
             const int p = (cy + ST_HALO) * ST_BX + (cx + ST_HALO);
-            reconstruct<ORDER>(sm, p, 1, true, lo, hi, P);
+            reconstruct<ORDER, Gm>(sm, p, 1, true, lo, hi, P);
             if (cx >= 0 && cx < ST_TX) sm[OFF_P + cy * ST_TX + cx] = P;
             side = sm + OFF_SX;
             idx = w;
@@ -322,8 +340,8 @@ __global__ void __launch_bounds__(ST_NT) stage_kernel(StageArgs a) {
             const int v = w - SX_N;
             const int cx = v % ST_TX, cy = v / ST_TX - 1;
             const int p = (cy + ST_HALO) * ST_BX + (cx + ST_HALO);
-            reconstruct<ORDER>(sm, p, ST_BX, false, lo, hi, P);
-            if (cy >= 0 && cy < ST_TY) sm[OFF_P + OWN + cy * ST_TX + cx] = P;
+            reconstruct<ORDER, Gm>(sm, p, ST_BX, false, lo, hi, P);
+            if (cy >= 0 && cy < ST_TY_) sm[OFF_P + OWN + cy * ST_TX + cx] = P;
             side = sm + OFF_SY;
             idx = v;
             n = SY_N;
@@ -340,7 +358,7 @@ __global__ void __launch_bounds__(ST_NT) stage_kernel(StageArgs a) {
     __syncthreads();
 
     // ---- P4: face fluxes, once per face (writes over the dead box) ----------------------------
-    for (int w = tid; w < FX_N + FY_N; w += ST_NT) {
+    for (int w = tid; w < FX_N + FY_N; w += NT) {
         Side l, r;
         float* out;
         int idx, n;
@@ -374,11 +392,9 @@ __global__ void __launch_bounds__(ST_NT) stage_kernel(StageArgs a) {
     __syncthreads();
 
     // ---- P5: per-cell update ------------------------------------------------------------------
-    float rmax = 0.f;
-    int nan_here = 0;
     const float* fx = sm + OFF_FX;
     const float* fy = sm + OFF_FY;
-    for (int c = tid; c < OWN; c += ST_NT) {
+    for (int c = tid; c < OWN; c += NT) {
         const int cx = c % ST_TX, cy = c / ST_TX;
         const int i = i0 + cx, j = j0 + cy;
         if (i >= g.nx || j >= g.ny) continue;
@@ -446,19 +462,38 @@ __global__ void __launch_bounds__(ST_NT) stage_kernel(StageArgs a) {
             }
         }
     }
-    if (!SGN && MODE != MODE_STAGE1) {
-        rmax = warp_max(rmax);
-        if (nan_here) s_nan = 1;  // benign race: every writer stores 1
-        if ((tid & 31) == 0) s_red[tid >> 5] = rmax;
-        __syncthreads();
-        if (tid == 0) {
-            float m = 0.f;
-            for (int w = 0; w < ST_NT / 32; w++) m = fmaxf(m, s_red[w]);
-            s_red[0] = m;
-        }
-        __syncthreads();
-        fold_rate_and_finish(a.ctl, s_red[0], s_nan, gridDim.x * gridDim.y);
+}
+
+// A finishing shallow-water stage: the block's CFL rate, folded into the device clock.
+template <int NT>
+__device__ __forceinline__ void stage_fold(Ctl* ctl, float rmax, int nan_here, unsigned nblocks) {
+    __shared__ float s_red[NT / 32];
+    __shared__ int s_nan;
+    if (threadIdx.x == 0) s_nan = 0;
+    __syncthreads();
+    rmax = warp_max(rmax);
+    if (nan_here) s_nan = 1;  // every writer stores 1
+    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = rmax;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float m = 0.f;
+        for (int w = 0; w < NT / 32; w++) m = fmaxf(m, s_red[w]);
+        s_red[0] = m;
     }
+    __syncthreads();
+    fold_rate_and_finish(ctl, s_red[0], s_nan, nblocks);
+}
+
+template <int MODE, int ORDER, bool SGN>
+__global__ void __launch_bounds__(ST_NT) stage_kernel(StageArgs a) {
+    extern __shared__ float4 smem4[];
+    float* sm = reinterpret_cast<float*>(smem4);
+    __shared__ StageShared ss;
+    if (!a.ctl->active) return;
+    float rmax = 0.f;
+    int nan_here = 0;
+    stage_tile<MODE, ORDER, SGN, ST_TY, ST_NT>(a, blockIdx.x * ST_TX, blockIdx.y * ST_TY, sm, ss, rmax, nan_here);
+    if (!SGN && MODE != MODE_STAGE1) stage_fold<ST_NT>(a.ctl, rmax, nan_here, gridDim.x * gridDim.y);
 }
 
 }  // namespace wcb

@@ -116,6 +116,12 @@ struct wc_solver {
     };
     std::vector<ProfEv> prof_live;
     std::vector<cudaEvent_t> prof_pool;
+    // One captured step, replayed by the device-resident stepping (not used while profiling).
+    cudaGraphExec_t step_graph = nullptr;
+    bool graph_failed = false;
+    // The device clock's stable_dt describes the resident state (set by every step's last kernel,
+    // cleared by an upload), so adaptive stepping need not recompute it.
+    bool rate_current = false;
 
     ~wc_solver() {
         void* bufs[] = {q0, q1, bed, prof, ycs, shallow, hn, pred, bv, w, r, p0, p1, ap, diag, cc, heff,
@@ -128,6 +134,7 @@ struct wc_solver {
             cudaEventDestroy(e.b);
         }
         for (auto e : prof_pool) cudaEventDestroy(e);
+        if (step_graph) cudaGraphExecDestroy(step_graph);
         if (own_stream) cudaStreamDestroy(own_stream);
     }
 };
@@ -280,15 +287,24 @@ wc_status launch_pcg(wc_solver* s, int mode, const float4* qold, float4* qout) {
     a.timeout_ns = BARRIER_TIMEOUT_NS;
     CK(cudaMemsetAsync(s->bar, 0, 2 * sizeof(unsigned), s->stream));
     ProfScope ps(s, 1);
-    void* args[] = {&a};
-    CK(cudaLaunchCooperativeKernel((void*)pcg_kernel, dim3(s->pcg_blocks), dim3(PG_NT), args, 0,
-                                   s->stream));
+    // A cooperative launch: every CTA is resident at once, so the grid barriers cannot deadlock.
+    cudaLaunchConfig_t lc{};
+    lc.gridDim = dim3(s->pcg_blocks);
+    lc.blockDim = dim3(PG_NT);
+    lc.dynamicSmemBytes = 0;
+    lc.stream = s->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    lc.attrs = attr;
+    lc.numAttrs = 1;
+    CK(cudaLaunchKernelEx(&lc, pcg_kernel, a));
     s->launches++;
     return WC_OK;
 }
 
 // One SSP-RK2 step (solver.rs:479-507) of size ctl->dt on the device-resident state q0.
-wc_status enqueue_step(wc_solver* s) {
+wc_status enqueue_step_direct(wc_solver* s) {
     if (s->order == WC_ORDER_FIRST) {
         TRY(launch_stage(s, MODE_FIRST, s->q0, s->q0, s->q1, false));
         if (s->sgn) TRY(launch_pcg(s, MODE_FIRST, s->q0, s->q1));
@@ -304,6 +320,44 @@ wc_status enqueue_step(wc_solver* s) {
     TRY(launch_pcg(s, MODE_STAGE1, s->q0, s->q1));
     TRY(launch_stage(s, MODE_STAGE1, s->q1, s->q0, s->q1, true));
     TRY(launch_pcg(s, MODE_STAGE2, s->q0, s->q0));
+    return WC_OK;
+}
+
+// Launches one step per kernel that enqueue_step_direct issues.
+int step_launches(const wc_solver* s) {
+    if (s->order == WC_ORDER_FIRST) return s->sgn ? 2 : 1;
+    return s->sgn ? 4 : 2;
+}
+
+// The same step through a CUDA graph captured at first use (launch gaps inside a graph are
+// shorter than between separate launches). Profiling runs the launches directly so that each
+// kernel gets its own events.
+wc_status enqueue_step(wc_solver* s) {
+    s->rate_current = true;
+    if (s->prof_on || s->graph_failed) return enqueue_step_direct(s);
+    if (!s->step_graph) {
+        cudaGraph_t graph = nullptr;
+        if (cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            cudaGetLastError();
+            s->graph_failed = true;
+            return enqueue_step_direct(s);
+        }
+        const unsigned long long before = s->launches;
+        wc_status st = enqueue_step_direct(s);
+        cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
+        s->launches = before;
+        if (st != WC_OK || e != cudaSuccess ||
+            cudaGraphInstantiate(&s->step_graph, graph, 0) != cudaSuccess) {
+            cudaGetLastError();
+            if (graph) cudaGraphDestroy(graph);
+            s->step_graph = nullptr;
+            s->graph_failed = true;
+            return enqueue_step_direct(s);
+        }
+        cudaGraphDestroy(graph);
+    }
+    CK(cudaGraphLaunch(s->step_graph, s->stream));
+    s->launches += step_launches(s);
     return WC_OK;
 }
 
@@ -620,6 +674,7 @@ wc_status wc_state_upload(wc_solver* s, const double* h, const double* hu, const
     TRY(stage_host(s, h, hu, hv));
     upload_kernel<<<aux_grid(s->ncell), AUX_NT, 0, s->stream>>>(s->g, s->st_h, s->st_hu, s->st_hv, s->q0);
     s->launches++;
+    s->rate_current = false;
     CK(cudaGetLastError());
     // The clock; a new state clears the error bits.
     TRY(read_ctl(s));
@@ -657,9 +712,13 @@ wc_status wc_step_device(wc_solver* s, double dt) {
 
 wc_status wc_step_n(wc_solver* s, uint64_t n_steps, double t_end) {
     if (!s) return set_err(WC_EINVAL, "null solver");
-    state_rate_kernel<<<aux_grid(s->ncell), AUX_NT, 0, s->stream>>>(s->g, s->q0, s->ctl);
+    if (!s->rate_current) {
+        state_rate_kernel<<<aux_grid(s->ncell), AUX_NT, 0, s->stream>>>(s->g, s->q0, s->ctl);
+        s->launches++;
+        s->rate_current = true;
+    }
     set_adaptive_kernel<<<1, 1, 0, s->stream>>>(s->ctl, t_end);
-    s->launches += 2;
+    s->launches++;
     for (uint64_t n = 0; n < n_steps; n++) TRY(enqueue_step(s));
     clear_adaptive_kernel<<<1, 1, 0, s->stream>>>(s->ctl);
     s->launches++;
