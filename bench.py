@@ -51,6 +51,56 @@ def workload(name: str):
     return {"config1": W.config1, "config2": W.config2, "config3": W.config3}[name]()
 
 
+def run_ensemble(args, world, rank, local):
+    """The 64-member ensemble (config 4): every timed step advances every member one step."""
+    import torch
+
+    from wavesim_b200 import Ensemble, Solver
+
+    torch.cuda.set_device(local)
+    ws = W.config4(seed=4 + 1000 * rank)
+    cells = sum(w.interior_cells() for w in ws)
+    ens = Ensemble([w.solver(Solver) for w in ws])
+    starts = [W.wave_train_state(w) for w in ws]
+    for m, s0 in enumerate(starts):
+        ens.upload(m, s0)
+    choice, tune_ms = ens.autotune(2)
+    ens.step_n(args.warmup)
+    ens.synchronize()
+    l0 = ens.launch_count()
+    it0 = [ens.member_stats(m)[0] for m in range(len(ws))]
+    torch.cuda.synchronize()
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    times = []
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            ens.step_n(1)
+            ens.synchronize()
+            times.append(time.perf_counter() - t0)
+    it1 = [ens.member_stats(m)[0] for m in range(len(ws))]
+    iters = sum(b.iterations - a.iterations for a, b in zip(it0, it1)) / max(1, sum(b.solves - a.solves for a, b in zip(it0, it1)))
+    total = sum(times)
+    value = cells * args.steps * world / total
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "ensemble_64_uneven_beaches", "members": len(ws), "cells": cells,
+                       "scheme": "fifth order + SGN", "preconditioner": "jacobi (plain PCG)", "tolerance": 1e-8,
+                       "pcg_iterations_per_solve": iters,
+                       "autotuned_variant": Ensemble.VARIANTS[choice], "autotune_ms_per_step": tune_ms,
+                       "timing": "host wall clock around each synchronised ensemble step",
+                       "l2": "flushed between timed steps (256 MiB write outside the timed region)"},
+            "gpu_launches": int(ens.launch_count() - l0),
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+
+
 def measured_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -345,7 +395,7 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="config2", choices=["config1", "config2", "config3"])
+    ap.add_argument("--workload", default="config2", choices=["config1", "config2", "config3", "config4"])
     ap.add_argument("--cpu-steps", type=int, default=40)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -354,6 +404,9 @@ def main():
     world, rank, local = dist_setup()
     if args.impl == "reference":
         run_reference(args, world, rank)
+        return
+    if args.workload == "config4":
+        run_ensemble(args, world, rank, local)
         return
     run_b200(args, world, rank, local)
 

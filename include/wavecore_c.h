@@ -220,6 +220,35 @@ wc_status wc_stable_dt_noalloc(const wc_grid* grid, double cfl, const double* d_
                                const double* d_hu, const double* d_hv, void* stream,
                                double* dt_out);
 
+/* ---- Ensembles (no counterpart in the reference, which runs one Solver per grid in turn,
+ * crates/wavesim/src/lib.rs:1813-1902) ------------------------------------------------------
+ * n independent runs, each with its own grid, bed (padded FP64) and configuration (second or
+ * fifth order), advanced together: every step of every member is one persistent cooperative
+ * launch, replayed from a CUDA graph, in which each member's own group of CTAs runs its whole
+ * SSP-RK2 step with its own adaptive time step, clock and PCG state. The stage tile shape and
+ * the CTAs per SM are chosen by an autotuner that times each compiled variant on the live state
+ * (then restores it); wc_ensemble_step_n runs it on first use. */
+typedef struct wc_ensemble wc_ensemble;
+wc_status wc_ensemble_create(uint64_t n, const wc_grid* grids, const double* const* beds,
+                             const wc_config* cfgs, wc_ensemble** out);
+void wc_ensemble_destroy(wc_ensemble* e);
+wc_status wc_ensemble_upload(wc_ensemble* e, uint64_t member, const double* h, const double* hu,
+                             const double* hv, double time);
+wc_status wc_ensemble_download(wc_ensemble* e, uint64_t member, double* h, double* hu, double* hv,
+                               double* time);
+/* Up to n_steps steps of every member, each of size min(stable_dt, t_end - time); a member stops
+ * once its time reaches t_end. Asynchronous. */
+wc_status wc_ensemble_step_n(wc_ensemble* e, uint64_t n_steps, double t_end);
+/* Time every variant over trial_steps steps and keep the fastest; *choice is its index (stage
+ * tile height 8 or 16 by CTAs per SM 1 or 2: 0 = 8/1, 1 = 8/2, 2 = 16/1, 3 = 16/2) and
+ * ms_per_step[4] the measured times (-1 for a variant that cannot run). */
+wc_status wc_ensemble_autotune(wc_ensemble* e, uint32_t trial_steps, int32_t* choice,
+                               double* ms_per_step);
+wc_status wc_ensemble_synchronize(wc_ensemble* e);
+wc_status wc_ensemble_member_stats(wc_ensemble* e, uint64_t member, wc_stats* stats,
+                                   double* time);
+uint64_t wc_ensemble_launch_count(const wc_ensemble* e);
+
 /* Kernel launches this solver has queued since it was created (for accounting). */
 uint64_t wc_launch_count(const wc_solver* s);
 /* Human-readable text of the last error on this thread ("" if none). */

@@ -41,7 +41,7 @@ struct PcgArgs {
     float2* p1;
     float2* ap;
     float2* diag;
-    double* part;     // [gridDim.x][4] CTA partials
+    double* part;     // [ncta][4] CTA partials
     unsigned* cnt;    // [0] arrivals, [1] released epoch; zeroed before each launch
     const float2* hn;
     const float2* pred;
@@ -61,19 +61,19 @@ struct PcgArgs {
 // and arrives; the last to arrive releases; every CTA then adds all partials in CTA order with
 // the same reduction tree, so all CTAs hold identical totals. Returns false if the wait timed out.
 __device__ bool reduce_barrier(const PcgArgs& a, unsigned& epoch, double v0, double v1, double v2,
-                               double* out, double* red) {
+                               double* out, double* red, int cta, int ncta) {
     __shared__ int s_ok;
     block_sum3<PG_NT>(v0, v1, v2, red);
     if (threadIdx.x == 0) {
         epoch += 1;
-        double* pp = a.part + 4 * (size_t)blockIdx.x;
+        double* pp = a.part + 4 * (size_t)cta;
         pp[0] = v0;
         pp[1] = v1;
         pp[2] = v2;
         __threadfence();
         int ok = 1;
         const unsigned arrived = atomicAdd(a.cnt, 1u) + 1u;
-        if (arrived == epoch * gridDim.x) {
+        if (arrived == epoch * (unsigned)ncta) {
             st_release_u32(a.cnt + 1, epoch);
         } else {
             const unsigned long long t0 = globaltimer_ns();
@@ -95,7 +95,7 @@ __device__ bool reduce_barrier(const PcgArgs& a, unsigned& epoch, double v0, dou
     __syncthreads();
     if (!s_ok) return false;
     double x = 0.0, y = 0.0, z = 0.0;
-    for (int b = threadIdx.x; b < (int)gridDim.x; b += PG_NT) {
+    for (int b = threadIdx.x; b < ncta; b += PG_NT) {
         const double* pp = a.part + 4 * (size_t)b;
         x += __ldcg(pp);
         y += __ldcg(pp + 1);
@@ -218,35 +218,36 @@ struct CellPrefetch {
     float2 p, ap, w, r, d;
 };
 
-__global__ void __launch_bounds__(PG_NT, 2) pcg_kernel(PcgArgs a) {
+// The solve and the stage epilogue, by the `ncta` CTAs (this one is number `cta`) that own this
+// run. `epoch` counts the run's grid barriers within the launch. Returns false if a bounded
+// wait expired (every CTA of the run then returns).
+__device__ __forceinline__ bool pcg_solve(const PcgArgs& a, int cta, int ncta, unsigned& epoch) {
     __shared__ TileSmem t;
     __shared__ double red[100];
     __shared__ float s_rate[PG_NT / 32];
     __shared__ int s_nan;
 
     Ctl* ctl = a.ctl;
-    if (!ctl->active) return;
     const DevGrid& g = a.g;
     const int tid = threadIdx.x;
     const int cx = tid % PG_TX, cy = tid / PG_TX;
     const int ntiles = a.tiles_x * a.tiles_y;
     const double dt = ctl->dt;
     const float dt_f = (float)dt;
-    unsigned epoch = 0;
     double tot[3];
     if (tid == 0) s_nan = 0;
     BoxPrefetch f;
 
     // ---- initial residual: r = b - A w (dispersion.rs:493-515) ---------------------------
     double bb = 0.0, rz_p = 0.0, rr_p = 0.0;
-    if ((int)blockIdx.x < ntiles) box_prefetch<true>(a, blockIdx.x, nullptr, true, f);
-    for (int tl = blockIdx.x; tl < ntiles; tl += gridDim.x) {
+    if (cta < ntiles) box_prefetch<true>(a, cta, nullptr, true, f);
+    for (int tl = cta; tl < ntiles; tl += ncta) {
         int i0, j0;
         tile_origin(a, tl, i0, j0);
         box_commit<true>(f, t, 0.f, true);
         const float he = f.he;
         __syncthreads();
-        if (tl + (int)gridDim.x < ntiles) box_prefetch<true>(a, tl + gridDim.x, nullptr, true, f);
+        if (tl + ncta < ntiles) box_prefetch<true>(a, tl + ncta, nullptr, true, f);
         const float2 aw = apply_a(g, t, cx, cy, he);
         const int i = i0 + cx, j = j0 + cy;
         if (i < g.nx && j < g.ny) {
@@ -268,7 +269,7 @@ __global__ void __launch_bounds__(PG_NT, 2) pcg_kernel(PcgArgs a) {
         }
         __syncthreads();
     }
-    if (!reduce_barrier(a, epoch, bb, rz_p, rr_p, tot, red)) return;
+    if (!reduce_barrier(a, epoch, bb, rz_p, rr_p, tot, red, cta, ncta)) return false;
     const double target = a.tol * sqrt(tot[0]) + 1e-10;
     double rz = tot[1];
     bool converged = sqrt(tot[2]) <= target;
@@ -281,14 +282,14 @@ __global__ void __launch_bounds__(PG_NT, 2) pcg_kernel(PcgArgs a) {
         const bool first = it == 0;
         // sweep A': p = z + beta p on the tile and its halo, then A p and <p, Ap>
         double pap = 0.0;
-        if ((int)blockIdx.x < ntiles) box_prefetch<false>(a, blockIdx.x, p_old, first, f);
-        for (int tl = blockIdx.x; tl < ntiles; tl += gridDim.x) {
+        if (cta < ntiles) box_prefetch<false>(a, cta, p_old, first, f);
+        for (int tl = cta; tl < ntiles; tl += ncta) {
             int i0, j0;
             tile_origin(a, tl, i0, j0);
             box_commit<false>(f, t, beta_f, first);
             const float he = f.he;
             __syncthreads();
-            if (tl + (int)gridDim.x < ntiles) box_prefetch<false>(a, tl + gridDim.x, p_old, first, f);
+            if (tl + ncta < ntiles) box_prefetch<false>(a, tl + ncta, p_old, first, f);
             const float2 av = apply_a(g, t, cx, cy, he);
             const int i = i0 + cx, j = j0 + cy;
             if (i < g.nx && j < g.ny) {
@@ -300,7 +301,7 @@ __global__ void __launch_bounds__(PG_NT, 2) pcg_kernel(PcgArgs a) {
             }
             __syncthreads();
         }
-        if (!reduce_barrier(a, epoch, pap, 0.0, 0.0, tot, red)) return;
+        if (!reduce_barrier(a, epoch, pap, 0.0, 0.0, tot, red, cta, ncta)) return false;
         const double alpha = rz / tot[0];
         const float alpha_f = (float)alpha;
         // sweep B: w += alpha p, r -= alpha Ap, <r, r> and <r, z>
@@ -319,10 +320,10 @@ __global__ void __launch_bounds__(PG_NT, 2) pcg_kernel(PcgArgs a) {
                 o.d = __ldcg(a.diag + k);
             }
         };
-        if ((int)blockIdx.x < ntiles) cell_load(blockIdx.x, c);
-        for (int tl = blockIdx.x; tl < ntiles; tl += gridDim.x) {
+        if (cta < ntiles) cell_load(cta, c);
+        for (int tl = cta; tl < ntiles; tl += ncta) {
             const CellPrefetch cur = c;
-            if (tl + (int)gridDim.x < ntiles) cell_load(tl + gridDim.x, c);
+            if (tl + ncta < ntiles) cell_load(tl + ncta, c);
             int i0, j0;
             tile_origin(a, tl, i0, j0);
             const int i = i0 + cx, j = j0 + cy;
@@ -339,14 +340,14 @@ __global__ void __launch_bounds__(PG_NT, 2) pcg_kernel(PcgArgs a) {
                 rzn += (double)r.x * (r.x / cur.d.x) + (double)r.y * (r.y / cur.d.y);
             }
         }
-        if (!reduce_barrier(a, epoch, rr, rzn, 0.0, tot, red)) return;
+        if (!reduce_barrier(a, epoch, rr, rzn, 0.0, tot, red, cta, ncta)) return false;
         it += 1;
         converged = sqrt(tot[0]) <= target;
         const double beta = tot[1] / rz;
         rz = tot[1];
         beta_f = (float)beta;
     }
-    if (blockIdx.x == 0 && tid == 0) {
+    if (cta == 0 && tid == 0) {
         ctl->solves += 1;
         ctl->iterations += (unsigned long long)it;
         if (!converged) ctl->unconverged += 1;
@@ -356,7 +357,7 @@ __global__ void __launch_bounds__(PG_NT, 2) pcg_kernel(PcgArgs a) {
     // ---- finish the stage from the solution (every w is final: the last reduction was a barrier)
     float rmax = 0.f;
     int nan_here = 0;
-    for (int tl = blockIdx.x; tl < ntiles; tl += gridDim.x) {
+    for (int tl = cta; tl < ntiles; tl += ncta) {
         int i0, j0;
         tile_origin(a, tl, i0, j0);
         const int i = i0 + cx, j = j0 + cy;
@@ -399,8 +400,15 @@ __global__ void __launch_bounds__(PG_NT, 2) pcg_kernel(PcgArgs a) {
             s_rate[0] = m;
         }
         __syncthreads();
-        fold_rate_and_finish(ctl, s_rate[0], s_nan, gridDim.x);
+        fold_rate_and_finish(ctl, s_rate[0], s_nan, (unsigned)ncta);
     }
+    return true;
+}
+
+__global__ void __launch_bounds__(PG_NT, 2) pcg_kernel(PcgArgs a) {
+    if (!a.ctl->active) return;
+    unsigned epoch = 0;
+    pcg_solve(a, blockIdx.x, gridDim.x, epoch);
 }
 
 }  // namespace wcb

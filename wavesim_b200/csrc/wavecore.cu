@@ -17,6 +17,7 @@
 #include "../../include/wavecore_c.h"
 #include "aux.cuh"
 #include "common.cuh"
+#include "ensemble.cuh"
 #include "pcg.cuh"
 #include "stage.cuh"
 
@@ -207,12 +208,15 @@ wc_status configure_kernels() {
     ATTR((stage_kernel<MODE_STAGE1, 0, true>), SMEM_SGN);
     ATTR((stage_kernel<MODE_STAGE1, 1, true>), SMEM_SGN);
     ATTR((stage_kernel<MODE_STAGE1, 2, true>), SMEM_SGN);
+    ATTR((ensemble_step_kernel<8, 1>), StageGeom<8>::SMEM_SGN);
+    ATTR((ensemble_step_kernel<8, 2>), StageGeom<8>::SMEM_SGN);
+    ATTR((ensemble_step_kernel<16, 1>), StageGeom<16>::SMEM_SGN);
+    ATTR((ensemble_step_kernel<16, 2>), StageGeom<16>::SMEM_SGN);
 #undef ATTR
     return WC_OK;
 }
 
-wc_status launch_stage(wc_solver* s, int mode, const float4* qin, const float4* qold, float4* qout,
-                       bool plus_dt) {
+StageArgs stage_args(const wc_solver* s, const float4* qin, const float4* qold, float4* qout, bool plus_dt) {
     StageArgs a{};
     a.g = s->g;
     a.qin = qin;
@@ -235,6 +239,12 @@ wc_status launch_stage(wc_solver* s, int mode, const float4* qin, const float4* 
     a.cc = s->cc;
     a.heff = s->heff;
     a.bv = s->bv;
+    return a;
+}
+
+wc_status launch_stage(wc_solver* s, int mode, const float4* qin, const float4* qold, float4* qout,
+                       bool plus_dt) {
+    const StageArgs a = stage_args(s, qin, qold, qout, plus_dt);
     dim3 grid((s->g.nx + ST_TX - 1) / ST_TX, (s->g.ny + ST_TY - 1) / ST_TY);
     dim3 block(ST_NT);
     cudaStream_t st = s->stream;
@@ -258,7 +268,7 @@ wc_status launch_stage(wc_solver* s, int mode, const float4* qin, const float4* 
     return WC_OK;
 }
 
-wc_status launch_pcg(wc_solver* s, int mode, const float4* qold, float4* qout) {
+PcgArgs pcg_args(const wc_solver* s, int mode, const float4* qold, float4* qout) {
     PcgArgs a{};
     a.g = s->g;
     a.cc = s->cc;
@@ -285,6 +295,11 @@ wc_status launch_pcg(wc_solver* s, int mode, const float4* qold, float4* qout) {
     a.tiles_y = s->pcg_tiles_y;
     a.damp = s->damp;
     a.timeout_ns = BARRIER_TIMEOUT_NS;
+    return a;
+}
+
+wc_status launch_pcg(wc_solver* s, int mode, const float4* qold, float4* qout) {
+    const PcgArgs a = pcg_args(s, mode, qold, qout);
     CK(cudaMemsetAsync(s->bar, 0, 2 * sizeof(unsigned), s->stream));
     ProfScope ps(s, 1);
     // A cooperative launch: every CTA is resident at once, so the grid barriers cannot deadlock.
@@ -865,5 +880,365 @@ wc_status wc_time_device(wc_solver* s, double* time_out) {
     *time_out = s->ctl_host->t;
     return WC_OK;
 }
+
+}  // extern "C"
+
+// ---- ensembles ------------------------------------------------------------------------------
+
+namespace {
+
+constexpr int EN_VARIANTS = 4;  // stage tile height {8, 16} x CTAs per SM {1, 2}
+
+struct EnVariant {
+    int ty, minb;
+    int ctas = 0;
+    std::vector<EnsembleMember> table;
+    EnsembleMember* d_table = nullptr;
+    int* d_cta_member = nullptr;
+    cudaGraphExec_t graph = nullptr;
+};
+
+template <int TY, int MINB>
+cudaError_t launch_ensemble_variant(int ctas, const EnsembleMember* table, const int* cta_member,
+                                    cudaStream_t st) {
+    cudaLaunchConfig_t lc{};
+    lc.gridDim = dim3(ctas);
+    lc.blockDim = dim3(EN_NT);
+    lc.dynamicSmemBytes = StageGeom<TY>::SMEM_SGN;
+    lc.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    lc.attrs = attr;
+    lc.numAttrs = 1;
+    return cudaLaunchKernelEx(&lc, ensemble_step_kernel<TY, MINB>, table, cta_member);
+}
+
+cudaError_t launch_variant(const EnVariant& v, cudaStream_t st) {
+    if (v.ty == 8 && v.minb == 1) return launch_ensemble_variant<8, 1>(v.ctas, v.d_table, v.d_cta_member, st);
+    if (v.ty == 8) return launch_ensemble_variant<8, 2>(v.ctas, v.d_table, v.d_cta_member, st);
+    if (v.minb == 1) return launch_ensemble_variant<16, 1>(v.ctas, v.d_table, v.d_cta_member, st);
+    return launch_ensemble_variant<16, 2>(v.ctas, v.d_table, v.d_cta_member, st);
+}
+
+int variant_occupancy(int ty, int minb) {
+    int occ = 0;
+    cudaError_t e;
+    if (ty == 8 && minb == 1) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ensemble_step_kernel<8, 1>, EN_NT, StageGeom<8>::SMEM_SGN);
+    else if (ty == 8) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ensemble_step_kernel<8, 2>, EN_NT, StageGeom<8>::SMEM_SGN);
+    else if (minb == 1) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ensemble_step_kernel<16, 1>, EN_NT, StageGeom<16>::SMEM_SGN);
+    else e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ensemble_step_kernel<16, 2>, EN_NT, StageGeom<16>::SMEM_SGN);
+    return e == cudaSuccess ? occ : 0;
+}
+
+}  // namespace
+
+struct wc_ensemble {
+    std::vector<wc_solver*> members;
+    cudaStream_t stream = nullptr;
+    unsigned* counters = nullptr;   // [members][2]: group barrier arrivals and released epoch
+    double* partials = nullptr;     // [members][max ctas][4]
+    int max_ctas = 0;
+    EnVariant var[EN_VARIANTS];
+    int chosen = -1;
+    double tune_ms[EN_VARIANTS] = {0, 0, 0, 0};
+    // snapshot of the resident states for tuning trials
+    std::vector<float4*> snap_q;
+    std::vector<float2*> snap_w;
+    unsigned long long launches = 0;
+
+    ~wc_ensemble() {
+        if (stream) cudaStreamSynchronize(stream);
+        for (auto& v : var) {
+            if (v.graph) cudaGraphExecDestroy(v.graph);
+            if (v.d_table) cudaFree(v.d_table);
+            if (v.d_cta_member) cudaFree(v.d_cta_member);
+        }
+        for (auto p : snap_q) cudaFree(p);
+        for (auto p : snap_w) cudaFree(p);
+        if (counters) cudaFree(counters);
+        if (partials) cudaFree(partials);
+        for (auto m : members) wc_solver_destroy(m);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+// Split `ctas` CTAs over the members in proportion to their cells (at least one each, at most
+// one per PCG tile), and fill the member table of one variant.
+wc_status build_variant(wc_ensemble* e, EnVariant& v, int ctas) {
+    const size_t n = e->members.size();
+    std::vector<double> cells(n);
+    double total = 0;
+    std::vector<int> cap(n);
+    for (size_t m = 0; m < n; m++) {
+        cells[m] = (double)e->members[m]->g.nx * e->members[m]->g.ny;
+        total += cells[m];
+        const int tiles_pcg = e->members[m]->pcg_tiles_x * e->members[m]->pcg_tiles_y;
+        const int tiles_st = ((e->members[m]->g.nx + ST_TX - 1) / ST_TX) * ((e->members[m]->g.ny + v.ty - 1) / v.ty);
+        cap[m] = std::max(1, std::min(e->max_ctas, std::max(tiles_pcg, tiles_st)));
+    }
+    std::vector<int> share(n);
+    int used = 0;
+    for (size_t m = 0; m < n; m++) {
+        share[m] = std::max(1, std::min(cap[m], (int)std::floor(ctas * cells[m] / total)));
+        used += share[m];
+    }
+    // hand out what is left to the members with the most cells per CTA
+    while (used < ctas) {
+        int best = -1;
+        double worst = -1;
+        for (size_t m = 0; m < n; m++)
+            if (share[m] < cap[m] && cells[m] / share[m] > worst) {
+                worst = cells[m] / share[m];
+                best = (int)m;
+            }
+        if (best < 0) break;
+        share[best]++;
+        used++;
+    }
+    v.ctas = used;
+    v.table.assign(n, EnsembleMember{});
+    std::vector<int> cta_member(used);
+    int first = 0;
+    for (size_t m = 0; m < n; m++) {
+        wc_solver* s = e->members[m];
+        EnsembleMember& M = v.table[m];
+        M.sgn = s->sgn;
+        M.order = s->order;
+        M.first_cta = first;
+        M.ncta = share[m];
+        for (int c = 0; c < share[m]; c++) cta_member[first + c] = (int)m;
+        first += share[m];
+        if (s->sgn) {
+            M.st[0] = stage_args(s, s->q0, s->q0, s->q1, false);
+            M.st[1] = stage_args(s, s->q1, s->q0, s->q1, true);
+        } else {
+            M.st[0] = stage_args(s, s->q0, s->q0, s->q1, false);
+            M.st[1] = stage_args(s, s->q1, s->q0, s->q0, true);
+        }
+        M.pcg[0] = pcg_args(s, MODE_STAGE1, s->q0, s->q1);
+        M.pcg[1] = pcg_args(s, MODE_STAGE2, s->q0, s->q0);
+        for (int k = 0; k < 2; k++) {
+            M.pcg[k].cnt = e->counters + 2 * m;
+            M.pcg[k].part = e->partials + 4 * (size_t)m * e->max_ctas;
+        }
+    }
+    if (!v.d_table) CK(cudaMalloc(&v.d_table, n * sizeof(EnsembleMember)));
+    if (!v.d_cta_member) CK(cudaMalloc(&v.d_cta_member, (size_t)e->max_ctas * EN_VARIANTS * sizeof(int)));
+    CK(cudaMemcpy(v.d_table, v.table.data(), n * sizeof(EnsembleMember), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(v.d_cta_member, cta_member.data(), used * sizeof(int), cudaMemcpyHostToDevice));
+    return WC_OK;
+}
+
+// One ensemble step through the variant's captured graph (counters cleared, then the launch).
+wc_status ensemble_step(wc_ensemble* e, EnVariant& v) {
+    if (!v.graph) {
+        cudaGraph_t graph = nullptr;
+        CK(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e1 = cudaMemsetAsync(e->counters, 0, 2 * e->members.size() * sizeof(unsigned), e->stream);
+        cudaError_t e2 = launch_variant(v, e->stream);
+        cudaError_t e3 = cudaStreamEndCapture(e->stream, &graph);
+        if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess)
+            return set_err(WC_ECUDA, std::string("capturing the ensemble step failed: ") +
+                                         cudaGetErrorString(e1 != cudaSuccess ? e1 : (e2 != cudaSuccess ? e2 : e3)));
+        cudaError_t e4 = cudaGraphInstantiate(&v.graph, graph, 0);
+        cudaGraphDestroy(graph);
+        CK(e4);
+    }
+    CK(cudaGraphLaunch(v.graph, e->stream));
+    e->launches++;
+    return WC_OK;
+}
+
+wc_status ensemble_prepare(wc_ensemble* e, double t_end) {
+    for (wc_solver* s : e->members) {
+        if (!s->rate_current) {
+            state_rate_kernel<<<aux_grid(s->ncell), AUX_NT, 0, e->stream>>>(s->g, s->q0, s->ctl);
+            s->rate_current = true;
+            e->launches++;
+        }
+        set_adaptive_kernel<<<1, 1, 0, e->stream>>>(s->ctl, t_end);
+        e->launches++;
+    }
+    CK(cudaGetLastError());
+    return WC_OK;
+}
+
+wc_status ensemble_finish(wc_ensemble* e) {
+    for (wc_solver* s : e->members) {
+        clear_adaptive_kernel<<<1, 1, 0, e->stream>>>(s->ctl);
+        e->launches++;
+    }
+    CK(cudaGetLastError());
+    return WC_OK;
+}
+
+// The autotuner: every compiled variant runs `trial` steps on a snapshot of the live state
+// (timed with events on the ensemble's stream), the state and clocks are restored after each,
+// and the fastest variant is kept.
+wc_status ensemble_tune(wc_ensemble* e, int trial) {
+    const size_t n = e->members.size();
+    if (e->snap_q.empty()) {
+        for (wc_solver* s : e->members) {
+            float4* q = nullptr;
+            float2* w = nullptr;
+            TRY(dalloc(&q, s->ncell));
+            if (s->sgn) TRY(dalloc(&w, s->ncell));
+            e->snap_q.push_back(q);
+            e->snap_w.push_back(w);
+        }
+    }
+    std::vector<Ctl> ctl(n);
+    for (size_t m = 0; m < n; m++) {
+        wc_solver* s = e->members[m];
+        CK(cudaMemcpyAsync(e->snap_q[m], s->q0, s->ncell * sizeof(float4), cudaMemcpyDeviceToDevice, e->stream));
+        if (s->sgn) CK(cudaMemcpyAsync(e->snap_w[m], s->w, s->ncell * sizeof(float2), cudaMemcpyDeviceToDevice, e->stream));
+        CK(cudaMemcpyAsync(&ctl[m], s->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, e->stream));
+    }
+    CK(cudaStreamSynchronize(e->stream));
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    double best = 1e300;
+    for (int k = 0; k < EN_VARIANTS; k++) {
+        if (e->var[k].ctas <= 0) {
+            e->tune_ms[k] = -1.0;
+            continue;
+        }
+        TRY(ensemble_prepare(e, INFINITY));
+        TRY(ensemble_step(e, e->var[k]));  // capture and warm
+        CK(cudaEventRecord(a, e->stream));
+        for (int t = 0; t < trial; t++) TRY(ensemble_step(e, e->var[k]));
+        CK(cudaEventRecord(b, e->stream));
+        CK(cudaEventSynchronize(b));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, a, b));
+        e->tune_ms[k] = ms / trial;
+        if (ms < best) {
+            best = ms;
+            e->chosen = k;
+        }
+        for (size_t m = 0; m < n; m++) {  // restore the state, the warm start and the clock
+            wc_solver* s = e->members[m];
+            CK(cudaMemcpyAsync(s->q0, e->snap_q[m], s->ncell * sizeof(float4), cudaMemcpyDeviceToDevice, e->stream));
+            if (s->sgn) CK(cudaMemcpyAsync(s->w, e->snap_w[m], s->ncell * sizeof(float2), cudaMemcpyDeviceToDevice, e->stream));
+            CK(cudaMemcpyAsync(s->ctl, &ctl[m], sizeof(Ctl), cudaMemcpyHostToDevice, e->stream));
+            s->rate_current = false;
+        }
+        CK(cudaStreamSynchronize(e->stream));
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (e->chosen < 0) return set_err(WC_ECUDA, "no ensemble kernel variant can run on this device");
+    TRY(ensemble_finish(e));
+    return WC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+wc_status wc_ensemble_create(uint64_t n, const wc_grid* grids, const double* const* beds,
+                             const wc_config* cfgs, wc_ensemble** out) {
+    if (!out) return set_err(WC_EINVAL, "out is null");
+    *out = nullptr;
+    if (n == 0 || !grids || !beds || !cfgs) return set_err(WC_EINVAL, "an ensemble needs members");
+    for (uint64_t m = 0; m < n; m++)
+        if (cfgs[m].order == WC_ORDER_FIRST)
+            return set_err(WC_EUNSUPPORTED, "ensemble members run second or fifth order (SSP-RK2)");
+    wc_ensemble* e = new wc_ensemble();
+    auto fail = [&](wc_status st) {
+        delete e;
+        return st;
+    };
+    if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return fail(set_err(WC_ECUDA, "cudaStreamCreate failed"));
+    for (uint64_t m = 0; m < n; m++) {
+        wc_solver* s = nullptr;
+        wc_status st = wc_solver_create(&grids[m], beds[m], &cfgs[m], &s);
+        if (st != WC_OK) return fail(st);
+        e->members.push_back(s);
+        s->stream = e->stream;  // members queue on the ensemble's stream
+    }
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int tys[2] = {8, 16};
+    int max_ctas = 0;
+    for (int k = 0; k < EN_VARIANTS; k++) {
+        e->var[k].ty = tys[k / 2];
+        e->var[k].minb = 1 + (k % 2);
+        const int occ = std::min(variant_occupancy(e->var[k].ty, e->var[k].minb), e->var[k].minb);
+        e->var[k].ctas = occ * sms;
+        max_ctas = std::max(max_ctas, e->var[k].ctas);
+    }
+    if (max_ctas <= 0) return fail(set_err(WC_ECUDA, "no ensemble kernel variant fits on this device"));
+    if ((int)n > max_ctas) return fail(set_err(WC_EUNSUPPORTED, "more members than co-resident CTAs"));
+    e->max_ctas = max_ctas;
+    wc_status st;
+    if ((st = dalloc(&e->counters, 2 * n)) != WC_OK) return fail(st);
+    if ((st = dalloc(&e->partials, 4 * n * (size_t)max_ctas)) != WC_OK) return fail(st);
+    for (int k = 0; k < EN_VARIANTS; k++) {
+        if (e->var[k].ctas <= 0) continue;
+        if ((st = build_variant(e, e->var[k], std::max((int)n, e->var[k].ctas))) != WC_OK) return fail(st);
+    }
+    *out = e;
+    return WC_OK;
+}
+
+void wc_ensemble_destroy(wc_ensemble* e) { delete e; }
+
+wc_status wc_ensemble_upload(wc_ensemble* e, uint64_t m, const double* h, const double* hu, const double* hv,
+                             double time) {
+    if (!e || m >= e->members.size()) return set_err(WC_EINVAL, "no such member");
+    return wc_state_upload(e->members[m], h, hu, hv, time);
+}
+
+wc_status wc_ensemble_download(wc_ensemble* e, uint64_t m, double* h, double* hu, double* hv, double* time) {
+    if (!e || m >= e->members.size()) return set_err(WC_EINVAL, "no such member");
+    return wc_state_download(e->members[m], h, hu, hv, time);
+}
+
+wc_status wc_ensemble_autotune(wc_ensemble* e, uint32_t trial_steps, int32_t* choice, double* ms_per_step) {
+    if (!e) return set_err(WC_EINVAL, "null ensemble");
+    TRY(ensemble_tune(e, (int)std::max<uint32_t>(1, trial_steps)));
+    if (choice) *choice = e->chosen;
+    if (ms_per_step)
+        for (int k = 0; k < EN_VARIANTS; k++) ms_per_step[k] = e->tune_ms[k];
+    return WC_OK;
+}
+
+wc_status wc_ensemble_step_n(wc_ensemble* e, uint64_t n_steps, double t_end) {
+    if (!e) return set_err(WC_EINVAL, "null ensemble");
+    if (e->chosen < 0) TRY(ensemble_tune(e, 2));
+    TRY(ensemble_prepare(e, t_end));
+    for (uint64_t k = 0; k < n_steps; k++) TRY(ensemble_step(e, e->var[e->chosen]));
+    TRY(ensemble_finish(e));
+    return WC_OK;
+}
+
+wc_status wc_ensemble_synchronize(wc_ensemble* e) {
+    if (!e) return set_err(WC_EINVAL, "null ensemble");
+    CK(cudaStreamSynchronize(e->stream));
+    for (wc_solver* s : e->members) TRY(status_of(s));
+    return WC_OK;
+}
+
+wc_status wc_ensemble_member_stats(wc_ensemble* e, uint64_t m, wc_stats* stats, double* time) {
+    if (!e || m >= e->members.size()) return set_err(WC_EINVAL, "no such member");
+    wc_solver* s = e->members[m];
+    TRY(read_ctl(s));
+    if (stats) {
+        stats->solves = s->ctl_host->solves;
+        stats->iterations = s->ctl_host->iterations;
+        stats->unconverged = s->ctl_host->unconverged;
+    }
+    if (time) *time = s->ctl_host->t;
+    return WC_OK;
+}
+
+uint64_t wc_ensemble_launch_count(const wc_ensemble* e) { return e ? e->launches : 0; }
 
 }  // extern "C"

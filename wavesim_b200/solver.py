@@ -49,6 +49,15 @@ EXPORTS = [
     "wc_launch_count",
     "wc_last_error",
     "wc_stable_dt_noalloc",
+    "wc_ensemble_create",
+    "wc_ensemble_destroy",
+    "wc_ensemble_upload",
+    "wc_ensemble_download",
+    "wc_ensemble_step_n",
+    "wc_ensemble_autotune",
+    "wc_ensemble_synchronize",
+    "wc_ensemble_member_stats",
+    "wc_ensemble_launch_count",
 ]
 
 
@@ -90,6 +99,20 @@ def load(path: str = LIB_PATH):
     L.wc_set_stream.argtypes = [V, V]
     L.wc_profile_enable.argtypes = [V, C.c_int32]
     L.wc_profile_read.argtypes = [V, C.POINTER(abi.wc_kernel_time)]
+    L.wc_ensemble_create.argtypes = [C.c_uint64, C.POINTER(abi.wc_grid), C.POINTER(D), C.POINTER(abi.wc_config), C.POINTER(V)]
+    L.wc_ensemble_destroy.argtypes = [V]
+    L.wc_ensemble_destroy.restype = None
+    L.wc_ensemble_upload.argtypes = [V, C.c_uint64, D, D, D, C.c_double]
+    L.wc_ensemble_download.argtypes = [V, C.c_uint64, D, D, D, D]
+    L.wc_ensemble_step_n.argtypes = [V, C.c_uint64, C.c_double]
+    L.wc_ensemble_autotune.argtypes = [V, C.c_uint32, C.POINTER(C.c_int32), D]
+    L.wc_ensemble_synchronize.argtypes = [V]
+    L.wc_ensemble_member_stats.argtypes = [V, C.c_uint64, C.POINTER(abi.wc_stats), D]
+    L.wc_ensemble_launch_count.argtypes = [V]
+    L.wc_ensemble_launch_count.restype = C.c_uint64
+    for name in ("wc_ensemble_create", "wc_ensemble_upload", "wc_ensemble_download", "wc_ensemble_step_n",
+                 "wc_ensemble_autotune", "wc_ensemble_synchronize", "wc_ensemble_member_stats"):
+        getattr(L, name).restype = C.c_int
     L.wc_stable_dt_noalloc.argtypes = [C.POINTER(abi.wc_grid), C.c_double, V, V, V, V, D]
     L.wc_stable_dt_noalloc.restype = C.c_int
     L.wc_launch_count.argtypes = [V]
@@ -252,3 +275,67 @@ class Solver(SolverConfig):
 
     def launch_count(self) -> int:
         return int(load().wc_launch_count(self._h()))
+
+
+class Ensemble:
+    """Independent runs advanced together, one persistent launch per step (`wc_ensemble_*`).
+
+    `members` are configured solvers (`Solver(grid, bed).with_...`); their configuration is
+    copied, each member gets its own device state. No counterpart in the reference, which runs one
+    `Solver` per grid in turn.
+    """
+
+    VARIANTS = ("tile 32x8, 1 CTA/SM", "tile 32x8, 2 CTAs/SM", "tile 32x16, 1 CTA/SM", "tile 32x16, 2 CTAs/SM")
+
+    def __init__(self, members):
+        L = load()
+        n = len(members)
+        grids = (abi.wc_grid * n)(*[m.grid.to_c() for m in members])
+        cfgs, keep = [], []
+        for m in members:
+            cfg, k = m._c_config()
+            cfgs.append(cfg)
+            keep.append(k)
+        carr = (abi.wc_config * n)(*cfgs)
+        beds = (abi.DPTR * n)(*[abi.dptr(m.bed.b) for m in members])
+        out = C.c_void_p()
+        _check(L.wc_ensemble_create(n, grids, beds, carr, C.byref(out)))
+        self._h = out
+        self.members = members
+        self.n = n
+
+    def __del__(self):
+        try:
+            if getattr(self, "_h", None):
+                load().wc_ensemble_destroy(self._h)
+        except Exception:
+            pass
+
+    def upload(self, m: int, s: State) -> None:
+        _check(load().wc_ensemble_upload(self._h, m, abi.dptr(s.h), abi.dptr(s.hu), abi.dptr(s.hv), float(s.time)))
+
+    def download(self, m: int, s: State) -> None:
+        t = C.c_double()
+        _check(load().wc_ensemble_download(self._h, m, abi.dptr(s.h), abi.dptr(s.hu), abi.dptr(s.hv), C.byref(t)))
+        s.time = t.value
+
+    def step_n(self, n: int, t_end: float = math.inf) -> None:
+        _check(load().wc_ensemble_step_n(self._h, int(n), float(t_end)))
+
+    def autotune(self, trial_steps: int = 2):
+        choice = C.c_int32()
+        ms = (C.c_double * 4)()
+        _check(load().wc_ensemble_autotune(self._h, int(trial_steps), C.byref(choice), ms))
+        return choice.value, list(ms)
+
+    def synchronize(self) -> None:
+        _check(load().wc_ensemble_synchronize(self._h))
+
+    def member_stats(self, m: int):
+        st = abi.wc_stats()
+        t = C.c_double()
+        _check(load().wc_ensemble_member_stats(self._h, m, C.byref(st), C.byref(t)))
+        return DispersionStats(st.solves, st.iterations, st.unconverged), t.value
+
+    def launch_count(self) -> int:
+        return int(load().wc_ensemble_launch_count(self._h))

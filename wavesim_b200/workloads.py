@@ -162,6 +162,40 @@ def config3(seed: int = 2025) -> Workload:
     return sgn_beach(2048, 1024, 2.0, seed, name="sgn_beach_2048x1024_dx2")
 
 
+def config4(seed: int = 4, members: int = 64, preconditioner: int = 0):
+    """64 runs of uneven grids (nx 512-2048, ny 256-1024, dx 2-3 m) on seeded rough plane beaches
+    (20 m shelf, 1:30 beach, Gaussian field sigma 0.5 m / 20 m), reflective y walls; per run the
+    swell angle ~ U(-20, 20) deg, T ~ U(8, 18) s, H ~ U(0.5, 4) m and a still-water offset
+    ~ U(-1, 1) m applied as a bed shift (as the reference's Bed::bathymetry(tide) does,
+    crates/waveio/src/bed.rs:239-246); fifth order + SGN to 1e-8."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for m in range(members):
+        nx = int(rng.integers(512 // 64, 2048 // 64 + 1)) * 64
+        ny = int(rng.integers(256 // 32, 1024 // 32 + 1)) * 32
+        dx = float(rng.uniform(2.0, 3.0))
+        angle = math.radians(float(rng.uniform(-20.0, 20.0)))
+        period = float(rng.uniform(8.0, 18.0))
+        height = float(rng.uniform(0.5, 4.0))
+        tide = float(rng.uniform(-1.0, 1.0))
+        grid = Grid(nx, ny, dx, dx)
+        lx = nx * dx
+        b = shelf_and_beach(grid, 20.0, 1.0 / 30.0, 0.85 * lx) + gaussian_field(nx, ny, dx, dx, 0.5, 20.0, seed * 1000 + m)
+        b = b - tide
+        bed = Bathymetry.from_interior(grid, b)
+        maker = WaveMaker(x=160.0, amplitude=height / 2.0, period=period, angle=angle, sigma=2.0 * dx, ramp_periods=4.0)
+        out.append(Workload(
+            name=f"ensemble_member_{m}_{nx}x{ny}",
+            grid=grid, bed=bed, order=Order.Fifth, cfl=0.4, manning=0.02, periodic_y=False,
+            sponges=[Sponge(int(round(100.0 / dx)), 1.5).edges(True, False, False, False)],
+            maker=maker,
+            dispersion=Dispersion(tolerance=1e-8, max_iterations=1000, preconditioner=preconditioner),
+            steps=3000,
+            meta={"dx": dx, "angle_deg": math.degrees(angle), "period": period, "height": height, "tide": tide},
+        ))
+    return out
+
+
 def wave_train_state(w: Workload, x_from: float | None = None, x_to: float | None = None) -> State:
     """A start that already holds the swell: still water plus a linear wave train of the maker's
     amplitude, direction and (offshore) wavenumber over the shelf, tapered to zero at both ends,
