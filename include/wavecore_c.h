@@ -249,6 +249,52 @@ wc_status wc_ensemble_member_stats(wc_ensemble* e, uint64_t member, wc_stats* st
                                    double* time);
 uint64_t wc_ensemble_launch_count(const wc_ensemble* e);
 
+/* ---- The learned preconditioner (no counterpart in the reference) ------------------------------
+ *
+ * The reference preconditions its dispersive CG with the Jacobi diagonal only
+ * (crates/wavecore/src/dispersion.rs:441-457, 493-545). These entry points add a trained
+ * alternative: a depth-gated linear 4-level U-net used inside a two-level cycle
+ *     z1 = w r / D,  z2 = z1 + mask N(D^-1 (r - A z1)),  z = z2 + w (r - A z2) / D   (w = 0.5)
+ * as the preconditioner of flexible CG, with the Jacobi solve's stopping rule; a solve that does
+ * not converge (or breaks down) is finished by Jacobi PCG from where it stopped, so the plain
+ * method stays the fallback and the judge of convergence. Training runs on
+ * the GPU by the library's own forward and backward kernels, on patches of SGN systems harvested
+ * from solver runs, minimising the energy norm of the cycle's error on random error fields. */
+typedef struct wc_lpc wc_lpc;
+
+/* channels[4]: feature maps per level, finest first (null: 8, 16, 32, 32); gate_hidden: width of
+ * the gate networks' hidden layer (8). Weights start scaled-normal from `seed`, biases at zero
+ * and the output layer at zero (an untrained network adds nothing to the Jacobi sweeps). */
+wc_status wc_lpc_create(const int32_t* channels, int32_t gate_hidden, uint64_t seed, wc_lpc** out);
+/* A network must outlive every solver it is attached to. */
+void wc_lpc_destroy(wc_lpc* l);
+uint64_t wc_lpc_num_params(const wc_lpc* l);
+/* The FP32 master weights, in the layout of wavesim_b200/lpc.py (UNetSpec.layers). Setting them
+ * resets the optimiser's moments. */
+wc_status wc_lpc_set_params(wc_lpc* l, const float* params, uint64_t n);
+wc_status wc_lpc_get_params(wc_lpc* l, float* params, uint64_t n);
+/* bf16 != 0 (default): the forward pass uses BF16-rounded weights; 0: the FP32 weights. */
+wc_status wc_lpc_set_rounding(wc_lpc* l, int32_t bf16);
+/* One forward and backward pass on host arrays, for checking gradients: x and feat are
+ * [n][2][h][w] (h, w multiples of 8), dy the output gradient of the same shape; returns the
+ * output y, the parameter gradient of sum(dy * y) (num_params values) and its input gradient. */
+wc_status wc_lpc_forward_backward(wc_lpc* l, int32_t n, int32_t h, int32_t w, const float* x,
+                                  const float* feat, const float* dy, float* y, float* grad,
+                                  float* dx);
+/* Copies the solver's current SGN system (c, h, bed; the one of its last solve) for training. */
+wc_status wc_lpc_harvest(wc_lpc* l, wc_solver* s);
+uint64_t wc_lpc_num_systems(const wc_lpc* l);
+/* `steps` Adam steps (learning rate lr) on batches of `batch` random patch x patch crops of the
+ * harvested systems with random error fields (`rough`: weight of the cell-scale noise in them);
+ * losses[steps] (may be null) receives every step's loss, the mean over the batch of
+ * <d, A d> / <e, A e> with d the cycle's error. Synchronous. */
+wc_status wc_lpc_train(wc_lpc* l, uint32_t steps, uint32_t batch, uint32_t patch, float lr,
+                       float rough, uint64_t seed, double* losses);
+/* Attach a network: the solver's dispersive solves become learned-preconditioned flexible CG.
+ * Null detaches it (Jacobi PCG). A solver created with WC_PC_LEARNED steps only once a network
+ * is attached. */
+wc_status wc_solver_set_lpc(wc_solver* s, wc_lpc* l);
+
 /* Kernel launches this solver has queued since it was created (for accounting). */
 uint64_t wc_launch_count(const wc_solver* s);
 /* Human-readable text of the last error on this thread ("" if none). */

@@ -1,8 +1,8 @@
-"""FP64 CPU forward and backward of the learned preconditioner's U-net (TEST INFRASTRUCTURE ONLY).
+"""FP64 CPU forward and backward of the learned preconditioner's network (TEST INFRASTRUCTURE ONLY).
 
 The learned preconditioner has no counterpart in the reference; its oracle is this restatement
-of the network in numpy FP64 (NCHW, zero padding, the architecture of wavesim_b200/lpc.py), used
-to check the device training kernels' forward values and gradients. Only tests/ import it.
+of the network of wavesim_b200/lpc.py in numpy FP64 (NCHW, zero padding), used to check the
+device training kernels' outputs and gradients. Only tests/ import it.
 """
 from __future__ import annotations
 
@@ -12,7 +12,7 @@ from wavesim_b200.lpc import UNetSpec
 
 
 def conv(x, w, b, k):
-    """x: (N, Ci, H, W); w: (Co, Ci, k, k); zero padding (k // 2)."""
+    """x: (N, Ci, H, W); w: (Co, Ci, k, k); zero padding (k // 2); b may be None."""
     n, ci, h, wd = x.shape
     co = w.shape[0]
     pad = k // 2
@@ -21,9 +21,10 @@ def conv(x, w, b, k):
     y = np.zeros((n, co, h, wd))
     for ty in range(k):
         for tx in range(k):
-            patch = xp[:, :, ty : ty + h, tx : tx + wd]
-            y += np.einsum("nchw,oc->nohw", patch, w[:, :, ty, tx])
-    return y + b[None, :, None, None]
+            y += np.einsum("nchw,oc->nohw", xp[:, :, ty : ty + h, tx : tx + wd], w[:, :, ty, tx])
+    if b is not None:
+        y += b[None, :, None, None]
+    return y
 
 
 def conv_bwd(x, w, dy, k):
@@ -39,8 +40,7 @@ def conv_bwd(x, w, dy, k):
             patch = xp[:, :, ty : ty + h, tx : tx + wd]
             dw[:, :, ty, tx] = np.einsum("nohw,nchw->oc", dy, patch)
             dxp[:, :, ty : ty + h, tx : tx + wd] += np.einsum("nohw,oc->nchw", dy, w[:, :, ty, tx])
-    db = dy.sum(axis=(0, 2, 3))
-    return dxp[:, :, pad : pad + h, pad : pad + wd], dw, db
+    return dxp[:, :, pad : pad + h, pad : pad + wd], dw, dy.sum(axis=(0, 2, 3))
 
 
 def pool(x):
@@ -65,85 +65,108 @@ def unpack(spec: UNetSpec, params):
     p = np.asarray(params, dtype=np.float64)
     out = {}
     for name, (w, b, co, ci, k) in spec.offsets().items():
-        out[name] = (p[w : w + co * ci * k * k].reshape(co, ci, k, k), p[b : b + co])
+        out[name] = (p[w : w + co * ci * k * k].reshape(co, ci, k, k), p[b : b + co] if b >= 0 else None)
     return out
 
 
-def forward(spec: UNetSpec, params, x):
-    """Returns (output (N, 2, H, W), cache for backward). H and W divisible by 2**(levels-1)."""
+def gates(spec: UNetSpec, P, feat):
+    """Gate maps per level and the cache for their backward."""
+    out, cache = [], []
+    f = feat
+    for l in range(spec.levels):
+        if l > 0:
+            f = pool(f)
+        wa, ba = P[f"gate{l}a"]
+        pre = conv(f, wa, ba, 3)
+        hid = np.maximum(pre, 0.0)
+        wb, bb = P[f"gate{l}b"]
+        z = conv(hid, wb, bb, 1)
+        g = 2.0 / (1.0 + np.exp(-z))
+        out.append(g)
+        cache.append((f, hid, g))
+    return out, cache
+
+
+def forward(spec: UNetSpec, params, x, feat):
+    """x: (N, 2, H, W) input; feat: (N, 2, H, W) = (h/H0, b/H0). Returns (y, cache)."""
     P = unpack(spec, params)
-    cache = {}
+    G, gcache = gates(spec, P, feat)
     L = spec.levels
+    cache = {"gcache": gcache, "G": G}
     enc = []
     cur = x
     for l in range(L):
         if l > 0:
             cur = pool(enc[-1])
         cache[f"in{l}"] = cur
-        wa, ba = P[f"enc{l}a"]
-        a = np.maximum(conv(cur, wa, ba, 3), 0.0)
+        a = conv(cur, P[f"enc{l}a"][0], None, 3)
         cache[f"enc{l}a"] = a
-        wb, bb = P[f"enc{l}b"]
-        e = np.maximum(conv(a, wb, bb, 3), 0.0)
-        cache[f"enc{l}b"] = e
+        u = conv(a, P[f"enc{l}b"][0], None, 3)
+        cache[f"enc{l}u"] = u
+        e = u * G[l]
         enc.append(e)
     d = enc[-1]
     for l in range(L - 2, -1, -1):
-        u = up(d)
-        cat = np.concatenate([u, enc[l]], axis=1)
+        cat = np.concatenate([up(d), enc[l]], axis=1)
         cache[f"cat{l}"] = cat
-        wa, ba = P[f"dec{l}a"]
-        a = np.maximum(conv(cat, wa, ba, 3), 0.0)
+        a = conv(cat, P[f"dec{l}a"][0], None, 3)
         cache[f"dec{l}a"] = a
-        wb, bb = P[f"dec{l}b"]
-        d = np.maximum(conv(a, wb, bb, 3), 0.0)
-        cache[f"dec{l}b"] = d
-    wo, bo = P["out"]
-    y = conv(d, wo, bo, 1)
+        u = conv(a, P[f"dec{l}b"][0], None, 3)
+        cache[f"dec{l}u"] = u
+        d = u * G[l]
+    cache["dec0"] = d
+    y = conv(d, P["out"][0], None, 1)
     return y, cache
 
 
 def backward(spec: UNetSpec, params, cache, dy):
-    """Gradient of sum(dy * output) with respect to the flat parameter vector and the input."""
+    """Gradient of sum(dy * output) w.r.t. the flat parameters and the input x."""
     P = unpack(spec, params)
     L = spec.levels
+    G = cache["G"]
     grads = {}
-    wo, bo = P["out"]
-    dd, dwo, dbo = conv_bwd(cache["dec0b"], wo, dy, 1)
-    grads["out"] = (dwo, dbo)
-    denc = [np.zeros_like(cache[f"enc{l}b"]) for l in range(L)]
-    # the decoder, from the finest level back towards the bottleneck (reverse of the forward)
+    dG = [np.zeros_like(g) for g in G]
+    dd, dwo, _ = conv_bwd(cache["dec0"], P["out"][0], dy, 1)
+    grads["out"] = (dwo, None)
+    denc = [None] * L
     for l in range(0, L - 1):
-        wb, bb = P[f"dec{l}b"]
-        dd = dd * (cache[f"dec{l}b"] > 0)
-        da, dwb, dbb = conv_bwd(cache[f"dec{l}a"], wb, dd, 3)
-        grads[f"dec{l}b"] = (dwb, dbb)
-        wa, ba = P[f"dec{l}a"]
-        da = da * (cache[f"dec{l}a"] > 0)
-        dcat, dwa, dba = conv_bwd(cache[f"cat{l}"], wa, da, 3)
-        grads[f"dec{l}a"] = (dwa, dba)
+        du = dd * G[l]
+        dG[l] += dd * cache[f"dec{l}u"]
+        da, dwb, _ = conv_bwd(cache[f"dec{l}a"], P[f"dec{l}b"][0], du, 3)
+        grads[f"dec{l}b"] = (dwb, None)
+        dcat, dwa, _ = conv_bwd(cache[f"cat{l}"], P[f"dec{l}a"][0], da, 3)
+        grads[f"dec{l}a"] = (dwa, None)
         cu = spec.channels[l + 1]
-        denc[l] += dcat[:, cu:]
-        dd = up_bwd(dcat[:, :cu])  # gradient into the next coarser decoder output
-    # the bottleneck output is enc[L-1]
-    denc[L - 1] += dd
+        denc[l] = dcat[:, cu:]
+        dd = up_bwd(dcat[:, :cu])
+    de = dd  # gradient into the bottleneck output enc[L-1]
     dx = None
     for l in range(L - 1, -1, -1):
-        de = denc[l] * (cache[f"enc{l}b"] > 0)
-        wb, bb = P[f"enc{l}b"]
-        da, dwb, dbb = conv_bwd(cache[f"enc{l}a"], wb, de, 3)
-        grads[f"enc{l}b"] = (dwb, dbb)
-        wa, ba = P[f"enc{l}a"]
-        da = da * (cache[f"enc{l}a"] > 0)
-        din, dwa, dba = conv_bwd(cache[f"in{l}"], wa, da, 3)
-        grads[f"enc{l}a"] = (dwa, dba)
+        if l < L - 1:
+            de = denc[l] + de_from_below
+        du = de * G[l]
+        dG[l] += de * cache[f"enc{l}u"]
+        da, dwb, _ = conv_bwd(cache[f"enc{l}a"], P[f"enc{l}b"][0], du, 3)
+        grads[f"enc{l}b"] = (dwb, None)
+        din, dwa, _ = conv_bwd(cache[f"in{l}"], P[f"enc{l}a"][0], da, 3)
+        grads[f"enc{l}a"] = (dwa, None)
         if l > 0:
-            denc[l - 1] += pool_bwd(din)
+            de_from_below = pool_bwd(din)
         else:
             dx = din
+    # gate networks
+    for l in range(L):
+        f, hid, g = cache["gcache"][l]
+        dz = dG[l] * g * (1.0 - g / 2.0)
+        dhid, dwb, dbb = conv_bwd(hid, P[f"gate{l}b"][0], dz, 1)
+        grads[f"gate{l}b"] = (dwb, dbb)
+        dpre = dhid * (hid > 0)
+        _, dwa, dba = conv_bwd(f, P[f"gate{l}a"][0], dpre, 3)
+        grads[f"gate{l}a"] = (dwa, dba)
     flat = np.zeros(spec.n_params())
     for name, (w, b, co, ci, k) in spec.offsets().items():
         gw, gb = grads[name]
         flat[w : w + co * ci * k * k] = gw.ravel()
-        flat[b : b + co] = gb
+        if b >= 0:
+            flat[b : b + co] = gb
     return flat, dx

@@ -1,0 +1,167 @@
+"""The learned preconditioner on the device: network gradients against the FP64 oracle, the
+flexible-CG solve against the Jacobi solve and the FP64 oracle, training, and what the trained
+network gains over the method without it.
+
+Tolerances (stated per test): FP32 device arithmetic against FP64 numpy, relative to the largest
+magnitude of each compared block.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import unet_oracle as U
+from oracle.oracle import OracleSolver
+from wavesim_b200 import LearnedPreconditioner, Solver
+from wavesim_b200 import workloads as W
+from wavesim_b200.lpc import UNetSpec, bf16_round, init_params
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-30))
+
+
+def random_params(spec, seed):
+    """Initial weights plus non-zero output layer and biases, so every gradient is exercised."""
+    rng = np.random.default_rng(seed)
+    p = init_params(spec, seed).astype(np.float64)
+    for name, (w, b, co, ci, k) in spec.offsets().items():
+        if name == "out":
+            p[w : w + co * ci * k * k] = rng.normal(0.0, 0.3, co * ci * k * k)
+        if b >= 0:
+            p[b : b + co] = rng.normal(0.0, 0.2, co)
+    return p.astype(np.float32)
+
+
+def batch(seed, n=2, h=16, w=24):
+    rng = np.random.default_rng(seed)
+    x = rng.normal(size=(n, 2, h, w)).astype(np.float32)
+    feat = np.stack([rng.uniform(0.0, 1.0, (n, h, w)), rng.uniform(-1.0, 0.2, (n, h, w))], axis=1).astype(np.float32)
+    dy = rng.normal(size=(n, 2, h, w)).astype(np.float32)
+    return x, feat, dy
+
+
+def test_network_forward_and_gradients_match_the_fp64_oracle():
+    spec = UNetSpec()
+    net = LearnedPreconditioner(spec)
+    net.set_rounding(False)
+    p = random_params(spec, 3)
+    net.set_params(p)
+    x, feat, dy = batch(4)
+    y, g, dx = net.forward_backward(x, feat, dy)
+    yo, cache = U.forward(spec, p.astype(np.float64), x.astype(np.float64), feat.astype(np.float64))
+    go, dxo = U.backward(spec, p.astype(np.float64), cache, dy.astype(np.float64))
+    assert rel(y, yo) < 2e-5
+    assert rel(dx, dxo) < 2e-5
+    for name, (w, b, co, ci, k) in spec.offsets().items():  # per layer, FP32 sums of ~1e3 terms
+        n = co * ci * k * k
+        assert rel(g[w : w + n], go[w : w + n]) < 1e-4, name
+        if b >= 0:
+            assert rel(g[b : b + co], go[b : b + co]) < 1e-4, name + " bias"
+
+
+def test_forward_uses_bf16_rounded_weights():
+    spec = UNetSpec()
+    net = LearnedPreconditioner(spec)
+    p = random_params(spec, 5)
+    net.set_params(p)  # rounding on by default
+    x, feat, dy = batch(6, n=1, h=32, w=32)
+    y, _, _ = net.forward_backward(x, feat, dy)
+    yr, _ = U.forward(spec, bf16_round(p).astype(np.float64), x.astype(np.float64), feat.astype(np.float64))
+    yf, _ = U.forward(spec, p.astype(np.float64), x.astype(np.float64), feat.astype(np.float64))
+    assert rel(y, yr) < 2e-5
+    assert rel(yr, yf) > 1e-4  # the rounding is visible: the test can tell the two apart
+    assert np.array_equal(net.get_params(), p)  # the master weights stay FP32
+
+
+def small_run(seed=11, nx=192, ny=96, tol=1e-8):
+    w = W.sgn_beach(nx, ny, 2.0, seed=seed, tolerance=tol, name=f"lpc_{nx}x{ny}")
+    return w, W.wave_train_state(w)
+
+
+def test_untrained_network_solve_matches_the_oracle():
+    # An untrained network (zero output layer) leaves flexible CG preconditioned by two Jacobi
+    # sweeps; the solution is the same system's, so the state matches the oracle as closely as
+    # the Jacobi build does (same tolerances as the SGN parity case).
+    w, s0 = small_run()
+    net = LearnedPreconditioner(UNetSpec(), seed=1)
+    gpu = w.solver(Solver)
+    gpu.set_preconditioner(net)
+    orc = w.solver(OracleSolver)
+    sg, so = s0.clone(), s0.clone()
+    g = w.grid
+    for _ in range(60):
+        dt = orc.stable_dt(so)
+        orc.step(so, dt)
+        gpu.step(sg, dt)
+    hg, ho = g.inner(sg.h), g.inner(so.h)
+    wet = (hg > 1e-3) & (ho > 1e-3)
+    d = np.abs(hg - ho)[wet]
+    assert d.max() < 3e-5
+    assert abs(sg.volume(g) - so.volume(g)) < 1e-5 * so.volume(g)
+    st = gpu.dispersion_stats()
+    assert st.solves == 120 and st.unconverged == 0
+
+
+def harvest(net, seeds=(21, 22, 23), steps=40, every=10, nx=256, ny=128):
+    for k, seed in enumerate(seeds):
+        w = W.sgn_beach(nx, ny, 2.0, seed=seed, height=1.0 + k, period=10.0 + 3 * k, angle_deg=-15.0 + 15 * k)
+        sol = w.solver(Solver)
+        s = W.wave_train_state(w)
+        sol.upload(s)
+        for _ in range(steps // every):
+            sol.step_n(every)
+            sol.synchronize()
+            net.harvest(sol)
+
+
+def test_training_lowers_the_loss():
+    net = LearnedPreconditioner(UNetSpec(), seed=2)
+    harvest(net)
+    assert net.n_systems == 12
+    before = net.train(0)
+    losses = net.train(300, batch=8, patch=64, lr=2e-3, seed=1)
+    assert before.size == 0 and np.all(np.isfinite(losses))
+    first, last = losses[:20].mean(), losses[-20:].mean()
+    assert last < 0.8 * first, (first, last)
+
+
+def test_trained_network_needs_fewer_iterations_than_jacobi():
+    net = LearnedPreconditioner(UNetSpec(), seed=2)
+    harvest(net)
+    net.train(600, batch=8, patch=64, lr=2e-3, seed=2)
+    w, s0 = small_run(seed=31, nx=256, ny=128)
+    plain = w.solver(Solver)
+    learned = w.solver(Solver)
+    learned.set_preconditioner(net)
+    sa, sb = s0.clone(), s0.clone()
+    for _ in range(20):
+        dt = plain.stable_dt(sa)
+        plain.step(sa, dt)
+        learned.step(sb, dt)
+    a, b = plain.dispersion_stats(), learned.dispersion_stats()
+    it_plain = a.iterations / a.solves
+    it_learned = b.iterations / b.solves
+    print(f"iterations per solve: Jacobi PCG {it_plain:.1f}, learned {it_learned:.1f}")
+    assert b.unconverged == 0
+    assert it_learned < 0.8 * it_plain
+    g = w.grid
+    assert np.max(np.abs(g.inner(sa.h) - g.inner(sb.h))) < 1e-5  # both solve to 1e-8
+
+
+def test_learned_solve_counts_its_iteration_kernels():
+    w, s0 = small_run(nx=128, ny=64)
+    net = LearnedPreconditioner(UNetSpec(), seed=1)
+    sol = w.solver(Solver)
+    sol.set_preconditioner(net)
+    sol.upload(s0)
+    n0 = sol.launch_count()
+    sol.step_n(3)
+    sol.synchronize()
+    st = sol.dispersion_stats()
+    n1 = sol.launch_count()
+    assert st.iterations > 0
+    assert n1 - n0 > 30 * st.iterations  # every iteration is ~30 kernels of the device library
+    assert math.isfinite(sol.time_device())

@@ -52,6 +52,7 @@ struct Ctl {
     unsigned long long solves, iterations, unconverged;
     int last_iterations;
     int pad_;
+    unsigned long long fcg_iterations;  // of them, learned flexible-CG iterations
 };
 
 struct SpongeDev {
@@ -80,6 +81,13 @@ __device__ __forceinline__ int wrap_idx(int j, int n) {
     int t = j % n;
     return t < 0 ? t + n : t;
 }
+
+// Scalars of the learned path's flexible CG, kept on the device so that iterations chain
+// without the host; `done` stops every later kernel of the solve.
+struct FcgScalars {
+    double bb, rr, pq, rp, zq, target, alpha, beta;
+    int converged, iterations, done, pad_;
+};
 
 struct Mapped {
     int k;        // linear index of the source cell

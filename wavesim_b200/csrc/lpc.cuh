@@ -1,0 +1,625 @@
+// lpc.cuh — kernels of the learned preconditioner: its network (inference and training) and
+// the patch-level SGN operator the training loss is measured with.
+//
+// No counterpart in the reference. Tensors are NCHW FP32; weights are [Co][Ci][K][K] and are
+// used as stored (the training loop stores BF16-rounded copies for the forward pass, so the
+// arithmetic is BF16 weights with FP32 accumulation). Zero padding at tensor edges.
+#pragma once
+
+#include "common.cuh"
+
+namespace wcb {
+
+enum ConvMode { CM_DIRECT = 0, CM_POOL = 1, CM_UP = 2 };
+enum ConvAct { ACT_NONE = 0, ACT_RELU = 1, ACT_SIG2 = 2 };
+
+struct ConvArgs {
+    const float* a;  // first input: ca channels; CM_POOL: at 2H x 2W (2x2 mean), CM_UP: at H/2 x W/2
+    int ca, amode;
+    const float* b;  // second input (concatenated after a), at H x W, or null
+    int cb;
+    const float* w;     // [co][ca + cb][k][k]
+    const float* bias;  // [co] or null
+    const float* gate;  // [n][co][H][W] or null: y = act(conv + bias) * gate
+    float* y;           // [n][co][H][W]
+    int co, H, W, N, act;
+};
+
+constexpr int CV_T = 16;   // output tile edge
+constexpr int CV_COB = 8;  // output channels per block
+constexpr int CV_CIB = 4;  // input channels staged per pass
+
+__device__ __forceinline__ float conv_input(const ConvArgs& p, int n, int c, int y, int x) {
+    if ((unsigned)y >= (unsigned)p.H || (unsigned)x >= (unsigned)p.W) return 0.f;
+    if (c < p.ca) {
+        if (p.amode == CM_DIRECT) return p.a[(((size_t)n * p.ca + c) * p.H + y) * p.W + x];
+        if (p.amode == CM_POOL) {
+            const int W2 = 2 * p.W;
+            const float* q = p.a + (((size_t)n * p.ca + c) * (2 * p.H) + 2 * y) * W2 + 2 * x;
+            return 0.25f * ((q[0] + q[1]) + (q[W2] + q[W2 + 1]));
+        }
+        const int Hh = p.H / 2, Wh = p.W / 2;
+        return p.a[(((size_t)n * p.ca + c) * Hh + y / 2) * Wh + x / 2];
+    }
+    return p.b[(((size_t)n * p.cb + (c - p.ca)) * p.H + y) * p.W + x];
+}
+
+template <int K>
+__global__ void __launch_bounds__(CV_T* CV_T) conv_fwd_kernel(ConvArgs p) {
+    constexpr int R = K / 2, TE = CV_T + 2 * R;
+    __shared__ float tile[CV_CIB][TE][TE];
+    __shared__ float wsm[CV_COB][CV_CIB][K * K];
+    const int ncog = (p.co + CV_COB - 1) / CV_COB;
+    const int n = blockIdx.z / ncog, cog = blockIdx.z % ncog;
+    const int x0 = blockIdx.x * CV_T, y0 = blockIdx.y * CV_T;
+    const int tx = threadIdx.x % CV_T, ty = threadIdx.x / CV_T;
+    const int ci_total = p.ca + p.cb;
+    float acc[CV_COB];
+#pragma unroll
+    for (int o = 0; o < CV_COB; o++) acc[o] = 0.f;
+    for (int c0 = 0; c0 < ci_total; c0 += CV_CIB) {
+        for (int q = threadIdx.x; q < CV_CIB * TE * TE; q += CV_T * CV_T) {
+            const int c = q / (TE * TE), r = q % (TE * TE);
+            const int yy = y0 + r / TE - R, xx = x0 + r % TE - R;
+            tile[c][r / TE][r % TE] = (c0 + c < ci_total) ? conv_input(p, n, c0 + c, yy, xx) : 0.f;
+        }
+        for (int q = threadIdx.x; q < CV_COB * CV_CIB * K * K; q += CV_T * CV_T) {
+            const int o = q / (CV_CIB * K * K), r = q % (CV_CIB * K * K);
+            const int c = r / (K * K), t = r % (K * K);
+            const int co = cog * CV_COB + o, ci = c0 + c;
+            wsm[o][c][t] = (co < p.co && ci < ci_total) ? p.w[((size_t)co * ci_total + ci) * K * K + t] : 0.f;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int c = 0; c < CV_CIB; c++)
+#pragma unroll
+            for (int t = 0; t < K * K; t++) {
+                const float v = tile[c][ty + t / K][tx + t % K];
+#pragma unroll
+                for (int o = 0; o < CV_COB; o++) acc[o] = fmaf(v, wsm[o][c][t], acc[o]);
+            }
+        __syncthreads();
+    }
+    const int x = x0 + tx, y = y0 + ty;
+    if (x >= p.W || y >= p.H) return;
+#pragma unroll
+    for (int o = 0; o < CV_COB; o++) {
+        const int co = cog * CV_COB + o;
+        if (co >= p.co) break;
+        float v = acc[o] + (p.bias ? p.bias[co] : 0.f);
+        if (p.act == ACT_RELU) v = fmaxf(v, 0.f);
+        else if (p.act == ACT_SIG2) v = 2.f / (1.f + expf(-v));
+        const size_t k = (((size_t)n * p.co + co) * p.H + y) * p.W + x;
+        if (p.gate) v *= p.gate[k];
+        p.y[k] = v;
+    }
+}
+
+// dw[co][ci][t] = sum over samples and pixels of dy[co] * x[ci] shifted by tap t; one block per
+// (co, ci) pair. x is the concatenation of xa (ca channels) and xb, both at H x W.
+template <int K>
+__global__ void __launch_bounds__(256) conv_wgrad_kernel(const float* __restrict__ dy, const float* __restrict__ xa,
+                                                         int ca, const float* __restrict__ xb, int cb, int co_n,
+                                                         int H, int W, int N, float* __restrict__ dw) {
+    constexpr int R = K / 2;
+    const int ci_total = ca + cb;
+    const int co = blockIdx.x / ci_total, ci = blockIdx.x % ci_total;
+    float acc[K * K];
+#pragma unroll
+    for (int t = 0; t < K * K; t++) acc[t] = 0.f;
+    const size_t plane = (size_t)H * W;
+    for (size_t q = threadIdx.x; q < (size_t)N * plane; q += blockDim.x) {
+        const int n = (int)(q / plane);
+        const int r = (int)(q % plane);
+        const int y = r / W, x = r % W;
+        const float g = dy[((size_t)n * co_n + co) * plane + r];
+        const float* src = ci < ca ? xa + ((size_t)n * ca + ci) * plane : xb + ((size_t)n * cb + (ci - ca)) * plane;
+#pragma unroll
+        for (int t = 0; t < K * K; t++) {
+            const int yy = y + t / K - R, xx = x + t % K - R;
+            if ((unsigned)yy < (unsigned)H && (unsigned)xx < (unsigned)W) acc[t] = fmaf(g, src[yy * W + xx], acc[t]);
+        }
+    }
+    __shared__ float red[K * K][8];
+#pragma unroll
+    for (int t = 0; t < K * K; t++) {
+        float v = acc[t];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0) red[t][threadIdx.x >> 5] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < K * K) {
+        float v = 0.f;
+        for (int w8 = 0; w8 < (int)(blockDim.x / 32); w8++) v += red[threadIdx.x][w8];
+        dw[((size_t)co * ci_total + ci) * K * K + threadIdx.x] += v;
+    }
+}
+
+__global__ void bias_grad_kernel(const float* __restrict__ dy, int co_n, int H, int W, int N, float* __restrict__ db) {
+    const int co = blockIdx.x;
+    const size_t plane = (size_t)H * W;
+    float s = 0.f;
+    for (size_t q = threadIdx.x; q < (size_t)N * plane; q += blockDim.x) {
+        const int n = (int)(q / plane);
+        s += dy[((size_t)n * co_n + co) * plane + q % plane];
+    }
+    __shared__ float red[8];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float v = 0.f;
+        for (int w8 = 0; w8 < (int)(blockDim.x / 32); w8++) v += red[w8];
+        db[co] += v;
+    }
+}
+
+// wt[ci][co][K-1-ty][K-1-tx] = w[co][ci][ty][tx]: the input gradient of a convolution is the
+// convolution of the output gradient with these weights.
+__global__ void transpose_weights_kernel(const float* __restrict__ w, int co_n, int ci_n, int K, float* __restrict__ wt) {
+    const int total = co_n * ci_n * K * K;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < total; q += gridDim.x * blockDim.x) {
+        const int t = q % (K * K), r = q / (K * K);
+        const int ci = r % ci_n, co = r / ci_n;
+        const int ty = t / K, tx = t % K;
+        wt[((size_t)ci * co_n + co) * K * K + (K - 1 - ty) * K + (K - 1 - tx)] = w[q];
+    }
+}
+
+// 2x2 mean pooling and nearest upsampling, their adjoints (pool_bwd = up / 4, up_bwd = sum).
+__global__ void pool2_kernel(const float* __restrict__ x, int NC, int H, int W, float* __restrict__ y, float scale,
+                             int add) {
+    // y at H/2 x W/2: scale * sum of the 2x2 block (scale 0.25: mean pooling; 1: the adjoint of up)
+    const int Hh = H / 2, Wh = W / 2;
+    const size_t total = (size_t)NC * Hh * Wh;
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
+        const int xx = (int)(q % Wh), yy = (int)((q / Wh) % Hh);
+        const size_t c = q / ((size_t)Hh * Wh);
+        const float* s = x + (c * H + 2 * yy) * W + 2 * xx;
+        const float v = scale * ((s[0] + s[1]) + (s[W] + s[W + 1]));
+        y[q] = add ? y[q] + v : v;
+    }
+}
+
+__global__ void up2_kernel(const float* __restrict__ x, int NC, int Hh, int Wh, float* __restrict__ y, float scale,
+                           int add) {
+    // y at 2Hh x 2Wh: scale * nearest value (scale 1: upsampling; 0.25: the adjoint of pooling)
+    const int H = 2 * Hh, W = 2 * Wh;
+    const size_t total = (size_t)NC * H * W;
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
+        const int xx = (int)(q % W), yy = (int)((q / W) % H);
+        const size_t c = q / ((size_t)H * W);
+        const float v = scale * x[(c * Hh + yy / 2) * Wh + xx / 2];
+        y[q] = add ? y[q] + v : v;
+    }
+}
+
+// Gate backward: u * g -> du = dy g, dg = dy u (dg accumulated); then through g = 2 sigmoid(z):
+// dz = dg * g (1 - g / 2).
+__global__ void gate_bwd_kernel(const float* __restrict__ dy, const float* __restrict__ u, const float* __restrict__ g,
+                                float* __restrict__ du, float* __restrict__ dg, size_t n) {
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+        du[q] = dy[q] * g[q];
+        dg[q] += dy[q] * u[q];
+    }
+}
+
+__global__ void sig2_relu_bwd_kernel(float* __restrict__ d, const float* __restrict__ y, size_t n, int act) {
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+        if (act == ACT_SIG2) d[q] *= y[q] * (1.f - 0.5f * y[q]);
+        else d[q] = y[q] > 0.f ? d[q] : 0.f;
+    }
+}
+
+// ---- the SGN operator on training patches (zero outside the patch) ------------------------
+
+struct PatchOp {
+    const float* c;     // [n][H][W]
+    const float* heff;  // [n][H][W]
+    const float* mask;  // [n][H][W]
+    int H, W, N;
+    float ix, iy, dx2i, dy2i;  // 0.5/dx, 0.5/dy, 0.25/dx^2, 0.25/dy^2
+};
+
+// out = A p on every patch cell (dispersion.rs:269-317 with zero values outside the patch).
+__global__ void patch_matvec_kernel(PatchOp op, const float* __restrict__ p, float* __restrict__ out) {
+    const size_t plane = (size_t)op.H * op.W;
+    const size_t total = (size_t)op.N * plane;
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
+        const int n = (int)(q / plane);
+        const int r = (int)(q % plane);
+        const int y = r / op.W, x = r % op.W;
+        const float* px = p + (size_t)n * 2 * plane;
+        const float* py = px + plane;
+        const float* c = op.c + (size_t)n * plane;
+        auto P = [&](const float* a, int yy, int xx) {
+            return ((unsigned)yy < (unsigned)op.H && (unsigned)xx < (unsigned)op.W) ? a[yy * op.W + xx] : 0.f;
+        };
+        auto f = [&](int yy, int xx) {
+            if ((unsigned)yy >= (unsigned)op.H || (unsigned)xx >= (unsigned)op.W) return 0.f;
+            return c[yy * op.W + xx] * ((P(px, yy, xx + 1) - P(px, yy, xx - 1)) * op.ix + (P(py, yy + 1, xx) - P(py, yy - 1, xx)) * op.iy);
+        };
+        const float m = op.mask[q], he = op.heff[q];
+        out[(size_t)n * 2 * plane + r] = m * (he * px[r] - (f(y, x + 1) - f(y, x - 1)) * op.ix);
+        out[(size_t)n * 2 * plane + plane + r] = m * (he * py[r] - (f(y + 1, x) - f(y - 1, x)) * op.iy);
+    }
+}
+
+// The Jacobi diagonal on patches (dispersion.rs:441-457), two planes per sample.
+__global__ void patch_diag_kernel(PatchOp op, float* __restrict__ d) {
+    const size_t plane = (size_t)op.H * op.W;
+    const size_t total = (size_t)op.N * plane;
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
+        const int n = (int)(q / plane);
+        const int r = (int)(q % plane);
+        const int y = r / op.W, x = r % op.W;
+        const float* c = op.c + (size_t)n * plane;
+        auto C = [&](int yy, int xx) {
+            return ((unsigned)yy < (unsigned)op.H && (unsigned)xx < (unsigned)op.W) ? c[yy * op.W + xx] : 0.f;
+        };
+        float dxv = 1.f, dyv = 1.f;
+        if (op.mask[q] != 0.f) {
+            dxv = op.heff[q] + (C(y, x + 1) + C(y, x - 1)) * op.dx2i;
+            dyv = op.heff[q] + (C(y + 1, x) + C(y - 1, x)) * op.dy2i;
+        }
+        d[(size_t)n * 2 * plane + r] = dxv;
+        d[(size_t)n * 2 * plane + plane + r] = dyv;
+    }
+}
+
+// Generic elementwise update on 2-plane fields: out = a * x + b * y * (mask?) / d^e ...
+// kept explicit: each use below names what it computes.
+__global__ void lincomb_kernel(float* __restrict__ out, const float* __restrict__ x, float ax,
+                               const float* __restrict__ y, float ay, const float* __restrict__ div_by,
+                               const float* __restrict__ mask, int mask_planes, size_t n, size_t plane) {
+    // out = ax * x + ay * y [/ div_by] [* mask (broadcast over 2 planes)]
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+        float v = ay * (y ? y[q] : 0.f);
+        if (div_by) v /= div_by[q];
+        if (mask) v *= mask[(q / (mask_planes * plane)) * plane + q % plane];
+        out[q] = (x ? ax * x[q] : 0.f) + v;
+    }
+}
+
+// Per-sample dots <a, b> over 2-plane fields, accumulated in FP64.
+__global__ void sample_dot_kernel(const float* __restrict__ a, const float* __restrict__ b, size_t per_sample,
+                                  double* __restrict__ out) {
+    const int n = blockIdx.y;
+    double s = 0.0;
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < per_sample; q += (size_t)gridDim.x * blockDim.x)
+        s += (double)a[n * per_sample + q] * b[n * per_sample + q];
+    __shared__ double red[8];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double v = 0.0;
+        for (int w8 = 0; w8 < (int)(blockDim.x / 32); w8++) v += red[w8];
+        atomicAdd(out + n, v);
+    }
+}
+
+// grad = -2 / (N E_n) * Ad  (the gradient of mean_n <d, A d>_n / E_n with respect to z, d = e - z)
+__global__ void loss_grad_kernel(const float* __restrict__ ad, const double* __restrict__ energy, int N,
+                                 size_t per_sample, float* __restrict__ g) {
+    const size_t total = (size_t)N * per_sample;
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
+        const int n = (int)(q / per_sample);
+        g[q] = (float)(-2.0 / ((double)N * energy[n])) * ad[q];
+    }
+}
+
+// Random error fields for training: white noise of a per-sample weight plus value noise at
+// scales 1..32 cells (bilinear between hashed lattice values), masked.
+__device__ __forceinline__ float hash_unit(unsigned long long k) {
+    k ^= k >> 33;
+    k *= 0xff51afd7ed558ccdull;
+    k ^= k >> 33;
+    k *= 0xc4ceb9fe1a85ec53ull;
+    k ^= k >> 33;
+    return (float)(k >> 40) * (1.0f / 16777216.0f) * 2.f - 1.f;
+}
+
+__global__ void random_field_kernel(float* __restrict__ e, const float* __restrict__ mask, int N, int H, int W,
+                                    unsigned long long seed, float rough) {
+    const size_t plane = (size_t)H * W;
+    const size_t total = (size_t)N * 2 * plane;
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
+        const int n = (int)(q / (2 * plane));
+        const int comp = (int)((q / plane) % 2);
+        const int r = (int)(q % plane);
+        const int y = r / W, x = r % W;
+        const unsigned long long base = seed * 1000003ull + (unsigned long long)(n * 2 + comp) * 7919ull;
+        const float wr = rough * 0.5f * (hash_unit(base ^ 0x51ull) + 1.f);
+        float v = wr * 1.7320508f * hash_unit(base * 31ull + (unsigned long long)r * 2654435761ull + 17ull);
+        for (int sc = 1, li = 0; sc <= 32; sc *= 2, li++) {
+            const float fy = (float)y / sc, fx = (float)x / sc;
+            const int iy = (int)floorf(fy), ixx = (int)floorf(fx);
+            const float ty = fy - iy, tx = fx - ixx;
+            auto L = [&](int a, int b) {
+                return hash_unit(base * 131ull + (unsigned long long)li * 1000003ull + (unsigned long long)(a + 64) * 92821ull +
+                                 (unsigned long long)(b + 64) * 68917ull);
+            };
+            const float lv = (1 - ty) * ((1 - tx) * L(iy, ixx) + tx * L(iy, ixx + 1)) + ty * ((1 - tx) * L(iy + 1, ixx) + tx * L(iy + 1, ixx + 1));
+            v += sqrtf((float)sc) * 1.7320508f * lv;
+        }
+        e[q] = v * mask[(size_t)n * plane + r];
+    }
+}
+
+// Nearest bfloat16 (ties to even) as a float: keep the top 16 bits after adding half an ulp of
+// the kept part (plus one if the kept part is odd). Finite inputs only (weights are finite).
+__device__ __forceinline__ float bf16_round(float x) {
+    const unsigned a = __float_as_uint(x);
+    return __uint_as_float((a + 0x7FFFu + ((a >> 16) & 1u)) & 0xFFFF0000u);
+}
+
+__global__ void adam_kernel(float* __restrict__ w, float* __restrict__ wq, const float* __restrict__ g, float* __restrict__ m,
+                            float* __restrict__ v, int n, float lr, float b1, float b2, float c1, float c2, float eps,
+                            int round_bf16) {
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        const float gg = g[q];
+        m[q] = b1 * m[q] + (1.f - b1) * gg;
+        v[q] = b2 * v[q] + (1.f - b2) * gg * gg;
+        w[q] -= lr * (m[q] * c1) / (sqrtf(v[q] * c2) + eps);
+        wq[q] = round_bf16 ? bf16_round(w[q]) : w[q];
+    }
+}
+
+__global__ void round_copy_kernel(const float* __restrict__ w, float* __restrict__ wq, int n, int round_bf16) {
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
+        wq[q] = round_bf16 ? bf16_round(w[q]) : w[q];
+}
+
+}  // namespace wcb
+
+namespace wcb {
+
+// ---- flexible CG with the learned preconditioner, on the solver's arrays ------------------
+//
+// Vectors are float2 (x, y components) over the interior with the solver's pitch; halo reads go
+// through the boundary mapping (vector ghosts: the wall-normal component flips sign), as in the
+// Jacobi solve. Scalars live on the device so that iterations chain without the host.
+
+
+// A v (dispersion.rs:269-317) one cell per thread, halo through the mapping.
+__global__ void fcg_matvec_kernel(DevGrid g, const float2* __restrict__ v, const float* __restrict__ cc,
+                                  const float* __restrict__ heff, float2* __restrict__ out,
+                                  const FcgScalars* __restrict__ sc) {
+    if (sc && sc->done) return;
+    const int n = g.nx * g.ny;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        const int i = c % g.nx, j = c / g.nx;
+        auto V = [&](int a, int b) {
+            const Mapped m = map_cell(g, a, b);
+            const float2 t = v[m.k];
+            return make_float2(t.x * m.sx, t.y * m.sy);
+        };
+        auto F = [&](int a, int b) {
+            const Mapped m = map_cell(g, a, b);
+            return cc[m.k] * ((V(a + 1, b).x - V(a - 1, b).x) * g.ix + (V(a, b + 1).y - V(a, b - 1).y) * g.iy);
+        };
+        const int k = j * g.pitch + i;
+        const float he = heff[k];
+        const float mask = he >= H_DISP_MIN ? 1.f : 0.f;
+        const float2 own = v[k];
+        float2 r;
+        r.x = mask * (he * own.x - (F(i + 1, j) - F(i - 1, j)) * g.ix);
+        r.y = mask * (he * own.y - (F(i, j + 1) - F(i, j - 1)) * g.iy);
+        out[k] = r;
+    }
+}
+
+// The Jacobi diagonal (dispersion.rs:441-457) and the warm start masked (:480-490).
+__global__ void fcg_setup_kernel(DevGrid g, const float* __restrict__ cc, const float* __restrict__ heff,
+                                 float2* __restrict__ diag, float2* __restrict__ w) {
+    const int n = g.nx * g.ny;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        const int i = c % g.nx, j = c / g.nx;
+        const int k = j * g.pitch + i;
+        const float he = heff[k];
+        float2 d = make_float2(1.f, 1.f);
+        if (he >= H_DISP_MIN) {
+            auto C = [&](int a, int b) { return cc[map_cell(g, a, b).k]; };
+            d.x = he + (C(i + 1, j) + C(i - 1, j)) * 0.25f / (g.dx * g.dx);
+            d.y = he + (C(i, j + 1) + C(i, j - 1)) * 0.25f / (g.dy * g.dy);
+        } else {
+            w[k] = make_float2(0.f, 0.f);
+        }
+        diag[k] = d;
+    }
+}
+
+// Up to three dot products of float2 fields, per-block FP64 partials (fixed partition), then
+// one block adds them in block order: reproducible.
+__global__ void fcg_dot_partial_kernel(DevGrid g, const float2* a0, const float2* b0, const float2* a1,
+                                       const float2* b1, const float2* a2, const float2* b2, double* part,
+                                       const FcgScalars* __restrict__ sc) {
+    if (sc && sc->done) return;
+    double s[3] = {0.0, 0.0, 0.0};
+    const int n = g.nx * g.ny;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        const int k = (c / g.nx) * g.pitch + c % g.nx;
+        const float2 x0 = a0[k], y0 = b0[k];
+        s[0] += (double)x0.x * y0.x + (double)x0.y * y0.y;
+        if (a1) {
+            const float2 x1 = a1[k], y1 = b1[k];
+            s[1] += (double)x1.x * y1.x + (double)x1.y * y1.y;
+        }
+        if (a2) {
+            const float2 x2 = a2[k], y2 = b2[k];
+            s[2] += (double)x2.x * y2.x + (double)x2.y * y2.y;
+        }
+    }
+    __shared__ double red[100];
+    block_sum3<256>(s[0], s[1], s[2], red);
+    if (threadIdx.x == 0) {
+        part[3 * blockIdx.x] = s[0];
+        part[3 * blockIdx.x + 1] = s[1];
+        part[3 * blockIdx.x + 2] = s[2];
+    }
+}
+
+enum FcgStep { FCG_INIT = 0, FCG_ALPHA = 1, FCG_RESID = 2, FCG_BETA = 3 };
+
+// Totals of the partials and the scalar logic of one point of the iteration. With `cond` set the
+// kernel also steers the graph's while-node: it continues while the solve is not done.
+__global__ void fcg_scalars_kernel(const double* part, int nblocks, FcgScalars* sc, int step, double tol,
+                                   long long max_it, cudaGraphConditionalHandle handle, int cond) {
+    if (sc->done && step != FCG_INIT) {
+        if (cond && threadIdx.x == 0) cudaGraphSetConditional(handle, 0u);
+        return;
+    }
+    double s[3] = {0.0, 0.0, 0.0};
+    for (int b = threadIdx.x; b < nblocks; b += 256)
+        for (int q = 0; q < 3; q++) s[q] += part[3 * b + q];
+    __shared__ double red[100];
+    block_sum3<256>(s[0], s[1], s[2], red);
+    if (threadIdx.x != 0) return;
+    if (step == FCG_INIT) {  // <b, b>, <r, r>
+        sc->bb = s[0];
+        sc->rr = s[1];
+        sc->target = tol * sqrt(s[0]) + 1e-10;
+        sc->iterations = 0;
+        sc->pq = 0.0;
+        sc->converged = sqrt(s[1]) <= sc->target;
+        sc->done = sc->converged || max_it <= 0;
+    } else if (step == FCG_ALPHA) {  // <p, q>, <r, p>
+        sc->pq = s[0];
+        sc->rp = s[1];
+        sc->alpha = s[1] / s[0];
+        if (!(s[0] > 0.0)) {  // breakdown: the solve stops unconverged (Jacobi PCG takes over)
+            sc->alpha = 0.0;
+            sc->done = 1;
+        }
+    } else if (step == FCG_RESID) {  // <r, r>
+        sc->rr = s[0];
+        sc->iterations += 1;
+        sc->converged = sqrt(s[0]) <= sc->target;
+        sc->done = sc->converged || sc->iterations >= max_it;
+    } else {  // <z, q>: the new direction is A-orthogonal to the previous one (none at first)
+        sc->zq = s[0];
+        sc->beta = sc->iterations == 0 ? 0.0 : -s[0] / sc->pq;
+    }
+    if (cond && (step == FCG_INIT || step == FCG_RESID)) cudaGraphSetConditional(handle, sc->done ? 0u : 1u);
+}
+
+// w += alpha p, r -= alpha q
+__global__ void fcg_update_kernel(DevGrid g, float2* w, float2* r, const float2* p, const float2* q, const FcgScalars* sc) {
+    if (sc->done) return;
+    const float a = (float)sc->alpha;
+    const int n = g.nx * g.ny;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        const int k = (c / g.nx) * g.pitch + c % g.nx;
+        float2 ww = w[k], rr = r[k];
+        const float2 pp = p[k], qq = q[k];
+        ww.x += a * pp.x;
+        ww.y += a * pp.y;
+        rr.x -= a * qq.x;
+        rr.y -= a * qq.y;
+        w[k] = ww;
+        r[k] = rr;
+    }
+}
+
+// p = z + beta p (the first direction: p = z)
+__global__ void fcg_direction_kernel(DevGrid g, float2* p, const float2* z, const FcgScalars* sc) {
+    if (sc->done) return;
+    const bool first = sc->iterations == 0;
+    const float b = first ? 0.f : (float)sc->beta;
+    const int n = g.nx * g.ny;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        const int k = (c / g.nx) * g.pitch + c % g.nx;
+        const float2 zz = z[k];
+        const float2 pp = first ? make_float2(0.f, 0.f) : p[k];
+        p[k] = make_float2(zz.x + b * pp.x, zz.y + b * pp.y);
+    }
+}
+
+// r = b - t (the initial residual)
+__global__ void fcg_residual_kernel(DevGrid g, const float2* b, const float2* t, float2* r) {
+    const int n = g.nx * g.ny;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        const int k = (c / g.nx) * g.pitch + c % g.nx;
+        const float2 bb = b[k], tt = t[k];
+        r[k] = make_float2(bb.x - tt.x, bb.y - tt.y);
+    }
+}
+
+// Preconditioner pieces. Network tensors are 2 planes of Hp x Wp (the interior, zero-padded to a
+// multiple of 8).
+// z1 = omega r / diag
+__global__ void lpc_jacobi_kernel(DevGrid g, const float2* r, const float2* d, float2* z, float omega, const FcgScalars* sc) {
+    if (sc->done) return;
+    const int n = g.nx * g.ny;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        const int k = (c / g.nx) * g.pitch + c % g.nx;
+        const float2 rr = r[k], dd = d[k];
+        z[k] = make_float2(omega * rr.x / dd.x, omega * rr.y / dd.y);
+    }
+}
+
+// the network input: (r - t) / diag, written as 2 planes
+__global__ void lpc_input_kernel(DevGrid g, const float2* r, const float2* t, const float2* d, float* x, int Hp, int Wp,
+                                 const FcgScalars* sc) {
+    if (sc->done) return;
+    const size_t plane = (size_t)Hp * Wp;
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < plane; q += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(q % Wp), j = (int)(q / Wp);
+        float vx = 0.f, vy = 0.f;
+        if (i < g.nx && j < g.ny) {
+            const int k = j * g.pitch + i;
+            const float2 rr = r[k], tt = t[k], dd = d[k];
+            vx = (rr.x - tt.x) / dd.x;
+            vy = (rr.y - tt.y) / dd.y;
+        }
+        x[q] = vx;
+        x[plane + q] = vy;
+    }
+}
+
+// z2 = z1 + mask * y (network output planes)
+__global__ void lpc_correct_kernel(DevGrid g, const float2* z1, const float* y, const float* heff, float2* z2, int Hp,
+                                   int Wp, const FcgScalars* sc) {
+    if (sc->done) return;
+    const size_t plane = (size_t)Hp * Wp;
+    const int n = g.nx * g.ny;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        const int i = c % g.nx, j = c / g.nx;
+        const int k = j * g.pitch + i;
+        const float m = heff[k] >= H_DISP_MIN ? 1.f : 0.f;
+        const size_t q = (size_t)j * Wp + i;
+        const float2 a = z1[k];
+        z2[k] = make_float2(a.x + m * y[q], a.y + m * y[plane + q]);
+    }
+}
+
+// z = z2 + omega (r - t) / diag
+__global__ void lpc_post_kernel(DevGrid g, const float2* z2, const float2* r, const float2* t, const float2* d, float2* z,
+                                float omega, const FcgScalars* sc) {
+    if (sc->done) return;
+    const int n = g.nx * g.ny;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        const int k = (c / g.nx) * g.pitch + c % g.nx;
+        const float2 a = z2[k], rr = r[k], tt = t[k], dd = d[k];
+        z[k] = make_float2(a.x + omega * (rr.x - tt.x) / dd.x, a.y + omega * (rr.y - tt.y) / dd.y);
+    }
+}
+
+// the features (h / H0, b / H0) as 2 planes
+__global__ void lpc_features_kernel(DevGrid g, const float* heff, const float* bed, float* f, int Hp, int Wp) {
+    const size_t plane = (size_t)Hp * Wp;
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < plane; q += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(q % Wp), j = (int)(q / Wp);
+        float a = 0.f, b = 0.f;
+        if (i < g.nx && j < g.ny) {
+            const int k = j * g.pitch + i;
+            a = heff[k] / 20.0f;
+            b = bed[k] / 20.0f;
+        }
+        f[q] = a;
+        f[plane + q] = b;
+    }
+}
+
+}  // namespace wcb

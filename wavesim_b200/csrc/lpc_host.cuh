@@ -1,0 +1,520 @@
+// lpc_host.cuh — host side of the learned preconditioner: the network (forward, backward, Adam)
+// over the kernels of lpc.cuh, and its training loop on SGN systems harvested from solves.
+//
+// No counterpart in the reference. The parameter layout is the one of wavesim_b200/lpc.py
+// (UNetSpec.layers): encoder convolutions, decoder convolutions, the 1x1 output, then per level
+// the gate network's 3x3 (with bias) and 1x1 (with bias) convolutions.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "lpc.cuh"
+
+namespace wcb {
+
+constexpr int LPC_LEVELS = 4;
+constexpr float LPC_H0 = 20.0f;
+// Damping of the cycle's Jacobi sweeps. The Jacobi-scaled operator's spectrum lies in (0, 4) for
+// square cells (Gershgorin: the width-2 x-x couplings and the x-y cross couplings add up to at
+// most 3 diagonals), so with w = 0.5 the zero network's cycle 2wD^-1 - w^2 D^-1 A D^-1 stays
+// positive definite; w = 0.8 is not (eigenvalues near 3 occur on real beds).
+constexpr float LPC_OMEGA = 0.5f;
+
+struct LpcLayer {
+    int w, b, co, ci, k;  // offsets into the parameter vector (b = -1: no bias)
+};
+
+inline dim3 ew_grid(size_t n) {
+    size_t b = (n + 255) / 256;
+    if (b > 148 * 32) b = 148 * 32;
+    if (b < 1) b = 1;
+    return dim3((unsigned)b);
+}
+
+// Device buffer that frees itself.
+struct DBuf {
+    float* p = nullptr;
+    size_t n = 0;
+    DBuf() = default;
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    cudaError_t alloc(size_t count) {
+        if (p) cudaFree(p);
+        n = count;
+        cudaError_t e = cudaMalloc(&p, (count ? count : 1) * sizeof(float));
+        if (e == cudaSuccess) e = cudaMemset(p, 0, (count ? count : 1) * sizeof(float));
+        return e;
+    }
+    ~DBuf() {
+        if (p) cudaFree(p);
+    }
+};
+
+struct LpcNet {
+    int ch[LPC_LEVELS] = {8, 16, 32, 32};
+    int hidden = 8;
+    int nparams = 0;
+    std::vector<LpcLayer> enc_a, enc_b, dec_a, dec_b, gate_a, gate_b;
+    LpcLayer out{};
+    const float* wq = nullptr;  // the weights the forward pass uses (owned by the model)
+    float* gw = nullptr;        // where backward accumulates the weight gradient
+
+    // activations for one batch shape
+    int N = 0, H = 0, W = 0;
+    DBuf F[LPC_LEVELS], HID[LPC_LEVELS], G[LPC_LEVELS];    // features, gate hidden, gates
+    DBuf X[LPC_LEVELS], A[LPC_LEVELS], U[LPC_LEVELS], E[LPC_LEVELS];  // encoder
+    DBuf UP[LPC_LEVELS], DA[LPC_LEVELS], DU[LPC_LEVELS], D[LPC_LEVELS];  // decoder
+    DBuf Y;
+    // gradients
+    DBuf dE[LPC_LEVELS], dD[LPC_LEVELS], dG[LPC_LEVELS], t0, t1, t2, wt;
+
+    void layout(const int* channels, int hid) {
+        for (int l = 0; l < LPC_LEVELS; l++) ch[l] = channels[l];
+        hidden = hid;
+        int off = 0;
+        auto add = [&](int co, int ci, int k, bool bias) {
+            LpcLayer L{off, -1, co, ci, k};
+            off += co * ci * k * k;
+            if (bias) {
+                L.b = off;
+                off += co;
+            }
+            return L;
+        };
+        enc_a.clear(); enc_b.clear(); dec_a.clear(); dec_b.clear(); gate_a.clear(); gate_b.clear();
+        int cin = 2;
+        for (int l = 0; l < LPC_LEVELS; l++) {
+            enc_a.push_back(add(ch[l], cin, 3, false));
+            enc_b.push_back(add(ch[l], ch[l], 3, false));
+            cin = ch[l];
+        }
+        dec_a.resize(LPC_LEVELS);
+        dec_b.resize(LPC_LEVELS);
+        for (int l = LPC_LEVELS - 2; l >= 0; l--) {
+            dec_a[l] = add(ch[l], ch[l + 1] + ch[l], 3, false);
+            dec_b[l] = add(ch[l], ch[l], 3, false);
+        }
+        out = add(2, ch[0], 1, false);
+        for (int l = 0; l < LPC_LEVELS; l++) {
+            gate_a.push_back(add(hidden, 2, 3, true));
+            gate_b.push_back(add(ch[l], hidden, 1, true));
+        }
+        nparams = off;
+    }
+
+    size_t max_weights() const {
+        size_t maxw = 0;
+        for (auto* L : {&enc_a, &enc_b, &dec_a, &dec_b, &gate_a, &gate_b})
+            for (auto& l : *L) maxw = std::max(maxw, (size_t)l.co * l.ci * l.k * l.k);
+        return maxw;
+    }
+
+    int h_of(int l) const { return H >> l; }
+    int w_of(int l) const { return W >> l; }
+    size_t sz(int l, int c) const { return (size_t)N * c * h_of(l) * w_of(l); }
+
+    // Activations for batch N of H x W (H, W divisible by 2^(levels-1)); `training` keeps the
+    // buffers the backward pass needs.
+    cudaError_t shape(int n, int h, int wd, bool training) {
+        N = n;
+        H = h;
+        W = wd;
+        cudaError_t e = cudaSuccess;
+        auto A_ = [&](DBuf& b, size_t c) {
+            if (e == cudaSuccess && b.n != c) e = b.alloc(c);
+        };
+        for (int l = 0; l < LPC_LEVELS; l++) {
+            A_(F[l], sz(l, 2));
+            A_(HID[l], sz(l, hidden));
+            A_(G[l], sz(l, ch[l]));
+            if (l == 0 || training) A_(X[l], sz(l, l == 0 ? 2 : ch[l - 1]));
+            A_(A[l], sz(l, ch[l]));
+            if (training) A_(U[l], sz(l, ch[l]));
+            A_(E[l], sz(l, ch[l]));
+            if (l < LPC_LEVELS - 1) {
+                if (training) A_(UP[l], sz(l, ch[l + 1]));
+                A_(DA[l], sz(l, ch[l]));
+                if (training) A_(DU[l], sz(l, ch[l]));
+                A_(D[l], sz(l, ch[l]));
+            }
+            if (training) {
+                A_(dE[l], sz(l, ch[l]));
+                A_(dD[l], sz(l, ch[l]));
+                A_(dG[l], sz(l, ch[l]));
+            }
+        }
+        A_(Y, sz(0, 2));
+        if (training) {
+            size_t big = 0;
+            for (int l = 0; l < LPC_LEVELS; l++) big = std::max(big, sz(l, ch[l] + (l + 1 < LPC_LEVELS ? ch[l + 1] : 0) + hidden + 2));
+            A_(t0, big);
+            A_(t1, big);
+            A_(t2, big);
+            A_(wt, max_weights());
+        }
+        return e;
+    }
+
+    cudaError_t conv(const float* a, int ca, int amode, const float* b, int cb, const LpcLayer& L, const float* weights,
+                     const float* gate, float* y, int level, int act, cudaStream_t st) const {
+        ConvArgs p{};
+        p.a = a;
+        p.ca = ca;
+        p.amode = amode;
+        p.b = b;
+        p.cb = cb;
+        p.w = weights + L.w;
+        p.bias = L.b >= 0 ? weights + L.b : nullptr;
+        p.gate = gate;
+        p.y = y;
+        p.co = L.co;
+        p.H = h_of(level);
+        p.W = w_of(level);
+        p.N = N;
+        p.act = act;
+        dim3 grid((p.W + CV_T - 1) / CV_T, (p.H + CV_T - 1) / CV_T, N * ((L.co + CV_COB - 1) / CV_COB));
+        if (L.k == 3) conv_fwd_kernel<3><<<grid, CV_T * CV_T, 0, st>>>(p);
+        else conv_fwd_kernel<1><<<grid, CV_T * CV_T, 0, st>>>(p);
+        return cudaGetLastError();
+    }
+
+    // Gates of every level from the features F[0] (h / H0, b / H0): constant within a solve.
+    cudaError_t gates(cudaStream_t st) {
+        cudaError_t e = cudaSuccess;
+        for (int l = 0; l < LPC_LEVELS && e == cudaSuccess; l++) {
+            if (l > 0) pool2_kernel<<<ew_grid(sz(l, 2)), 256, 0, st>>>(F[l - 1].p, N * 2, h_of(l - 1), w_of(l - 1), F[l].p, 0.25f, 0);
+            e = conv(F[l].p, 2, CM_DIRECT, nullptr, 0, gate_a[l], wq, nullptr, HID[l].p, l, ACT_RELU, st);
+            if (e == cudaSuccess) e = conv(HID[l].p, hidden, CM_DIRECT, nullptr, 0, gate_b[l], wq, nullptr, G[l].p, l, ACT_SIG2, st);
+        }
+        return e;
+    }
+
+    // Y = N(X[0]) with the gates already in G. `keep`: materialise what backward needs
+    // (pooled inputs, upsampled skips, pre-gate maps); otherwise pooling and upsampling are read
+    // on the fly by the convolutions and the gate is applied in their epilogue.
+    cudaError_t forward(cudaStream_t st, bool keep) {
+        cudaError_t e = cudaSuccess;
+        for (int l = 0; l < LPC_LEVELS && e == cudaSuccess; l++) {
+            const int cin = l == 0 ? 2 : ch[l - 1];
+            const float* in = l == 0 ? X[0].p : E[l - 1].p;
+            int mode = l == 0 ? CM_DIRECT : CM_POOL;
+            if (keep && l > 0) {
+                pool2_kernel<<<ew_grid(sz(l, cin)), 256, 0, st>>>(E[l - 1].p, N * cin, h_of(l - 1), w_of(l - 1), X[l].p, 0.25f, 0);
+                in = X[l].p;
+                mode = CM_DIRECT;
+            }
+            e = conv(in, cin, mode, nullptr, 0, enc_a[l], wq, nullptr, A[l].p, l, ACT_NONE, st);
+            if (e != cudaSuccess) break;
+            if (keep) {
+                e = conv(A[l].p, ch[l], CM_DIRECT, nullptr, 0, enc_b[l], wq, nullptr, U[l].p, l, ACT_NONE, st);
+                if (e == cudaSuccess) e = product(E[l].p, U[l].p, G[l].p, sz(l, ch[l]), st);  // E = U * G
+            } else {
+                e = conv(A[l].p, ch[l], CM_DIRECT, nullptr, 0, enc_b[l], wq, G[l].p, E[l].p, l, ACT_NONE, st);
+            }
+        }
+        for (int l = LPC_LEVELS - 2; l >= 0 && e == cudaSuccess; l--) {
+            const float* below = (l == LPC_LEVELS - 2) ? E[l + 1].p : D[l + 1].p;
+            const float* a_in = below;
+            int mode = CM_UP;
+            if (keep) {
+                up2_kernel<<<ew_grid(sz(l, ch[l + 1])), 256, 0, st>>>(below, N * ch[l + 1], h_of(l + 1), w_of(l + 1), UP[l].p, 1.f, 0);
+                a_in = UP[l].p;
+                mode = CM_DIRECT;
+            }
+            e = conv(a_in, ch[l + 1], mode, E[l].p, ch[l], dec_a[l], wq, nullptr, DA[l].p, l, ACT_NONE, st);
+            if (e != cudaSuccess) break;
+            if (keep) {
+                e = conv(DA[l].p, ch[l], CM_DIRECT, nullptr, 0, dec_b[l], wq, nullptr, DU[l].p, l, ACT_NONE, st);
+                if (e == cudaSuccess) e = product(D[l].p, DU[l].p, G[l].p, sz(l, ch[l]), st);  // D = DU * G
+            } else {
+                e = conv(DA[l].p, ch[l], CM_DIRECT, nullptr, 0, dec_b[l], wq, G[l].p, D[l].p, l, ACT_NONE, st);
+            }
+        }
+        if (e == cudaSuccess) e = conv(D[0].p, ch[0], CM_DIRECT, nullptr, 0, out, wq, nullptr, Y.p, 0, ACT_NONE, st);
+        return e;
+    }
+
+    static cudaError_t product(float* y, const float* u, const float* g, size_t n, cudaStream_t st);
+    static cudaError_t accumulate(float* y, const float* x, size_t n, cudaStream_t st);
+
+    // dx = input gradient of the convolution L (weights transposed into wt), dW accumulated.
+    cudaError_t conv_bwd(const float* dy, const float* xa, int ca, const float* xb, int cb, const LpcLayer& L,
+                         float* dx, int level, cudaStream_t st) {
+        const int ci = ca + cb;
+        if (dx) {
+            transpose_weights_kernel<<<ew_grid((size_t)L.co * ci * L.k * L.k), 256, 0, st>>>(wq + L.w, L.co, ci, L.k, wt.p);
+            LpcLayer T{0, -1, ci, L.co, L.k};
+            cudaError_t e = conv(dy, L.co, CM_DIRECT, nullptr, 0, T, wt.p, nullptr, dx, level, ACT_NONE, st);
+            if (e != cudaSuccess) return e;
+        }
+        if (L.k == 3)
+            conv_wgrad_kernel<3><<<L.co * ci, 256, 0, st>>>(dy, xa, ca, xb, cb, L.co, h_of(level), w_of(level), N, gw + L.w);
+        else
+            conv_wgrad_kernel<1><<<L.co * ci, 256, 0, st>>>(dy, xa, ca, xb, cb, L.co, h_of(level), w_of(level), N, gw + L.w);
+        if (L.b >= 0) bias_grad_kernel<<<L.co, 256, 0, st>>>(dy, L.co, h_of(level), w_of(level), N, gw + L.b);
+        return cudaGetLastError();
+    }
+
+    // Gradients of sum(dY * Y) into g (which the caller zeroes) and, if dX0 is given, into X[0].
+    cudaError_t backward(const float* dY, float* dX0, cudaStream_t st) {
+        cudaError_t e;
+        for (int l = 0; l < LPC_LEVELS; l++) {
+            cudaMemsetAsync(dE[l].p, 0, dE[l].n * sizeof(float), st);
+            cudaMemsetAsync(dG[l].p, 0, dG[l].n * sizeof(float), st);
+        }
+        if ((e = conv_bwd(dY, D[0].p, ch[0], nullptr, 0, out, dD[0].p, 0, st)) != cudaSuccess) return e;
+        for (int l = 0; l < LPC_LEVELS - 1; l++) {
+            const size_t n = sz(l, ch[l]);
+            gate_bwd_kernel<<<ew_grid(n), 256, 0, st>>>(dD[l].p, DU[l].p, G[l].p, t0.p, dG[l].p, n);  // t0 = dDU
+            if ((e = conv_bwd(t0.p, DA[l].p, ch[l], nullptr, 0, dec_b[l], t1.p, l, st)) != cudaSuccess) return e;  // t1 = dDA
+            if ((e = conv_bwd(t1.p, UP[l].p, ch[l + 1], E[l].p, ch[l], dec_a[l], t2.p, l, st)) != cudaSuccess) return e;  // t2 = dcat
+            // dE[l] += dcat[:, C_{l+1}:]; dD[l+1] = up_bwd(dcat[:, :C_{l+1}])
+            const size_t plane = (size_t)h_of(l) * w_of(l);
+            for (int n_ = 0; n_ < N; n_++) {
+                const float* src = t2.p + ((size_t)n_ * (ch[l + 1] + ch[l]) + ch[l + 1]) * plane;
+                float* dst = dE[l].p + (size_t)n_ * ch[l] * plane;
+                if ((e = accumulate(dst, src, (size_t)ch[l] * plane, st)) != cudaSuccess) return e;
+                float* dbelow = (l + 1 == LPC_LEVELS - 1) ? dE[l + 1].p : dD[l + 1].p;
+                pool2_kernel<<<ew_grid((size_t)ch[l + 1] * plane / 4), 256, 0, st>>>(
+                    t2.p + (size_t)n_ * (ch[l + 1] + ch[l]) * plane, ch[l + 1], h_of(l), w_of(l),
+                    dbelow + (size_t)n_ * ch[l + 1] * plane / 4, 1.f, (l + 1 == LPC_LEVELS - 1) ? 1 : 0);
+            }
+        }
+        for (int l = LPC_LEVELS - 1; l >= 0; l--) {
+            const size_t n = sz(l, ch[l]);
+            gate_bwd_kernel<<<ew_grid(n), 256, 0, st>>>(dE[l].p, U[l].p, G[l].p, t0.p, dG[l].p, n);  // t0 = dU
+            if ((e = conv_bwd(t0.p, A[l].p, ch[l], nullptr, 0, enc_b[l], t1.p, l, st)) != cudaSuccess) return e;  // t1 = dA
+            const int cin = l == 0 ? 2 : ch[l - 1];
+            float* dx = (l == 0) ? dX0 : t2.p;
+            if ((e = conv_bwd(t1.p, X[l].p, cin, nullptr, 0, enc_a[l], dx, l, st)) != cudaSuccess) return e;
+            if (l > 0)  // dE[l-1] += pool_bwd(dX[l]) = up(dX[l]) / 4
+                up2_kernel<<<ew_grid(sz(l - 1, cin)), 256, 0, st>>>(t2.p, N * cin, h_of(l), w_of(l), dE[l - 1].p, 0.25f, 1);
+        }
+        for (int l = 0; l < LPC_LEVELS; l++) {
+            const size_t n = sz(l, ch[l]);
+            sig2_relu_bwd_kernel<<<ew_grid(n), 256, 0, st>>>(dG[l].p, G[l].p, n, ACT_SIG2);  // dG -> dZ
+            if ((e = conv_bwd(dG[l].p, HID[l].p, hidden, nullptr, 0, gate_b[l], t1.p, l, st)) != cudaSuccess) return e;
+            const size_t nh = sz(l, hidden);
+            sig2_relu_bwd_kernel<<<ew_grid(nh), 256, 0, st>>>(t1.p, HID[l].p, nh, ACT_RELU);
+            if ((e = conv_bwd(t1.p, F[l].p, 2, nullptr, 0, gate_a[l], nullptr, l, st)) != cudaSuccess) return e;
+        }
+        return cudaGetLastError();
+    }
+};
+
+__global__ void product_kernel(float* __restrict__ y, const float* __restrict__ u, const float* __restrict__ g, size_t n) {
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x)
+        y[q] = u[q] * g[q];
+}
+
+__global__ void accumulate_kernel(float* __restrict__ y, const float* __restrict__ x, size_t n) {
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) y[q] += x[q];
+}
+
+inline cudaError_t LpcNet::product(float* y, const float* u, const float* g, size_t n, cudaStream_t st) {
+    product_kernel<<<ew_grid(n), 256, 0, st>>>(y, u, g, n);
+    return cudaGetLastError();
+}
+
+inline cudaError_t LpcNet::accumulate(float* y, const float* x, size_t n, cudaStream_t st) {
+    accumulate_kernel<<<ew_grid(n), 256, 0, st>>>(y, x, n);
+    return cudaGetLastError();
+}
+
+// ---- training --------------------------------------------------------------------------
+
+// A patch of a harvested system: c, heff and the bed cropped into the batch tensors, the mask
+// (h >= 5 cm) and the features (h / H0, b / H0).
+__global__ void crop_kernel(const float* __restrict__ c, const float* __restrict__ heff, const float* __restrict__ bed,
+                            int pitch, int x0, int y0, int H, int W, float* __restrict__ oc, float* __restrict__ oheff,
+                            float* __restrict__ omask, float* __restrict__ ofeat) {
+    const int plane = H * W;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < plane; q += gridDim.x * blockDim.x) {
+        const int y = q / W, x = q % W;
+        const size_t k = (size_t)(y0 + y) * pitch + (x0 + x);
+        const float he = heff[k];
+        oc[q] = c[k];
+        oheff[q] = he;
+        omask[q] = he >= H_DISP_MIN ? 1.f : 0.f;
+        ofeat[q] = he / LPC_H0;
+        ofeat[plane + q] = bed[k] / LPC_H0;
+    }
+}
+
+struct LpcSystem {
+    int nx, ny, pitch;
+    float dx, dy;
+    DBuf c, heff, bed;
+};
+
+struct LpcTrainer {
+    int N = 0, H = 0, W = 0;
+    float dx = 1.f, dy = 1.f;
+    DBuf c, heff, mask, e, r, dg, z1, tmp, zj, z2, z, dd, ad, ae, gz, gz2;
+    double* sums = nullptr;  // [2][N]: <d, A d>, <e, A e>
+    ~LpcTrainer() {
+        if (sums) cudaFree(sums);
+    }
+    cudaError_t shape(int n, int h, int w) {
+        N = n;
+        H = h;
+        W = w;
+        const size_t one = (size_t)n * h * w, two = 2 * one;
+        cudaError_t er = cudaSuccess;
+        for (DBuf* b : {&c, &heff, &mask}) if (er == cudaSuccess && b->n != one) er = b->alloc(one);
+        for (DBuf* b : {&e, &r, &dg, &z1, &tmp, &zj, &z2, &z, &dd, &ad, &ae, &gz, &gz2})
+            if (er == cudaSuccess && b->n != two) er = b->alloc(two);
+        if (er == cudaSuccess) {
+            if (sums) cudaFree(sums);
+            er = cudaMalloc(&sums, 2 * n * sizeof(double));
+        }
+        return er;
+    }
+    PatchOp op() const {
+        PatchOp o;
+        o.c = c.p;
+        o.heff = heff.p;
+        o.mask = mask.p;
+        o.H = H;
+        o.W = W;
+        o.N = N;
+        o.ix = 0.5f / dx;
+        o.iy = 0.5f / dy;
+        o.dx2i = 0.25f / (dx * dx);
+        o.dy2i = 0.25f / (dy * dy);
+        return o;
+    }
+};
+
+// out = ax * x + ay * y / d * mask over 2-plane fields of N samples (any of y's modifiers null).
+inline void fld(float* out, const float* x, float ax, const float* y, float ay, const float* d, const float* mask, int N,
+                size_t plane, cudaStream_t st) {
+    const size_t n = (size_t)N * 2 * plane;
+    lincomb_kernel<<<ew_grid(n), 256, 0, st>>>(out, x, ax, y, ay, d, mask, 2, n, plane);
+}
+
+
+// loss[step] = mean over samples of <d, A d> / <e, A e>
+__global__ void lpc_loss_kernel(const double* __restrict__ sums, int N, double* __restrict__ out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double l = 0.0;
+    for (int n = 0; n < N; n++) l += sums[n] / fmax(sums[N + n], 1e-300);
+    *out = l / N;
+}
+
+// The trained network and what training needs: parameters with Adam moments, harvested systems,
+// the batch buffers.
+struct LpcModel {
+    LpcNet net;      // layout; activations of the training batch
+    DBuf w, wq, g, m, v;
+    int adam_t = 0;
+    int round_bf16 = 1;
+    std::vector<LpcSystem*> systems;
+    LpcTrainer tr;
+    double* dloss = nullptr;  // the loss of every step of a training call
+    size_t dloss_n = 0;
+    unsigned long long rng = 0x9e3779b97f4a7c15ull;
+    cudaStream_t st = nullptr;
+
+    ~LpcModel() {
+        for (auto* q : systems) delete q;
+        if (dloss) cudaFree(dloss);
+        if (st) cudaStreamDestroy(st);
+    }
+
+    cudaError_t init(const int* channels, int hidden) {
+        net.layout(channels, hidden);
+        cudaError_t e;
+        for (DBuf* b : {&w, &wq, &g, &m, &v})
+            if ((e = b->alloc(net.nparams)) != cudaSuccess) return e;
+        net.wq = wq.p;
+        net.gw = g.p;
+        return cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    }
+
+    // The forward copy from the master weights (BF16-rounded unless rounding is off).
+    cudaError_t refresh() {
+        round_copy_kernel<<<ew_grid(net.nparams), 256, 0, st>>>(w.p, wq.p, net.nparams, round_bf16);
+        return cudaGetLastError();
+    }
+
+    unsigned long long next() {
+        rng ^= rng << 13;
+        rng ^= rng >> 7;
+        rng ^= rng << 17;
+        return rng;
+    }
+
+    // One step of training: N patches of H x W from random systems and offsets, one random error
+    // field each, the loss mean_n <d, A d>_n / <e, A e>_n of the cycle's error d = e - M A e, its
+    // gradient through the cycle and the network, an Adam update.
+    cudaError_t train_step(int N, int H, int W, float lr, double* loss_slot, float rough) {
+        cudaError_t e;
+        if (tr.N != N || tr.H != H || tr.W != W)
+            if ((e = tr.shape(N, H, W)) != cudaSuccess) return e;
+        if ((e = net.shape(N, H, W, true)) != cudaSuccess) return e;
+        const size_t plane = (size_t)H * W, per = 2 * plane;
+        // one grid spacing per batch: the systems of a random one's spacing
+        const LpcSystem* s0 = systems[next() % systems.size()];
+        std::vector<const LpcSystem*> pool;
+        for (auto* q : systems)
+            if (q->dx == s0->dx && q->dy == s0->dy && q->nx >= W && q->ny >= H) pool.push_back(q);
+        if (pool.empty()) return cudaErrorInvalidValue;
+        for (int n = 0; n < N; n++) {
+            const LpcSystem* sy = pool[next() % pool.size()];
+            const int x0 = (int)(next() % (unsigned long long)(sy->nx - W + 1));
+            const int y0 = (int)(next() % (unsigned long long)(sy->ny - H + 1));
+            crop_kernel<<<ew_grid(plane), 256, 0, st>>>(sy->c.p, sy->heff.p, sy->bed.p, sy->pitch, x0, y0, H, W,
+                                                        tr.c.p + n * plane, tr.heff.p + n * plane,
+                                                        tr.mask.p + n * plane, net.F[0].p + n * per);
+        }
+        tr.dx = s0->dx;
+        tr.dy = s0->dy;
+        const PatchOp op = tr.op();
+        const size_t tot = (size_t)N * per;
+        const float om = LPC_OMEGA;
+        random_field_kernel<<<ew_grid(tot), 256, 0, st>>>(tr.e.p, tr.mask.p, N, H, W, next(), rough);
+        patch_matvec_kernel<<<ew_grid(N * plane), 256, 0, st>>>(op, tr.e.p, tr.r.p);   // r = A e
+        patch_diag_kernel<<<ew_grid(N * plane), 256, 0, st>>>(op, tr.dg.p);
+        fld(tr.z1.p, nullptr, 0.f, tr.r.p, om, tr.dg.p, nullptr, N, plane, st);       // z1 = w r / D
+        patch_matvec_kernel<<<ew_grid(N * plane), 256, 0, st>>>(op, tr.z1.p, tr.tmp.p);
+        fld(tr.zj.p, tr.r.p, 1.f, tr.tmp.p, -1.f, nullptr, nullptr, N, plane, st);      // r - A z1
+        fld(net.X[0].p, nullptr, 0.f, tr.zj.p, 1.f, tr.dg.p, nullptr, N, plane, st);     // / D
+        if ((e = net.gates(st)) != cudaSuccess) return e;
+        if ((e = net.forward(st, true)) != cudaSuccess) return e;
+        fld(tr.z2.p, tr.z1.p, 1.f, net.Y.p, 1.f, nullptr, tr.mask.p, N, plane, st);     // z2 = z1 + m Y
+        patch_matvec_kernel<<<ew_grid(N * plane), 256, 0, st>>>(op, tr.z2.p, tr.tmp.p);
+        fld(tr.dd.p, tr.r.p, 1.f, tr.tmp.p, -1.f, nullptr, nullptr, N, plane, st);      // r - A z2
+        fld(tr.z.p, tr.z2.p, 1.f, tr.dd.p, om, tr.dg.p, nullptr, N, plane, st);         // z
+        fld(tr.dd.p, tr.e.p, 1.f, tr.z.p, -1.f, nullptr, nullptr, N, plane, st);        // d = e - z
+        patch_matvec_kernel<<<ew_grid(N * plane), 256, 0, st>>>(op, tr.dd.p, tr.ad.p);  // A d
+        cudaMemsetAsync(tr.sums, 0, 2 * N * sizeof(double), st);
+        const dim3 dg((unsigned)std::min<size_t>((per + 255) / 256, 64), (unsigned)N);
+        sample_dot_kernel<<<dg, 256, 0, st>>>(tr.dd.p, tr.ad.p, per, tr.sums);
+        sample_dot_kernel<<<dg, 256, 0, st>>>(tr.e.p, tr.r.p, per, tr.sums + N);
+        lpc_loss_kernel<<<1, 32, 0, st>>>(tr.sums, N, loss_slot);
+        if (lr <= 0.f) return cudaGetLastError();
+        // dL/dz = -2 A d / (N E_n); through z = z2 + w (r - A z2) / D: dz2 = dz - w A (dz / D);
+        // through z2 = z1 + m Y: dY = m dz2.
+        loss_grad_kernel<<<ew_grid(tot), 256, 0, st>>>(tr.ad.p, tr.sums + N, N, per, tr.gz.p);
+        fld(tr.tmp.p, nullptr, 0.f, tr.gz.p, 1.f, tr.dg.p, nullptr, N, plane, st);
+        patch_matvec_kernel<<<ew_grid(N * plane), 256, 0, st>>>(op, tr.tmp.p, tr.zj.p);
+        fld(tr.gz2.p, tr.gz.p, 1.f, tr.zj.p, -om, nullptr, nullptr, N, plane, st);
+        fld(tr.gz2.p, nullptr, 0.f, tr.gz2.p, 1.f, nullptr, tr.mask.p, N, plane, st);
+        cudaMemsetAsync(g.p, 0, g.n * sizeof(float), st);
+        if ((e = net.backward(tr.gz2.p, nullptr, st)) != cudaSuccess) return e;
+        adam_t += 1;
+        const float b1 = 0.9f, b2 = 0.999f;
+        const float c1 = (float)(1.0 / (1.0 - pow((double)b1, adam_t)));
+        const float c2 = (float)(1.0 / (1.0 - pow((double)b2, adam_t)));
+        adam_kernel<<<ew_grid(net.nparams), 256, 0, st>>>(w.p, wq.p, g.p, m.p, v.p, net.nparams, lr, b1, b2, c1, c2,
+                                                          1e-8f, round_bf16);
+        return cudaGetLastError();
+    }
+};
+
+}  // namespace wcb

@@ -49,6 +49,7 @@ struct PcgArgs {
     float4* qout;
     const float* bed;
     Ctl* ctl;
+    const FcgScalars* fcg;  // non-null: the solve ran in the learned path's kernels; finish only
     double tol;
     long long max_iter;
     int mode;         // StageMode
@@ -59,14 +60,17 @@ struct PcgArgs {
 
 // Grid-wide sum of up to three values that is also a barrier. Each CTA publishes its partials
 // and arrives; the last to arrive releases; every CTA then adds all partials in CTA order with
-// the same reduction tree, so all CTAs hold identical totals. Returns false if the wait timed out.
+// the same reduction tree, so all CTAs hold identical totals. Partials alternate between two
+// banks by epoch parity: a CTA that has left barrier e can reach barrier e+1 while a slower CTA
+// still reads the partials of e, but it cannot reach e+2 before every CTA has arrived at e+1,
+// i.e. finished reading e. Returns false if the wait timed out.
 __device__ bool reduce_barrier(const PcgArgs& a, unsigned& epoch, double v0, double v1, double v2,
                                double* out, double* red, int cta, int ncta) {
     __shared__ int s_ok;
     block_sum3<PG_NT>(v0, v1, v2, red);
+    epoch += 1;  // every thread keeps the count: it selects the bank below
     if (threadIdx.x == 0) {
-        epoch += 1;
-        double* pp = a.part + 4 * (size_t)cta;
+        double* pp = a.part + 4 * ((size_t)cta + (epoch & 1u) * (size_t)ncta);
         pp[0] = v0;
         pp[1] = v1;
         pp[2] = v2;
@@ -95,8 +99,9 @@ __device__ bool reduce_barrier(const PcgArgs& a, unsigned& epoch, double v0, dou
     __syncthreads();
     if (!s_ok) return false;
     double x = 0.0, y = 0.0, z = 0.0;
+    const double* bank = a.part + 4 * (size_t)(epoch & 1u) * (size_t)ncta;
     for (int b = threadIdx.x; b < ncta; b += PG_NT) {
-        const double* pp = a.part + 4 * (size_t)b;
+        const double* pp = bank + 4 * (size_t)b;
         x += __ldcg(pp);
         y += __ldcg(pp + 1);
         z += __ldcg(pp + 2);
@@ -238,116 +243,123 @@ __device__ __forceinline__ bool pcg_solve(const PcgArgs& a, int cta, int ncta, u
     if (tid == 0) s_nan = 0;
     BoxPrefetch f;
 
-    // ---- initial residual: r = b - A w (dispersion.rs:493-515) ---------------------------
-    double bb = 0.0, rz_p = 0.0, rr_p = 0.0;
-    if (cta < ntiles) box_prefetch<true>(a, cta, nullptr, true, f);
-    for (int tl = cta; tl < ntiles; tl += ncta) {
-        int i0, j0;
-        tile_origin(a, tl, i0, j0);
-        box_commit<true>(f, t, 0.f, true);
-        const float he = f.he;
-        __syncthreads();
-        if (tl + ncta < ntiles) box_prefetch<true>(a, tl + ncta, nullptr, true, f);
-        const float2 aw = apply_a(g, t, cx, cy, he);
-        const int i = i0 + cx, j = j0 + cy;
-        if (i < g.nx && j < g.ny) {
-            const int k = j * g.pitch + i;
-            const int pc = (cy + 1) * PC_W + (cx + 1);
-            float2 d = make_float2(1.f, 1.f);
-            if (he >= H_DISP_MIN) {
-                d.x = he + (t.scc[pc + 1] + t.scc[pc - 1]) * 0.25f / (g.dx * g.dx);
-                d.y = he + (t.scc[pc + PC_W] + t.scc[pc - PC_W]) * 0.25f / (g.dy * g.dy);
-            }
-            const float2 b = __ldg(a.bv + k);
-            const float2 r = make_float2(b.x - aw.x, b.y - aw.y);
-            a.w[k] = t.sv[(cy + 2) * PB_W + (cx + 2)];  // the warm start, masked
-            a.diag[k] = d;
-            a.r[k] = r;
-            bb += (double)b.x * b.x + (double)b.y * b.y;
-            rz_p += (double)r.x * (r.x / d.x) + (double)r.y * (r.y / d.y);
-            rr_p += (double)r.x * r.x + (double)r.y * r.y;
-        }
-        __syncthreads();
-    }
-    if (!reduce_barrier(a, epoch, bb, rz_p, rr_p, tot, red, cta, ncta)) return false;
-    const double target = a.tol * sqrt(tot[0]) + 1e-10;
-    double rz = tot[1];
-    bool converged = sqrt(tot[2]) <= target;
     long long it = 0;
-    float beta_f = 0.f;
-
-    while (!converged && it < a.max_iter) {
-        const float2* p_old = (it & 1) ? a.p1 : a.p0;
-        float2* p_new = (it & 1) ? a.p0 : a.p1;
-        const bool first = it == 0;
-        // sweep A': p = z + beta p on the tile and its halo, then A p and <p, Ap>
-        double pap = 0.0;
-        if (cta < ntiles) box_prefetch<false>(a, cta, p_old, first, f);
+    bool converged = false;
+    if (a.fcg && a.fcg->converged) {  // solved by the learned flexible CG: finish only
+        converged = true;
+    } else {  // the Jacobi solve; after a learned solve that failed, from where that one stopped
+        // ---- initial residual: r = b - A w (dispersion.rs:493-515) ---------------------------
+        double bb = 0.0, rz_p = 0.0, rr_p = 0.0;
+        if (cta < ntiles) box_prefetch<true>(a, cta, nullptr, true, f);
         for (int tl = cta; tl < ntiles; tl += ncta) {
             int i0, j0;
             tile_origin(a, tl, i0, j0);
-            box_commit<false>(f, t, beta_f, first);
+            box_commit<true>(f, t, 0.f, true);
             const float he = f.he;
             __syncthreads();
-            if (tl + ncta < ntiles) box_prefetch<false>(a, tl + ncta, p_old, first, f);
-            const float2 av = apply_a(g, t, cx, cy, he);
+            if (tl + ncta < ntiles) box_prefetch<true>(a, tl + ncta, nullptr, true, f);
+            const float2 aw = apply_a(g, t, cx, cy, he);
             const int i = i0 + cx, j = j0 + cy;
             if (i < g.nx && j < g.ny) {
                 const int k = j * g.pitch + i;
-                const float2 p = t.sv[(cy + 2) * PB_W + (cx + 2)];
-                p_new[k] = p;
-                a.ap[k] = av;
-                pap += (double)p.x * av.x + (double)p.y * av.y;
+                const int pc = (cy + 1) * PC_W + (cx + 1);
+                float2 d = make_float2(1.f, 1.f);
+                if (he >= H_DISP_MIN) {
+                    d.x = he + (t.scc[pc + 1] + t.scc[pc - 1]) * 0.25f / (g.dx * g.dx);
+                    d.y = he + (t.scc[pc + PC_W] + t.scc[pc - PC_W]) * 0.25f / (g.dy * g.dy);
+                }
+                const float2 b = __ldg(a.bv + k);
+                const float2 r = make_float2(b.x - aw.x, b.y - aw.y);
+                a.w[k] = t.sv[(cy + 2) * PB_W + (cx + 2)];  // the warm start, masked
+                a.diag[k] = d;
+                a.r[k] = r;
+                bb += (double)b.x * b.x + (double)b.y * b.y;
+                rz_p += (double)r.x * (r.x / d.x) + (double)r.y * (r.y / d.y);
+                rr_p += (double)r.x * r.x + (double)r.y * r.y;
             }
             __syncthreads();
         }
-        if (!reduce_barrier(a, epoch, pap, 0.0, 0.0, tot, red, cta, ncta)) return false;
-        const double alpha = rz / tot[0];
-        const float alpha_f = (float)alpha;
-        // sweep B: w += alpha p, r -= alpha Ap, <r, r> and <r, z>
-        double rr = 0.0, rzn = 0.0;
-        CellPrefetch c{};
-        auto cell_load = [&](int tl, CellPrefetch& o) {
-            int i0, j0;
-            tile_origin(a, tl, i0, j0);
-            const int i = i0 + cx, j = j0 + cy;
-            if (i < g.nx && j < g.ny) {
-                const int k = j * g.pitch + i;
-                o.p = __ldcg(p_new + k);
-                o.ap = __ldcg(a.ap + k);
-                o.w = __ldcg(a.w + k);
-                o.r = __ldcg(a.r + k);
-                o.d = __ldcg(a.diag + k);
+        if (!reduce_barrier(a, epoch, bb, rz_p, rr_p, tot, red, cta, ncta)) return false;
+        const double target = a.tol * sqrt(tot[0]) + 1e-10;
+        double rz = tot[1];
+        converged = sqrt(tot[2]) <= target;
+        float beta_f = 0.f;
+
+        while (!converged && it < a.max_iter) {
+            const float2* p_old = (it & 1) ? a.p1 : a.p0;
+            float2* p_new = (it & 1) ? a.p0 : a.p1;
+            const bool first = it == 0;
+            // sweep A': p = z + beta p on the tile and its halo, then A p and <p, Ap>
+            double pap = 0.0;
+            if (cta < ntiles) box_prefetch<false>(a, cta, p_old, first, f);
+            for (int tl = cta; tl < ntiles; tl += ncta) {
+                int i0, j0;
+                tile_origin(a, tl, i0, j0);
+                box_commit<false>(f, t, beta_f, first);
+                const float he = f.he;
+                __syncthreads();
+                if (tl + ncta < ntiles) box_prefetch<false>(a, tl + ncta, p_old, first, f);
+                const float2 av = apply_a(g, t, cx, cy, he);
+                const int i = i0 + cx, j = j0 + cy;
+                if (i < g.nx && j < g.ny) {
+                    const int k = j * g.pitch + i;
+                    const float2 p = t.sv[(cy + 2) * PB_W + (cx + 2)];
+                    p_new[k] = p;
+                    a.ap[k] = av;
+                    pap += (double)p.x * av.x + (double)p.y * av.y;
+                }
+                __syncthreads();
             }
-        };
-        if (cta < ntiles) cell_load(cta, c);
-        for (int tl = cta; tl < ntiles; tl += ncta) {
-            const CellPrefetch cur = c;
-            if (tl + ncta < ntiles) cell_load(tl + ncta, c);
-            int i0, j0;
-            tile_origin(a, tl, i0, j0);
-            const int i = i0 + cx, j = j0 + cy;
-            if (i < g.nx && j < g.ny) {
-                const int k = j * g.pitch + i;
-                float2 w = cur.w, r = cur.r;
-                w.x += alpha_f * cur.p.x;
-                w.y += alpha_f * cur.p.y;
-                r.x -= alpha_f * cur.ap.x;
-                r.y -= alpha_f * cur.ap.y;
-                a.w[k] = w;
-                a.r[k] = r;
-                rr += (double)r.x * r.x + (double)r.y * r.y;
-                rzn += (double)r.x * (r.x / cur.d.x) + (double)r.y * (r.y / cur.d.y);
+            if (!reduce_barrier(a, epoch, pap, 0.0, 0.0, tot, red, cta, ncta)) return false;
+            const double alpha = rz / tot[0];
+            const float alpha_f = (float)alpha;
+            // sweep B: w += alpha p, r -= alpha Ap, <r, r> and <r, z>
+            double rr = 0.0, rzn = 0.0;
+            CellPrefetch c{};
+            auto cell_load = [&](int tl, CellPrefetch& o) {
+                int i0, j0;
+                tile_origin(a, tl, i0, j0);
+                const int i = i0 + cx, j = j0 + cy;
+                if (i < g.nx && j < g.ny) {
+                    const int k = j * g.pitch + i;
+                    o.p = __ldcg(p_new + k);
+                    o.ap = __ldcg(a.ap + k);
+                    o.w = __ldcg(a.w + k);
+                    o.r = __ldcg(a.r + k);
+                    o.d = __ldcg(a.diag + k);
+                }
+            };
+            if (cta < ntiles) cell_load(cta, c);
+            for (int tl = cta; tl < ntiles; tl += ncta) {
+                const CellPrefetch cur = c;
+                if (tl + ncta < ntiles) cell_load(tl + ncta, c);
+                int i0, j0;
+                tile_origin(a, tl, i0, j0);
+                const int i = i0 + cx, j = j0 + cy;
+                if (i < g.nx && j < g.ny) {
+                    const int k = j * g.pitch + i;
+                    float2 w = cur.w, r = cur.r;
+                    w.x += alpha_f * cur.p.x;
+                    w.y += alpha_f * cur.p.y;
+                    r.x -= alpha_f * cur.ap.x;
+                    r.y -= alpha_f * cur.ap.y;
+                    a.w[k] = w;
+                    a.r[k] = r;
+                    rr += (double)r.x * r.x + (double)r.y * r.y;
+                    rzn += (double)r.x * (r.x / cur.d.x) + (double)r.y * (r.y / cur.d.y);
+                }
             }
+            if (!reduce_barrier(a, epoch, rr, rzn, 0.0, tot, red, cta, ncta)) return false;
+            it += 1;
+            converged = sqrt(tot[0]) <= target;
+            const double beta = tot[1] / rz;
+            rz = tot[1];
+            beta_f = (float)beta;
         }
-        if (!reduce_barrier(a, epoch, rr, rzn, 0.0, tot, red, cta, ncta)) return false;
-        it += 1;
-        converged = sqrt(tot[0]) <= target;
-        const double beta = tot[1] / rz;
-        rz = tot[1];
-        beta_f = (float)beta;
     }
+    if (a.fcg) it += a.fcg->iterations;
     if (cta == 0 && tid == 0) {
+        if (a.fcg) ctl->fcg_iterations += (unsigned long long)a.fcg->iterations;
         ctl->solves += 1;
         ctl->iterations += (unsigned long long)it;
         if (!converged) ctl->unconverged += 1;

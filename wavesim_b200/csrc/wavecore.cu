@@ -18,6 +18,7 @@
 #include "aux.cuh"
 #include "common.cuh"
 #include "ensemble.cuh"
+#include "lpc_host.cuh"
 #include "pcg.cuh"
 #include "stage.cuh"
 
@@ -119,16 +120,32 @@ struct wc_solver {
     std::vector<cudaEvent_t> prof_pool;
     // One captured step, replayed by the device-resident stepping (not used while profiling).
     cudaGraphExec_t step_graph = nullptr;
+    unsigned long long graph_launches = 0;  // kernels of one replay (a while-node's body: per iteration)
     bool graph_failed = false;
     // The device clock's stable_dt describes the resident state (set by every step's last kernel,
     // cleared by an upload), so adaptive stepping need not recompute it.
     bool rate_current = false;
+    // The learned preconditioner (WC_PC_LEARNED): the attached network (not owned), its
+    // activations at this grid's size and the flexible CG's extra buffers.
+    int pc = WC_PC_JACOBI;
+    LpcModel* lpc = nullptr;
+    LpcNet lnet;
+    int lpc_hp = 0, lpc_wp = 0;
+    float2* tv = nullptr;
+    FcgScalars* fsc = nullptr;
+    double* fpart = nullptr;
+    int* done_host = nullptr;
+    cudaStream_t body_stream = nullptr;
+    unsigned long long fcg_body_launches = 0;  // kernels per flexible-CG iteration
+    unsigned long long fcg_iter_base = 0;      // flexible-CG iterations before the network was attached
 
     ~wc_solver() {
         void* bufs[] = {q0, q1, bed, prof, ycs, shallow, hn, pred, bv, w, r, p0, p1, ap, diag, cc, heff,
-                        part, bar, ctl, st_h, st_hu, st_hv, r64, diag_bands, diag_done, diag_out};
+                        part, bar, ctl, st_h, st_hu, st_hv, r64, diag_bands, diag_done, diag_out, tv, fsc, fpart};
         for (void* b : bufs)
             if (b) cudaFree(b);
+        if (done_host) cudaFreeHost(done_host);
+        if (body_stream) cudaStreamDestroy(body_stream);
         if (ctl_host) cudaFreeHost(ctl_host);
         for (auto& e : prof_live) {
             cudaEventDestroy(e.a);
@@ -268,8 +285,9 @@ wc_status launch_stage(wc_solver* s, int mode, const float4* qin, const float4* 
     return WC_OK;
 }
 
-PcgArgs pcg_args(const wc_solver* s, int mode, const float4* qold, float4* qout) {
+PcgArgs pcg_args(const wc_solver* s, int mode, const float4* qold, float4* qout, const FcgScalars* fcg = nullptr) {
     PcgArgs a{};
+    a.fcg = fcg;
     a.g = s->g;
     a.cc = s->cc;
     a.heff = s->heff;
@@ -298,8 +316,8 @@ PcgArgs pcg_args(const wc_solver* s, int mode, const float4* qold, float4* qout)
     return a;
 }
 
-wc_status launch_pcg(wc_solver* s, int mode, const float4* qold, float4* qout) {
-    const PcgArgs a = pcg_args(s, mode, qold, qout);
+wc_status launch_pcg(wc_solver* s, int mode, const float4* qold, float4* qout, const FcgScalars* fcg = nullptr) {
+    const PcgArgs a = pcg_args(s, mode, qold, qout, fcg);
     CK(cudaMemsetAsync(s->bar, 0, 2 * sizeof(unsigned), s->stream));
     ProfScope ps(s, 1);
     // A cooperative launch: every CTA is resident at once, so the grid barriers cannot deadlock.
@@ -318,11 +336,150 @@ wc_status launch_pcg(wc_solver* s, int mode, const float4* qold, float4* qout) {
     return WC_OK;
 }
 
+// ---- the learned path: flexible CG with the network preconditioner --------------------------
+//
+// Same system, warm start and stopping rule as the Jacobi solve (dispersion.rs:493-545); the
+// preconditioner is the two-level cycle of the network (lpc.cuh), so directions are
+// A-orthogonalised against the previous one (flexible CG). An iteration is a chain of ordinary
+// kernels; in a captured step the chain is the body of a graph while-node whose condition the
+// residual kernel sets, so the loop runs on the device without the host.
+
+constexpr int FCG_BLOCKS = 148 * 4;
+
+int fcg_blocks(const wc_solver* s) {
+    const size_t n = (size_t)s->grid.nx * s->grid.ny;
+    return (int)std::max<size_t>(1, std::min<size_t>(FCG_BLOCKS, (n + 255) / 256));
+}
+
+#define FCG_LAUNCH(...)                 \
+    do {                                \
+        __VA_ARGS__;                    \
+        s->launches++;                  \
+        CK(cudaGetLastError());         \
+    } while (0)
+
+// dots of up to three pairs, totalled by the scalars kernel at `step`
+wc_status fcg_dots(wc_solver* s, cudaStream_t st, int step, const float2* a0, const float2* b0, const float2* a1,
+                   const float2* b1, cudaGraphConditionalHandle h, int cond) {
+    const int nb = fcg_blocks(s);
+    const FcgScalars* guard = step == FCG_INIT ? nullptr : s->fsc;
+    FCG_LAUNCH(fcg_dot_partial_kernel<<<nb, 256, 0, st>>>(s->g, a0, b0, a1, b1, nullptr, nullptr, s->fpart, guard));
+    FCG_LAUNCH(fcg_scalars_kernel<<<1, 256, 0, st>>>(s->fpart, nb, s->fsc, step, s->disp.tolerance,
+                                                     (long long)s->disp.max_iterations, h, cond));
+    return WC_OK;
+}
+
+// Before the loop: diagonal, warm start, r = b - A w, the norms, the network's gates.
+wc_status fcg_pre(wc_solver* s, cudaStream_t st, cudaGraphConditionalHandle h, int cond) {
+    const int nb = fcg_blocks(s);
+    FCG_LAUNCH(fcg_setup_kernel<<<nb, 256, 0, st>>>(s->g, s->cc, s->heff, s->diag, s->w));
+    FCG_LAUNCH(fcg_matvec_kernel<<<nb, 256, 0, st>>>(s->g, s->w, s->cc, s->heff, s->tv, nullptr));
+    FCG_LAUNCH(fcg_residual_kernel<<<nb, 256, 0, st>>>(s->g, s->bv, s->tv, s->r));
+    TRY(fcg_dots(s, st, FCG_INIT, s->bv, s->bv, s->r, s->r, h, cond));
+    const size_t plane = (size_t)s->lpc_hp * s->lpc_wp;
+    FCG_LAUNCH(lpc_features_kernel<<<ew_grid(plane), 256, 0, st>>>(s->g, s->heff, s->bed, s->lnet.F[0].p, s->lpc_hp,
+                                                                   s->lpc_wp));
+    CK(s->lnet.gates(st));
+    s->launches += 2 * LPC_LEVELS + (LPC_LEVELS - 1);
+    return WC_OK;
+}
+
+// One iteration: z = M r, p = z + beta p, q = A p, alpha, w and r, the residual norm.
+wc_status fcg_body(wc_solver* s, cudaStream_t st, cudaGraphConditionalHandle h, int cond) {
+    const DevGrid& g = s->g;
+    const int nb = fcg_blocks(s);
+    FcgScalars* sc = s->fsc;
+    float2 *z = s->p1, *p = s->p0, *q = s->ap;
+    const int hp = s->lpc_hp, wp = s->lpc_wp;
+    const size_t plane = (size_t)hp * wp;
+    FCG_LAUNCH(lpc_jacobi_kernel<<<nb, 256, 0, st>>>(g, s->r, s->diag, z, LPC_OMEGA, sc));
+    FCG_LAUNCH(fcg_matvec_kernel<<<nb, 256, 0, st>>>(g, z, s->cc, s->heff, s->tv, sc));
+    FCG_LAUNCH(lpc_input_kernel<<<ew_grid(plane), 256, 0, st>>>(g, s->r, s->tv, s->diag, s->lnet.X[0].p, hp, wp, sc));
+    CK(s->lnet.forward(st, false));
+    s->launches += 2 * LPC_LEVELS + 2 * (LPC_LEVELS - 1) + 1;
+    FCG_LAUNCH(lpc_correct_kernel<<<nb, 256, 0, st>>>(g, z, s->lnet.Y.p, s->heff, z, hp, wp, sc));
+    FCG_LAUNCH(fcg_matvec_kernel<<<nb, 256, 0, st>>>(g, z, s->cc, s->heff, s->tv, sc));
+    FCG_LAUNCH(lpc_post_kernel<<<nb, 256, 0, st>>>(g, z, s->r, s->tv, s->diag, z, LPC_OMEGA, sc));
+    TRY(fcg_dots(s, st, FCG_BETA, z, q, nullptr, nullptr, h, 0));
+    FCG_LAUNCH(fcg_direction_kernel<<<nb, 256, 0, st>>>(g, p, z, sc));
+    FCG_LAUNCH(fcg_matvec_kernel<<<nb, 256, 0, st>>>(g, p, s->cc, s->heff, q, sc));
+    TRY(fcg_dots(s, st, FCG_ALPHA, p, q, s->r, p, h, 0));
+    FCG_LAUNCH(fcg_update_kernel<<<nb, 256, 0, st>>>(g, s->w, s->r, p, q, sc));
+    TRY(fcg_dots(s, st, FCG_RESID, s->r, s->r, nullptr, nullptr, h, cond));
+    return WC_OK;
+}
+
+wc_status launch_fcg(wc_solver* s, int mode, const float4* qold, float4* qout) {
+    cudaStream_t st = s->stream;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(st, &cs));
+    const bool graph = cs == cudaStreamCaptureStatusActive;
+    cudaGraphConditionalHandle h = 0;
+    if (graph) {
+        cudaGraph_t cg = nullptr;
+        CK(cudaStreamGetCaptureInfo(st, &cs, nullptr, &cg, nullptr, nullptr));
+        CK(cudaGraphConditionalHandleCreate(&h, cg, 0, cudaGraphCondAssignDefault));
+    }
+    {
+        ProfScope ps(s, 1);
+        TRY(fcg_pre(s, st, h, graph ? 1 : 0));
+        if (graph) {
+            cudaGraph_t cg = nullptr;
+            const cudaGraphNode_t* deps = nullptr;
+            size_t nd = 0;
+            CK(cudaStreamGetCaptureInfo(st, &cs, nullptr, &cg, &deps, &nd));
+            cudaGraphNodeParams np{};
+            np.type = cudaGraphNodeTypeConditional;
+            np.conditional.handle = h;
+            np.conditional.type = cudaGraphCondTypeWhile;
+            np.conditional.size = 1;
+            cudaGraphNode_t node = nullptr;
+            CK(cudaGraphAddNode(&node, cg, deps, nd, &np));
+            CK(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+            cudaGraph_t body = np.conditional.phGraph_out[0];
+            CK(cudaStreamBeginCaptureToGraph(s->body_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+            const unsigned long long before = s->launches;
+            const wc_status bs = fcg_body(s, s->body_stream, h, 1);
+            cudaGraph_t captured = nullptr;
+            const cudaError_t e = cudaStreamEndCapture(s->body_stream, &captured);
+            s->fcg_body_launches = s->launches - before;
+            s->launches = before;  // body launches are counted per executed iteration
+            if (bs != WC_OK) return bs;
+            CK(e);
+        } else {
+            // Without a graph: iterations in chunks, the host looks at `done` between them; the
+            // kernels of iterations past the end return at once.
+            const long long max_it = (long long)s->disp.max_iterations;
+            for (long long k = 0; k < max_it;) {
+                const long long chunk = std::min<long long>(4, max_it - k);
+                const unsigned long long before = s->launches;
+                for (long long c = 0; c < chunk; c++) TRY(fcg_body(s, st, 0, 0));
+                s->fcg_body_launches = (s->launches - before) / (unsigned long long)chunk;
+                s->launches = before;
+                k += chunk;
+                CK(cudaMemcpyAsync(s->done_host, &s->fsc->done, sizeof(int), cudaMemcpyDeviceToHost, st));
+                CK(cudaStreamSynchronize(st));
+                if (*s->done_host) break;
+            }
+        }
+    }
+    return launch_pcg(s, mode, qold, qout, s->fsc);
+}
+
+// The dispersive solve of one stage by the configured method.
+wc_status launch_solve(wc_solver* s, int mode, const float4* qold, float4* qout) {
+    if (s->pc == WC_PC_LEARNED) {
+        if (!s->lpc) return set_err(WC_EINVAL, "the learned preconditioner is selected but no network is attached");
+        return launch_fcg(s, mode, qold, qout);
+    }
+    return launch_pcg(s, mode, qold, qout);
+}
+
 // One SSP-RK2 step (solver.rs:479-507) of size ctl->dt on the device-resident state q0.
 wc_status enqueue_step_direct(wc_solver* s) {
     if (s->order == WC_ORDER_FIRST) {
         TRY(launch_stage(s, MODE_FIRST, s->q0, s->q0, s->q1, false));
-        if (s->sgn) TRY(launch_pcg(s, MODE_FIRST, s->q0, s->q1));
+        if (s->sgn) TRY(launch_solve(s, MODE_FIRST, s->q0, s->q1));
         CK(cudaMemcpyAsync(s->q0, s->q1, s->ncell * sizeof(float4), cudaMemcpyDeviceToDevice, s->stream));
         return WC_OK;
     }
@@ -332,21 +489,12 @@ wc_status enqueue_step_direct(wc_solver* s) {
         return WC_OK;
     }
     TRY(launch_stage(s, MODE_STAGE1, s->q0, s->q0, s->q1, false));
-    TRY(launch_pcg(s, MODE_STAGE1, s->q0, s->q1));
+    TRY(launch_solve(s, MODE_STAGE1, s->q0, s->q1));
     TRY(launch_stage(s, MODE_STAGE1, s->q1, s->q0, s->q1, true));
-    TRY(launch_pcg(s, MODE_STAGE2, s->q0, s->q0));
+    TRY(launch_solve(s, MODE_STAGE2, s->q0, s->q0));
     return WC_OK;
 }
 
-// Launches one step per kernel that enqueue_step_direct issues.
-int step_launches(const wc_solver* s) {
-    if (s->order == WC_ORDER_FIRST) return s->sgn ? 2 : 1;
-    return s->sgn ? 4 : 2;
-}
-
-// The same step through a CUDA graph captured at first use (launch gaps inside a graph are
-// shorter than between separate launches). Profiling runs the launches directly so that each
-// kernel gets its own events.
 wc_status enqueue_step(wc_solver* s) {
     s->rate_current = true;
     if (s->prof_on || s->graph_failed) return enqueue_step_direct(s);
@@ -360,6 +508,7 @@ wc_status enqueue_step(wc_solver* s) {
         const unsigned long long before = s->launches;
         wc_status st = enqueue_step_direct(s);
         cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
+        s->graph_launches = s->launches - before;
         s->launches = before;
         if (st != WC_OK || e != cudaSuccess ||
             cudaGraphInstantiate(&s->step_graph, graph, 0) != cudaSuccess) {
@@ -372,7 +521,7 @@ wc_status enqueue_step(wc_solver* s) {
         cudaGraphDestroy(graph);
     }
     CK(cudaGraphLaunch(s->step_graph, s->stream));
-    s->launches += step_launches(s);
+    s->launches += s->graph_launches;
     return WC_OK;
 }
 
@@ -445,7 +594,17 @@ void wc_dispersion_default(wc_dispersion* d) {
 
 const char* wc_last_error(void) { return g_err.c_str(); }
 
-uint64_t wc_launch_count(const wc_solver* s) { return s ? s->launches : 0; }
+uint64_t wc_launch_count(const wc_solver* s) {
+    if (!s) return 0;
+    uint64_t n = s->launches;
+    if (s->fcg_body_launches) {  // flexible-CG iterations run as while-node bodies: count them
+        Ctl c{};
+        if (cudaMemcpyAsync(&c, s->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s->stream) == cudaSuccess &&
+            cudaStreamSynchronize(s->stream) == cudaSuccess)
+            n += s->fcg_body_launches * (c.fcg_iterations - s->fcg_iter_base);
+    }
+    return n;
+}
 
 wc_status wc_solver_create(const wc_grid* grid, const double* bed_padded, const wc_config* cfg,
                            wc_solver** out) {
@@ -461,8 +620,8 @@ wc_status wc_solver_create(const wc_grid* grid, const double* bed_padded, const 
         return set_err(WC_EUNSUPPORTED, "at most 8 sponges are supported");
     if (cfg->n_sponges && !cfg->sponges) return set_err(WC_EINVAL, "sponges is null");
     if (cfg->dispersion) {
-        if (cfg->dispersion->preconditioner != WC_PC_JACOBI)
-            return set_err(WC_EUNSUPPORTED, "this build's solver takes the Jacobi preconditioner");
+        if (cfg->dispersion->preconditioner != WC_PC_JACOBI && cfg->dispersion->preconditioner != WC_PC_LEARNED)
+            return set_err(WC_EINVAL, "unknown preconditioner");
         if (!(cfg->dispersion->tolerance >= 0.0)) return set_err(WC_EINVAL, "tolerance must be >= 0");
     }
     TRY(configure_kernels());
@@ -495,7 +654,10 @@ wc_status wc_solver_create(const wc_grid* grid, const double* bed_padded, const 
     s->order = cfg->order;
     s->cfl = cfg->cfl;
     s->sgn = cfg->dispersion ? 1 : 0;
-    if (cfg->dispersion) s->disp = *cfg->dispersion;
+    if (cfg->dispersion) {
+        s->disp = *cfg->dispersion;
+        s->pc = cfg->dispersion->preconditioner;
+    }
     else wc_dispersion_default(&s->disp);
     const wc_breaking& b = s->disp.breaking;  // Breaking::default() for shallow water (solver.rs:618-623)
     s->br.er_lo = (float)b.eta_ratio_lo;
@@ -623,7 +785,7 @@ wc_status wc_solver_create(const wc_grid* grid, const double* bed_padded, const 
         s->pcg_tiles_y = (ny + PG_TY - 1) / PG_TY;
         const int tiles = s->pcg_tiles_x * s->pcg_tiles_y;
         s->pcg_blocks = std::max(1, std::min(tiles, sms * std::min(occ, 4)));
-        ALLOC(s->part, 4 * (size_t)s->pcg_blocks);
+        ALLOC(s->part, 8 * (size_t)s->pcg_blocks);
         ALLOC(s->bar, 2);
     }
 #undef ALLOC
@@ -1022,7 +1184,7 @@ wc_status build_variant(wc_ensemble* e, EnVariant& v, int ctas) {
         M.pcg[1] = pcg_args(s, MODE_STAGE2, s->q0, s->q0);
         for (int k = 0; k < 2; k++) {
             M.pcg[k].cnt = e->counters + 2 * m;
-            M.pcg[k].part = e->partials + 4 * (size_t)m * e->max_ctas;
+            M.pcg[k].part = e->partials + 8 * (size_t)m * e->max_ctas;
         }
     }
     if (!v.d_table) CK(cudaMalloc(&v.d_table, n * sizeof(EnsembleMember)));
@@ -1179,7 +1341,7 @@ wc_status wc_ensemble_create(uint64_t n, const wc_grid* grids, const double* con
     e->max_ctas = max_ctas;
     wc_status st;
     if ((st = dalloc(&e->counters, 2 * n)) != WC_OK) return fail(st);
-    if ((st = dalloc(&e->partials, 4 * n * (size_t)max_ctas)) != WC_OK) return fail(st);
+    if ((st = dalloc(&e->partials, 8 * n * (size_t)max_ctas)) != WC_OK) return fail(st);
     for (int k = 0; k < EN_VARIANTS; k++) {
         if (e->var[k].ctas <= 0) continue;
         if ((st = build_variant(e, e->var[k], std::max((int)n, e->var[k].ctas))) != WC_OK) return fail(st);
@@ -1240,5 +1402,233 @@ wc_status wc_ensemble_member_stats(wc_ensemble* e, uint64_t m, wc_stats* stats, 
 }
 
 uint64_t wc_ensemble_launch_count(const wc_ensemble* e) { return e ? e->launches : 0; }
+
+}  // extern "C"
+
+// ---- the learned preconditioner ---------------------------------------------------------------
+
+struct wc_lpc {
+    LpcModel m;
+};
+
+namespace {
+
+wc_status lpc_ck(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) return set_err(WC_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    return WC_OK;
+}
+
+// Scaled normal weights (standard deviation sqrt(1 / fan-in)), zero biases, a zero output layer:
+// the untrained network adds nothing to the two Jacobi sweeps.
+void lpc_init_host(const LpcNet& net, uint64_t seed, std::vector<float>& p) {
+    p.assign(net.nparams, 0.f);
+    unsigned long long st = seed * 0x9e3779b97f4a7c15ull + 0x632be59bd9b4e019ull;
+    auto uni = [&]() {
+        st ^= st << 13;
+        st ^= st >> 7;
+        st ^= st << 17;
+        return ((st >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+    };
+    auto fill = [&](const LpcLayer& L) {
+        const double sd = std::sqrt(1.0 / (L.ci * L.k * L.k));
+        for (int q = 0; q < L.co * L.ci * L.k * L.k; q++) {
+            const double u1 = uni(), u2 = uni();  // Box-Muller
+            p[L.w + q] = (float)(sd * std::sqrt(-2.0 * std::log(u1)) * std::cos(TAU * u2));
+        }
+    };
+    for (auto* L : {&net.enc_a, &net.enc_b, &net.dec_a, &net.dec_b, &net.gate_a, &net.gate_b})
+        for (auto& l : *L)
+            if (l.co > 0) fill(l);
+}
+
+}  // namespace
+
+extern "C" {
+
+wc_status wc_lpc_create(const int32_t* channels, int32_t gate_hidden, uint64_t seed, wc_lpc** out) {
+    if (!out) return set_err(WC_EINVAL, "out is null");
+    *out = nullptr;
+    int ch[LPC_LEVELS] = {8, 16, 32, 32};
+    if (channels)
+        for (int l = 0; l < LPC_LEVELS; l++) ch[l] = channels[l];
+    for (int l = 0; l < LPC_LEVELS; l++)
+        if (ch[l] < 1 || ch[l] > 256) return set_err(WC_EINVAL, "channels must be in 1..256");
+    if (gate_hidden < 1 || gate_hidden > 256) return set_err(WC_EINVAL, "gate_hidden must be in 1..256");
+    wc_lpc* l = new wc_lpc();
+    wc_status st = lpc_ck(l->m.init(ch, gate_hidden), "network allocation");
+    if (st == WC_OK) {
+        std::vector<float> p;
+        lpc_init_host(l->m.net, seed, p);
+        st = lpc_ck(cudaMemcpy(l->m.w.p, p.data(), p.size() * sizeof(float), cudaMemcpyHostToDevice), "upload");
+        if (st == WC_OK) st = lpc_ck(l->m.refresh(), "refresh");
+        if (st == WC_OK) st = lpc_ck(cudaStreamSynchronize(l->m.st), "init");
+    }
+    if (st != WC_OK) {
+        delete l;
+        return st;
+    }
+    *out = l;
+    return WC_OK;
+}
+
+void wc_lpc_destroy(wc_lpc* l) {
+    if (l) cudaStreamSynchronize(l->m.st);
+    delete l;
+}
+
+uint64_t wc_lpc_num_params(const wc_lpc* l) { return l ? (uint64_t)l->m.net.nparams : 0; }
+
+wc_status wc_lpc_set_params(wc_lpc* l, const float* params, uint64_t n) {
+    if (!l || !params) return set_err(WC_EINVAL, "null argument");
+    if (n != (uint64_t)l->m.net.nparams) return set_err(WC_EINVAL, "parameter count mismatch");
+    LpcModel& m = l->m;
+    TRY(lpc_ck(cudaMemcpyAsync(m.w.p, params, n * sizeof(float), cudaMemcpyHostToDevice, m.st), "upload"));
+    TRY(lpc_ck(cudaMemsetAsync(m.m.p, 0, n * sizeof(float), m.st), "memset"));
+    TRY(lpc_ck(cudaMemsetAsync(m.v.p, 0, n * sizeof(float), m.st), "memset"));
+    m.adam_t = 0;
+    TRY(lpc_ck(m.refresh(), "refresh"));
+    return lpc_ck(cudaStreamSynchronize(m.st), "set_params");
+}
+
+wc_status wc_lpc_get_params(wc_lpc* l, float* params, uint64_t n) {
+    if (!l || !params) return set_err(WC_EINVAL, "null argument");
+    if (n != (uint64_t)l->m.net.nparams) return set_err(WC_EINVAL, "parameter count mismatch");
+    TRY(lpc_ck(cudaMemcpyAsync(params, l->m.w.p, n * sizeof(float), cudaMemcpyDeviceToHost, l->m.st), "download"));
+    return lpc_ck(cudaStreamSynchronize(l->m.st), "get_params");
+}
+
+wc_status wc_lpc_set_rounding(wc_lpc* l, int32_t bf16) {
+    if (!l) return set_err(WC_EINVAL, "null network");
+    l->m.round_bf16 = bf16 ? 1 : 0;
+    TRY(lpc_ck(l->m.refresh(), "refresh"));
+    return lpc_ck(cudaStreamSynchronize(l->m.st), "set_rounding");
+}
+
+wc_status wc_lpc_forward_backward(wc_lpc* l, int32_t n, int32_t h, int32_t w, const float* x, const float* feat,
+                                  const float* dy, float* y, float* grad, float* dx) {
+    if (!l || !x || !feat || !dy || !y || !grad || !dx) return set_err(WC_EINVAL, "null argument");
+    const int div = 1 << (LPC_LEVELS - 1);
+    if (n < 1 || h < div || w < div || h % div || w % div)
+        return set_err(WC_EINVAL, "batch must be >= 1 and patch sides positive multiples of 8");
+    LpcModel& m = l->m;
+    LpcNet& net = m.net;
+    cudaStream_t st = m.st;
+    const size_t per = (size_t)n * 2 * h * w;
+    TRY(lpc_ck(net.shape(n, h, w, true), "activations"));
+    DBuf ddy, ddx;
+    TRY(lpc_ck(ddy.alloc(per), "alloc"));
+    TRY(lpc_ck(ddx.alloc(per), "alloc"));
+    TRY(lpc_ck(cudaMemcpyAsync(net.X[0].p, x, per * sizeof(float), cudaMemcpyHostToDevice, st), "upload"));
+    TRY(lpc_ck(cudaMemcpyAsync(net.F[0].p, feat, per * sizeof(float), cudaMemcpyHostToDevice, st), "upload"));
+    TRY(lpc_ck(cudaMemcpyAsync(ddy.p, dy, per * sizeof(float), cudaMemcpyHostToDevice, st), "upload"));
+    TRY(lpc_ck(net.gates(st), "gates"));
+    TRY(lpc_ck(net.forward(st, true), "forward"));
+    TRY(lpc_ck(cudaMemsetAsync(m.g.p, 0, m.g.n * sizeof(float), st), "memset"));
+    TRY(lpc_ck(net.backward(ddy.p, ddx.p, st), "backward"));
+    TRY(lpc_ck(cudaMemcpyAsync(y, net.Y.p, per * sizeof(float), cudaMemcpyDeviceToHost, st), "download"));
+    TRY(lpc_ck(cudaMemcpyAsync(grad, m.g.p, (size_t)net.nparams * sizeof(float), cudaMemcpyDeviceToHost, st), "download"));
+    TRY(lpc_ck(cudaMemcpyAsync(dx, ddx.p, per * sizeof(float), cudaMemcpyDeviceToHost, st), "download"));
+    return lpc_ck(cudaStreamSynchronize(st), "forward_backward");
+}
+
+wc_status wc_lpc_harvest(wc_lpc* l, wc_solver* s) {
+    if (!l || !s) return set_err(WC_EINVAL, "null argument");
+    if (!s->sgn) return set_err(WC_EINVAL, "the solver has no dispersive solve to harvest");
+    TRY(lpc_ck(cudaStreamSynchronize(s->stream), "harvest"));
+    auto* q = new LpcSystem();
+    q->nx = (int)s->grid.nx;
+    q->ny = (int)s->grid.ny;
+    q->pitch = s->g.pitch;
+    q->dx = (float)s->grid.dx;
+    q->dy = (float)s->grid.dy;
+    wc_status st = WC_OK;
+    for (auto pr : {std::make_pair(&q->c, (const float*)s->cc), std::make_pair(&q->heff, (const float*)s->heff),
+                    std::make_pair(&q->bed, (const float*)s->bed)}) {
+        if (st == WC_OK) st = lpc_ck(pr.first->alloc(s->ncell), "alloc");
+        if (st == WC_OK)
+            st = lpc_ck(cudaMemcpy(pr.first->p, pr.second, s->ncell * sizeof(float), cudaMemcpyDeviceToDevice), "copy");
+    }
+    if (st != WC_OK) {
+        delete q;
+        return st;
+    }
+    l->m.systems.push_back(q);
+    return WC_OK;
+}
+
+uint64_t wc_lpc_num_systems(const wc_lpc* l) { return l ? l->m.systems.size() : 0; }
+
+wc_status wc_lpc_train(wc_lpc* l, uint32_t steps, uint32_t batch, uint32_t patch, float lr, float rough, uint64_t seed,
+                       double* losses) {
+    if (!l) return set_err(WC_EINVAL, "null network");
+    LpcModel& m = l->m;
+    if (m.systems.empty()) return set_err(WC_EINVAL, "no harvested systems");
+    const uint32_t div = 1u << (LPC_LEVELS - 1);
+    if (batch < 1 || batch > 4096 || patch < div || patch % div || patch > 4096)
+        return set_err(WC_EINVAL, "batch must be in 1..4096 and the patch side a multiple of 8 up to 4096");
+    bool fits = false;
+    for (auto* q : m.systems) fits = fits || ((uint32_t)q->nx >= patch && (uint32_t)q->ny >= patch);
+    if (!fits) return set_err(WC_EINVAL, "no harvested system is as large as the patch");
+    if (steps == 0) return WC_OK;
+    if (m.dloss_n < steps) {
+        if (m.dloss) cudaFree(m.dloss);
+        m.dloss = nullptr;
+        m.dloss_n = 0;
+        TRY(lpc_ck(cudaMalloc(&m.dloss, steps * sizeof(double)), "alloc"));
+        m.dloss_n = steps;
+    }
+    m.rng = seed * 0x9e3779b97f4a7c15ull + 0x2545f4914f6cdd1dull;
+    if (m.rng == 0) m.rng = 1;
+    for (uint32_t k = 0; k < steps; k++) {
+        const cudaError_t e = m.train_step((int)batch, (int)patch, (int)patch, lr, m.dloss + k, rough);
+        if (e == cudaErrorInvalidValue) return set_err(WC_EINVAL, "no harvested system of one spacing fits the patch");
+        TRY(lpc_ck(e, "training step"));
+    }
+    if (losses)
+        TRY(lpc_ck(cudaMemcpyAsync(losses, m.dloss, steps * sizeof(double), cudaMemcpyDeviceToHost, m.st), "download"));
+    return lpc_ck(cudaStreamSynchronize(m.st), "train");
+}
+
+wc_status wc_solver_set_lpc(wc_solver* s, wc_lpc* l) {
+    if (!s) return set_err(WC_EINVAL, "null solver");
+    if (!s->sgn) return set_err(WC_EINVAL, "the solver has no dispersive solve");
+    CK(cudaStreamSynchronize(s->stream));
+    Ctl c{};
+    CK(cudaMemcpy(&c, s->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost));
+    if (s->fcg_body_launches) s->launches += s->fcg_body_launches * (c.fcg_iterations - s->fcg_iter_base);
+    s->fcg_body_launches = 0;
+    if (s->step_graph) {  // the captured step names the previous method's buffers
+        cudaGraphExecDestroy(s->step_graph);
+        s->step_graph = nullptr;
+    }
+    if (!l) {
+        s->lpc = nullptr;
+        s->pc = WC_PC_JACOBI;
+        return WC_OK;
+    }
+    if (l->m.net.nparams == 0) return set_err(WC_EINVAL, "network not initialised");
+    const int div = 1 << (LPC_LEVELS - 1);
+    s->lpc_hp = ((int)s->grid.ny + div - 1) / div * div;
+    s->lpc_wp = ((int)s->grid.nx + div - 1) / div * div;
+    s->lnet.layout(l->m.net.ch, l->m.net.hidden);
+    s->lnet.wq = l->m.wq.p;
+    s->lnet.gw = nullptr;
+    CK(s->lnet.shape(1, s->lpc_hp, s->lpc_wp, false));
+    if (!s->tv) {
+        CK(cudaMalloc(&s->tv, s->ncell * sizeof(float2)));
+        CK(cudaMemset(s->tv, 0, s->ncell * sizeof(float2)));
+        CK(cudaMalloc(&s->fsc, sizeof(FcgScalars)));
+        CK(cudaMemset(s->fsc, 0, sizeof(FcgScalars)));
+        CK(cudaMalloc(&s->fpart, 3 * FCG_BLOCKS * sizeof(double)));
+        CK(cudaMallocHost(&s->done_host, sizeof(int)));
+        CK(cudaStreamCreateWithFlags(&s->body_stream, cudaStreamNonBlocking));
+    }
+    // training and inference may run on different streams: the weights are final from here
+    CK(cudaStreamSynchronize(l->m.st));
+    s->lpc = &l->m;
+    s->pc = WC_PC_LEARNED;
+    s->fcg_iter_base = c.fcg_iterations;  // the kernels per iteration are counted at the first solve
+    return WC_OK;
+}
 
 }  // extern "C"

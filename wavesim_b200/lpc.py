@@ -1,21 +1,26 @@
-"""The learned preconditioner: a small 4-level convolutional U-net.
+"""The learned preconditioner of the SGN solve: a depth-gated linear U-net in a two-level cycle.
 
 No counterpart in the reference (its dispersive solve is Jacobi-preconditioned CG,
-crates/wavecore/src/dispersion.rs:493-545). The network maps the SGN residual r = (rx, ry), with
-the depth and bed, to a correction of the Jacobi step:
+crates/wavecore/src/dispersion.rs:493-545). Given a residual r of the system
+h w - grad(c div w) = r, the preconditioner returns
 
-    z = r / diag + (s / H0) * mask * N(h / H0, b / H0, rx / s, ry / s),   s = rms(r)
+    z1 = omega r / diag                       damped Jacobi sweep
+    z2 = z1 + mask * N(diag^-1 (r - A z1))    the network's correction
+    z  = z2 + omega (r - A z2) / diag         damped Jacobi sweep
 
-so an untrained network (last layer zero) is exactly the Jacobi preconditioner, and scaling r
-scales z. N is a U-net: on each of 4 levels two 3x3 convolutions with ReLU, 2x2 average pooling
-down, nearest-neighbour upsampling and concatenation with the skip up, two 3x3 convolutions per
-decoder level, and a 1x1 convolution to 2 channels. Weights are stored in FP32 for training and
-used in BF16; accumulation is FP32. It is applied inside flexible CG (Polak-Ribiere beta), which
-stays correct for a preconditioner that is not a fixed symmetric matrix, with the same stopping
-rule as the plain solve.
+N is a 4-level U-net of 3x3 convolutions without biases or activations, so z depends linearly
+on r (Krylov methods need that: a network that is nonlinear in r stalled flexible CG in
+experiments), and scaling r scales z. What it cannot see from r — the depth-dependent
+coefficients — enters through gates: at every level the feature maps are multiplied by
+G_l = 2 sigmoid(conv1x1(relu(conv3x3(F_l)))) of F_0 = (h / H0, b / H0), pooled to the level.
+Encoder: two convolutions then the gate; 2x2 average pooling down; decoder: nearest-neighbour
+upsampling, concatenation with the skip, two convolutions, the gate; a 1x1 convolution to 2
+channels. Weights are trained in FP32 and used in BF16; accumulation is FP32. The last layer
+starts at zero, so an untrained network leaves the two Jacobi sweeps. It is applied inside
+flexible CG (the previous direction A-orthogonalised out), with the plain solve's stopping rule.
 
-This module holds the architecture's parameter layout, shared by the device kernels, the
-training loop and the FP64 CPU reference used to check gradients.
+This module holds the parameter layout shared by the device kernels, the training loop and the
+FP64 CPU reference used to check gradients.
 """
 from __future__ import annotations
 
@@ -24,68 +29,77 @@ from dataclasses import dataclass
 import numpy as np
 
 DEPTH_SCALE = 20.0  # H0, metres
+OMEGA = 0.5         # damping of the Jacobi sweeps (keeps the cycle positive definite)
+GATE_HIDDEN = 8     # channels of the gate networks' hidden layer
 
 
 @dataclass(frozen=True)
 class UNetSpec:
     channels: tuple = (8, 16, 32, 32)  # feature maps per level, finest first
-    in_ch: int = 4
+    in_ch: int = 2
     out_ch: int = 2
+    feat_ch: int = 2
+    gate_hidden: int = GATE_HIDDEN
 
     @property
     def levels(self) -> int:
         return len(self.channels)
 
     def layers(self):
-        """(name, c_out, c_in, kernel) in parameter order."""
+        """(name, c_out, c_in, kernel, has_bias) in parameter order."""
         c = self.channels
         out = []
         cin = self.in_ch
         for l in range(self.levels):
-            out.append((f"enc{l}a", c[l], cin, 3))
-            out.append((f"enc{l}b", c[l], c[l], 3))
+            out.append((f"enc{l}a", c[l], cin, 3, False))
+            out.append((f"enc{l}b", c[l], c[l], 3, False))
             cin = c[l]
         for l in range(self.levels - 2, -1, -1):
-            out.append((f"dec{l}a", c[l], c[l + 1] + c[l], 3))
-            out.append((f"dec{l}b", c[l], c[l], 3))
-        out.append(("out", self.out_ch, c[0], 1))
+            out.append((f"dec{l}a", c[l], c[l + 1] + c[l], 3, False))
+            out.append((f"dec{l}b", c[l], c[l], 3, False))
+        out.append(("out", self.out_ch, c[0], 1, False))
+        for l in range(self.levels):
+            out.append((f"gate{l}a", self.gate_hidden, self.feat_ch, 3, True))
+            out.append((f"gate{l}b", c[l], self.gate_hidden, 1, True))
         return out
 
     def offsets(self):
-        """{name: (w_offset, b_offset, c_out, c_in, k)} into the flat parameter vector."""
+        """{name: (w_offset, b_offset or -1, c_out, c_in, k)} into the flat parameter vector."""
         off = 0
         table = {}
-        for name, co, ci, k in self.layers():
+        for name, co, ci, k, has_b in self.layers():
             w = off
             off += co * ci * k * k
-            b = off
-            off += co
+            b = -1
+            if has_b:
+                b = off
+                off += co
             table[name] = (w, b, co, ci, k)
         return table
 
     def n_params(self) -> int:
-        n = 0
-        for _, co, ci, k in self.layers():
-            n += co * ci * k * k + co
-        return n
+        return sum(co * ci * k * k + (co if hb else 0) for _, co, ci, k, hb in self.layers())
 
     def flops_per_cell(self) -> float:
-        """Multiply-adds x2 per finest-level cell for one application."""
+        """2 x multiply-adds per finest-level cell of one application (gates excluded: they are
+        computed once per solve)."""
         f = 0.0
-        for name, co, ci, k in self.layers():
-            level = int(name[3]) if name != "out" else 0
+        for name, co, ci, k, _ in self.layers():
+            if name.startswith("gate"):
+                continue
+            level = 0 if name == "out" else int(name[3])
             f += 2.0 * co * ci * k * k / (4.0 ** level)
         return f
 
 
 def init_params(spec: UNetSpec, seed: int = 0) -> np.ndarray:
-    """He-normal weights, zero biases, and a zero output layer (the network starts as Jacobi)."""
+    """Scaled normal weights, zero biases, a zero output layer (the network starts at zero)."""
     rng = np.random.default_rng(seed)
     p = np.zeros(spec.n_params(), dtype=np.float32)
     for name, (w, b, co, ci, k) in spec.offsets().items():
         if name == "out":
             continue
-        std = np.sqrt(2.0 / (ci * k * k))
+        std = np.sqrt(1.0 / (ci * k * k))
         p[w : w + co * ci * k * k] = rng.normal(0.0, std, co * ci * k * k).astype(np.float32)
     return p
 

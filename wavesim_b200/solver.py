@@ -58,6 +58,17 @@ EXPORTS = [
     "wc_ensemble_synchronize",
     "wc_ensemble_member_stats",
     "wc_ensemble_launch_count",
+    "wc_lpc_create",
+    "wc_lpc_destroy",
+    "wc_lpc_num_params",
+    "wc_lpc_set_params",
+    "wc_lpc_get_params",
+    "wc_lpc_set_rounding",
+    "wc_lpc_forward_backward",
+    "wc_lpc_harvest",
+    "wc_lpc_num_systems",
+    "wc_lpc_train",
+    "wc_solver_set_lpc",
 ]
 
 
@@ -115,6 +126,24 @@ def load(path: str = LIB_PATH):
         getattr(L, name).restype = C.c_int
     L.wc_stable_dt_noalloc.argtypes = [C.POINTER(abi.wc_grid), C.c_double, V, V, V, V, D]
     L.wc_stable_dt_noalloc.restype = C.c_int
+    F = C.POINTER(C.c_float)
+    L.wc_lpc_create.argtypes = [C.POINTER(C.c_int32), C.c_int32, C.c_uint64, C.POINTER(V)]
+    L.wc_lpc_destroy.argtypes = [V]
+    L.wc_lpc_destroy.restype = None
+    L.wc_lpc_num_params.argtypes = [V]
+    L.wc_lpc_num_params.restype = C.c_uint64
+    L.wc_lpc_set_params.argtypes = [V, F, C.c_uint64]
+    L.wc_lpc_get_params.argtypes = [V, F, C.c_uint64]
+    L.wc_lpc_set_rounding.argtypes = [V, C.c_int32]
+    L.wc_lpc_forward_backward.argtypes = [V, C.c_int32, C.c_int32, C.c_int32, F, F, F, F, F, F]
+    L.wc_lpc_harvest.argtypes = [V, V]
+    L.wc_lpc_num_systems.argtypes = [V]
+    L.wc_lpc_num_systems.restype = C.c_uint64
+    L.wc_lpc_train.argtypes = [V, C.c_uint32, C.c_uint32, C.c_uint32, C.c_float, C.c_float, C.c_uint64, D]
+    L.wc_solver_set_lpc.argtypes = [V, V]
+    for name in ("wc_lpc_create", "wc_lpc_set_params", "wc_lpc_get_params", "wc_lpc_set_rounding",
+                 "wc_lpc_forward_backward", "wc_lpc_harvest", "wc_lpc_train", "wc_solver_set_lpc"):
+        getattr(L, name).restype = C.c_int
     L.wc_launch_count.argtypes = [V]
     L.wc_launch_count.restype = C.c_uint64
     L.wc_last_error.restype = C.c_char_p
@@ -273,8 +302,100 @@ class Solver(SolverConfig):
         _check(load().wc_time_device(self._h(), C.byref(t)))
         return t.value
 
+    def set_preconditioner(self, net: "LearnedPreconditioner | None") -> None:
+        """Attach a trained network (learned-preconditioned flexible CG) or detach it (None:
+        Jacobi PCG, the reference's method)."""
+        _check(load().wc_solver_set_lpc(self._h(), net._handle if net is not None else None))
+        self._lpc = net  # keep it alive while attached
+
     def launch_count(self) -> int:
         return int(load().wc_launch_count(self._h()))
+
+
+def _fptr(a: np.ndarray):
+    assert a.dtype == np.float32 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+class LearnedPreconditioner:
+    """The network preconditioner of the dispersive solve (`wc_lpc_*`; no counterpart in the
+    reference, whose solve is Jacobi-preconditioned CG, dispersion.rs:493-545).
+
+    Its parameter layout is `lpc.UNetSpec`; it is trained on the GPU on SGN systems harvested
+    from solvers (`harvest`, `train`) and attached to a solver with `Solver.set_preconditioner`.
+    It must outlive the solvers it is attached to (a solver keeps a reference)."""
+
+    def __init__(self, spec=None, seed: int = 0):
+        from .lpc import UNetSpec
+
+        self.spec = spec or UNetSpec()
+        ch = (C.c_int32 * 4)(*self.spec.channels)
+        out = C.c_void_p()
+        _check(load().wc_lpc_create(ch, int(self.spec.gate_hidden), int(seed), C.byref(out)))
+        self._handle = out
+
+    def __del__(self):
+        try:
+            if getattr(self, "_handle", None):
+                load().wc_lpc_destroy(self._handle)
+            self._handle = None
+        except Exception:
+            pass
+
+    @property
+    def n_params(self) -> int:
+        return int(load().wc_lpc_num_params(self._handle))
+
+    def get_params(self) -> np.ndarray:
+        p = np.zeros(self.n_params, dtype=np.float32)
+        _check(load().wc_lpc_get_params(self._handle, _fptr(p), p.size))
+        return p
+
+    def set_params(self, p) -> None:
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        _check(load().wc_lpc_set_params(self._handle, _fptr(p), p.size))
+
+    def set_rounding(self, bf16: bool) -> None:
+        _check(load().wc_lpc_set_rounding(self._handle, 1 if bf16 else 0))
+
+    def forward_backward(self, x, feat, dy):
+        """(y, parameter gradient, input gradient) of one pass on [n][2][h][w] arrays."""
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        feat = np.ascontiguousarray(feat, dtype=np.float32)
+        dy = np.ascontiguousarray(dy, dtype=np.float32)
+        n, c, h, w = x.shape
+        assert c == 2 and feat.shape == x.shape and dy.shape == x.shape
+        y = np.zeros_like(x)
+        dx = np.zeros_like(x)
+        g = np.zeros(self.n_params, dtype=np.float32)
+        _check(load().wc_lpc_forward_backward(self._handle, n, h, w, _fptr(x), _fptr(feat), _fptr(dy), _fptr(y),
+                                              _fptr(g), _fptr(dx)))
+        return y, g, dx
+
+    def harvest(self, solver: "Solver") -> None:
+        """Keep the solver's current SGN system (that of its last solve) for training."""
+        _check(load().wc_lpc_harvest(self._handle, solver._h()))
+
+    @property
+    def n_systems(self) -> int:
+        return int(load().wc_lpc_num_systems(self._handle))
+
+    def train(self, steps: int, batch: int = 16, patch: int = 64, lr: float = 2e-3, rough: float = 1.0,
+              seed: int = 0) -> np.ndarray:
+        """Adam steps on random patches of the harvested systems; returns every step's loss."""
+        losses = np.zeros(max(int(steps), 1), dtype=np.float64)
+        _check(load().wc_lpc_train(self._handle, int(steps), int(batch), int(patch), float(lr), float(rough),
+                                   int(seed), abi.dptr(losses)))
+        return losses[: int(steps)]
+
+    def save(self, path: str) -> None:
+        np.save(path, self.get_params())
+
+    @classmethod
+    def load_params(cls, path: str, spec=None):
+        net = cls(spec)
+        net.set_params(np.load(path))
+        return net
 
 
 class Ensemble:
