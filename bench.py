@@ -110,6 +110,16 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
+def peak_tensor():
+    """Dense BF16 tensor throughput (TFLOP/s), burst figure: the network is timed per application."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["bf16_tflops"]), "measured (cuBLAS bf16, burst)"
+    except Exception:
+        return 1590.0, "fallback"
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
 
@@ -238,31 +248,21 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
-def run_b200(args, world, rank, local):
+def measure_arm(w, args, world, stream, flush, net=None):
+    """One arm (Jacobi PCG, or the learned preconditioner when `net` is given): device-timed
+    steps, the per-kernel profiled pass, the end-to-end pass through `wc_step`."""
     import torch
 
     from wavesim_b200 import Solver
 
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
-    w = workload(args.workload)
-    stream = torch.cuda.Stream()  # a real stream handle: the solver and the events share it
-    torch.cuda.set_stream(stream)
+    dist = torch.distributed if world > 1 else None
     sol = w.solver(Solver)
     sol.set_stream(stream.cuda_stream)
+    if net is not None:
+        sol.set_preconditioner(net)
     s0 = W.wave_train_state(w)
     sol.upload(s0)
-    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
-
-    # warm-up: adaptive steps on the device
-    sol.step_n(args.warmup)
+    sol.step_n(args.warmup)  # warm-up: adaptive steps on the device
     sol.synchronize()
     st0 = sol.dispersion_stats()
     l0 = sol.launch_count()
@@ -270,7 +270,7 @@ def run_b200(args, world, rank, local):
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    with ClockSampler(local) as clocks:
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clocks:
         for k in range(args.steps):
             flush.zero_()
             ev[k][0].record(stream)
@@ -291,20 +291,20 @@ def run_b200(args, world, rank, local):
     prof = sol.profile_read()
     sol.profile(False)
     st2 = sol.dispersion_stats()
-    total_ms = sum(step_ms)
-    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    t = torch.tensor([sum(step_ms)], dtype=torch.float64, device="cuda")
     if dist:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dist.barrier()
     total_ms_max = float(t.item())
     cells = w.interior_cells()
-    value = cells * args.steps * world / (total_ms_max / 1e3)
 
     # end to end through the reference-facing call, pinned host FP64 arrays
     pin = lambda a: torch.from_numpy(a).pin_memory().numpy()  # noqa: E731
     hs = State(pin(s0.h), pin(s0.hu), pin(s0.hv), pin(s0.breaking), s0.time)
     e2e_sol = w.solver(Solver)
     e2e_sol.set_stream(stream.cuda_stream)
+    if net is not None:
+        e2e_sol.set_preconditioner(net)
     dt = 0.5 * sol.stable_dt_device()
     for _ in range(2):
         e2e_sol.step(hs, dt)
@@ -317,34 +317,119 @@ def run_b200(args, world, rank, local):
     te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
     if dist:
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = cells * n_e2e * world / float(te.item())
-    npad = w.grid.cells()
+    per_solve = lambda a, b: (b.iterations - a.iterations) / max(1, b.solves - a.solves) if b else 0.0  # noqa: E731
+    return {
+        "value": cells * args.steps * world / (total_ms_max / 1e3),
+        "ms_per_step": total_ms_max / args.steps,
+        "iterations_per_solve": per_solve(st0, st1),
+        "iterations_per_solve_profiled": per_solve(st1, st2),
+        "unconverged": (st2.unconverged - st0.unconverged) if st2 else 0,
+        "prof": prof,
+        "launches": int(launches),
+        "clocks": clocks.summary(),
+        "e2e": {"value": cells * n_e2e * world / float(te.item()), "unit": UNIT,
+                "h2d_bytes_per_step": 3 * w.grid.cells() * 8, "d2h_bytes_per_step": 3 * w.grid.cells() * 8,
+                "steps": n_e2e, "path": "wc_step on pinned host FP64 arrays (upload, step, download per call)"},
+    }
+
+
+def eta_errors(w, net, steps: int):
+    """Max |eta - eta_oracle| over wet cells after `steps` steps from the wave-train start (the
+    oracle's dt sequence), for Jacobi PCG and the learned preconditioner."""
+    from oracle.oracle import OracleSolver, set_threads
+
+    from wavesim_b200 import Solver
+
+    set_threads(0)
+    orc = w.solver(OracleSolver)
+    arms = {"plain_pcg": w.solver(Solver), "learned": w.solver(Solver)}
+    arms["learned"].set_preconditioner(net)
+    s0 = W.wave_train_state(w)
+    so = s0.clone()
+    ss = {k: s0.clone() for k in arms}
+    for _ in range(steps):
+        dt = orc.stable_dt(so)
+        orc.step(so, dt)
+        for k, sol in arms.items():
+            sol.step(ss[k], dt)
+    g = w.grid
+    ho = g.inner(so.h)
+    out = {}
+    for k, s in ss.items():
+        hg = g.inner(s.h)
+        wet = (hg > 1e-3) & (ho > 1e-3)
+        out[k] = float(np.abs(hg - ho)[wet].max())
+    out["steps"] = steps
+    return out
+
+
+def run_b200(args, world, rank, local):
+    import torch
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    w = workload(args.workload)
+    stream = torch.cuda.Stream()  # a real stream handle: the solvers and the events share it
+    torch.cuda.set_stream(stream)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    learned = args.pc == "learned" and w.dispersion is not None
+
+    net, train_rec = None, None
+    if learned:
+        from wavesim_b200.train_lpc import trained_network
+
+        torch.cuda.synchronize()
+        net, train_rec = trained_network(dx=w.grid.dx, steps=args.train_steps, seed=0)
+        torch.cuda.synchronize()
+    arm = measure_arm(w, args, world, stream, flush, net)
+    plain = measure_arm(w, args, world, stream, flush, None) if learned else None
 
     line = None
     if rank == 0:
-        iters = (st1.iterations - st0.iterations) / max(1, st1.solves - st0.solves) if st1 else 0.0
-        iters_prof = (st2.iterations - st1.iterations) / max(1, st2.solves - st1.solves) if st1 else 0.0
+        cells = w.interior_cells()
+        prof = arm["prof"]
         solve_n, solve_ms = prof["solve"]
         stage_n, stage_ms = prof["stage"]
+        net_n, net_ms = prof.get("network", (0, 0.0))
         peak, peak_kind = measured_peaks()
-        if solve_n and solve_ms >= stage_ms:
-            per_cell = SOLVE_INIT_BYTES + SOLVE_ITER_BYTES * iters_prof + SOLVE_FINISH_BYTES
-            dom = {"kernel": "pcg_kernel (persistent dispersive solve)", "launches": solve_n, "avg_ms": solve_ms / solve_n,
-                   "bytes_per_cell": per_cell}
+        iters_prof = arm["iterations_per_solve_profiled"]
+        if learned and net_ms >= max(solve_ms, stage_ms):
+            from wavesim_b200.lpc import UNetSpec
+
+            flops = UNetSpec().flops_per_cell() * w.grid.nx * w.grid.ny
+            tflops = flops / (net_ms / net_n / 1e3) / 1e12
+            roof = {"bound": "compute (FP32 CUDA-core convolutions)", "kernel": "conv_fwd_kernel chain (one network application)",
+                    "achieved": tflops, "unit": "TFLOP/s", "flops_per_cell": UNetSpec().flops_per_cell(),
+                    "avg_ms": net_ms / net_n, "traffic": None}
+            bf16 = peak_tensor()
+            roof.update({"peak": bf16[0], "frac": tflops / bf16[0], "peak_source": bf16[1]})
         else:
-            per_cell = STAGE_BYTES_SGN if w.dispersion else STAGE_BYTES_SWE
-            dom = {"kernel": "stage_kernel (fused RK stage)", "launches": stage_n, "avg_ms": stage_ms / max(1, stage_n),
-                   "bytes_per_cell": per_cell}
-        achieved = per_cell * cells / (dom["avg_ms"] / 1e3) / 1e9
-        ck = clocks.summary()
+            if solve_n and solve_ms >= stage_ms:
+                per_cell = SOLVE_INIT_BYTES + SOLVE_ITER_BYTES * iters_prof + SOLVE_FINISH_BYTES
+                dom = {"kernel": "pcg_kernel (persistent dispersive solve)", "launches": solve_n,
+                       "avg_ms": solve_ms / solve_n, "bytes_per_cell": per_cell}
+            else:
+                per_cell = STAGE_BYTES_SGN if w.dispersion else STAGE_BYTES_SWE
+                dom = {"kernel": "stage_kernel (fused RK stage)", "launches": stage_n,
+                       "avg_ms": stage_ms / max(1, stage_n), "bytes_per_cell": per_cell}
+            achieved = per_cell * cells / (dom["avg_ms"] / 1e3) / 1e9
+            roof = {"bound": "hbm", "kernel": dom["kernel"], "achieved": achieved, "peak": peak, "unit": "GB/s",
+                    "frac": achieved / peak, "peak_source": peak_kind, "algorithmic_bytes_per_cell": dom["bytes_per_cell"],
+                    "avg_ms": dom["avg_ms"], "traffic": None}
         line = {
             "metric": METRIC,
-            "value": value,
+            "value": arm["value"],
             "unit": UNIT,
             "n_gpus": world,
             "steps": args.steps,
             "warmup": args.warmup,
-            "ms_per_step": total_ms_max / args.steps,
+            "ms_per_step": arm["ms_per_step"],
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
@@ -353,37 +438,41 @@ def run_b200(args, world, rank, local):
             "config": {
                 "workload": w.name, "nx": w.grid.nx, "ny": w.grid.ny, "dx_m": w.grid.dx,
                 "scheme": "fifth order + SGN" if w.dispersion else "second order SWE",
-                "preconditioner": "jacobi (plain PCG)" if w.dispersion else None,
+                "preconditioner": ("learned (gated linear U-net in a two-level cycle, flexible CG)" if learned
+                                   else "jacobi (plain PCG)") if w.dispersion else None,
                 "tolerance": w.dispersion.tolerance if w.dispersion else None,
-                "pcg_iterations_per_solve": iters,
+                "pcg_iterations_per_solve": arm["iterations_per_solve"],
+                "unconverged_solves": arm["unconverged"],
                 "l2": "flushed between timed steps (256 MiB write outside the timed events)",
                 "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                 **{k: v for k, v in w.meta.items() if k != "bed"},
             },
-            "roofline": {
-                "bound": "hbm",
-                "kernel": dom["kernel"],
-                "achieved": achieved,
-                "peak": peak,
-                "unit": "GB/s",
-                "frac": achieved / peak,
-                "peak_source": peak_kind,
-                "algorithmic_bytes_per_cell": dom["bytes_per_cell"],
-                "traffic": None,
-            },
+            "roofline": roof,
             "kernel_ms_per_step": {"stage": stage_ms / args.steps, "solve": solve_ms / args.steps,
-                                   "other": prof["other"][1] / args.steps,
-                                   "source": "profiled pass of the same number of steps after the timed pass"},
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 3 * npad * 8,
-                    "d2h_bytes_per_step": 3 * npad * 8, "steps": n_e2e,
-                    "path": "wc_step on pinned host FP64 arrays (upload, step, download per call)"},
-            "gpu_launches": int(launches),
-            "clocks": ck,
+                                   "network": net_ms / args.steps, "other": prof["other"][1] / args.steps,
+                                   "source": "profiled pass of the same number of steps after the timed pass "
+                                             "(direct launches; the learned solve syncs with the host every 4 iterations there)"},
+            "e2e": arm["e2e"],
+            "gpu_launches": arm["launches"],
+            "clocks": arm["clocks"],
         }
+        if learned:
+            line["plain_pcg"] = {
+                "value": plain["value"], "ms_per_step": plain["ms_per_step"],
+                "iterations_per_solve": plain["iterations_per_solve"], "unconverged_solves": plain["unconverged"],
+                "e2e": plain["e2e"]["value"], "gpu_launches": plain["launches"], "clocks": plain["clocks"],
+                "kernel_ms_per_step": {k: v[1] / args.steps for k, v in plain["prof"].items()},
+            }
+            line["learned_vs_plain"] = arm["value"] / plain["value"]
+            line["training"] = train_rec
+            if args.eta_steps > 0:
+                line["eta_max_abs_err_vs_fp64_oracle_m"] = eta_errors(w, net, args.eta_steps)
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(w, args.cpu_steps)
         print(json.dumps(line), flush=True)
-    if dist:
+    if world > 1:
+        import torch.distributed as dist
+
         dist.barrier()
         dist.destroy_process_group()
     return line
@@ -395,7 +484,11 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="config2", choices=["config1", "config2", "config3", "config4"])
+    ap.add_argument("--workload", default="config3", choices=["config1", "config2", "config3", "config4"])
+    ap.add_argument("--pc", default="learned", choices=["learned", "jacobi"],
+                    help="learned: time the learned preconditioner and plain PCG side by side (SGN workloads)")
+    ap.add_argument("--train-steps", type=int, default=3000)
+    ap.add_argument("--eta-steps", type=int, default=10)
     ap.add_argument("--cpu-steps", type=int, default=40)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

@@ -196,13 +196,16 @@ wc_status wc_set_stream(wc_solver* s, void* stream);
 /* Per-kernel device timing (no counterpart in the reference). While enabled, every launch of
  * the step is bracketed by CUDA events on the solver's stream; wc_profile_read synchronises and
  * returns, per kernel kind, the launch count and the summed device milliseconds since the last
- * enable. Kinds: 0 = RK-stage stencil kernel, 1 = dispersive solve kernel, 2 = other. */
+ * enable. Kinds: 0 = RK-stage stencil kernel, 1 = dispersive solve (for the learned
+ * preconditioner: its vector kernels and the stage epilogue), 2 = other, 3 = the learned
+ * preconditioner's network (one count per application). */
 typedef struct wc_kernel_time {
     uint64_t launches;
     double total_ms;
 } wc_kernel_time;
+#define WC_KERNEL_KINDS 4
 wc_status wc_profile_enable(wc_solver* s, int32_t on);
-wc_status wc_profile_read(wc_solver* s, wc_kernel_time out[3]);
+wc_status wc_profile_read(wc_solver* s, wc_kernel_time out[WC_KERNEL_KINDS]);
 
 /* No counterpart in the reference: wc_stable_dt for callers that cannot allocate device memory
  * when they need the time step, such as code running while a CUDA stream capture is open (where

@@ -115,7 +115,7 @@ class wc_kernel_time(C.Structure):
     _fields_ = [("launches", C.c_uint64), ("total_ms", C.c_double)]
 
 
-KERNEL_KINDS = ("stage", "solve", "other")
+KERNEL_KINDS = ("stage", "solve", "other", "network")
 
 DPTR = C.POINTER(C.c_double)
 

@@ -392,11 +392,18 @@ wc_status fcg_body(wc_solver* s, cudaStream_t st, cudaGraphConditionalHandle h, 
     float2 *z = s->p1, *p = s->p0, *q = s->ap;
     const int hp = s->lpc_hp, wp = s->lpc_wp;
     const size_t plane = (size_t)hp * wp;
-    FCG_LAUNCH(lpc_jacobi_kernel<<<nb, 256, 0, st>>>(g, s->r, s->diag, z, LPC_OMEGA, sc));
-    FCG_LAUNCH(fcg_matvec_kernel<<<nb, 256, 0, st>>>(g, z, s->cc, s->heff, s->tv, sc));
-    FCG_LAUNCH(lpc_input_kernel<<<ew_grid(plane), 256, 0, st>>>(g, s->r, s->tv, s->diag, s->lnet.X[0].p, hp, wp, sc));
-    CK(s->lnet.forward(st, false));
-    s->launches += 2 * LPC_LEVELS + 2 * (LPC_LEVELS - 1) + 1;
+    {
+        ProfScope ps(s, 1);
+        FCG_LAUNCH(lpc_jacobi_kernel<<<nb, 256, 0, st>>>(g, s->r, s->diag, z, LPC_OMEGA, sc));
+        FCG_LAUNCH(fcg_matvec_kernel<<<nb, 256, 0, st>>>(g, z, s->cc, s->heff, s->tv, sc));
+        FCG_LAUNCH(lpc_input_kernel<<<ew_grid(plane), 256, 0, st>>>(g, s->r, s->tv, s->diag, s->lnet.X[0].p, hp, wp, sc));
+    }
+    {
+        ProfScope ps(s, 3);
+        CK(s->lnet.forward(st, false));
+        s->launches += 2 * LPC_LEVELS + 2 * (LPC_LEVELS - 1) + 1;
+    }
+    ProfScope ps(s, 1);
     FCG_LAUNCH(lpc_correct_kernel<<<nb, 256, 0, st>>>(g, z, s->lnet.Y.p, s->heff, z, hp, wp, sc));
     FCG_LAUNCH(fcg_matvec_kernel<<<nb, 256, 0, st>>>(g, z, s->cc, s->heff, s->tv, sc));
     FCG_LAUNCH(lpc_post_kernel<<<nb, 256, 0, st>>>(g, z, s->r, s->tv, s->diag, z, LPC_OMEGA, sc));
@@ -421,8 +428,10 @@ wc_status launch_fcg(wc_solver* s, int mode, const float4* qold, float4* qout) {
         CK(cudaGraphConditionalHandleCreate(&h, cg, 0, cudaGraphCondAssignDefault));
     }
     {
-        ProfScope ps(s, 1);
-        TRY(fcg_pre(s, st, h, graph ? 1 : 0));
+        {
+            ProfScope ps(s, 1);
+            TRY(fcg_pre(s, st, h, graph ? 1 : 0));
+        }
         if (graph) {
             cudaGraph_t cg = nullptr;
             const cudaGraphNode_t* deps = nullptr;
@@ -826,10 +835,10 @@ wc_status wc_profile_enable(wc_solver* s, int32_t on) {
     return WC_OK;
 }
 
-wc_status wc_profile_read(wc_solver* s, wc_kernel_time out[3]) {
+wc_status wc_profile_read(wc_solver* s, wc_kernel_time out[WC_KERNEL_KINDS]) {
     if (!s || !out) return set_err(WC_EINVAL, "null argument");
     CK(cudaStreamSynchronize(s->stream));
-    for (int k = 0; k < 3; k++) out[k] = wc_kernel_time{0, 0.0};
+    for (int k = 0; k < WC_KERNEL_KINDS; k++) out[k] = wc_kernel_time{0, 0.0};
     for (auto& e : s->prof_live) {
         float ms = 0.f;
         CK(cudaEventElapsedTime(&ms, e.a, e.b));

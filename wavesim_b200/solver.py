@@ -280,9 +280,9 @@ class Solver(SolverConfig):
 
     def profile_read(self) -> dict:
         """{kind: (launches, total device ms)} since profiling was enabled."""
-        out = (abi.wc_kernel_time * 3)()
+        out = (abi.wc_kernel_time * len(abi.KERNEL_KINDS))()
         _check(load().wc_profile_read(self._h(), out))
-        return {abi.KERNEL_KINDS[k]: (int(out[k].launches), float(out[k].total_ms)) for k in range(3)}
+        return {abi.KERNEL_KINDS[k]: (int(out[k].launches), float(out[k].total_ms)) for k in range(len(abi.KERNEL_KINDS))}
 
     def synchronize(self) -> None:
         _check(load().wc_synchronize(self._h()))
