@@ -284,6 +284,13 @@ wc_status wc_lpc_set_rounding(wc_lpc* l, int32_t bf16);
 wc_status wc_lpc_forward_backward(wc_lpc* l, int32_t n, int32_t h, int32_t w, const float* x,
                                   const float* feat, const float* dy, float* y, float* grad,
                                   float* dx);
+/* The training objective on given patches, for checking its gradient: c, heff and bed are
+ * [n][h][w] (the mask h >= 5 cm and the features h / 20 m, b / 20 m are derived as for harvested
+ * crops), e the error fields [n][2][h][w]; returns the loss (as wc_lpc_train defines it) and its
+ * gradient with respect to the parameters (num_params values). */
+wc_status wc_lpc_loss_grad(wc_lpc* l, int32_t n, int32_t h, int32_t w, const float* c,
+                           const float* heff, const float* bed, const float* e, double dx, double dy,
+                           double* loss, float* grad);
 /* Copies the solver's current SGN system (c, h, bed; the one of its last solve) for training. */
 wc_status wc_lpc_harvest(wc_lpc* l, wc_solver* s);
 uint64_t wc_lpc_num_systems(const wc_lpc* l);

@@ -170,3 +170,65 @@ def backward(spec: UNetSpec, params, cache, dy):
         if b >= 0:
             flat[b : b + co] = gb
     return flat, dx
+
+
+# ---- the training objective: the two-level cycle on patches ------------------------------------
+
+H_DISP_MIN = 0.05
+
+
+def _shift(a, dy, dx):
+    """out[..., y, x] = a[..., y + dy, x + dx], zero outside."""
+    out = np.zeros_like(a)
+    h, w = a.shape[-2:]
+    ys, yd = (slice(dy, h), slice(0, h - dy)) if dy >= 0 else (slice(0, h + dy), slice(-dy, h))
+    xs, xd = (slice(dx, w), slice(0, w - dx)) if dx >= 0 else (slice(0, w + dx), slice(-dx, w))
+    out[..., yd, xd] = a[..., ys, xs]
+    return out
+
+
+def patch_matvec(c, heff, mask, p, dx, dy):
+    """A p of crates/wavecore/src/dispersion.rs:269-317 on patches (N, H, W), zero outside."""
+    ix, iy = 0.5 / dx, 0.5 / dy
+    px, py = p[:, 0], p[:, 1]
+    f = c * ((_shift(px, 0, 1) - _shift(px, 0, -1)) * ix + (_shift(py, 1, 0) - _shift(py, -1, 0)) * iy)
+    ax = mask * (heff * px - (_shift(f, 0, 1) - _shift(f, 0, -1)) * ix)
+    ay = mask * (heff * py - (_shift(f, 1, 0) - _shift(f, -1, 0)) * iy)
+    return np.stack([ax, ay], axis=1)
+
+
+def patch_diag(c, heff, mask, dx, dy):
+    """The Jacobi diagonal (dispersion.rs:441-457) on patches; 1 where the mask is off."""
+    dxv = np.where(mask > 0, heff + (_shift(c, 0, 1) + _shift(c, 0, -1)) * 0.25 / (dx * dx), 1.0)
+    dyv = np.where(mask > 0, heff + (_shift(c, 1, 0) + _shift(c, -1, 0)) * 0.25 / (dy * dy), 1.0)
+    return np.stack([dxv, dyv], axis=1)
+
+
+def cycle_loss_grad(spec: UNetSpec, params, c, heff, bed, e, dx, dy, omega):
+    """Loss mean_n <d, A d>_n / <e, A e>_n of the cycle z = M A e (d = e - z) and its gradient
+    with respect to the flat parameters. c, heff, bed: (N, H, W); e: (N, 2, H, W). A patch
+    without a wet cell (<e, A e> = 0) contributes nothing."""
+    c, heff, bed, e = (np.asarray(a, dtype=np.float64) for a in (c, heff, bed, e))
+    mask = (heff >= H_DISP_MIN).astype(np.float64)
+    feat = np.stack([heff / 20.0, bed / 20.0], axis=1)
+    A = lambda v: patch_matvec(c, heff, mask, v, dx, dy)  # noqa: E731
+    D = patch_diag(c, heff, mask, dx, dy)
+    m2 = mask[:, None]
+    r = A(e)
+    z1 = omega * r / D
+    x = (r - A(z1)) / D
+    y, cache = forward(spec, params, x, feat)
+    z2 = z1 + m2 * y
+    z = z2 + omega * (r - A(z2)) / D
+    d = e - z
+    ad = A(d)
+    n = e.shape[0]
+    num = np.einsum("nchw,nchw->n", d, ad)
+    den = np.einsum("nchw,nchw->n", e, r)
+    ok = den > 0.0
+    safe = np.where(ok, den, 1.0)
+    loss = float(np.sum(np.where(ok, num / safe, 0.0)) / n)
+    gz = np.where(ok[:, None, None, None], -2.0 * ad / (n * safe[:, None, None, None]), 0.0)
+    gz2 = gz - omega * A(gz / D)
+    grads, _ = backward(spec, params, cache, m2 * gz2)
+    return loss, grads

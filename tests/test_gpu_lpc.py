@@ -76,6 +76,34 @@ def test_forward_uses_bf16_rounded_weights():
     assert np.array_equal(net.get_params(), p)  # the master weights stay FP32
 
 
+def test_training_loss_and_gradient_match_the_fp64_oracle():
+    # The whole training objective (the cycle on patches, the energy-norm loss) and its gradient
+    # through the cycle and the network, against the FP64 oracle (FP32 weights on both sides).
+    from wavesim_b200.lpc import OMEGA
+
+    spec = UNetSpec()
+    net = LearnedPreconditioner(spec)
+    net.set_rounding(False)
+    p = random_params(spec, 7)
+    net.set_params(p)
+    rng = np.random.default_rng(8)
+    n, h, w = 3, 32, 40
+    depth = rng.uniform(-0.3, 8.0, (n, h, w)).astype(np.float32)
+    depth[2] = -1.0  # an all-dry patch contributes nothing
+    heff = np.maximum(depth, 1e-8).astype(np.float32)
+    c = np.where(depth < 0.05, 0.0, depth**3 / 3.0).astype(np.float32)
+    bed = (-depth).astype(np.float32)
+    e = (rng.normal(size=(n, 2, h, w)) * (heff >= 0.05)[:, None]).astype(np.float32)
+    loss, g = net.loss_grad(c, heff, bed, e, 2.0, 2.0)
+    lo, go = U.cycle_loss_grad(spec, p.astype(np.float64), c, heff, bed, e, 2.0, 2.0, OMEGA)
+    assert abs(loss - lo) < 1e-5 * abs(lo)
+    for name, (wo, b, co, ci, k) in spec.offsets().items():
+        m = co * ci * k * k
+        assert rel(g[wo : wo + m], go[wo : wo + m]) < 2e-4, name
+        if b >= 0:
+            assert rel(g[b : b + co], go[b : b + co]) < 2e-4, name + " bias"
+
+
 def small_run(seed=11, nx=192, ny=96, tol=1e-8):
     w = W.sgn_beach(nx, ny, 2.0, seed=seed, tolerance=tol, name=f"lpc_{nx}x{ny}")
     return w, W.wave_train_state(w)
@@ -125,7 +153,7 @@ def test_training_lowers_the_loss():
     losses = net.train(300, batch=8, patch=64, lr=2e-3, seed=1)
     assert before.size == 0 and np.all(np.isfinite(losses))
     first, last = losses[:20].mean(), losses[-20:].mean()
-    assert last < 0.8 * first, (first, last)
+    assert last < 0.5 * first, (first, last)
 
 
 def test_trained_network_needs_fewer_iterations_than_jacobi():

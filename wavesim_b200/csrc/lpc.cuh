@@ -25,7 +25,9 @@ struct ConvArgs {
     int co, H, W, N, act;
 };
 
-constexpr int CV_T = 16;   // output tile edge
+constexpr int CV_TH = 16;  // threads per tile edge (16 x 16 = 256 threads)
+constexpr int CV_P = 2;    // output pixels per thread along each axis (2 x 2)
+constexpr int CV_T = CV_TH * CV_P;  // output tile edge (32)
 constexpr int CV_COB = 8;  // output channels per block
 constexpr int CV_CIB = 4;  // input channels staged per pass
 
@@ -44,55 +46,81 @@ __device__ __forceinline__ float conv_input(const ConvArgs& p, int n, int c, int
     return p.b[(((size_t)n * p.cb + (c - p.ca)) * p.H + y) * p.W + x];
 }
 
+// Direct convolution, register-blocked: a block computes a 32 x 32 tile of 8 output channels;
+// each thread a 2 x 2 patch of all 8, from a (2 + K - 1)^2 window of every staged input channel
+// held in registers and the 8 weights of a tap read as two float4 (broadcast).
 template <int K>
-__global__ void __launch_bounds__(CV_T* CV_T) conv_fwd_kernel(ConvArgs p) {
-    constexpr int R = K / 2, TE = CV_T + 2 * R;
-    __shared__ float tile[CV_CIB][TE][TE];
-    __shared__ float wsm[CV_COB][CV_CIB][K * K];
+__global__ void __launch_bounds__(CV_TH* CV_TH) conv_fwd_kernel(ConvArgs p) {
+    constexpr int R = K / 2, TE = CV_T + 2 * R, WIN = CV_P + K - 1;
+    __shared__ float tile[CV_CIB][TE][TE + 1];
+    __shared__ __align__(16) float wsm[CV_CIB][K * K][CV_COB];
     const int ncog = (p.co + CV_COB - 1) / CV_COB;
     const int n = blockIdx.z / ncog, cog = blockIdx.z % ncog;
     const int x0 = blockIdx.x * CV_T, y0 = blockIdx.y * CV_T;
-    const int tx = threadIdx.x % CV_T, ty = threadIdx.x / CV_T;
+    const int tx = threadIdx.x % CV_TH, ty = threadIdx.x / CV_TH;
     const int ci_total = p.ca + p.cb;
-    float acc[CV_COB];
+    float acc[CV_P][CV_P][CV_COB];
 #pragma unroll
-    for (int o = 0; o < CV_COB; o++) acc[o] = 0.f;
+    for (int a = 0; a < CV_P; a++)
+#pragma unroll
+        for (int b = 0; b < CV_P; b++)
+#pragma unroll
+            for (int o = 0; o < CV_COB; o++) acc[a][b][o] = 0.f;
     for (int c0 = 0; c0 < ci_total; c0 += CV_CIB) {
-        for (int q = threadIdx.x; q < CV_CIB * TE * TE; q += CV_T * CV_T) {
+        for (int q = threadIdx.x; q < CV_CIB * TE * TE; q += CV_TH * CV_TH) {
             const int c = q / (TE * TE), r = q % (TE * TE);
             const int yy = y0 + r / TE - R, xx = x0 + r % TE - R;
             tile[c][r / TE][r % TE] = (c0 + c < ci_total) ? conv_input(p, n, c0 + c, yy, xx) : 0.f;
         }
-        for (int q = threadIdx.x; q < CV_COB * CV_CIB * K * K; q += CV_T * CV_T) {
-            const int o = q / (CV_CIB * K * K), r = q % (CV_CIB * K * K);
+        for (int q = threadIdx.x; q < CV_COB * CV_CIB * K * K; q += CV_TH * CV_TH) {
+            const int o = q % CV_COB, r = q / CV_COB;
             const int c = r / (K * K), t = r % (K * K);
             const int co = cog * CV_COB + o, ci = c0 + c;
-            wsm[o][c][t] = (co < p.co && ci < ci_total) ? p.w[((size_t)co * ci_total + ci) * K * K + t] : 0.f;
+            wsm[c][t][o] = (co < p.co && ci < ci_total) ? p.w[((size_t)co * ci_total + ci) * K * K + t] : 0.f;
         }
         __syncthreads();
 #pragma unroll
-        for (int c = 0; c < CV_CIB; c++)
+        for (int c = 0; c < CV_CIB; c++) {
+            float win[WIN][WIN];
+#pragma unroll
+            for (int a = 0; a < WIN; a++)
+#pragma unroll
+                for (int b = 0; b < WIN; b++) win[a][b] = tile[c][CV_P * ty + a][CV_P * tx + b];
 #pragma unroll
             for (int t = 0; t < K * K; t++) {
-                const float v = tile[c][ty + t / K][tx + t % K];
+                const float4 w0 = *reinterpret_cast<const float4*>(&wsm[c][t][0]);
+                const float4 w1 = *reinterpret_cast<const float4*>(&wsm[c][t][4]);
+                const float wv[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
 #pragma unroll
-                for (int o = 0; o < CV_COB; o++) acc[o] = fmaf(v, wsm[o][c][t], acc[o]);
+                for (int a = 0; a < CV_P; a++)
+#pragma unroll
+                    for (int b = 0; b < CV_P; b++) {
+                        const float v = win[a + t / K][b + t % K];
+#pragma unroll
+                        for (int o = 0; o < CV_COB; o++) acc[a][b][o] = fmaf(v, wv[o], acc[a][b][o]);
+                    }
             }
+        }
         __syncthreads();
     }
-    const int x = x0 + tx, y = y0 + ty;
-    if (x >= p.W || y >= p.H) return;
 #pragma unroll
-    for (int o = 0; o < CV_COB; o++) {
-        const int co = cog * CV_COB + o;
-        if (co >= p.co) break;
-        float v = acc[o] + (p.bias ? p.bias[co] : 0.f);
-        if (p.act == ACT_RELU) v = fmaxf(v, 0.f);
-        else if (p.act == ACT_SIG2) v = 2.f / (1.f + expf(-v));
-        const size_t k = (((size_t)n * p.co + co) * p.H + y) * p.W + x;
-        if (p.gate) v *= p.gate[k];
-        p.y[k] = v;
-    }
+    for (int a = 0; a < CV_P; a++)
+#pragma unroll
+        for (int b = 0; b < CV_P; b++) {
+            const int x = x0 + CV_P * tx + b, y = y0 + CV_P * ty + a;
+            if (x >= p.W || y >= p.H) continue;
+#pragma unroll
+            for (int o = 0; o < CV_COB; o++) {
+                const int co = cog * CV_COB + o;
+                if (co >= p.co) break;
+                float v = acc[a][b][o] + (p.bias ? p.bias[co] : 0.f);
+                if (p.act == ACT_RELU) v = fmaxf(v, 0.f);
+                else if (p.act == ACT_SIG2) v = 2.f / (1.f + expf(-v));
+                const size_t k = (((size_t)n * p.co + co) * p.H + y) * p.W + x;
+                if (p.gate) v *= p.gate[k];
+                p.y[k] = v;
+            }
+        }
 }
 
 // dw[co][ci][t] = sum over samples and pixels of dy[co] * x[ci] shifted by tap t; one block per
@@ -299,13 +327,14 @@ __global__ void sample_dot_kernel(const float* __restrict__ a, const float* __re
     }
 }
 
-// grad = -2 / (N E_n) * Ad  (the gradient of mean_n <d, A d>_n / E_n with respect to z, d = e - z)
+// grad = -2 / (N E_n) * Ad  (the gradient of mean_n <d, A d>_n / E_n with respect to z, d = e - z;
+// a patch without a wet cell has E_n = 0 and contributes nothing)
 __global__ void loss_grad_kernel(const float* __restrict__ ad, const double* __restrict__ energy, int N,
                                  size_t per_sample, float* __restrict__ g) {
     const size_t total = (size_t)N * per_sample;
     for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
         const int n = (int)(q / per_sample);
-        g[q] = (float)(-2.0 / ((double)N * energy[n])) * ad[q];
+        g[q] = energy[n] > 0.0 ? (float)(-2.0 / ((double)N * energy[n])) * ad[q] : 0.f;
     }
 }
 

@@ -177,8 +177,8 @@ struct LpcNet {
         p.N = N;
         p.act = act;
         dim3 grid((p.W + CV_T - 1) / CV_T, (p.H + CV_T - 1) / CV_T, N * ((L.co + CV_COB - 1) / CV_COB));
-        if (L.k == 3) conv_fwd_kernel<3><<<grid, CV_T * CV_T, 0, st>>>(p);
-        else conv_fwd_kernel<1><<<grid, CV_T * CV_T, 0, st>>>(p);
+        if (L.k == 3) conv_fwd_kernel<3><<<grid, CV_TH * CV_TH, 0, st>>>(p);
+        else conv_fwd_kernel<1><<<grid, CV_TH * CV_TH, 0, st>>>(p);
         return cudaGetLastError();
     }
 
@@ -329,9 +329,9 @@ inline cudaError_t LpcNet::accumulate(float* y, const float* x, size_t n, cudaSt
 
 // A patch of a harvested system: c, heff and the bed cropped into the batch tensors, the mask
 // (h >= 5 cm) and the features (h / H0, b / H0).
-__global__ void crop_kernel(const float* __restrict__ c, const float* __restrict__ heff, const float* __restrict__ bed,
-                            int pitch, int x0, int y0, int H, int W, float* __restrict__ oc, float* __restrict__ oheff,
-                            float* __restrict__ omask, float* __restrict__ ofeat) {
+// (c may be oc and heff oheff: every element is read before it is written.)
+__global__ void crop_kernel(const float* c, const float* heff, const float* __restrict__ bed, int pitch, int x0, int y0,
+                            int H, int W, float* oc, float* oheff, float* __restrict__ omask, float* __restrict__ ofeat) {
     const int plane = H * W;
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < plane; q += gridDim.x * blockDim.x) {
         const int y = q / W, x = q % W;
@@ -402,7 +402,7 @@ inline void fld(float* out, const float* x, float ax, const float* y, float ay, 
 __global__ void lpc_loss_kernel(const double* __restrict__ sums, int N, double* __restrict__ out) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     double l = 0.0;
-    for (int n = 0; n < N; n++) l += sums[n] / fmax(sums[N + n], 1e-300);
+    for (int n = 0; n < N; n++) l += sums[N + n] > 0.0 ? sums[n] / sums[N + n] : 0.0;  // all-dry patch: 0
     *out = l / N;
 }
 
@@ -449,16 +449,19 @@ struct LpcModel {
         return rng;
     }
 
-    // One step of training: N patches of H x W from random systems and offsets, one random error
-    // field each, the loss mean_n <d, A d>_n / <e, A e>_n of the cycle's error d = e - M A e, its
-    // gradient through the cycle and the network, an Adam update.
-    cudaError_t train_step(int N, int H, int W, float lr, double* loss_slot, float rough) {
+    cudaError_t shape_batch(int N, int H, int W) {
         cudaError_t e;
         if (tr.N != N || tr.H != H || tr.W != W)
             if ((e = tr.shape(N, H, W)) != cudaSuccess) return e;
-        if ((e = net.shape(N, H, W, true)) != cudaSuccess) return e;
+        return net.shape(N, H, W, true);
+    }
+
+    // A training batch: N patches of H x W from random systems and offsets (all of one grid
+    // spacing), one random error field each.
+    cudaError_t sample_batch(int N, int H, int W, float rough) {
+        cudaError_t e;
+        if ((e = shape_batch(N, H, W)) != cudaSuccess) return e;
         const size_t plane = (size_t)H * W, per = 2 * plane;
-        // one grid spacing per batch: the systems of a random one's spacing
         const LpcSystem* s0 = systems[next() % systems.size()];
         std::vector<const LpcSystem*> pool;
         for (auto* q : systems)
@@ -474,10 +477,19 @@ struct LpcModel {
         }
         tr.dx = s0->dx;
         tr.dy = s0->dy;
+        random_field_kernel<<<ew_grid((size_t)N * per), 256, 0, st>>>(tr.e.p, tr.mask.p, N, H, W, next(), rough);
+        return cudaGetLastError();
+    }
+
+    // The loss mean_n <d, A d>_n / <e, A e>_n of the cycle's error d = e - M A e on the batch in
+    // tr (c, heff, mask, e) and net.F[0] (features), into *loss_slot; with `grad`, its gradient
+    // through the cycle and the network into g.
+    cudaError_t loss_grad(double* loss_slot, bool grad) {
+        cudaError_t e;
+        const int N = tr.N, H = tr.H, W = tr.W;
+        const size_t plane = (size_t)H * W, per = 2 * plane, tot = (size_t)N * per;
         const PatchOp op = tr.op();
-        const size_t tot = (size_t)N * per;
         const float om = LPC_OMEGA;
-        random_field_kernel<<<ew_grid(tot), 256, 0, st>>>(tr.e.p, tr.mask.p, N, H, W, next(), rough);
         patch_matvec_kernel<<<ew_grid(N * plane), 256, 0, st>>>(op, tr.e.p, tr.r.p);   // r = A e
         patch_diag_kernel<<<ew_grid(N * plane), 256, 0, st>>>(op, tr.dg.p);
         fld(tr.z1.p, nullptr, 0.f, tr.r.p, om, tr.dg.p, nullptr, N, plane, st);       // z1 = w r / D
@@ -497,7 +509,7 @@ struct LpcModel {
         sample_dot_kernel<<<dg, 256, 0, st>>>(tr.dd.p, tr.ad.p, per, tr.sums);
         sample_dot_kernel<<<dg, 256, 0, st>>>(tr.e.p, tr.r.p, per, tr.sums + N);
         lpc_loss_kernel<<<1, 32, 0, st>>>(tr.sums, N, loss_slot);
-        if (lr <= 0.f) return cudaGetLastError();
+        if (!grad) return cudaGetLastError();
         // dL/dz = -2 A d / (N E_n); through z = z2 + w (r - A z2) / D: dz2 = dz - w A (dz / D);
         // through z2 = z1 + m Y: dY = m dz2.
         loss_grad_kernel<<<ew_grid(tot), 256, 0, st>>>(tr.ad.p, tr.sums + N, N, per, tr.gz.p);
@@ -507,6 +519,10 @@ struct LpcModel {
         fld(tr.gz2.p, nullptr, 0.f, tr.gz2.p, 1.f, nullptr, tr.mask.p, N, plane, st);
         cudaMemsetAsync(g.p, 0, g.n * sizeof(float), st);
         if ((e = net.backward(tr.gz2.p, nullptr, st)) != cudaSuccess) return e;
+        return cudaGetLastError();
+    }
+
+    cudaError_t adam_step(float lr) {
         adam_t += 1;
         const float b1 = 0.9f, b2 = 0.999f;
         const float c1 = (float)(1.0 / (1.0 - pow((double)b1, adam_t)));
@@ -514,6 +530,14 @@ struct LpcModel {
         adam_kernel<<<ew_grid(net.nparams), 256, 0, st>>>(w.p, wq.p, g.p, m.p, v.p, net.nparams, lr, b1, b2, c1, c2,
                                                           1e-8f, round_bf16);
         return cudaGetLastError();
+    }
+
+    // One step of training: a batch, the loss and its gradient, an Adam update.
+    cudaError_t train_step(int N, int H, int W, float lr, double* loss_slot, float rough) {
+        cudaError_t e;
+        if ((e = sample_batch(N, H, W, rough)) != cudaSuccess) return e;
+        if ((e = loss_grad(loss_slot, lr > 0.f)) != cudaSuccess) return e;
+        return lr > 0.f ? adam_step(lr) : cudaSuccess;
     }
 };
 

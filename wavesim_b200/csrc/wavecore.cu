@@ -1598,6 +1598,43 @@ wc_status wc_lpc_train(wc_lpc* l, uint32_t steps, uint32_t batch, uint32_t patch
     return lpc_ck(cudaStreamSynchronize(m.st), "train");
 }
 
+wc_status wc_lpc_loss_grad(wc_lpc* l, int32_t n, int32_t h, int32_t w, const float* c, const float* heff,
+                           const float* bed, const float* e, double dx, double dy, double* loss, float* grad) {
+    if (!l || !c || !heff || !bed || !e || !loss || !grad) return set_err(WC_EINVAL, "null argument");
+    const int div = 1 << (LPC_LEVELS - 1);
+    if (n < 1 || h < div || w < div || h % div || w % div)
+        return set_err(WC_EINVAL, "batch must be >= 1 and patch sides positive multiples of 8");
+    if (!(dx > 0.0 && dy > 0.0)) return set_err(WC_EINVAL, "cell size must be positive");
+    LpcModel& m = l->m;
+    cudaStream_t st = m.st;
+    TRY(lpc_ck(m.shape_batch(n, h, w), "activations"));
+    const size_t plane = (size_t)n * h * w;
+    DBuf dbed;
+    TRY(lpc_ck(dbed.alloc(plane), "alloc"));
+    TRY(lpc_ck(cudaMemcpyAsync(m.tr.c.p, c, plane * sizeof(float), cudaMemcpyHostToDevice, st), "upload"));
+    TRY(lpc_ck(cudaMemcpyAsync(m.tr.heff.p, heff, plane * sizeof(float), cudaMemcpyHostToDevice, st), "upload"));
+    TRY(lpc_ck(cudaMemcpyAsync(dbed.p, bed, plane * sizeof(float), cudaMemcpyHostToDevice, st), "upload"));
+    TRY(lpc_ck(cudaMemcpyAsync(m.tr.e.p, e, 2 * plane * sizeof(float), cudaMemcpyHostToDevice, st), "upload"));
+    for (int k = 0; k < n; k++) {  // mask and features of each patch, as the crops make them
+        const size_t hw = (size_t)h * w;
+        crop_kernel<<<ew_grid(hw), 256, 0, st>>>(m.tr.c.p + k * hw, m.tr.heff.p + k * hw, dbed.p + k * hw, w, 0, 0, h, w,
+                                                 m.tr.c.p + k * hw, m.tr.heff.p + k * hw, m.tr.mask.p + k * hw,
+                                                 m.net.F[0].p + 2 * k * hw);
+    }
+    m.tr.dx = (float)dx;
+    m.tr.dy = (float)dy;
+    double* dl = nullptr;
+    TRY(lpc_ck(cudaMalloc(&dl, sizeof(double)), "alloc"));
+    wc_status stt = lpc_ck(m.loss_grad(dl, true), "loss_grad");
+    if (stt == WC_OK) stt = lpc_ck(cudaMemcpyAsync(loss, dl, sizeof(double), cudaMemcpyDeviceToHost, st), "download");
+    if (stt == WC_OK)
+        stt = lpc_ck(cudaMemcpyAsync(grad, m.g.p, (size_t)m.net.nparams * sizeof(float), cudaMemcpyDeviceToHost, st),
+                     "download");
+    if (stt == WC_OK) stt = lpc_ck(cudaStreamSynchronize(st), "loss_grad");
+    cudaFree(dl);
+    return stt;
+}
+
 wc_status wc_solver_set_lpc(wc_solver* s, wc_lpc* l) {
     if (!s) return set_err(WC_EINVAL, "null solver");
     if (!s->sgn) return set_err(WC_EINVAL, "the solver has no dispersive solve");

@@ -65,6 +65,7 @@ EXPORTS = [
     "wc_lpc_get_params",
     "wc_lpc_set_rounding",
     "wc_lpc_forward_backward",
+    "wc_lpc_loss_grad",
     "wc_lpc_harvest",
     "wc_lpc_num_systems",
     "wc_lpc_train",
@@ -136,13 +137,15 @@ def load(path: str = LIB_PATH):
     L.wc_lpc_get_params.argtypes = [V, F, C.c_uint64]
     L.wc_lpc_set_rounding.argtypes = [V, C.c_int32]
     L.wc_lpc_forward_backward.argtypes = [V, C.c_int32, C.c_int32, C.c_int32, F, F, F, F, F, F]
+    L.wc_lpc_loss_grad.argtypes = [V, C.c_int32, C.c_int32, C.c_int32, F, F, F, F, C.c_double, C.c_double, D, F]
     L.wc_lpc_harvest.argtypes = [V, V]
     L.wc_lpc_num_systems.argtypes = [V]
     L.wc_lpc_num_systems.restype = C.c_uint64
     L.wc_lpc_train.argtypes = [V, C.c_uint32, C.c_uint32, C.c_uint32, C.c_float, C.c_float, C.c_uint64, D]
     L.wc_solver_set_lpc.argtypes = [V, V]
     for name in ("wc_lpc_create", "wc_lpc_set_params", "wc_lpc_get_params", "wc_lpc_set_rounding",
-                 "wc_lpc_forward_backward", "wc_lpc_harvest", "wc_lpc_train", "wc_solver_set_lpc"):
+                 "wc_lpc_forward_backward", "wc_lpc_loss_grad", "wc_lpc_harvest", "wc_lpc_train",
+                 "wc_solver_set_lpc"):
         getattr(L, name).restype = C.c_int
     L.wc_launch_count.argtypes = [V]
     L.wc_launch_count.restype = C.c_uint64
@@ -371,6 +374,18 @@ class LearnedPreconditioner:
         _check(load().wc_lpc_forward_backward(self._handle, n, h, w, _fptr(x), _fptr(feat), _fptr(dy), _fptr(y),
                                               _fptr(g), _fptr(dx)))
         return y, g, dx
+
+    def loss_grad(self, c, heff, bed, e, dx: float, dy: float):
+        """The training loss of patches (c, heff, bed: [n][h][w]; error fields e: [n][2][h][w])
+        and its parameter gradient."""
+        c, heff, bed, e = (np.ascontiguousarray(a, dtype=np.float32) for a in (c, heff, bed, e))
+        n, h, w = c.shape
+        assert heff.shape == c.shape and bed.shape == c.shape and e.shape == (n, 2, h, w)
+        loss = C.c_double()
+        g = np.zeros(self.n_params, dtype=np.float32)
+        _check(load().wc_lpc_loss_grad(self._handle, n, h, w, _fptr(c), _fptr(heff), _fptr(bed), _fptr(e), float(dx),
+                                       float(dy), C.byref(loss), _fptr(g)))
+        return loss.value, g
 
     def harvest(self, solver: "Solver") -> None:
         """Keep the solver's current SGN system (that of its last solve) for training."""
