@@ -385,7 +385,10 @@ def run_b200(args, world, rank, local):
         from wavesim_b200.train_lpc import trained_network
 
         torch.cuda.synchronize()
-        net, train_rec = trained_network(dx=w.grid.dx, steps=args.train_steps, seed=0)
+        from wavesim_b200.lpc import UNetSpec
+
+        spec = UNetSpec(channels=tuple(int(c) for c in args.lpc_channels.split(",")), stride=args.lpc_stride)
+        net, train_rec = trained_network(dx=w.grid.dx, steps=args.train_steps, seed=0, spec=spec)
         torch.cuda.synchronize()
     arm = measure_arm(w, args, world, stream, flush, net)
     plain = measure_arm(w, args, world, stream, flush, None) if learned else None
@@ -400,12 +403,11 @@ def run_b200(args, world, rank, local):
         peak, peak_kind = measured_peaks()
         iters_prof = arm["iterations_per_solve_profiled"]
         if learned and net_ms >= max(solve_ms, stage_ms):
-            from wavesim_b200.lpc import UNetSpec
-
-            flops = UNetSpec().flops_per_cell() * w.grid.nx * w.grid.ny
+            spec = net.spec
+            flops = spec.flops_per_cell() / spec.stride**2 * w.grid.nx * w.grid.ny
             tflops = flops / (net_ms / net_n / 1e3) / 1e12
             roof = {"bound": "compute (FP32 CUDA-core convolutions)", "kernel": "conv_fwd_kernel chain (one network application)",
-                    "achieved": tflops, "unit": "TFLOP/s", "flops_per_cell": UNetSpec().flops_per_cell(),
+                    "achieved": tflops, "unit": "TFLOP/s", "flops_per_cell": spec.flops_per_cell() / spec.stride**2,
                     "avg_ms": net_ms / net_n, "traffic": None}
             bf16 = peak_tensor()
             roof.update({"peak": bf16[0], "frac": tflops / bf16[0], "peak_source": bf16[1]})
@@ -488,6 +490,8 @@ def main():
     ap.add_argument("--pc", default="learned", choices=["learned", "jacobi"],
                     help="learned: time the learned preconditioner and plain PCG side by side (SGN workloads)")
     ap.add_argument("--train-steps", type=int, default=3000)
+    ap.add_argument("--lpc-stride", type=int, default=1, choices=[1, 2, 4])
+    ap.add_argument("--lpc-channels", default="8,16,32,32")
     ap.add_argument("--eta-steps", type=int, default=10)
     ap.add_argument("--cpu-steps", type=int, default=40)
     ap.add_argument("--no-cpu-baseline", action="store_true")

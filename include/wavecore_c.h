@@ -266,9 +266,12 @@ uint64_t wc_ensemble_launch_count(const wc_ensemble* e);
 typedef struct wc_lpc wc_lpc;
 
 /* channels[4]: feature maps per level, finest first (null: 8, 16, 32, 32); gate_hidden: width of
- * the gate networks' hidden layer (8). Weights start scaled-normal from `seed`, biases at zero
- * and the output layer at zero (an untrained network adds nothing to the Jacobi sweeps). */
-wc_status wc_lpc_create(const int32_t* channels, int32_t gate_hidden, uint64_t seed, wc_lpc** out);
+ * the gate networks' hidden layer (8); stride 1, 2 or 4: the network runs on a grid that many
+ * times coarser than the solver's (its input is the block mean of D^-1 (r - A z1), its output is
+ * added at every cell of the block). Weights start scaled-normal from `seed`, biases at zero and
+ * the output layer at zero (an untrained network adds nothing to the Jacobi sweeps). */
+wc_status wc_lpc_create(const int32_t* channels, int32_t gate_hidden, int32_t stride,
+                        uint64_t seed, wc_lpc** out);
 /* A network must outlive every solver it is attached to. */
 void wc_lpc_destroy(wc_lpc* l);
 uint64_t wc_lpc_num_params(const wc_lpc* l);

@@ -207,7 +207,8 @@ def patch_diag(c, heff, mask, dx, dy):
 def cycle_loss_grad(spec: UNetSpec, params, c, heff, bed, e, dx, dy, omega):
     """Loss mean_n <d, A d>_n / <e, A e>_n of the cycle z = M A e (d = e - z) and its gradient
     with respect to the flat parameters. c, heff, bed: (N, H, W); e: (N, 2, H, W). A patch
-    without a wet cell (<e, A e> = 0) contributes nothing."""
+    without a wet cell (<e, A e> = 0) contributes nothing. With spec.stride S > 1 the network
+    sees S x S block means of its input and features and its output is repeated over the block."""
     c, heff, bed, e = (np.asarray(a, dtype=np.float64) for a in (c, heff, bed, e))
     mask = (heff >= H_DISP_MIN).astype(np.float64)
     feat = np.stack([heff / 20.0, bed / 20.0], axis=1)
@@ -217,8 +218,11 @@ def cycle_loss_grad(spec: UNetSpec, params, c, heff, bed, e, dx, dy, omega):
     r = A(e)
     z1 = omega * r / D
     x = (r - A(z1)) / D
-    y, cache = forward(spec, params, x, feat)
-    z2 = z1 + m2 * y
+    S = spec.stride
+    pool_s = lambda a: a.reshape(a.shape[0], a.shape[1], a.shape[2] // S, S, a.shape[3] // S, S).mean(axis=(3, 5))  # noqa: E731
+    up_s = lambda a: np.repeat(np.repeat(a, S, axis=2), S, axis=3)  # noqa: E731
+    y, cache = forward(spec, params, pool_s(x), pool_s(feat))
+    z2 = z1 + m2 * up_s(y)
     z = z2 + omega * (r - A(z2)) / D
     d = e - z
     ad = A(d)
@@ -230,5 +234,5 @@ def cycle_loss_grad(spec: UNetSpec, params, c, heff, bed, e, dx, dy, omega):
     loss = float(np.sum(np.where(ok, num / safe, 0.0)) / n)
     gz = np.where(ok[:, None, None, None], -2.0 * ad / (n * safe[:, None, None, None]), 0.0)
     gz2 = gz - omega * A(gz / D)
-    grads, _ = backward(spec, params, cache, m2 * gz2)
+    grads, _ = backward(spec, params, cache, pool_s(m2 * gz2) * (S * S))  # adjoint of up_s: block sums
     return loss, grads

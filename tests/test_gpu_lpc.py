@@ -104,6 +104,32 @@ def test_training_loss_and_gradient_match_the_fp64_oracle():
             assert rel(g[b : b + co], go[b : b + co]) < 2e-4, name + " bias"
 
 
+def test_strided_training_loss_and_gradient_match_the_fp64_oracle():
+    # The network on a grid twice coarser: block-mean input and features, output repeated.
+    from dataclasses import replace
+
+    from wavesim_b200.lpc import OMEGA
+
+    spec = replace(UNetSpec(), stride=2)
+    net = LearnedPreconditioner(spec)
+    net.set_rounding(False)
+    p = random_params(spec, 9)
+    net.set_params(p)
+    rng = np.random.default_rng(10)
+    n, h, w = 2, 32, 48
+    depth = rng.uniform(-0.3, 8.0, (n, h, w)).astype(np.float32)
+    heff = np.maximum(depth, 1e-8).astype(np.float32)
+    c = np.where(depth < 0.05, 0.0, depth**3 / 3.0).astype(np.float32)
+    bed = (-depth).astype(np.float32)
+    e = (rng.normal(size=(n, 2, h, w)) * (heff >= 0.05)[:, None]).astype(np.float32)
+    loss, g = net.loss_grad(c, heff, bed, e, 2.0, 2.0)
+    lo, go = U.cycle_loss_grad(spec, p.astype(np.float64), c, heff, bed, e, 2.0, 2.0, OMEGA)
+    assert abs(loss - lo) < 1e-5 * abs(lo)
+    for name, (wo, b, co, ci, k) in spec.offsets().items():
+        m = co * ci * k * k
+        assert rel(g[wo : wo + m], go[wo : wo + m]) < 2e-4, name
+
+
 def small_run(seed=11, nx=192, ny=96, tol=1e-8):
     w = W.sgn_beach(nx, ny, 2.0, seed=seed, tolerance=tol, name=f"lpc_{nx}x{ny}")
     return w, W.wave_train_state(w)

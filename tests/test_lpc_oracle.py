@@ -77,3 +77,20 @@ def test_an_all_dry_patch_contributes_nothing():
     l, g = U.cycle_loss_grad(SPEC, p, c, heff, bed, e, 2.0, 2.0, OMEGA)
     assert np.isfinite(l) and np.all(np.isfinite(g))
     assert abs(l - l2 / 2) < 1e-12 and np.allclose(g, g2 / 2, rtol=1e-9, atol=1e-15)
+
+
+def test_strided_cycle_loss_gradient_matches_finite_differences():
+    from dataclasses import replace
+
+    spec = replace(SPEC, stride=2)
+    p = params(9)
+    c, heff, bed, e = patches(10, n=2, h=32, w=32)
+    loss, g = U.cycle_loss_grad(spec, p, c, heff, bed, e, 2.0, 2.0, OMEGA)
+    rng = np.random.default_rng(11)
+    for idx in rng.choice(p.size, 10, replace=False):
+        q1, q2 = p.copy(), p.copy()
+        q1[idx] += 1e-6
+        q2[idx] -= 1e-6
+        l1 = U.cycle_loss_grad(spec, q1, c, heff, bed, e, 2.0, 2.0, OMEGA)[0]
+        l2 = U.cycle_loss_grad(spec, q2, c, heff, bed, e, 2.0, 2.0, OMEGA)[0]
+        assert abs((l1 - l2) / 2e-6 - g[idx]) < 1e-6 + 1e-5 * abs(g[idx]), idx

@@ -26,10 +26,8 @@ struct ConvArgs {
 };
 
 constexpr int CV_TH = 16;  // threads per tile edge (16 x 16 = 256 threads)
-constexpr int CV_P = 2;    // output pixels per thread along each axis (2 x 2)
-constexpr int CV_T = CV_TH * CV_P;  // output tile edge (32)
 constexpr int CV_COB = 8;  // output channels per block
-constexpr int CV_CIB = 4;  // input channels staged per pass
+constexpr int CV_CIB = 8;  // input channels staged per pass
 
 __device__ __forceinline__ float conv_input(const ConvArgs& p, int n, int c, int y, int x) {
     if ((unsigned)y >= (unsigned)p.H || (unsigned)x >= (unsigned)p.W) return 0.f;
@@ -46,31 +44,33 @@ __device__ __forceinline__ float conv_input(const ConvArgs& p, int n, int c, int
     return p.b[(((size_t)n * p.cb + (c - p.ca)) * p.H + y) * p.W + x];
 }
 
-// Direct convolution, register-blocked: a block computes a 32 x 32 tile of 8 output channels;
-// each thread a 2 x 2 patch of all 8, from a (2 + K - 1)^2 window of every staged input channel
-// held in registers and the 8 weights of a tap read as two float4 (broadcast).
-template <int K>
+// Direct convolution, register-blocked: a block computes a (16 P) x (16 P) tile of 8 output
+// channels; each thread a P x P patch of all 8, from a (P + K - 1)^2 window of every staged input
+// channel held in registers and the 8 weights of a tap read as two float4 (broadcast). P = 2 on
+// large maps; P = 1 on the coarse levels, where a 32 x 32 tile would leave most SMs idle.
+template <int K, int P>
 __global__ void __launch_bounds__(CV_TH* CV_TH) conv_fwd_kernel(ConvArgs p) {
-    constexpr int R = K / 2, TE = CV_T + 2 * R, WIN = CV_P + K - 1;
+    constexpr int T = CV_TH * P, R = K / 2, TE = T + 2 * R, WIN = P + K - 1;
     __shared__ float tile[CV_CIB][TE][TE + 1];
     __shared__ __align__(16) float wsm[CV_CIB][K * K][CV_COB];
     const int ncog = (p.co + CV_COB - 1) / CV_COB;
     const int n = blockIdx.z / ncog, cog = blockIdx.z % ncog;
-    const int x0 = blockIdx.x * CV_T, y0 = blockIdx.y * CV_T;
+    const int x0 = blockIdx.x * T, y0 = blockIdx.y * T;
     const int tx = threadIdx.x % CV_TH, ty = threadIdx.x / CV_TH;
     const int ci_total = p.ca + p.cb;
-    float acc[CV_P][CV_P][CV_COB];
+    float acc[P][P][CV_COB];
 #pragma unroll
-    for (int a = 0; a < CV_P; a++)
+    for (int a = 0; a < P; a++)
 #pragma unroll
-        for (int b = 0; b < CV_P; b++)
+        for (int b = 0; b < P; b++)
 #pragma unroll
             for (int o = 0; o < CV_COB; o++) acc[a][b][o] = 0.f;
     for (int c0 = 0; c0 < ci_total; c0 += CV_CIB) {
-        for (int q = threadIdx.x; q < CV_CIB * TE * TE; q += CV_TH * CV_TH) {
+        const int nc = min(CV_CIB, ci_total - c0);
+        for (int q = threadIdx.x; q < nc * TE * TE; q += CV_TH * CV_TH) {
             const int c = q / (TE * TE), r = q % (TE * TE);
             const int yy = y0 + r / TE - R, xx = x0 + r % TE - R;
-            tile[c][r / TE][r % TE] = (c0 + c < ci_total) ? conv_input(p, n, c0 + c, yy, xx) : 0.f;
+            tile[c][r / TE][r % TE] = conv_input(p, n, c0 + c, yy, xx);
         }
         for (int q = threadIdx.x; q < CV_COB * CV_CIB * K * K; q += CV_TH * CV_TH) {
             const int o = q % CV_COB, r = q / CV_COB;
@@ -79,22 +79,21 @@ __global__ void __launch_bounds__(CV_TH* CV_TH) conv_fwd_kernel(ConvArgs p) {
             wsm[c][t][o] = (co < p.co && ci < ci_total) ? p.w[((size_t)co * ci_total + ci) * K * K + t] : 0.f;
         }
         __syncthreads();
-#pragma unroll
-        for (int c = 0; c < CV_CIB; c++) {
+        for (int c = 0; c < nc; c++) {
             float win[WIN][WIN];
 #pragma unroll
             for (int a = 0; a < WIN; a++)
 #pragma unroll
-                for (int b = 0; b < WIN; b++) win[a][b] = tile[c][CV_P * ty + a][CV_P * tx + b];
+                for (int b = 0; b < WIN; b++) win[a][b] = tile[c][P * ty + a][P * tx + b];
 #pragma unroll
             for (int t = 0; t < K * K; t++) {
                 const float4 w0 = *reinterpret_cast<const float4*>(&wsm[c][t][0]);
                 const float4 w1 = *reinterpret_cast<const float4*>(&wsm[c][t][4]);
                 const float wv[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
 #pragma unroll
-                for (int a = 0; a < CV_P; a++)
+                for (int a = 0; a < P; a++)
 #pragma unroll
-                    for (int b = 0; b < CV_P; b++) {
+                    for (int b = 0; b < P; b++) {
                         const float v = win[a + t / K][b + t % K];
 #pragma unroll
                         for (int o = 0; o < CV_COB; o++) acc[a][b][o] = fmaf(v, wv[o], acc[a][b][o]);
@@ -104,10 +103,10 @@ __global__ void __launch_bounds__(CV_TH* CV_TH) conv_fwd_kernel(ConvArgs p) {
         __syncthreads();
     }
 #pragma unroll
-    for (int a = 0; a < CV_P; a++)
+    for (int a = 0; a < P; a++)
 #pragma unroll
-        for (int b = 0; b < CV_P; b++) {
-            const int x = x0 + CV_P * tx + b, y = y0 + CV_P * ty + a;
+        for (int b = 0; b < P; b++) {
+            const int x = x0 + P * tx + b, y = y0 + P * ty + a;
             if (x >= p.W || y >= p.H) continue;
 #pragma unroll
             for (int o = 0; o < CV_COB; o++) {
@@ -236,6 +235,34 @@ __global__ void sig2_relu_bwd_kernel(float* __restrict__ d, const float* __restr
     for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
         if (act == ACT_SIG2) d[q] *= y[q] * (1.f - 0.5f * y[q]);
         else d[q] = y[q] > 0.f ? d[q] : 0.f;
+    }
+}
+
+// The network can run on a grid S times coarser than the solver's: its input is the S x S block
+// mean, its output is read back at the block's every cell (nearest). Their adjoints: the block
+// sum times `scale` (1: the adjoint of nearest upsampling), nearest upsampling times `scale`.
+__global__ void pool_s_kernel(const float* __restrict__ x, int NC, int H, int W, int S, float* __restrict__ y,
+                              float scale) {
+    const int Hc = H / S, Wc = W / S;
+    const size_t total = (size_t)NC * Hc * Wc;
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
+        const int xx = (int)(q % Wc), yy = (int)((q / Wc) % Hc);
+        const size_t c = q / ((size_t)Hc * Wc);
+        const float* s = x + (c * H + (size_t)yy * S) * W + (size_t)xx * S;
+        float v = 0.f;
+        for (int a = 0; a < S; a++)
+            for (int b = 0; b < S; b++) v += s[(size_t)a * W + b];
+        y[q] = scale * v;
+    }
+}
+
+__global__ void up_s_kernel(const float* __restrict__ x, int NC, int Hc, int Wc, int S, float* __restrict__ y) {
+    const int H = Hc * S, W = Wc * S;
+    const size_t total = (size_t)NC * H * W;
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
+        const int xx = (int)(q % W), yy = (int)((q / W) % H);
+        const size_t c = q / ((size_t)H * W);
+        y[q] = x[(c * Hc + yy / S) * Wc + xx / S];
     }
 }
 
@@ -588,28 +615,34 @@ __global__ void lpc_jacobi_kernel(DevGrid g, const float2* r, const float2* d, f
     }
 }
 
-// the network input: (r - t) / diag, written as 2 planes
+// the network input: (r - t) / diag, as 2 planes of Hp x Wp (the S x S block means; zero
+// outside the interior)
 __global__ void lpc_input_kernel(DevGrid g, const float2* r, const float2* t, const float2* d, float* x, int Hp, int Wp,
-                                 const FcgScalars* sc) {
+                                 int S, const FcgScalars* sc) {
     if (sc->done) return;
     const size_t plane = (size_t)Hp * Wp;
+    const float inv = 1.f / (float)(S * S);
     for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < plane; q += (size_t)gridDim.x * blockDim.x) {
-        const int i = (int)(q % Wp), j = (int)(q / Wp);
+        const int i0 = (int)(q % Wp) * S, j0 = (int)(q / Wp) * S;
         float vx = 0.f, vy = 0.f;
-        if (i < g.nx && j < g.ny) {
-            const int k = j * g.pitch + i;
-            const float2 rr = r[k], tt = t[k], dd = d[k];
-            vx = (rr.x - tt.x) / dd.x;
-            vy = (rr.y - tt.y) / dd.y;
-        }
-        x[q] = vx;
-        x[plane + q] = vy;
+        for (int a = 0; a < S; a++)
+            for (int b = 0; b < S; b++) {
+                const int i = i0 + b, j = j0 + a;
+                if (i < g.nx && j < g.ny) {
+                    const int k = j * g.pitch + i;
+                    const float2 rr = r[k], tt = t[k], dd = d[k];
+                    vx += (rr.x - tt.x) / dd.x;
+                    vy += (rr.y - tt.y) / dd.y;
+                }
+            }
+        x[q] = vx * inv;
+        x[plane + q] = vy * inv;
     }
 }
 
-// z2 = z1 + mask * y (network output planes)
+// z2 = z1 + mask * y (network output planes, read at the cell's block)
 __global__ void lpc_correct_kernel(DevGrid g, const float2* z1, const float* y, const float* heff, float2* z2, int Hp,
-                                   int Wp, const FcgScalars* sc) {
+                                   int Wp, int S, const FcgScalars* sc) {
     if (sc->done) return;
     const size_t plane = (size_t)Hp * Wp;
     const int n = g.nx * g.ny;
@@ -617,7 +650,7 @@ __global__ void lpc_correct_kernel(DevGrid g, const float2* z1, const float* y, 
         const int i = c % g.nx, j = c / g.nx;
         const int k = j * g.pitch + i;
         const float m = heff[k] >= H_DISP_MIN ? 1.f : 0.f;
-        const size_t q = (size_t)j * Wp + i;
+        const size_t q = (size_t)(j / S) * Wp + i / S;
         const float2 a = z1[k];
         z2[k] = make_float2(a.x + m * y[q], a.y + m * y[plane + q]);
     }
@@ -635,19 +668,24 @@ __global__ void lpc_post_kernel(DevGrid g, const float2* z2, const float2* r, co
     }
 }
 
-// the features (h / H0, b / H0) as 2 planes
-__global__ void lpc_features_kernel(DevGrid g, const float* heff, const float* bed, float* f, int Hp, int Wp) {
+// the features (h / H0, b / H0) as 2 planes (S x S block means, zero outside the interior)
+__global__ void lpc_features_kernel(DevGrid g, const float* heff, const float* bed, float* f, int Hp, int Wp, int S) {
     const size_t plane = (size_t)Hp * Wp;
+    const float inv = 1.f / (20.0f * (float)(S * S));
     for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < plane; q += (size_t)gridDim.x * blockDim.x) {
-        const int i = (int)(q % Wp), j = (int)(q / Wp);
+        const int i0 = (int)(q % Wp) * S, j0 = (int)(q / Wp) * S;
         float a = 0.f, b = 0.f;
-        if (i < g.nx && j < g.ny) {
-            const int k = j * g.pitch + i;
-            a = heff[k] / 20.0f;
-            b = bed[k] / 20.0f;
-        }
-        f[q] = a;
-        f[plane + q] = b;
+        for (int u = 0; u < S; u++)
+            for (int v = 0; v < S; v++) {
+                const int i = i0 + v, j = j0 + u;
+                if (i < g.nx && j < g.ny) {
+                    const int k = j * g.pitch + i;
+                    a += heff[k];
+                    b += bed[k];
+                }
+            }
+        f[q] = a * inv;
+        f[plane + q] = b * inv;
     }
 }
 

@@ -176,9 +176,18 @@ struct LpcNet {
         p.W = w_of(level);
         p.N = N;
         p.act = act;
-        dim3 grid((p.W + CV_T - 1) / CV_T, (p.H + CV_T - 1) / CV_T, N * ((L.co + CV_COB - 1) / CV_COB));
-        if (L.k == 3) conv_fwd_kernel<3><<<grid, CV_TH * CV_TH, 0, st>>>(p);
-        else conv_fwd_kernel<1><<<grid, CV_TH * CV_TH, 0, st>>>(p);
+        // 32 x 32 tiles while they give every SM a few blocks, 16 x 16 below
+        const int groups = N * ((L.co + CV_COB - 1) / CV_COB);
+        const bool big = (size_t)((p.W + 31) / 32) * ((p.H + 31) / 32) * groups >= 4 * 148;
+        const int T = big ? 2 * CV_TH : CV_TH;
+        dim3 grid((p.W + T - 1) / T, (p.H + T - 1) / T, groups);
+        if (L.k == 3) {
+            if (big) conv_fwd_kernel<3, 2><<<grid, CV_TH * CV_TH, 0, st>>>(p);
+            else conv_fwd_kernel<3, 1><<<grid, CV_TH * CV_TH, 0, st>>>(p);
+        } else {
+            if (big) conv_fwd_kernel<1, 2><<<grid, CV_TH * CV_TH, 0, st>>>(p);
+            else conv_fwd_kernel<1, 1><<<grid, CV_TH * CV_TH, 0, st>>>(p);
+        }
         return cudaGetLastError();
     }
 
@@ -354,7 +363,8 @@ struct LpcSystem {
 struct LpcTrainer {
     int N = 0, H = 0, W = 0;
     float dx = 1.f, dy = 1.f;
-    DBuf c, heff, mask, e, r, dg, z1, tmp, zj, z2, z, dd, ad, ae, gz, gz2;
+    int S = 1;  // the network's grid is S times coarser
+    DBuf c, heff, mask, e, r, dg, z1, tmp, zj, z2, z, dd, ad, feat, yf, gz, gz2, dyc;
     double* sums = nullptr;  // [2][N]: <d, A d>, <e, A e>
     ~LpcTrainer() {
         if (sums) cudaFree(sums);
@@ -366,8 +376,9 @@ struct LpcTrainer {
         const size_t one = (size_t)n * h * w, two = 2 * one;
         cudaError_t er = cudaSuccess;
         for (DBuf* b : {&c, &heff, &mask}) if (er == cudaSuccess && b->n != one) er = b->alloc(one);
-        for (DBuf* b : {&e, &r, &dg, &z1, &tmp, &zj, &z2, &z, &dd, &ad, &ae, &gz, &gz2})
+        for (DBuf* b : {&e, &r, &dg, &z1, &tmp, &zj, &z2, &z, &dd, &ad, &feat, &yf, &gz, &gz2})
             if (er == cudaSuccess && b->n != two) er = b->alloc(two);
+        if (er == cudaSuccess && dyc.n != two / (S * S)) er = dyc.alloc(two / (S * S));
         if (er == cudaSuccess) {
             if (sums) cudaFree(sums);
             er = cudaMalloc(&sums, 2 * n * sizeof(double));
@@ -413,6 +424,7 @@ struct LpcModel {
     DBuf w, wq, g, m, v;
     int adam_t = 0;
     int round_bf16 = 1;
+    int stride = 1;  // the network runs on a grid this many times coarser than the solver's
     std::vector<LpcSystem*> systems;
     LpcTrainer tr;
     double* dloss = nullptr;  // the loss of every step of a training call
@@ -426,7 +438,9 @@ struct LpcModel {
         if (st) cudaStreamDestroy(st);
     }
 
-    cudaError_t init(const int* channels, int hidden) {
+    cudaError_t init(const int* channels, int hidden, int S) {
+        stride = S;
+        tr.S = S;
         net.layout(channels, hidden);
         cudaError_t e;
         for (DBuf* b : {&w, &wq, &g, &m, &v})
@@ -453,7 +467,19 @@ struct LpcModel {
         cudaError_t e;
         if (tr.N != N || tr.H != H || tr.W != W)
             if ((e = tr.shape(N, H, W)) != cudaSuccess) return e;
-        return net.shape(N, H, W, true);
+        return net.shape(N, H / stride, W / stride, true);
+    }
+
+    // where crops put the features: the network's input directly, or the fine-grid buffer
+    float* fine_features() { return stride == 1 ? net.F[0].p : tr.feat.p; }
+
+    // the network's features from the fine ones (block means)
+    cudaError_t pool_features() {
+        if (stride == 1) return cudaSuccess;
+        const size_t nc = (size_t)tr.N * 2 * (tr.H / stride) * (tr.W / stride);
+        pool_s_kernel<<<ew_grid(nc), 256, 0, st>>>(tr.feat.p, tr.N * 2, tr.H, tr.W, stride, net.F[0].p,
+                                                   1.f / (float)(stride * stride));
+        return cudaGetLastError();
     }
 
     // A training batch: N patches of H x W from random systems and offsets (all of one grid
@@ -473,12 +499,12 @@ struct LpcModel {
             const int y0 = (int)(next() % (unsigned long long)(sy->ny - H + 1));
             crop_kernel<<<ew_grid(plane), 256, 0, st>>>(sy->c.p, sy->heff.p, sy->bed.p, sy->pitch, x0, y0, H, W,
                                                         tr.c.p + n * plane, tr.heff.p + n * plane,
-                                                        tr.mask.p + n * plane, net.F[0].p + n * per);
+                                                        tr.mask.p + n * plane, fine_features() + n * per);
         }
         tr.dx = s0->dx;
         tr.dy = s0->dy;
         random_field_kernel<<<ew_grid((size_t)N * per), 256, 0, st>>>(tr.e.p, tr.mask.p, N, H, W, next(), rough);
-        return cudaGetLastError();
+        return pool_features();
     }
 
     // The loss mean_n <d, A d>_n / <e, A e>_n of the cycle's error d = e - M A e on the batch in
@@ -495,10 +521,22 @@ struct LpcModel {
         fld(tr.z1.p, nullptr, 0.f, tr.r.p, om, tr.dg.p, nullptr, N, plane, st);       // z1 = w r / D
         patch_matvec_kernel<<<ew_grid(N * plane), 256, 0, st>>>(op, tr.z1.p, tr.tmp.p);
         fld(tr.zj.p, tr.r.p, 1.f, tr.tmp.p, -1.f, nullptr, nullptr, N, plane, st);      // r - A z1
-        fld(net.X[0].p, nullptr, 0.f, tr.zj.p, 1.f, tr.dg.p, nullptr, N, plane, st);     // / D
+        const int S = stride;
+        const size_t coarse = tot / (S * S);
+        if (S == 1) {
+            fld(net.X[0].p, nullptr, 0.f, tr.zj.p, 1.f, tr.dg.p, nullptr, N, plane, st);  // / D
+        } else {
+            fld(tr.z2.p, nullptr, 0.f, tr.zj.p, 1.f, tr.dg.p, nullptr, N, plane, st);
+            pool_s_kernel<<<ew_grid(coarse), 256, 0, st>>>(tr.z2.p, N * 2, H, W, S, net.X[0].p, 1.f / (float)(S * S));
+        }
         if ((e = net.gates(st)) != cudaSuccess) return e;
         if ((e = net.forward(st, true)) != cudaSuccess) return e;
-        fld(tr.z2.p, tr.z1.p, 1.f, net.Y.p, 1.f, nullptr, tr.mask.p, N, plane, st);     // z2 = z1 + m Y
+        const float* yfine = net.Y.p;
+        if (S > 1) {
+            up_s_kernel<<<ew_grid(tot), 256, 0, st>>>(net.Y.p, N * 2, H / S, W / S, S, tr.yf.p);
+            yfine = tr.yf.p;
+        }
+        fld(tr.z2.p, tr.z1.p, 1.f, yfine, 1.f, nullptr, tr.mask.p, N, plane, st);       // z2 = z1 + m Y
         patch_matvec_kernel<<<ew_grid(N * plane), 256, 0, st>>>(op, tr.z2.p, tr.tmp.p);
         fld(tr.dd.p, tr.r.p, 1.f, tr.tmp.p, -1.f, nullptr, nullptr, N, plane, st);      // r - A z2
         fld(tr.z.p, tr.z2.p, 1.f, tr.dd.p, om, tr.dg.p, nullptr, N, plane, st);         // z
@@ -517,8 +555,13 @@ struct LpcModel {
         patch_matvec_kernel<<<ew_grid(N * plane), 256, 0, st>>>(op, tr.tmp.p, tr.zj.p);
         fld(tr.gz2.p, tr.gz.p, 1.f, tr.zj.p, -om, nullptr, nullptr, N, plane, st);
         fld(tr.gz2.p, nullptr, 0.f, tr.gz2.p, 1.f, nullptr, tr.mask.p, N, plane, st);
+        const float* dy = tr.gz2.p;
+        if (S > 1) {  // through the nearest upsampling: block sums
+            pool_s_kernel<<<ew_grid(coarse), 256, 0, st>>>(tr.gz2.p, N * 2, H, W, S, tr.dyc.p, 1.f);
+            dy = tr.dyc.p;
+        }
         cudaMemsetAsync(g.p, 0, g.n * sizeof(float), st);
-        if ((e = net.backward(tr.gz2.p, nullptr, st)) != cudaSuccess) return e;
+        if ((e = net.backward(dy, nullptr, st)) != cudaSuccess) return e;
         return cudaGetLastError();
     }
 

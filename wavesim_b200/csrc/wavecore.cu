@@ -378,7 +378,7 @@ wc_status fcg_pre(wc_solver* s, cudaStream_t st, cudaGraphConditionalHandle h, i
     TRY(fcg_dots(s, st, FCG_INIT, s->bv, s->bv, s->r, s->r, h, cond));
     const size_t plane = (size_t)s->lpc_hp * s->lpc_wp;
     FCG_LAUNCH(lpc_features_kernel<<<ew_grid(plane), 256, 0, st>>>(s->g, s->heff, s->bed, s->lnet.F[0].p, s->lpc_hp,
-                                                                   s->lpc_wp));
+                                                                   s->lpc_wp, s->lpc->stride));
     CK(s->lnet.gates(st));
     s->launches += 2 * LPC_LEVELS + (LPC_LEVELS - 1);
     return WC_OK;
@@ -396,7 +396,8 @@ wc_status fcg_body(wc_solver* s, cudaStream_t st, cudaGraphConditionalHandle h, 
         ProfScope ps(s, 1);
         FCG_LAUNCH(lpc_jacobi_kernel<<<nb, 256, 0, st>>>(g, s->r, s->diag, z, LPC_OMEGA, sc));
         FCG_LAUNCH(fcg_matvec_kernel<<<nb, 256, 0, st>>>(g, z, s->cc, s->heff, s->tv, sc));
-        FCG_LAUNCH(lpc_input_kernel<<<ew_grid(plane), 256, 0, st>>>(g, s->r, s->tv, s->diag, s->lnet.X[0].p, hp, wp, sc));
+        FCG_LAUNCH(lpc_input_kernel<<<ew_grid(plane), 256, 0, st>>>(g, s->r, s->tv, s->diag, s->lnet.X[0].p, hp, wp,
+                                                                    s->lpc->stride, sc));
     }
     {
         ProfScope ps(s, 3);
@@ -404,7 +405,7 @@ wc_status fcg_body(wc_solver* s, cudaStream_t st, cudaGraphConditionalHandle h, 
         s->launches += 2 * LPC_LEVELS + 2 * (LPC_LEVELS - 1) + 1;
     }
     ProfScope ps(s, 1);
-    FCG_LAUNCH(lpc_correct_kernel<<<nb, 256, 0, st>>>(g, z, s->lnet.Y.p, s->heff, z, hp, wp, sc));
+    FCG_LAUNCH(lpc_correct_kernel<<<nb, 256, 0, st>>>(g, z, s->lnet.Y.p, s->heff, z, hp, wp, s->lpc->stride, sc));
     FCG_LAUNCH(fcg_matvec_kernel<<<nb, 256, 0, st>>>(g, z, s->cc, s->heff, s->tv, sc));
     FCG_LAUNCH(lpc_post_kernel<<<nb, 256, 0, st>>>(g, z, s->r, s->tv, s->diag, z, LPC_OMEGA, sc));
     TRY(fcg_dots(s, st, FCG_BETA, z, q, nullptr, nullptr, h, 0));
@@ -1454,7 +1455,7 @@ void lpc_init_host(const LpcNet& net, uint64_t seed, std::vector<float>& p) {
 
 extern "C" {
 
-wc_status wc_lpc_create(const int32_t* channels, int32_t gate_hidden, uint64_t seed, wc_lpc** out) {
+wc_status wc_lpc_create(const int32_t* channels, int32_t gate_hidden, int32_t stride, uint64_t seed, wc_lpc** out) {
     if (!out) return set_err(WC_EINVAL, "out is null");
     *out = nullptr;
     int ch[LPC_LEVELS] = {8, 16, 32, 32};
@@ -1463,8 +1464,9 @@ wc_status wc_lpc_create(const int32_t* channels, int32_t gate_hidden, uint64_t s
     for (int l = 0; l < LPC_LEVELS; l++)
         if (ch[l] < 1 || ch[l] > 256) return set_err(WC_EINVAL, "channels must be in 1..256");
     if (gate_hidden < 1 || gate_hidden > 256) return set_err(WC_EINVAL, "gate_hidden must be in 1..256");
+    if (stride != 1 && stride != 2 && stride != 4) return set_err(WC_EINVAL, "stride must be 1, 2 or 4");
     wc_lpc* l = new wc_lpc();
-    wc_status st = lpc_ck(l->m.init(ch, gate_hidden), "network allocation");
+    wc_status st = lpc_ck(l->m.init(ch, gate_hidden, stride), "network allocation");
     if (st == WC_OK) {
         std::vector<float> p;
         lpc_init_host(l->m.net, seed, p);
@@ -1572,9 +1574,9 @@ wc_status wc_lpc_train(wc_lpc* l, uint32_t steps, uint32_t batch, uint32_t patch
     if (!l) return set_err(WC_EINVAL, "null network");
     LpcModel& m = l->m;
     if (m.systems.empty()) return set_err(WC_EINVAL, "no harvested systems");
-    const uint32_t div = 1u << (LPC_LEVELS - 1);
+    const uint32_t div = (1u << (LPC_LEVELS - 1)) * (uint32_t)m.stride;
     if (batch < 1 || batch > 4096 || patch < div || patch % div || patch > 4096)
-        return set_err(WC_EINVAL, "batch must be in 1..4096 and the patch side a multiple of 8 up to 4096");
+        return set_err(WC_EINVAL, "batch must be in 1..4096 and the patch side a multiple of 8 x stride up to 4096");
     bool fits = false;
     for (auto* q : m.systems) fits = fits || ((uint32_t)q->nx >= patch && (uint32_t)q->ny >= patch);
     if (!fits) return set_err(WC_EINVAL, "no harvested system is as large as the patch");
@@ -1601,11 +1603,11 @@ wc_status wc_lpc_train(wc_lpc* l, uint32_t steps, uint32_t batch, uint32_t patch
 wc_status wc_lpc_loss_grad(wc_lpc* l, int32_t n, int32_t h, int32_t w, const float* c, const float* heff,
                            const float* bed, const float* e, double dx, double dy, double* loss, float* grad) {
     if (!l || !c || !heff || !bed || !e || !loss || !grad) return set_err(WC_EINVAL, "null argument");
-    const int div = 1 << (LPC_LEVELS - 1);
-    if (n < 1 || h < div || w < div || h % div || w % div)
-        return set_err(WC_EINVAL, "batch must be >= 1 and patch sides positive multiples of 8");
-    if (!(dx > 0.0 && dy > 0.0)) return set_err(WC_EINVAL, "cell size must be positive");
     LpcModel& m = l->m;
+    const int div = (1 << (LPC_LEVELS - 1)) * m.stride;
+    if (n < 1 || h < div || w < div || h % div || w % div)
+        return set_err(WC_EINVAL, "batch must be >= 1 and patch sides positive multiples of 8 x stride");
+    if (!(dx > 0.0 && dy > 0.0)) return set_err(WC_EINVAL, "cell size must be positive");
     cudaStream_t st = m.st;
     TRY(lpc_ck(m.shape_batch(n, h, w), "activations"));
     const size_t plane = (size_t)n * h * w;
@@ -1619,8 +1621,9 @@ wc_status wc_lpc_loss_grad(wc_lpc* l, int32_t n, int32_t h, int32_t w, const flo
         const size_t hw = (size_t)h * w;
         crop_kernel<<<ew_grid(hw), 256, 0, st>>>(m.tr.c.p + k * hw, m.tr.heff.p + k * hw, dbed.p + k * hw, w, 0, 0, h, w,
                                                  m.tr.c.p + k * hw, m.tr.heff.p + k * hw, m.tr.mask.p + k * hw,
-                                                 m.net.F[0].p + 2 * k * hw);
+                                                 m.fine_features() + 2 * k * hw);
     }
+    TRY(lpc_ck(m.pool_features(), "features"));
     m.tr.dx = (float)dx;
     m.tr.dy = (float)dy;
     double* dl = nullptr;
@@ -1654,8 +1657,9 @@ wc_status wc_solver_set_lpc(wc_solver* s, wc_lpc* l) {
     }
     if (l->m.net.nparams == 0) return set_err(WC_EINVAL, "network not initialised");
     const int div = 1 << (LPC_LEVELS - 1);
-    s->lpc_hp = ((int)s->grid.ny + div - 1) / div * div;
-    s->lpc_wp = ((int)s->grid.nx + div - 1) / div * div;
+    const int S = l->m.stride;  // the network's grid: ceil(n / S) cells, padded to a multiple of 8
+    s->lpc_hp = ((int)s->grid.ny + div * S - 1) / (div * S) * div;
+    s->lpc_wp = ((int)s->grid.nx + div * S - 1) / (div * S) * div;
     s->lnet.layout(l->m.net.ch, l->m.net.hidden);
     s->lnet.wq = l->m.wq.p;
     s->lnet.gw = nullptr;

@@ -40,6 +40,7 @@ class UNetSpec:
     out_ch: int = 2
     feat_ch: int = 2
     gate_hidden: int = GATE_HIDDEN
+    stride: int = 1  # the network's grid is this many times coarser than the solver's (1, 2, 4)
 
     @property
     def levels(self) -> int:
@@ -81,8 +82,8 @@ class UNetSpec:
         return sum(co * ci * k * k + (co if hb else 0) for _, co, ci, k, hb in self.layers())
 
     def flops_per_cell(self) -> float:
-        """2 x multiply-adds per finest-level cell of one application (gates excluded: they are
-        computed once per solve)."""
+        """2 x multiply-adds per cell of the network's finest level for one application (gates
+        excluded: they are computed once per solve). Per solver cell: divide by stride**2."""
         f = 0.0
         for name, co, ci, k, _ in self.layers():
             if name.startswith("gate"):

@@ -128,7 +128,7 @@ def load(path: str = LIB_PATH):
     L.wc_stable_dt_noalloc.argtypes = [C.POINTER(abi.wc_grid), C.c_double, V, V, V, V, D]
     L.wc_stable_dt_noalloc.restype = C.c_int
     F = C.POINTER(C.c_float)
-    L.wc_lpc_create.argtypes = [C.POINTER(C.c_int32), C.c_int32, C.c_uint64, C.POINTER(V)]
+    L.wc_lpc_create.argtypes = [C.POINTER(C.c_int32), C.c_int32, C.c_int32, C.c_uint64, C.POINTER(V)]
     L.wc_lpc_destroy.argtypes = [V]
     L.wc_lpc_destroy.restype = None
     L.wc_lpc_num_params.argtypes = [V]
@@ -334,7 +334,7 @@ class LearnedPreconditioner:
         self.spec = spec or UNetSpec()
         ch = (C.c_int32 * 4)(*self.spec.channels)
         out = C.c_void_p()
-        _check(load().wc_lpc_create(ch, int(self.spec.gate_hidden), int(seed), C.byref(out)))
+        _check(load().wc_lpc_create(ch, int(self.spec.gate_hidden), int(self.spec.stride), int(seed), C.byref(out)))
         self._handle = out
 
     def __del__(self):

@@ -45,10 +45,11 @@ def harvest_runs(net: LearnedPreconditioner, runs: int = 8, nx: int = 512, ny: i
             "seconds": time.perf_counter() - t0}
 
 
-def train(net: LearnedPreconditioner, steps: int = 3000, batch: int = 16, patch: int = 64, lr: float = 2e-3,
+def train(net: LearnedPreconditioner, steps: int = 3000, batch: int = 16, patch: int = 0, lr: float = 2e-3,
           seed: int = 0) -> dict:
     """Adam with the learning rate dropped by 4 for the last quarter; returns the loss record."""
     t0 = time.perf_counter()
+    patch = patch or 64 * net.spec.stride  # the network sees 64 x 64 patches of its own grid
     main = int(math.ceil(0.75 * steps))
     l1 = net.train(main, batch=batch, patch=patch, lr=lr, seed=seed)
     l2 = net.train(steps - main, batch=batch, patch=patch, lr=lr / 4.0, seed=seed + 1)
