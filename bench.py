@@ -48,7 +48,8 @@ STAGE_BYTES_SWE = (36 + 52) / 2                 # stage 1 / stage 2 (RK average 
 
 
 def workload(name: str):
-    return {"config1": W.config1, "config2": W.config2, "config3": W.config3}[name]()
+    return {"config1": W.config1, "config2": W.config2, "config3": W.config3, "config5": W.config5,
+            "swe4096": W.swe_large}[name]()
 
 
 def run_ensemble(args, world, rank, local):
@@ -486,7 +487,7 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="config3", choices=["config1", "config2", "config3", "config4"])
+    ap.add_argument("--workload", default="config3", choices=["config1", "config2", "config3", "config4", "config5", "swe4096"])
     ap.add_argument("--pc", default="learned", choices=["learned", "jacobi"],
                     help="learned: time the learned preconditioner and plain PCG side by side (SGN workloads)")
     ap.add_argument("--train-steps", type=int, default=3000)

@@ -152,6 +152,63 @@ def sgn_beach(nx: int, ny: int, dx: float, seed: int, tolerance: float = 1e-8, h
     )
 
 
+def swe_beach(nx: int, ny: int, dx: float, seed: int, name: str | None = None, steps: int = 2000) -> Workload:
+    """The non-dispersive stencil at scale: the beach of `sgn_beach` (20 m shelf, 1:30 beach,
+    Gaussian field sigma 0.5 m / 20 m, periodic y) with the plain method of the first
+    configuration: second order (MUSCL-MC + HLL), SSP-RK2, CFL 0.45, no dispersion, Manning 0.02;
+    maker H = 1 m, T = 12 s at normal incidence; a 100 m offshore sponge."""
+    grid = Grid(nx, ny, dx, dx)
+    lx = nx * dx
+    b = shelf_and_beach(grid, 20.0, 1.0 / 30.0, 0.85 * lx) + gaussian_field(nx, ny, dx, dx, 0.5, 20.0, seed)
+    bed = Bathymetry.from_interior(grid, b)
+    maker_x = min(160.0, 0.15 * lx)
+    return Workload(
+        name=name or f"swe_beach_{nx}x{ny}_dx{dx:g}",
+        grid=grid, bed=bed, order=Order.Second, cfl=0.45, manning=0.02, periodic_y=True,
+        sponges=[Sponge(int(round(100.0 / dx)), 1.5).edges(True, False, False, False)],
+        maker=WaveMaker(x=maker_x, amplitude=0.5, period=12.0, angle=0.0, sigma=2.0 * dx, ramp_periods=4.0),
+        dispersion=None, steps=steps,
+        meta={"seed": seed, "bed": "20 m shelf + 1:30 beach (shore at 0.85 Lx) + Gaussian field sigma 0.5 m, corr 20 m"},
+    )
+
+
+def swe_large(seed: int = 7) -> Workload:
+    """4096 x 4096 at 2 m of the non-dispersive stencil (16.8 M cells, the size of the largest
+    configuration)."""
+    return swe_beach(4096, 4096, 2.0, seed, name="swe_beach_4096x4096_dx2")
+
+
+def config5(seed: int = 2026, preconditioner: int = 0) -> Workload:
+    """4096 x 4096 at 1 m: a 1:30 plane beach behind a 20 m shelf plus a ridged random field
+    (sigma 1 m, correlation 10 m) and a Gaussian shoal (radius 150 m) whose crest is 1 m deep;
+    fifth order + SGN to 1e-8 with the breaking switch; maker H = 3 m, T = 16 s at the angle
+    nearest 10 degrees that fits the periodic width; 10000 steps."""
+    nx = ny = 4096
+    dx = 1.0
+    grid = Grid(nx, ny, dx, dx)
+    lx, ly = nx * dx, ny * dx
+    X, Y = grid.centres()
+    base = shelf_and_beach(grid, 20.0, 1.0 / 30.0, 0.85 * lx)
+    shoal_x = 0.5 * lx
+    base_at_shoal = float(np.maximum(-20.0, (shoal_x - 0.85 * lx) / 30.0))
+    shoal = (-1.0 - base_at_shoal) * np.exp(-((X - shoal_x) ** 2 + (Y - 0.5 * ly) ** 2) / (150.0**2))
+    b = np.maximum(base + shoal, np.minimum(base, -1.0)) + ridged_field(nx, ny, dx, dx, 1.0, 10.0, seed)
+    bed = Bathymetry.from_interior(grid, b)
+    maker_x = 160.0
+    i_m = int(round(maker_x / dx - 0.5))
+    depth = -b[ny // 2, i_m]
+    omega = 2.0 * math.pi / 16.0
+    angle, turns = snapped_angle(omega, depth, ly, math.radians(10.0), True)
+    maker = WaveMaker(x=maker_x, amplitude=1.5, period=16.0, angle=angle, sigma=2.0 * dx, ramp_periods=4.0)
+    return Workload(
+        name="sgn_reef_4096x4096_dx1", grid=grid, bed=bed, order=Order.Fifth, cfl=0.4, manning=0.02,
+        periodic_y=True, sponges=[Sponge(100, 1.5).edges(True, False, False, False)], maker=maker,
+        dispersion=Dispersion(tolerance=1e-8, max_iterations=1000, preconditioner=preconditioner), steps=10000,
+        meta={"seed": seed, "maker_depth_m": depth, "angle_deg": math.degrees(angle), "alongshore_turns": turns,
+              "bed": "20 m shelf + 1:30 beach + ridged field sigma 1 m / 10 m + shoal to 1 m depth"},
+    )
+
+
 def config2(seed: int = 2024) -> Workload:
     """1024x512 at 2 m, fifth order + SGN by Jacobi PCG to 1e-8, periodic y, H=2 m, T=14 s."""
     return sgn_beach(1024, 512, 2.0, seed, name="sgn_beach_1024x512_dx2")
