@@ -41,8 +41,8 @@ L2_FLUSH_BYTES = 256 << 20
 
 # Algorithmic bytes per interior cell (FP32 state with a compensated depth).
 STAGE_BYTES_SGN = 16 + 4 + 8 + 8 + 4 + 4 + 8   # read q, b; write hn, pred, c, heff, b-vector
-SOLVE_INIT_BYTES = 8 + 4 + 4 + 8 + 8 + 8 + 8 + 8  # read w, c, heff, b; write w, r, p, diag
-SOLVE_ITER_BYTES = 24 + 56 + 32                 # sweeps A, B, C
+SOLVE_INIT_BYTES = (8 + 4 + 4 + 8 + 8 + 8 + 8) + (8 + 8 + 4 + 4 + 8)  # r = b - A w; then q0 = A (r / diag)
+SOLVE_ITER_BYTES = (8 * 4 + 8 * 2 + 4 * 2) + 8 * 5  # read r, q, s, diag, p, w, c, heff; write p, w, s, r, q
 SOLVE_FINISH_BYTES = (44 + 60) / 2              # stage 1 / stage 2 epilogue, averaged
 STAGE_BYTES_SWE = (36 + 52) / 2                 # stage 1 / stage 2 (RK average + damping)
 

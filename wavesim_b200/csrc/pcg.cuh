@@ -2,13 +2,13 @@
 //
 // The reference solves  h w - grad(c div w) = r  by Jacobi-preconditioned conjugate gradients
 // from the previous solution, stopping when ||r|| <= tol ||b|| + 1e-10 or after max_iterations
-// (crates/wavecore/src/dispersion.rs:493-545). The recurrences here are the same; the sweeps
-// are arranged for the GPU:
-//   init   r = b - A w, diag, <b,b>, <r,z>, <r,r>           (z = r / diag, recomputed)
-//   A'     p = z + beta p (on the tile and a 2-cell halo), Ap, <p,Ap>
-//   B      w += alpha p, r -= alpha Ap, <r,r>, <r,z>
-// two grid-wide reductions per iteration. p is double-buffered: sweep A' reads the previous p
-// around its tile while other CTAs write the new one.
+// (crates/wavecore/src/dispersion.rs:493-545). This kernel runs the same method in its
+// single-reduction (Chronopoulos-Gear) form, which has the same iterates in exact arithmetic:
+//   init   r = b - A w, the inverse diagonal, <b,b>, <r,r>             (one reduction)
+//          q = A (r / diag), <r, u>, <u, q>                              (one reduction)
+//   iter   p = u + beta p, s = q + beta s, w += alpha p, r -= alpha s,
+//          u = r / diag, q = A u, <r,u>, <u,q>, <r,r>                    (one reduction)
+// one sweep and one grid-wide reduction per iteration instead of the textbook's two.
 //
 // Every CTA owns a fixed set of 32x16 tiles for the whole solve, and every sweep is software-
 // pipelined: the next tile's halo box is loaded into registers while the current tile computes.
@@ -37,10 +37,13 @@ struct PcgArgs {
     const float2* bv;
     float2* w;
     float2* r;
-    float2* p0;       // p, double-buffered
+    float2* p0;       // p (the CG sweep's search direction; own cells only)
     float2* p1;
+    float2* rb[2];    // the CG sweep's banks of r (bank 0 is r), s = A p and q = A (r / diag)
+    float2* sb[2];
+    float2* qb[2];
     float2* ap;
-    float2* diag;
+    float2* diag;     // the inverse Jacobi diagonal (written by the initial sweep)
     double* part;     // [ncta][4] CTA partials
     unsigned* cnt;    // [0] arrivals, [1] released epoch; zeroed before each launch
     const float2* hn;
@@ -117,6 +120,7 @@ struct TileSmem {
     float2 sv[PB_N];
     float scc[PC_N];
     float sf[PC_N];
+    float2 sr[PB_N], ss[PB_N], su[PB_N];  // the CG sweep's r', s and u = r / diag on the box
 };
 
 constexpr int PB_PER = (PB_N + PG_NT - 1) / PG_NT;  // box positions per thread
@@ -126,7 +130,8 @@ constexpr int PC_PER = (PC_N + PG_NT - 1) / PG_NT;
 // and the moment the tile's shared memory is free: the next tile's loads overlap this tile's
 // arithmetic.
 struct BoxPrefetch {
-    float2 v0[PB_PER], v1[PB_PER], v2[PB_PER];
+    float2 v0[PB_PER];
+    float he_box[PB_PER];
     float sx[PB_PER], sy[PB_PER];
     float c[PC_PER];
     float he;
@@ -137,11 +142,9 @@ __device__ __forceinline__ void tile_origin(const PcgArgs& a, int tl, int& i0, i
     j0 = (tl / a.tiles_x) * PG_TY;
 }
 
-// INIT: v0 = warm start w, v1.x = heff at the box position. Otherwise: v0 = r, v1 = diag,
-// v2 = previous p.
-template <bool INIT>
-__device__ __forceinline__ void box_prefetch(const PcgArgs& a, int tl, const float2* p_old, bool first,
-                                             BoxPrefetch& f) {
+// The initial sweep's loads for a tile: the warm start w and heff on the box, c on the tile
+// plus 1, heff of the own cell.
+__device__ __forceinline__ void box_prefetch_init(const PcgArgs& a, int tl, BoxPrefetch& f) {
     int i0, j0;
     tile_origin(a, tl, i0, j0);
     const DevGrid& g = a.g;
@@ -152,14 +155,8 @@ __device__ __forceinline__ void box_prefetch(const PcgArgs& a, int tl, const flo
             const Mapped m = map_cell(g, i0 - 2 + q % PB_W, j0 - 2 + q / PB_W);
             f.sx[n] = m.sx;
             f.sy[n] = m.sy;
-            if (INIT) {
-                f.v0[n] = a.w[m.k];
-                f.v1[n].x = __ldg(a.heff + m.k);
-            } else {
-                f.v0[n] = __ldcg(a.r + m.k);
-                f.v1[n] = __ldcg(a.diag + m.k);
-                if (!first) f.v2[n] = __ldcg(p_old + m.k);
-            }
+            f.v0[n] = a.w[m.k];
+            f.he_box[n] = __ldg(a.heff + m.k);
         }
     }
 #pragma unroll
@@ -174,22 +171,13 @@ __device__ __forceinline__ void box_prefetch(const PcgArgs& a, int tl, const flo
     f.he = (i < g.nx && j < g.ny) ? __ldg(a.heff + j * g.pitch + i) : 0.f;
 }
 
-template <bool INIT>
-__device__ __forceinline__ void box_commit(const BoxPrefetch& f, TileSmem& t, float beta, bool first) {
+// The warm start masked (dispersion.rs:480-490) and signed for ghost positions; c.
+__device__ __forceinline__ void box_commit_init(const BoxPrefetch& f, TileSmem& t) {
 #pragma unroll
     for (int n = 0; n < PB_PER; n++) {
         const int q = threadIdx.x + n * PG_NT;
         if (q < PB_N) {
-            float2 v;
-            if (INIT) {
-                v = f.v1[n].x >= H_DISP_MIN ? f.v0[n] : make_float2(0.f, 0.f);  // dispersion.rs:480-490
-            } else {
-                v = make_float2(f.v0[n].x / f.v1[n].x, f.v0[n].y / f.v1[n].y);  // z = r / diag
-                if (!first) {
-                    v.x += beta * f.v2[n].x;
-                    v.y += beta * f.v2[n].y;
-                }
-            }
+            const float2 v = f.he_box[n] >= H_DISP_MIN ? f.v0[n] : make_float2(0.f, 0.f);
             t.sv[q] = make_float2(v.x * f.sx[n], v.y * f.sy[n]);
         }
     }
@@ -218,10 +206,85 @@ __device__ __forceinline__ float2 apply_a(const DevGrid& g, TileSmem& t, int cx,
     return av;
 }
 
-// Own-cell vectors of sweep B, prefetched one tile ahead.
-struct CellPrefetch {
-    float2 p, ap, w, r, d;
+// One CG sweep's loads for a tile, taken one tile ahead: r, q = A u and the previous s on the
+// box (tile plus 2 cells), the inverse diagonal there, c on the tile plus 1, and the own cell's p, w.
+struct CgPrefetch {
+    float2 r[PB_PER], q[PB_PER], s[PB_PER], d[PB_PER];
+    float sx[PB_PER], sy[PB_PER];
+    float c[PC_PER];
+    float he;
+    float2 p, x;
 };
+
+__device__ __forceinline__ void cg_prefetch(const PcgArgs& a, int tl, int rb, bool init, bool first, CgPrefetch& f) {
+    int i0, j0;
+    tile_origin(a, tl, i0, j0);
+    const DevGrid& g = a.g;
+#pragma unroll
+    for (int n = 0; n < PB_PER; n++) {
+        const int q = threadIdx.x + n * PG_NT;
+        if (q < PB_N) {
+            const Mapped m = map_cell(g, i0 - 2 + q % PB_W, j0 - 2 + q / PB_W);
+            f.sx[n] = m.sx;
+            f.sy[n] = m.sy;
+            f.r[n] = __ldcg(a.rb[rb] + m.k);
+            f.d[n] = __ldcg(a.diag + m.k);
+            if (!init) {
+                f.q[n] = __ldcg(a.qb[rb] + m.k);
+                if (!first) f.s[n] = __ldcg(a.sb[rb] + m.k);
+            }
+        }
+    }
+#pragma unroll
+    for (int n = 0; n < PC_PER; n++) {
+        const int q = threadIdx.x + n * PG_NT;
+        if (q < PC_N) {
+            const Mapped m = map_cell(g, i0 - 1 + q % PC_W, j0 - 1 + q / PC_W);
+            f.c[n] = __ldg(a.cc + m.k);
+        }
+    }
+    const int i = i0 + threadIdx.x % PG_TX, j = j0 + threadIdx.x / PG_TX;
+    const bool own = i < g.nx && j < g.ny;
+    const int k = j * g.pitch + i;
+    f.he = own ? __ldg(a.heff + k) : 0.f;
+    if (!init && own) {
+        f.x = __ldcg(a.w + k);
+        if (!first) f.p = __ldcg(a.p0 + k);
+    }
+}
+
+// s = q + beta s, r' = r - alpha s and u' = r' / diag at every box position (the diagonal is
+// stored inverted) (the halo's copies
+// are this CTA's own recomputation from the old banks); u' (signed for ghost positions) feeds
+// A u'; s, r' and u = r / diag are kept for the own cells.
+__device__ __forceinline__ void cg_commit(const CgPrefetch& f, TileSmem& t, float alpha, float beta, bool init, bool first) {
+#pragma unroll
+    for (int n = 0; n < PB_PER; n++) {
+        const int q = threadIdx.x + n * PG_NT;
+        if (q < PB_N) {
+            const float2 r = f.r[n], d = f.d[n];
+            float2 rn = r;
+            if (!init) {
+                float2 sk = f.q[n];
+                if (!first) {
+                    sk.x += beta * f.s[n].x;
+                    sk.y += beta * f.s[n].y;
+                }
+                rn = make_float2(r.x - alpha * sk.x, r.y - alpha * sk.y);
+                t.ss[q] = sk;
+                t.su[q] = make_float2(r.x * d.x, r.y * d.y);
+            }
+            t.sr[q] = rn;
+            t.sv[q] = make_float2(rn.x * d.x * f.sx[n], rn.y * d.y * f.sy[n]);
+        }
+    }
+#pragma unroll
+    for (int n = 0; n < PC_PER; n++) {
+        const int q = threadIdx.x + n * PG_NT;
+        if (q < PC_N) t.scc[q] = f.c[n];
+    }
+}
+
 
 // The solve and the stage epilogue, by the `ncta` CTAs (this one is number `cta`) that own this
 // run. `epoch` counts the run's grid barriers within the launch. Returns false if a bounded
@@ -249,15 +312,15 @@ __device__ __forceinline__ bool pcg_solve(const PcgArgs& a, int cta, int ncta, u
         converged = true;
     } else {  // the Jacobi solve; after a learned solve that failed, from where that one stopped
         // ---- initial residual: r = b - A w (dispersion.rs:493-515) ---------------------------
-        double bb = 0.0, rz_p = 0.0, rr_p = 0.0;
-        if (cta < ntiles) box_prefetch<true>(a, cta, nullptr, true, f);
+        double bb = 0.0, rr_p = 0.0;
+        if (cta < ntiles) box_prefetch_init(a, cta, f);
         for (int tl = cta; tl < ntiles; tl += ncta) {
             int i0, j0;
             tile_origin(a, tl, i0, j0);
-            box_commit<true>(f, t, 0.f, true);
+            box_commit_init(f, t);
             const float he = f.he;
             __syncthreads();
-            if (tl + ncta < ntiles) box_prefetch<true>(a, tl + ncta, nullptr, true, f);
+            if (tl + ncta < ntiles) box_prefetch_init(a, tl + ncta, f);
             const float2 aw = apply_a(g, t, cx, cy, he);
             const int i = i0 + cx, j = j0 + cy;
             if (i < g.nx && j < g.ny) {
@@ -271,90 +334,82 @@ __device__ __forceinline__ bool pcg_solve(const PcgArgs& a, int cta, int ncta, u
                 const float2 b = __ldg(a.bv + k);
                 const float2 r = make_float2(b.x - aw.x, b.y - aw.y);
                 a.w[k] = t.sv[(cy + 2) * PB_W + (cx + 2)];  // the warm start, masked
-                a.diag[k] = d;
+                a.diag[k] = make_float2(1.f / d.x, 1.f / d.y);  // the CG sweeps multiply by the inverse
                 a.r[k] = r;
                 bb += (double)b.x * b.x + (double)b.y * b.y;
-                rz_p += (double)r.x * (r.x / d.x) + (double)r.y * (r.y / d.y);
                 rr_p += (double)r.x * r.x + (double)r.y * r.y;
             }
             __syncthreads();
         }
-        if (!reduce_barrier(a, epoch, bb, rz_p, rr_p, tot, red, cta, ncta)) return false;
+        if (!reduce_barrier(a, epoch, bb, 0.0, rr_p, tot, red, cta, ncta)) return false;
         const double target = a.tol * sqrt(tot[0]) + 1e-10;
-        double rz = tot[1];
         converged = sqrt(tot[2]) <= target;
-        float beta_f = 0.f;
-
+        // ---- single-reduction CG (Chronopoulos-Gear form of the same Jacobi PCG) --------------
+        // With u = r / diag and q = A u, the direction's image s = A p obeys s = q + beta s, and
+        // <p, s> = delta - beta gamma / alpha_prev (gamma = <r, u>, delta = <u, q>), so one sweep
+        // per iteration does p = u + beta p, s = q + beta s, w += alpha p, r -= alpha s,
+        // u = r / diag, q = A u and the three dots, with one grid reduction. r, s and q are read
+        // on a 2-cell halo and alternate between two banks by iteration; the halo's new u is
+        // recomputed from the old banks, so no CTA waits for its neighbours within a sweep.
+        // Sweep "first" (k = -1) only forms q0 = A u0 and gamma0, delta0 from r0.
+        double gamma = 0.0, delta = 0.0, alpha_prev = 1.0, beta = 0.0;
+        CgPrefetch cf;
+        auto cg_sweep = [&](int k, float alpha_f, float beta_f, double* dots) -> bool {
+            const bool init = k < 0;
+            const bool first = k == 0;
+            const int rb = init ? 0 : (k & 1), wb = init ? 0 : ((k + 1) & 1);
+            double g1 = 0.0, g2 = 0.0, g3 = 0.0;
+            if (cta < ntiles) cg_prefetch(a, cta, rb, init, first, cf);
+            for (int tl = cta; tl < ntiles; tl += ncta) {
+                int i0, j0;
+                tile_origin(a, tl, i0, j0);
+                cg_commit(cf, t, alpha_f, beta_f, init, first);
+                const float he = cf.he;
+                const float2 p_own = cf.p, w_own = cf.x;
+                __syncthreads();
+                if (tl + ncta < ntiles) cg_prefetch(a, tl + ncta, rb, init, first, cf);
+                const float2 q = apply_a(g, t, cx, cy, he);
+                const int i = i0 + cx, j = j0 + cy;
+                if (i < g.nx && j < g.ny) {
+                    const int kk = j * g.pitch + i;
+                    const int c0 = (cy + 2) * PB_W + (cx + 2);
+                    const float2 u = t.sv[c0];
+                    const float2 r = t.sr[c0];
+                    if (!init) {
+                        const float2 sk = t.ss[c0], uk = t.su[c0];
+                        float2 pk = uk;
+                        if (!first) {
+                            pk.x += beta_f * p_own.x;
+                            pk.y += beta_f * p_own.y;
+                        }
+                        a.p0[kk] = pk;
+                        a.w[kk] = make_float2(w_own.x + alpha_f * pk.x, w_own.y + alpha_f * pk.y);
+                        a.sb[wb][kk] = sk;
+                        a.rb[wb][kk] = r;
+                    }
+                    a.qb[wb][kk] = q;
+                    g1 += (double)r.x * u.x + (double)r.y * u.y;
+                    g2 += (double)u.x * q.x + (double)u.y * q.y;
+                    g3 += (double)r.x * r.x + (double)r.y * r.y;
+                }
+                __syncthreads();
+            }
+            return reduce_barrier(a, epoch, g1, g2, g3, dots, red, cta, ncta);
+        };
+        if (!converged) {
+            if (!cg_sweep(-1, 0.f, 0.f, tot)) return false;
+            gamma = tot[0];
+            delta = tot[1];
+        }
         while (!converged && it < a.max_iter) {
-            const float2* p_old = (it & 1) ? a.p1 : a.p0;
-            float2* p_new = (it & 1) ? a.p0 : a.p1;
-            const bool first = it == 0;
-            // sweep A': p = z + beta p on the tile and its halo, then A p and <p, Ap>
-            double pap = 0.0;
-            if (cta < ntiles) box_prefetch<false>(a, cta, p_old, first, f);
-            for (int tl = cta; tl < ntiles; tl += ncta) {
-                int i0, j0;
-                tile_origin(a, tl, i0, j0);
-                box_commit<false>(f, t, beta_f, first);
-                const float he = f.he;
-                __syncthreads();
-                if (tl + ncta < ntiles) box_prefetch<false>(a, tl + ncta, p_old, first, f);
-                const float2 av = apply_a(g, t, cx, cy, he);
-                const int i = i0 + cx, j = j0 + cy;
-                if (i < g.nx && j < g.ny) {
-                    const int k = j * g.pitch + i;
-                    const float2 p = t.sv[(cy + 2) * PB_W + (cx + 2)];
-                    p_new[k] = p;
-                    a.ap[k] = av;
-                    pap += (double)p.x * av.x + (double)p.y * av.y;
-                }
-                __syncthreads();
-            }
-            if (!reduce_barrier(a, epoch, pap, 0.0, 0.0, tot, red, cta, ncta)) return false;
-            const double alpha = rz / tot[0];
-            const float alpha_f = (float)alpha;
-            // sweep B: w += alpha p, r -= alpha Ap, <r, r> and <r, z>
-            double rr = 0.0, rzn = 0.0;
-            CellPrefetch c{};
-            auto cell_load = [&](int tl, CellPrefetch& o) {
-                int i0, j0;
-                tile_origin(a, tl, i0, j0);
-                const int i = i0 + cx, j = j0 + cy;
-                if (i < g.nx && j < g.ny) {
-                    const int k = j * g.pitch + i;
-                    o.p = __ldcg(p_new + k);
-                    o.ap = __ldcg(a.ap + k);
-                    o.w = __ldcg(a.w + k);
-                    o.r = __ldcg(a.r + k);
-                    o.d = __ldcg(a.diag + k);
-                }
-            };
-            if (cta < ntiles) cell_load(cta, c);
-            for (int tl = cta; tl < ntiles; tl += ncta) {
-                const CellPrefetch cur = c;
-                if (tl + ncta < ntiles) cell_load(tl + ncta, c);
-                int i0, j0;
-                tile_origin(a, tl, i0, j0);
-                const int i = i0 + cx, j = j0 + cy;
-                if (i < g.nx && j < g.ny) {
-                    const int k = j * g.pitch + i;
-                    float2 w = cur.w, r = cur.r;
-                    w.x += alpha_f * cur.p.x;
-                    w.y += alpha_f * cur.p.y;
-                    r.x -= alpha_f * cur.ap.x;
-                    r.y -= alpha_f * cur.ap.y;
-                    a.w[k] = w;
-                    a.r[k] = r;
-                    rr += (double)r.x * r.x + (double)r.y * r.y;
-                    rzn += (double)r.x * (r.x / cur.d.x) + (double)r.y * (r.y / cur.d.y);
-                }
-            }
-            if (!reduce_barrier(a, epoch, rr, rzn, 0.0, tot, red, cta, ncta)) return false;
+            const double alpha = it == 0 ? gamma / delta : gamma / (delta - beta * gamma / alpha_prev);
+            if (!cg_sweep((int)it, (float)alpha, (float)beta, tot)) return false;
             it += 1;
-            converged = sqrt(tot[0]) <= target;
-            const double beta = tot[1] / rz;
-            rz = tot[1];
-            beta_f = (float)beta;
+            converged = sqrt(tot[2]) <= target;
+            beta = tot[0] / gamma;
+            gamma = tot[0];
+            delta = tot[1];
+            alpha_prev = alpha;
         }
     }
     if (a.fcg) it += a.fcg->iterations;

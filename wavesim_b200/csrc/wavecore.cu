@@ -97,6 +97,7 @@ struct wc_solver {
     uint8_t* shallow = nullptr;
     float2 *hn = nullptr, *pred = nullptr, *bv = nullptr, *w = nullptr, *r = nullptr, *p0 = nullptr,
            *p1 = nullptr, *ap = nullptr, *diag = nullptr;
+    float2 *r2 = nullptr, *s_a = nullptr, *s_b = nullptr, *q_a = nullptr, *q_b = nullptr;  // CG banks
     float *cc = nullptr, *heff = nullptr;
     double* part = nullptr;   // CTA partials of the solve's reductions
     unsigned* bar = nullptr;  // grid-barrier counters: arrivals, released epoch
@@ -141,7 +142,8 @@ struct wc_solver {
 
     ~wc_solver() {
         void* bufs[] = {q0, q1, bed, prof, ycs, shallow, hn, pred, bv, w, r, p0, p1, ap, diag, cc, heff,
-                        part, bar, ctl, st_h, st_hu, st_hv, r64, diag_bands, diag_done, diag_out, tv, fsc, fpart};
+                        part, bar, ctl, st_h, st_hu, st_hv, r64, diag_bands, diag_done, diag_out, tv, fsc, fpart,
+                        r2, s_a, s_b, q_a, q_b};
         for (void* b : bufs)
             if (b) cudaFree(b);
         if (done_host) cudaFreeHost(done_host);
@@ -298,6 +300,12 @@ PcgArgs pcg_args(const wc_solver* s, int mode, const float4* qold, float4* qout,
     a.p1 = s->p1;
     a.ap = s->ap;
     a.diag = s->diag;
+    a.rb[0] = s->r;
+    a.rb[1] = s->r2;
+    a.sb[0] = s->s_a;
+    a.sb[1] = s->s_b;
+    a.qb[0] = s->q_a;
+    a.qb[1] = s->q_b;
     a.part = s->part;
     a.cnt = s->bar;
     a.hn = s->hn;
@@ -784,6 +792,11 @@ wc_status wc_solver_create(const wc_grid* grid, const double* bed_padded, const 
         ALLOC(s->p1, s->ncell);
         ALLOC(s->ap, s->ncell);
         ALLOC(s->diag, s->ncell);
+        ALLOC(s->r2, s->ncell);
+        ALLOC(s->s_a, s->ncell);
+        ALLOC(s->s_b, s->ncell);
+        ALLOC(s->q_a, s->ncell);
+        ALLOC(s->q_b, s->ncell);
         ALLOC(s->cc, s->ncell);
         ALLOC(s->heff, s->ncell);
         int dev = 0, sms = 0, occ = 0;
