@@ -105,8 +105,9 @@ __device__ __forceinline__ Mapped map_cell(const DevGrid& g, int i, int j) {
     return m;
 }
 
-// solver.rs:90-92
-__device__ __forceinline__ float velocity(float h, float hm) { return h > H_DRY ? hm / h : 0.f; }
+// solver.rs:90-92, with the fast single-precision division (two ulps; the FP32 state is already
+// further from the FP64 reference than that).
+__device__ __forceinline__ float velocity(float h, float hm) { return h > H_DRY ? __fdividef(hm, h) : 0.f; }
 
 // A compensated depth (hi + lo as FP32) widened to FP64, and packed back.
 __device__ __forceinline__ double depth64(float4 q) { return (double)q.x + (double)q.y; }

@@ -28,7 +28,7 @@
 namespace wcb {
 
 constexpr int ST_TX = 32, ST_HALO = 4, ST_BX = ST_TX + 2 * ST_HALO;
-constexpr int ST_TY = 16;  // tile height of the standalone stage kernel
+constexpr int ST_TY = 8;   // tile height of the standalone stage kernel (measured best of 4, 8, 16)
 constexpr int ST_NT = 256; // its block size
 
 // Tile geometry for a TX x TY tile (TX = 32) and the shared-memory layout of one tile, in floats.
@@ -199,7 +199,7 @@ __device__ __forceinline__ void hll_face(const Side& l, const Side& r, float& F0
     } else if (sr <= 0.f) {
         F0 = qr; F2 = tr; RR = mr; RL = mr + dp;
     } else {
-        const float inv = 1.f / (sr - sl);
+        const float inv = __fdividef(1.f, sr - sl);
         const float du0 = hr - hl, du1 = qr - ql, du2 = hr * r.ut - hl * l.ut;
         const float df0 = qr - ql, df1 = (mr - ml) + dp, df2 = tr - tl;
         F0 = ql + sl * (sr * du0 - df0) * inv;
