@@ -31,10 +31,13 @@ constexpr int ST_TX = 32, ST_HALO = 4, ST_BX = ST_TX + 2 * ST_HALO;
 constexpr int ST_TY = 8;   // tile height of the standalone stage kernel (measured best of 4, 8, 16)
 constexpr int ST_NT = 256; // its block size
 
-// Tile geometry for a TX x TY tile (TX = 32) and the shared-memory layout of one tile, in floats.
-template <int TY>
+// Tile geometry for a TX x TY tile (TX = 32) with an H-cell halo (4 for the fifth order and the
+// dispersive coefficients, 2 suffices for second order) and the shared-memory layout of one tile,
+// in floats.
+template <int TY, int H = ST_HALO>
 struct StageGeom {
-    static constexpr int BY = TY + 2 * ST_HALO, NB = ST_BX * BY;
+    static constexpr int HALO = H, BX = ST_TX + 2 * H;
+    static constexpr int BY = TY + 2 * H, NB = BX * BY;
     static constexpr int SX_W = ST_TX + 2, SX_N = SX_W * TY;   // x reconstructions: cx in [-1, TX]
     static constexpr int SY_H = TY + 2, SY_N = ST_TX * SY_H;   // y reconstructions: cy in [-1, TY]
     static constexpr int FX_W = ST_TX + 1, FX_N = FX_W * TY;   // x faces
@@ -52,12 +55,18 @@ struct StageGeom {
     static constexpr int OFF_F = OFF_C + CF_N;
     static constexpr int SMEM_SWE = OFF_DIV * 4;
     static constexpr int SMEM_SGN = (OFF_F + CF_N) * 4;
-    // Face fluxes reuse the box (dead after P3): 4 arrays of FX_N, then 4 of FY_N.
+    // Face fluxes reuse the box (dead after P3; the phi slot too, read only in P3): 4 arrays of
+    // FX_N, then 4 of FY_N.
     static constexpr int OFF_FX = 0, OFF_FY = 4 * FX_N;
-    static_assert(4 * FX_N + 4 * FY_N <= 5 * NB, "face arrays must fit in the box");
+    static_assert(4 * FX_N + 4 * FY_N <= 6 * NB, "face arrays must fit in the box");
 };
 
-constexpr int SMEM_SWE = StageGeom<ST_TY>::SMEM_SWE;
+// The halo a stage variant needs.
+template <int ORDER, bool SGN>
+constexpr int stage_halo() { return (ORDER == 2 || SGN) ? ST_HALO : 2; }
+
+constexpr int SMEM_SWE = StageGeom<ST_TY>::SMEM_SWE;                // fifth order
+constexpr int SMEM_SWE2 = StageGeom<ST_TY, 2>::SMEM_SWE;            // first and second order
 constexpr int SMEM_SGN = StageGeom<ST_TY>::SMEM_SGN;
 
 enum StageMode { MODE_STAGE1 = 0, MODE_STAGE2 = 1, MODE_FIRST = 2 };
@@ -153,9 +162,12 @@ __device__ __forceinline__ void reconstruct(const float* __restrict__ sm, int p,
         blend = fminf(blend, phi[p + 2 * s]);
     }
     float elo, ehi, ulo, uhi, tlo, thi;
-    face_values(eta[p - 2 * s], eta[p - s], eta[p], eta[p + s], eta[p + 2 * s], blend, elo, ehi);
-    face_values(un[p - 2 * s], un[p - s], un[p], un[p + s], un[p + 2 * s], blend, ulo, uhi);
-    face_values(ut[p - 2 * s], ut[p - s], ut[p], ut[p + s], ut[p + 2 * s], blend, tlo, thi);
+    // The outer stencil points are read only by the fifth order (blend > 0), and only its tiles
+    // carry the halo that holds them.
+    const int s2 = ORDER == 2 ? 2 * s : s;
+    face_values(eta[p - s2], eta[p - s], eta[p], eta[p + s], eta[p + s2], blend, elo, ehi);
+    face_values(un[p - s2], un[p - s], un[p], un[p + s], un[p + s2], blend, ulo, uhi);
+    face_values(ut[p - s2], ut[p - s], ut[p], ut[p + s], ut[p + s2], blend, tlo, thi);
     const float sz = 0.25f * (bb[p + s] - bb[p - s]);
     const float zlo = bb[p] - sz, zhi = bb[p] + sz;
     const float hlo = elo - zlo, hhi = ehi - zhi;
@@ -219,8 +231,8 @@ struct StageShared {
 template <int MODE, int ORDER, bool SGN, int TY, int NT>
 __device__ __forceinline__ void stage_tile(const StageArgs& a, int i0, int j0, float* sm,
                                            StageShared& ss, float& rmax, int& nan_here) {
-    using Gm = StageGeom<TY>;
-    constexpr int ST_BY = Gm::BY, ST_NB = Gm::NB;
+    using Gm = StageGeom<TY, stage_halo<ORDER, SGN>()>;
+    constexpr int ST_BX = Gm::BX, ST_BY = Gm::BY, ST_NB = Gm::NB, ST_HALO = Gm::HALO;
     constexpr int SX_W = Gm::SX_W, SX_N = Gm::SX_N, SY_N = Gm::SY_N, FX_W = Gm::FX_W;
     constexpr int FX_N = Gm::FX_N, FY_N = Gm::FY_N, DV_W = Gm::DV_W, DV_N = Gm::DV_N;
     constexpr int CF_W = Gm::CF_W, CF_N = Gm::CF_N, OWN = Gm::OWN;

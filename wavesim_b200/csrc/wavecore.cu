@@ -219,11 +219,11 @@ wc_status configure_kernels() {
     if (done) return st;
     done = true;
 #define ATTR(K, B) CK(cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, B))
-    ATTR((stage_kernel<MODE_STAGE1, 1, false>), SMEM_SWE);
+    ATTR((stage_kernel<MODE_STAGE1, 1, false>), SMEM_SWE2);
     ATTR((stage_kernel<MODE_STAGE1, 2, false>), SMEM_SWE);
-    ATTR((stage_kernel<MODE_STAGE2, 1, false>), SMEM_SWE);
+    ATTR((stage_kernel<MODE_STAGE2, 1, false>), SMEM_SWE2);
     ATTR((stage_kernel<MODE_STAGE2, 2, false>), SMEM_SWE);
-    ATTR((stage_kernel<MODE_FIRST, 0, false>), SMEM_SWE);
+    ATTR((stage_kernel<MODE_FIRST, 0, false>), SMEM_SWE2);
     ATTR((stage_kernel<MODE_STAGE1, 0, true>), SMEM_SGN);
     ATTR((stage_kernel<MODE_STAGE1, 1, true>), SMEM_SGN);
     ATTR((stage_kernel<MODE_STAGE1, 2, true>), SMEM_SGN);
@@ -274,12 +274,12 @@ wc_status launch_stage(wc_solver* s, int mode, const float4* qin, const float4* 
         else if (o == 1) stage_kernel<MODE_STAGE1, 1, true><<<grid, block, SMEM_SGN, st>>>(a);
         else stage_kernel<MODE_STAGE1, 2, true><<<grid, block, SMEM_SGN, st>>>(a);
     } else if (mode == MODE_FIRST) {
-        stage_kernel<MODE_FIRST, 0, false><<<grid, block, SMEM_SWE, st>>>(a);
+        stage_kernel<MODE_FIRST, 0, false><<<grid, block, SMEM_SWE2, st>>>(a);
     } else if (mode == MODE_STAGE1) {
-        if (o == 1) stage_kernel<MODE_STAGE1, 1, false><<<grid, block, SMEM_SWE, st>>>(a);
+        if (o == 1) stage_kernel<MODE_STAGE1, 1, false><<<grid, block, SMEM_SWE2, st>>>(a);
         else stage_kernel<MODE_STAGE1, 2, false><<<grid, block, SMEM_SWE, st>>>(a);
     } else {
-        if (o == 1) stage_kernel<MODE_STAGE2, 1, false><<<grid, block, SMEM_SWE, st>>>(a);
+        if (o == 1) stage_kernel<MODE_STAGE2, 1, false><<<grid, block, SMEM_SWE2, st>>>(a);
         else stage_kernel<MODE_STAGE2, 2, false><<<grid, block, SMEM_SWE, st>>>(a);
     }
     s->launches++;
