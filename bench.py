@@ -359,7 +359,11 @@ def eta_errors(w, net, steps: int):
     for k, s in ss.items():
         hg = g.inner(s.h)
         wet = (hg > 1e-3) & (ho > 1e-3)
-        out[k] = float(np.abs(hg - ho)[wet].max())
+        d = np.abs(hg - ho)[wet]
+        st = arms[k].dispersion_stats()
+        out[k] = {"max": float(d.max()), "rms": float(np.sqrt(np.mean(d * d))), "cells_over_1mm": int((d > 1e-3).sum()),
+                  "nan_cells": int(np.isnan(hg).sum()), "iterations_per_solve": st.iterations / max(1, st.solves),
+                  "unconverged": st.unconverged}
     out["steps"] = steps
     return out
 

@@ -219,3 +219,24 @@ def test_learned_solve_counts_its_iteration_kernels():
     assert st.iterations > 0
     assert n1 - n0 > 30 * st.iterations  # every iteration is ~30 kernels of the device library
     assert math.isfinite(sol.time_device())
+
+
+def test_solvers_sharing_a_network_agree_bit_for_bit():
+    # Regression: set-up copies and memsets used to run on the legacy stream and could land after
+    # the first kernels on the solver's non-blocking stream (a solver then stepped on a partly
+    # uploaded bed). Every solver built from the same inputs must now step identically.
+    w, s0 = small_run(seed=41, nx=256, ny=128)
+    net = LearnedPreconditioner(UNetSpec(), seed=3)
+    outs = []
+    keep = []
+    for k in range(4):
+        sol = w.solver(Solver)
+        sol.set_preconditioner(net)
+        s = s0.clone()
+        for _ in range(5):
+            sol.step(s, 0.05)
+        outs.append(s.h.copy())
+        if k % 2 == 0:
+            keep.append(sol)
+    for o in outs[1:]:
+        assert np.array_equal(o, outs[0])

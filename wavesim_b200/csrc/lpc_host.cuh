@@ -47,6 +47,8 @@ struct DBuf {
         n = count;
         cudaError_t e = cudaMalloc(&p, (count ? count : 1) * sizeof(float));
         if (e == cudaSuccess) e = cudaMemset(p, 0, (count ? count : 1) * sizeof(float));
+        // the memset runs on the legacy stream; the users of the buffer run on non-blocking ones
+        if (e == cudaSuccess) e = cudaStreamSynchronize(0);
         return e;
     }
     ~DBuf() {

@@ -166,6 +166,9 @@ wc_status dalloc(T** p, size_t n) {
     cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
     if (e != cudaSuccess) return set_err(WC_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
     e = cudaMemset(*p, 0, n * sizeof(T));
+    // cudaMemset and pageable cudaMemcpy run on the legacy stream and may return before they
+    // finish; the solvers' streams are non-blocking, so wait here rather than race them.
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
     if (e != cudaSuccess) return set_err(WC_ECUDA, std::string("cudaMemset: ") + cudaGetErrorString(e));
     return WC_OK;
 }
@@ -771,7 +774,8 @@ wc_status wc_solver_create(const wc_grid* grid, const double* bed_padded, const 
             ycs[jj] = make_float2((float)std::cos(s->drive.ky * y), (float)std::sin(s->drive.ky * y));
         }
         if (cudaMemcpy(s->prof, prof.data(), pitch * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(s->ycs, ycs.data(), ny * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess)
+            cudaMemcpy(s->ycs, ycs.data(), ny * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaStreamSynchronize(0) != cudaSuccess)
             return fail(set_err(WC_ECUDA, "maker tables upload failed"));
     }
     if (cfg->shallow_cells) {
@@ -779,7 +783,8 @@ wc_status wc_solver_create(const wc_grid* grid, const double* bed_padded, const 
         std::vector<uint8_t> m(s->ncell, 0);
         for (int jj = 0; jj < ny; jj++)
             for (int ii = 0; ii < nx; ii++) m[(size_t)jj * pitch + ii] = cfg->shallow_cells[(size_t)jj * nx + ii] ? 1 : 0;
-        if (cudaMemcpy(s->shallow, m.data(), s->ncell, cudaMemcpyHostToDevice) != cudaSuccess)
+        if (cudaMemcpy(s->shallow, m.data(), s->ncell, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaStreamSynchronize(0) != cudaSuccess)
             return fail(set_err(WC_ECUDA, "shallow-cell mask upload failed"));
     }
     if (s->sgn) {
@@ -816,7 +821,8 @@ wc_status wc_solver_create(const wc_grid* grid, const double* bed_padded, const 
         return fail(set_err(WC_ENOMEM, "cudaMallocHost failed"));
 
     // The bed, interior only, FP32.
-    if (cudaMemcpy(s->st_h, bed_padded, s->npad * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+    if (cudaMemcpy(s->st_h, bed_padded, s->npad * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaStreamSynchronize(0) != cudaSuccess)
         return fail(set_err(WC_ECUDA, "bed upload failed"));
     pack_f32_kernel<<<aux_grid(s->ncell), AUX_NT, 0, s->stream>>>(s->g, s->st_h, s->bed);
     s->launches++;
@@ -1214,6 +1220,7 @@ wc_status build_variant(wc_ensemble* e, EnVariant& v, int ctas) {
     if (!v.d_cta_member) CK(cudaMalloc(&v.d_cta_member, (size_t)e->max_ctas * EN_VARIANTS * sizeof(int)));
     CK(cudaMemcpy(v.d_table, v.table.data(), n * sizeof(EnsembleMember), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(v.d_cta_member, cta_member.data(), used * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaStreamSynchronize(0));
     return WC_OK;
 }
 
@@ -1484,6 +1491,7 @@ wc_status wc_lpc_create(const int32_t* channels, int32_t gate_hidden, int32_t st
         std::vector<float> p;
         lpc_init_host(l->m.net, seed, p);
         st = lpc_ck(cudaMemcpy(l->m.w.p, p.data(), p.size() * sizeof(float), cudaMemcpyHostToDevice), "upload");
+        if (st == WC_OK) st = lpc_ck(cudaStreamSynchronize(0), "upload");
         if (st == WC_OK) st = lpc_ck(l->m.refresh(), "refresh");
         if (st == WC_OK) st = lpc_ck(cudaStreamSynchronize(l->m.st), "init");
     }
@@ -1572,6 +1580,7 @@ wc_status wc_lpc_harvest(wc_lpc* l, wc_solver* s) {
         if (st == WC_OK)
             st = lpc_ck(cudaMemcpy(pr.first->p, pr.second, s->ncell * sizeof(float), cudaMemcpyDeviceToDevice), "copy");
     }
+    if (st == WC_OK) st = lpc_ck(cudaStreamSynchronize(0), "copy");  // device copies return early
     if (st != WC_OK) {
         delete q;
         return st;
@@ -1682,6 +1691,7 @@ wc_status wc_solver_set_lpc(wc_solver* s, wc_lpc* l) {
         CK(cudaMemset(s->tv, 0, s->ncell * sizeof(float2)));
         CK(cudaMalloc(&s->fsc, sizeof(FcgScalars)));
         CK(cudaMemset(s->fsc, 0, sizeof(FcgScalars)));
+        CK(cudaStreamSynchronize(0));
         CK(cudaMalloc(&s->fpart, 3 * FCG_BLOCKS * sizeof(double)));
         CK(cudaMallocHost(&s->done_host, sizeof(int)));
         CK(cudaStreamCreateWithFlags(&s->body_stream, cudaStreamNonBlocking));
