@@ -46,6 +46,11 @@ SOLVE_ITER_BYTES = (8 * 4 + 8 * 2 + 4 * 2) + 8 * 5  # read r, q, s, diag, p, w, 
 SOLVE_FINISH_BYTES = (44 + 60) / 2              # stage 1 / stage 2 epilogue, averaged
 STAGE_BYTES_SWE = (36 + 52) / 2                 # stage 1 / stage 2 (RK average + damping)
 
+# DRAM bytes per cell measured by ncu (one capture each; scaled to a launch by cells, and by
+# iterations for the solve): profiles/network_conv_2048x1024.md, profiles/pcg_kernel_sgn_2048x1024.md.
+NETWORK_DRAM_BYTES_PER_CELL = 1.0265e9 / (2048 * 1024)   # one application of the U-net
+PCG_DRAM_BYTES_PER_CELL_ITER = 10.52e9 / (2048 * 1024 * 57)  # one iteration of the solve
+
 
 def workload(name: str):
     return {"config1": W.config1, "config2": W.config2, "config3": W.config3, "config5": W.config5,
@@ -393,7 +398,12 @@ def run_b200(args, world, rank, local):
         from wavesim_b200.lpc import UNetSpec
 
         spec = UNetSpec(channels=tuple(int(c) for c in args.lpc_channels.split(",")), stride=args.lpc_stride)
-        net, train_rec = trained_network(dx=w.grid.dx, steps=args.train_steps, seed=0, spec=spec)
+        if args.train_steps > 0:
+            net, train_rec = trained_network(dx=w.grid.dx, steps=args.train_steps, seed=0, spec=spec)
+        else:  # an untrained network (profiling runs: same kernels, no harvest or training launches)
+            from wavesim_b200 import LearnedPreconditioner
+
+            net, train_rec = LearnedPreconditioner(spec, seed=0), {"untrained": True}
         torch.cuda.synchronize()
     arm = measure_arm(w, args, world, stream, flush, net)
     plain = measure_arm(w, args, world, stream, flush, None) if learned else None
@@ -413,7 +423,9 @@ def run_b200(args, world, rank, local):
             tflops = flops / (net_ms / net_n / 1e3) / 1e12
             roof = {"bound": "compute (FP32 CUDA-core convolutions)", "kernel": "conv_fwd_kernel chain (one network application)",
                     "achieved": tflops, "unit": "TFLOP/s", "flops_per_cell": spec.flops_per_cell() / spec.stride**2,
-                    "avg_ms": net_ms / net_n, "traffic": None}
+                    "avg_ms": net_ms / net_n,
+                    "traffic": NETWORK_DRAM_BYTES_PER_CELL * w.grid.nx * w.grid.ny / spec.stride**2,
+                    "traffic_source": "ncu DRAM bytes of one application at 2048x1024, scaled by cells"}
             bf16 = peak_tensor()
             roof.update({"peak": bf16[0], "frac": tflops / bf16[0], "peak_source": bf16[1]})
         else:
@@ -426,9 +438,14 @@ def run_b200(args, world, rank, local):
                 dom = {"kernel": "stage_kernel (fused RK stage)", "launches": stage_n,
                        "avg_ms": stage_ms / max(1, stage_n), "bytes_per_cell": per_cell}
             achieved = per_cell * cells / (dom["avg_ms"] / 1e3) / 1e9
+            traffic = None
+            if dom["kernel"].startswith("pcg_kernel"):
+                traffic = PCG_DRAM_BYTES_PER_CELL_ITER * iters_prof * cells
             roof = {"bound": "hbm", "kernel": dom["kernel"], "achieved": achieved, "peak": peak, "unit": "GB/s",
                     "frac": achieved / peak, "peak_source": peak_kind, "algorithmic_bytes_per_cell": dom["bytes_per_cell"],
-                    "avg_ms": dom["avg_ms"], "traffic": None}
+                    "avg_ms": dom["avg_ms"], "traffic": traffic,
+                    "traffic_source": "ncu DRAM bytes per cell and iteration of one solve at 2048x1024, scaled by cells "
+                                      "and iterations" if traffic else None}
         line = {
             "metric": METRIC,
             "value": arm["value"],
