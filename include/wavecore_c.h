@@ -308,6 +308,41 @@ wc_status wc_lpc_train(wc_lpc* l, uint32_t steps, uint32_t batch, uint32_t patch
  * is attached. */
 wc_status wc_solver_set_lpc(wc_solver* s, wc_lpc* l);
 
+/* ---- Per-step statistics and frames ------------------------------------------------------------
+ *
+ * The reference's driver records statistics after every step of a run in a host loop over the
+ * grid (crates/wavesim/src/lib.rs:1276-1301, Stage::record; 899-931, Stats; 1095-1169,
+ * FirstHarmonic) and writes frames of the surface and the breaking indicator
+ * (lib.rs:1348-1380, frame_if_due). A recorder keeps the same per-cell sums on the device and is
+ * updated by kernels appended to every step of its solver (host-array or device-resident). */
+typedef struct wc_recorder wc_recorder;
+
+typedef struct wc_record_summary {
+    double seconds;        /* recorded time */
+    uint64_t waves;        /* whole wave periods closed */
+    int32_t has_harmonic;  /* 0: too little time to separate a mean, a cosine and a sine */
+    int32_t has_unsettled;
+    double unsettled;      /* lib.rs:1316-1338: median relative change of the per-wave height per period */
+} wc_record_summary;
+
+/* Start recording the solver's steps: statistics count from time `from`; `period` is the swell's
+ * period (per-wave heights and the first harmonic). One recorder per solver; it must be destroyed
+ * before the solver, or it is detached and inert once the solver is gone. */
+wc_status wc_recorder_create(wc_solver* s, double from, double period, wc_recorder** out);
+void wc_recorder_destroy(wc_recorder* r);
+/* The statistics so far, interior row-major arrays of nx*ny values (any may be null): the surface's
+ * maximum and minimum, the mean crest-to-trough height per wave (NaN before a whole wave), the
+ * fraction of the recorded time spent breaking (indicator >= 0.8, lib.rs:1222) and, in
+ * `harmonic` (2 values per cell), the first harmonic's (a, -b) of eta = m + a cos wt + b sin wt
+ * (NaN while has_harmonic is 0). */
+wc_status wc_recorder_read(wc_recorder* r, wc_record_summary* summary, double* eta_max,
+                           double* eta_min, double* wave_height, double* breaking_fraction,
+                           double* harmonic);
+/* A frame of the resident state (lib.rs:1348-1380): eta = h + b and the breaking indicator as
+ * FP32, interior row-major, and the highest surface above `tide` among cells deeper than 1 mm.
+ * Returns WC_ENAN (frame still written) when the surface is not finite or more than 100 m up. */
+wc_status wc_frame(wc_solver* s, double tide, float* eta, float* breaking, double* rise);
+
 /* Kernel launches this solver has queued since it was created (for accounting). */
 uint64_t wc_launch_count(const wc_solver* s);
 /* Human-readable text of the last error on this thread ("" if none). */

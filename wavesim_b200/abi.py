@@ -123,3 +123,8 @@ DPTR = C.POINTER(C.c_double)
 def dptr(a):
     """Pointer to the data of a C-contiguous float64 numpy array."""
     return a.ctypes.data_as(DPTR)
+
+
+class wc_record_summary(C.Structure):
+    _fields_ = [("seconds", C.c_double), ("waves", C.c_uint64), ("has_harmonic", C.c_int32),
+                ("has_unsettled", C.c_int32), ("unsettled", C.c_double)]

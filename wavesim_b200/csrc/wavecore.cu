@@ -20,6 +20,7 @@
 #include "ensemble.cuh"
 #include "lpc_host.cuh"
 #include "pcg.cuh"
+#include "record.cuh"
 #include "stage.cuh"
 
 using namespace wcb;
@@ -139,11 +140,15 @@ struct wc_solver {
     cudaStream_t body_stream = nullptr;
     unsigned long long fcg_body_launches = 0;  // kernels per flexible-CG iteration
     unsigned long long fcg_iter_base = 0;      // flexible-CG iterations before the network was attached
+    // Per-step statistics (wc_recorder): recorded after every step when attached.
+    struct wc_recorder* rec = nullptr;
+    float* frame = nullptr;  // staging of wc_frame: eta and the breaking indicator, FP32
 
-    ~wc_solver() {
+    ~wc_solver();
+    void free_all() {
         void* bufs[] = {q0, q1, bed, prof, ycs, shallow, hn, pred, bv, w, r, p0, p1, ap, diag, cc, heff,
                         part, bar, ctl, st_h, st_hu, st_hv, r64, diag_bands, diag_done, diag_out, tv, fsc, fpart,
-                        r2, s_a, s_b, q_a, q_b};
+                        r2, s_a, s_b, q_a, q_b, frame};
         for (void* b : bufs)
             if (b) cudaFree(b);
         if (done_host) cudaFreeHost(done_host);
@@ -497,7 +502,9 @@ wc_status launch_solve(wc_solver* s, int mode, const float4* qold, float4* qout)
 }
 
 // One SSP-RK2 step (solver.rs:479-507) of size ctl->dt on the device-resident state q0.
-wc_status enqueue_step_direct(wc_solver* s) {
+wc_status enqueue_record(wc_solver* s);
+
+wc_status enqueue_step_kernels(wc_solver* s) {
     if (s->order == WC_ORDER_FIRST) {
         TRY(launch_stage(s, MODE_FIRST, s->q0, s->q0, s->q1, false));
         if (s->sgn) TRY(launch_solve(s, MODE_FIRST, s->q0, s->q1));
@@ -513,6 +520,12 @@ wc_status enqueue_step_direct(wc_solver* s) {
     TRY(launch_solve(s, MODE_STAGE1, s->q0, s->q1));
     TRY(launch_stage(s, MODE_STAGE1, s->q1, s->q0, s->q1, true));
     TRY(launch_solve(s, MODE_STAGE2, s->q0, s->q0));
+    return WC_OK;
+}
+
+wc_status enqueue_step_direct(wc_solver* s) {
+    TRY(enqueue_step_kernels(s));
+    if (s->rec) TRY(enqueue_record(s));
     return WC_OK;
 }
 
@@ -1701,6 +1714,248 @@ wc_status wc_solver_set_lpc(wc_solver* s, wc_lpc* l) {
     s->lpc = &l->m;
     s->pc = WC_PC_LEARNED;
     s->fcg_iter_base = c.fcg_iterations;  // the kernels per iteration are counted at the first solve
+    return WC_OK;
+}
+
+}  // extern "C"
+
+// ---- per-step statistics and frames -----------------------------------------------------------
+
+struct wc_recorder {
+    wc_solver* s = nullptr;  // cleared when the solver goes first
+    RecDev* rd = nullptr;
+    RecArrays ra{};
+    double* block = nullptr;  // one allocation behind every array of ra
+    size_t cells = 0;
+    ~wc_recorder() {
+        if (rd) cudaFree(rd);
+        if (block) cudaFree(block);
+    }
+};
+
+wc_solver::~wc_solver() {
+    if (rec) rec->s = nullptr;
+    free_all();
+}
+
+namespace {
+
+wc_status enqueue_record(wc_solver* s) {
+    wc_recorder* r = s->rec;
+    const size_t cells = r->cells;
+    const unsigned blocks = (unsigned)std::min<size_t>(148 * 8, (cells + 255) / 256);
+    record_cells_kernel<<<blocks, 256, 0, s->stream>>>(s->g, s->q0, s->bed, s->br, s->ctl, r->rd, r->ra);
+    record_finish_kernel<<<1, 32, 0, s->stream>>>(s->ctl, r->rd);
+    s->launches += 2;
+    CK(cudaGetLastError());
+    return WC_OK;
+}
+
+__global__ void fill_kernel(double* a, size_t n, double v) {
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) a[q] = v;
+}
+
+// eta = h + b and the breaking indicator of the resident state, FP32, interior row-major.
+__global__ void frame_kernel(DevGrid g, const float4* __restrict__ q, const float* __restrict__ bed, BreakingDev br,
+                             float* __restrict__ eta, float* __restrict__ brk, float* __restrict__ depth) {
+    const size_t cells = (size_t)g.nx * g.ny;
+    for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < cells; c += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(c % g.nx), j = (int)(c / g.nx);
+        const int k = j * g.pitch + i;
+        const double h = depth64(q[k]);
+        eta[c] = (float)(h + (double)bed[k]);
+        brk[c] = breaking_off(g, q, bed, br, i, j);
+        depth[c] = (float)h;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+wc_status wc_recorder_create(wc_solver* s, double from, double period, wc_recorder** out) {
+    if (!out) return set_err(WC_EINVAL, "out is null");
+    *out = nullptr;
+    if (!s) return set_err(WC_EINVAL, "null solver");
+    if (!(period > 0.0) || !std::isfinite(period)) return set_err(WC_EINVAL, "period must be positive");
+    if (s->rec) return set_err(WC_EINVAL, "the solver already has a recorder");
+    CK(cudaStreamSynchronize(s->stream));
+    Ctl c{};
+    CK(cudaMemcpy(&c, s->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost));
+    auto* r = new wc_recorder();
+    auto fail = [&](wc_status st) {
+        delete r;
+        return st;
+    };
+    r->s = s;
+    r->cells = (size_t)s->grid.nx * s->grid.ny;
+    const size_t n = r->cells;
+    if (cudaMalloc(&r->block, 11 * n * sizeof(double)) != cudaSuccess || cudaMalloc(&r->rd, sizeof(RecDev)) != cudaSuccess)
+        return fail(set_err(WC_ENOMEM, "recorder allocation failed"));
+    double* b = r->block;
+    r->ra.eta_max = b;
+    r->ra.eta_min = b + n;
+    r->ra.wave_max = b + 2 * n;
+    r->ra.wave_min = b + 3 * n;
+    r->ra.wave_sum = b + 4 * n;
+    r->ra.wave_first = b + 5 * n;
+    r->ra.wave_last = b + 6 * n;
+    r->ra.breaking_seconds = b + 7 * n;
+    r->ra.harm = b + 8 * n;
+    const unsigned blocks = (unsigned)std::min<size_t>(148 * 8, (n + 255) / 256);
+    fill_kernel<<<blocks, 256, 0, s->stream>>>(r->ra.eta_max, n, -INFINITY);
+    fill_kernel<<<blocks, 256, 0, s->stream>>>(r->ra.eta_min, n, INFINITY);
+    fill_kernel<<<blocks, 256, 0, s->stream>>>(r->ra.wave_max, n, -INFINITY);
+    fill_kernel<<<blocks, 256, 0, s->stream>>>(r->ra.wave_min, n, INFINITY);
+    if (cudaMemsetAsync(r->ra.wave_sum, 0, 7 * n * sizeof(double), s->stream) != cudaSuccess)
+        return fail(set_err(WC_ECUDA, "recorder set-up failed"));
+    // lib.rs:1255-1268: the first wave ends a period after the later of the start and `from`
+    RecDev d{};
+    d.from = from;
+    d.period = period;
+    d.omega = TAU / period;
+    d.next_wave = std::max(from, c.t) + period;
+    d.t_last = c.t;
+    if (cudaMemcpyAsync(r->rd, &d, sizeof d, cudaMemcpyHostToDevice, s->stream) != cudaSuccess ||
+        cudaStreamSynchronize(s->stream) != cudaSuccess)
+        return fail(set_err(WC_ECUDA, "recorder set-up failed"));
+    if (s->step_graph) {  // the captured step gains the recording kernels
+        cudaGraphExecDestroy(s->step_graph);
+        s->step_graph = nullptr;
+    }
+    s->rec = r;
+    *out = r;
+    return WC_OK;
+}
+
+void wc_recorder_destroy(wc_recorder* r) {
+    if (!r) return;
+    if (r->s) {
+        cudaStreamSynchronize(r->s->stream);
+        if (r->s->rec == r) {
+            r->s->rec = nullptr;
+            if (r->s->step_graph) {
+                cudaGraphExecDestroy(r->s->step_graph);
+                r->s->step_graph = nullptr;
+            }
+        }
+    }
+    delete r;
+}
+
+wc_status wc_recorder_read(wc_recorder* r, wc_record_summary* sum, double* eta_max, double* eta_min,
+                           double* wave_height, double* breaking_fraction, double* harmonic) {
+    if (!r || !r->s) return set_err(WC_EINVAL, "null recorder");
+    wc_solver* s = r->s;
+    const size_t n = r->cells;
+    CK(cudaStreamSynchronize(s->stream));
+    RecDev d{};
+    CK(cudaMemcpy(&d, r->rd, sizeof d, cudaMemcpyDeviceToHost));
+    auto get = [&](const double* src, std::vector<double>& v) -> wc_status {
+        v.resize(n);
+        CK(cudaMemcpy(v.data(), src, n * sizeof(double), cudaMemcpyDeviceToHost));
+        return WC_OK;
+    };
+    if (eta_max) CK(cudaMemcpy(eta_max, r->ra.eta_max, n * sizeof(double), cudaMemcpyDeviceToHost));
+    if (eta_min) CK(cudaMemcpy(eta_min, r->ra.eta_min, n * sizeof(double), cudaMemcpyDeviceToHost));
+    std::vector<double> first, last, tmp;
+    // lib.rs:1303-1314: the mean per-wave height, NaN before a whole wave has passed
+    if (wave_height) {
+        TRY(get(r->ra.wave_sum, tmp));
+        for (size_t c = 0; c < n; c++) wave_height[c] = d.waves > 0 ? tmp[c] / (double)d.waves : NAN;
+    }
+    // lib.rs:1340-1344
+    if (breaking_fraction) {
+        TRY(get(r->ra.breaking_seconds, tmp));
+        const double t = std::max(d.seconds, 2.2250738585072014e-308);
+        for (size_t c = 0; c < n; c++) breaking_fraction[c] = tmp[c] / t;
+    }
+    // FirstHarmonic::amplitudes (lib.rs:1132-1168): (a, -b) per cell from the 3x3 normal equations
+    int has_harmonic = 0;
+    if (harmonic || sum) {
+        const double S = d.moments[0], C = d.moments[1], N = d.moments[2], CC = d.moments[3], CS = d.moments[4],
+                     SS = d.moments[5];
+        const double m[3][3] = {{S, C, N}, {C, CC, CS}, {N, CS, SS}};
+        auto cof = [&](int rr, int k) {
+            const int r1 = (rr + 1) % 3, r2 = (rr + 2) % 3, k1 = (k + 1) % 3, k2 = (k + 2) % 3;
+            return m[r1][k1] * m[r2][k2] - m[r1][k2] * m[r2][k1];
+        };
+        double det = 0.0;
+        for (int k = 0; k < 3; k++) det += m[0][k] * cof(0, k);
+        has_harmonic = !(std::isnan(det) || det <= 1e-3 * S * S * S / 4.0);
+        if (harmonic) {
+            std::vector<double> h3(3 * n);
+            CK(cudaMemcpy(h3.data(), r->ra.harm, 3 * n * sizeof(double), cudaMemcpyDeviceToHost));
+            for (size_t c = 0; c < n; c++) {
+                if (!has_harmonic) {
+                    harmonic[2 * c] = harmonic[2 * c + 1] = NAN;
+                    continue;
+                }
+                const double e[3] = {h3[c], h3[n + c], h3[2 * n + c]};
+                auto row = [&](int rr) {
+                    double v = 0.0;
+                    for (int k = 0; k < 3; k++) v += cof(k, rr) / det * e[k];
+                    return v;
+                };
+                harmonic[2 * c] = row(1);
+                harmonic[2 * c + 1] = -row(2);
+            }
+        }
+    }
+    if (sum) {
+        sum->seconds = d.seconds;
+        sum->waves = (uint64_t)d.waves;
+        sum->has_harmonic = has_harmonic;
+        // lib.rs:1316-1338: median over the middle half of the rows, cells with a first wave
+        // above 0.3 m, of |last / first - 1| / (waves - 1)
+        sum->has_unsettled = 0;
+        sum->unsettled = NAN;
+        if (d.waves >= 2) {
+            TRY(get(r->ra.wave_first, first));
+            TRY(get(r->ra.wave_last, last));
+            const size_t nx = s->grid.nx, ny = s->grid.ny;
+            std::vector<double> change;
+            for (size_t j = ny / 4; j < ny - ny / 4; j++)
+                for (size_t i = 0; i < nx; i++) {
+                    const size_t c = j * nx + i;
+                    if (first[c] > 0.3) change.push_back(std::fabs(last[c] / first[c] - 1.0) / (double)(d.waves - 1));
+                }
+            if (!change.empty()) {
+                std::sort(change.begin(), change.end());
+                sum->unsettled = change[change.size() / 2];
+                sum->has_unsettled = 1;
+            }
+        }
+    }
+    return WC_OK;
+}
+
+wc_status wc_frame(wc_solver* s, double tide, float* eta, float* breaking, double* rise) {
+    if (!s || !eta || !breaking || !rise) return set_err(WC_EINVAL, "null argument");
+    const size_t n = (size_t)s->grid.nx * s->grid.ny;
+    if (!s->frame) {
+        CK(cudaMalloc(&s->frame, 3 * n * sizeof(float)));
+    }
+    const unsigned blocks = (unsigned)std::min<size_t>(148 * 8, (n + 255) / 256);
+    frame_kernel<<<blocks, 256, 0, s->stream>>>(s->g, s->q0, s->bed, s->br, s->frame, s->frame + n, s->frame + 2 * n);
+    s->launches++;
+    CK(cudaGetLastError());
+    std::vector<float> depth(n);
+    CK(cudaMemcpyAsync(eta, s->frame, n * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaMemcpyAsync(breaking, s->frame + n, n * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaMemcpyAsync(depth.data(), s->frame + 2 * n, n * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    // lib.rs:1350-1366: the highest surface over still water among wet cells; a surface that is
+    // not finite or more than 100 m up means the run is unstable
+    double up = 0.0;
+    bool finite = true;
+    for (size_t c = 0; c < n; c++) {
+        if (!std::isfinite(eta[c])) finite = false;
+        if (depth[c] > 1e-3f) up = std::max(up, (double)eta[c] - tide);
+    }
+    *rise = up;
+    if (!finite || !std::isfinite(up) || up > 100.0)
+        return set_err(WC_ENAN, "the surface is not finite or more than 100 m above still water");
     return WC_OK;
 }
 

@@ -70,6 +70,10 @@ EXPORTS = [
     "wc_lpc_num_systems",
     "wc_lpc_train",
     "wc_solver_set_lpc",
+    "wc_recorder_create",
+    "wc_recorder_destroy",
+    "wc_recorder_read",
+    "wc_frame",
 ]
 
 
@@ -146,6 +150,13 @@ def load(path: str = LIB_PATH):
     for name in ("wc_lpc_create", "wc_lpc_set_params", "wc_lpc_get_params", "wc_lpc_set_rounding",
                  "wc_lpc_forward_backward", "wc_lpc_loss_grad", "wc_lpc_harvest", "wc_lpc_train",
                  "wc_solver_set_lpc"):
+        getattr(L, name).restype = C.c_int
+    L.wc_recorder_create.argtypes = [V, C.c_double, C.c_double, C.POINTER(V)]
+    L.wc_recorder_destroy.argtypes = [V]
+    L.wc_recorder_destroy.restype = None
+    L.wc_recorder_read.argtypes = [V, C.POINTER(abi.wc_record_summary), D, D, D, D, D]
+    L.wc_frame.argtypes = [V, C.c_double, F, F, D]
+    for name in ("wc_recorder_create", "wc_recorder_read", "wc_frame"):
         getattr(L, name).restype = C.c_int
     L.wc_launch_count.argtypes = [V]
     L.wc_launch_count.restype = C.c_uint64
@@ -305,6 +316,18 @@ class Solver(SolverConfig):
         _check(load().wc_time_device(self._h(), C.byref(t)))
         return t.value
 
+    def frame(self, tide: float = 0.0):
+        """A frame of the resident state (crates/wavesim/src/lib.rs:1348-1380): eta and the
+        breaking indicator, FP32 (ny, nx), and the highest surface above `tide` over wet cells.
+        Raises when the surface is not finite or more than 100 m up (the driver's Unstable)."""
+        n = self.grid.nx * self.grid.ny
+        eta = np.zeros(n, dtype=np.float32)
+        brk = np.zeros(n, dtype=np.float32)
+        rise = C.c_double()
+        _check(load().wc_frame(self._h(), float(tide), _fptr(eta), _fptr(brk), C.byref(rise)))
+        shape = (self.grid.ny, self.grid.nx)
+        return eta.reshape(shape), brk.reshape(shape), rise.value
+
     def set_preconditioner(self, net: "LearnedPreconditioner | None") -> None:
         """Attach a trained network (learned-preconditioned flexible CG) or detach it (None:
         Jacobi PCG, the reference's method)."""
@@ -411,6 +434,50 @@ class LearnedPreconditioner:
         net = cls(spec)
         net.set_params(np.load(path))
         return net
+
+
+class Recorder:
+    """Per-step statistics of a solver's run (`wc_recorder_*`): the reference driver's
+    `Stage::record` (crates/wavesim/src/lib.rs:1276-1301) kept on the device. Every step the solver
+    takes after this is created (host arrays or device-resident) is recorded."""
+
+    def __init__(self, solver: "Solver", start_from: float, period: float):
+        out = C.c_void_p()
+        _check(load().wc_recorder_create(solver._h(), float(start_from), float(period), C.byref(out)))
+        self._handle = out
+        self._solver = solver  # the solver must outlive the recorder
+        self.grid = solver.grid
+
+    def close(self):
+        if getattr(self, "_handle", None):
+            load().wc_recorder_destroy(self._handle)
+        self._handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def read(self) -> dict:
+        """seconds, waves, unsettled (or None) and the per-cell (ny, nx) arrays eta_max, eta_min,
+        wave_height (None before a whole wave), breaking_fraction and harmonic (complex a - ib,
+        or None while the samples cannot separate it)."""
+        n = self.grid.nx * self.grid.ny
+        arrs = {k: np.zeros(n) for k in ("eta_max", "eta_min", "wave_height", "breaking_fraction")}
+        harm = np.zeros(2 * n)
+        sm = abi.wc_record_summary()
+        _check(load().wc_recorder_read(self._handle, C.byref(sm), *(abi.dptr(arrs[k]) for k in
+                                       ("eta_max", "eta_min", "wave_height", "breaking_fraction")), abi.dptr(harm)))
+        shape = (self.grid.ny, self.grid.nx)
+        out = {k: v.reshape(shape) for k, v in arrs.items()}
+        if sm.waves == 0:
+            out["wave_height"] = None
+        out["harmonic"] = (harm[0::2] + 1j * harm[1::2]).reshape(shape) if sm.has_harmonic else None
+        out["seconds"] = sm.seconds
+        out["waves"] = int(sm.waves)
+        out["unsettled"] = sm.unsettled if sm.has_unsettled else None
+        return out
 
 
 class Ensemble:
