@@ -287,6 +287,11 @@ wc_status wc_lpc_set_rounding(wc_lpc* l, int32_t bf16);
 wc_status wc_lpc_forward_backward(wc_lpc* l, int32_t n, int32_t h, int32_t w, const float* x,
                                   const float* feat, const float* dy, float* y, float* grad,
                                   float* dx);
+/* The network's output (inference: no training state kept) on host arrays x and feat,
+ * [n][2][h][w] (h, w multiples of 8). tensor != 0: BF16 activations on the tensor cores, as the
+ * solver applies it; 0: FP32 FMA, as training does. */
+wc_status wc_lpc_forward(wc_lpc* l, int32_t n, int32_t h, int32_t w, const float* x,
+                         const float* feat, int32_t tensor, float* y);
 /* The training objective on given patches, for checking its gradient: c, heff and bed are
  * [n][h][w] (the mask h >= 5 cm and the features h / 20 m, b / 20 m are derived as for harvested
  * crops), e the error fields [n][2][h][w]; returns the loss (as wc_lpc_train defines it) and its

@@ -76,6 +76,22 @@ def test_forward_uses_bf16_rounded_weights():
     assert np.array_equal(net.get_params(), p)  # the master weights stay FP32
 
 
+def test_tensor_core_inference_matches_the_oracle_to_bf16():
+    # The solver's network: BF16 activations on the tensor cores, FP32 accumulation. Against the
+    # FP64 oracle with the same (BF16-rounded) weights: a few BF16 roundings per layer.
+    spec = UNetSpec()
+    net = LearnedPreconditioner(spec)
+    p = random_params(spec, 11)
+    net.set_params(p)
+    x, feat, _ = batch(12, n=2, h=32, w=48)
+    yt = net.forward(x, feat, tensor=True)
+    yf = net.forward(x, feat, tensor=False)
+    yo, _ = U.forward(spec, bf16_round(p).astype(np.float64), x.astype(np.float64), feat.astype(np.float64))
+    assert rel(yf, yo) < 2e-5
+    assert rel(yt, yo) < 3e-2
+    assert rel(yt, yo) > 1e-5  # the tensor path does round to BF16
+
+
 def test_training_loss_and_gradient_match_the_fp64_oracle():
     # The whole training objective (the cycle on patches, the energy-norm loss) and its gradient
     # through the cycle and the network, against the FP64 oracle (FP32 weights on both sides).

@@ -19,6 +19,7 @@ struct ConvArgs {
     const float* b;  // second input (concatenated after a), at H x W, or null
     int cb;
     const float* w;     // [co][ca + cb][k][k]
+    const unsigned short* wre;  // the same as BF16 in the tensor-core kernel's [8 tiles][k k CP] order, or null
     const float* bias;  // [co] or null
     const float* gate;  // [n][co][H][W] or null: y = act(conv + bias) * gate
     float* y;           // [n][co][H][W]
@@ -120,6 +121,125 @@ __global__ void __launch_bounds__(CV_TH* CV_TH) conv_fwd_kernel(ConvArgs p) {
                 p.y[k] = v;
             }
         }
+}
+
+// ---- inference convolution on the tensor cores ------------------------------------------------
+//
+// The same convolution as conv_fwd_kernel as an implicit GEMM on BF16 tensor-core MMAs
+// (mma.sync m16n8k16, FP32 accumulation): M = pixels (one row of 16 per MMA), N = output channels
+// (tiles of 8), K = taps x input channels (k = tap * CP + c, channels padded to CP, a multiple of
+// 16, so one K step is 16 channels of one tap). The block stages its 16 x 8 pixel tile plus halo
+// with the channels innermost (pixel stride CP + 2 halves: conflict-free 32-bit reads of channel
+// pairs) and all weights reordered to the same K, BF16, in shared memory; each warp owns two
+// pixel rows. The small channel counts of this network leave it memory-bound: the tensor cores
+// take the arithmetic off the FMA pipes.
+constexpr int CM_TX = 16, CM_TY = 16, CM_NT = 256, CM_NMAX = 8;  // N tiles of 8: up to 64 channels
+
+__device__ __forceinline__ unsigned short bf16_bits(float x) {  // nearest, ties to even (finite x)
+    const unsigned a = __float_as_uint(x);
+    return (unsigned short)((a + 0x7FFFu + ((a >> 16) & 1u)) >> 16);
+}
+
+__device__ __forceinline__ void mma_bf16_16816(float* d, const unsigned* a, const unsigned* b) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+__host__ __device__ inline int conv_mma_cp(int ci) { return (ci + 15) / 16 * 16; }
+
+// Shared memory of one block (bytes): inputs [TY + 2R][TX + 2R][CP + 2], weights [8 nt][KK CP].
+__host__ __device__ inline size_t conv_mma_smem(int ci, int co, int kk) {
+    const int r = kk == 9 ? 1 : 0, cp = conv_mma_cp(ci);
+    return ((size_t)(CM_TY + 2 * r) * (CM_TX + 2 * r) * (cp + 2) + (size_t)((co + 7) / 8) * 8 * kk * cp) * 2;
+}
+
+// The weights [co][ci][tap] (FP32 holding BF16 values) as BF16 in the order [8 ntl][tap CP + c].
+__global__ void conv_mma_weights_kernel(const float* __restrict__ w, int co_n, int ci_n, int kk, int ntl,
+                                        unsigned short* __restrict__ out) {
+    const int cp = conv_mma_cp(ci_n), kp = kk * cp;
+    const int total = ntl * 8 * kp;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < total; q += gridDim.x * blockDim.x) {
+        const int co = q / kp, k = q % kp;
+        const int tap = k / cp, c = k - tap * cp;
+        out[q] = (co < co_n && c < ci_n) ? (unsigned short)(__float_as_uint(w[((size_t)co * ci_n + c) * kk + tap]) >> 16)
+                                        : (unsigned short)0;
+    }
+}
+
+template <int KK, int NTL>  // taps: 9 (3x3) or 1 (1x1); N tiles of 8 channels: 1, 2, 4 or 8
+__global__ void __launch_bounds__(CM_NT) conv_mma_kernel(ConvArgs p) {
+    constexpr int R = KK == 9 ? 1 : 0, EW = CM_TX + 2 * R, EH = CM_TY + 2 * R;
+    extern __shared__ __align__(16) unsigned short cm_smem[];
+    const int ci_total = p.ca + p.cb;
+    const int CP = conv_mma_cp(ci_total), PS = CP + 2, Kp = KK * CP;
+    constexpr int ntiles = NTL;
+    unsigned short* in_s = cm_smem;                         // [EH][EW][PS]
+    unsigned short* w_s = cm_smem + (size_t)EH * EW * PS;   // [8 ntiles][Kp]
+    const int n = blockIdx.z;
+    const int x0 = blockIdx.x * CM_TX, y0 = blockIdx.y * CM_TY;
+    for (int q = threadIdx.x; q < CP * EH * EW; q += CM_NT) {  // x fastest: coalesced reads
+        const int c = q / (EH * EW), r = q % (EH * EW);
+        const float v = c < ci_total ? conv_input(p, n, c, y0 + r / EW - R, x0 + r % EW - R) : 0.f;
+        in_s[r * PS + c] = bf16_bits(v);
+    }
+    {  // the weights, already in this kernel's order: 16-byte copies (8 tiles x Kp is a multiple of 8)
+        const uint4* src = reinterpret_cast<const uint4*>(p.wre);
+        uint4* dst = reinterpret_cast<uint4*>(w_s);
+        for (int q = threadIdx.x; q < ntiles * Kp; q += CM_NT) dst[q] = __ldg(src + q);
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int grp = lane >> 2, tig = lane & 3;
+    float acc[2][NTL][4];
+#pragma unroll
+    for (int r = 0; r < 2; r++)
+#pragma unroll
+        for (int t = 0; t < NTL; t++)
+#pragma unroll
+            for (int e = 0; e < 4; e++) acc[r][t][e] = 0.f;
+    for (int kb = 0; kb < Kp; kb += 16) {
+        const int tap = kb / CP, c0 = kb - tap * CP + tig * 2;
+        const int dy = KK == 9 ? tap / 3 : 0, dx = KK == 9 ? tap - 3 * (tap / 3) : 0;
+        unsigned b[NTL][2];
+#pragma unroll
+        for (int t = 0; t < NTL; t++) {
+            const unsigned* wrow = reinterpret_cast<const unsigned*>(w_s + (size_t)(t * 8 + grp) * Kp + kb + tig * 2);
+            b[t][0] = wrow[0];
+            b[t][1] = wrow[4];  // k + 8
+        }
+#pragma unroll
+        for (int r = 0; r < 2; r++) {
+            const int row = warp * 2 + r + dy;
+            const unsigned* lo = reinterpret_cast<const unsigned*>(in_s + ((size_t)row * EW + grp + dx) * PS + c0);
+            const unsigned* hi = reinterpret_cast<const unsigned*>(in_s + ((size_t)row * EW + grp + 8 + dx) * PS + c0);
+            const unsigned a[4] = {lo[0], hi[0], lo[4], hi[4]};  // (pixel, k..k+1), (pixel+8, ..), (+8 channels)
+#pragma unroll
+            for (int t = 0; t < NTL; t++) mma_bf16_16816(acc[r][t], a, b[t]);
+        }
+    }
+    // D[pixel][channel]: pixels grp and grp + 8 of the warp's two rows, channels tig * 2 + {0, 1}
+#pragma unroll
+    for (int r = 0; r < 2; r++) {
+        const int y = y0 + warp * 2 + r;
+#pragma unroll
+        for (int t = 0; t < NTL; t++) {
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                const int x = x0 + grp + (e >= 2 ? 8 : 0);
+                const int co = t * 8 + tig * 2 + (e & 1);
+                if (x >= p.W || y >= p.H || co >= p.co) continue;
+                float v = acc[r][t][e] + (p.bias ? p.bias[co] : 0.f);
+                if (p.act == ACT_RELU) v = fmaxf(v, 0.f);
+                else if (p.act == ACT_SIG2) v = 2.f / (1.f + expf(-v));
+                const size_t kidx = (((size_t)n * p.co + co) * p.H + y) * p.W + x;
+                if (p.gate) v *= p.gate[kidx];
+                p.y[kidx] = v;
+            }
+        }
+    }
 }
 
 // dw[co][ci][t] = sum over samples and pixels of dy[co] * x[ci] shifted by tap t; one block per

@@ -28,6 +28,24 @@ struct LpcLayer {
     int w, b, co, ci, k;  // offsets into the parameter vector (b = -1: no bias)
 };
 
+constexpr size_t CONV_MMA_SMEM_MAX = 160 * 1024;
+
+// The tensor-core convolution's shared-memory limit, set once per process before any capture.
+inline cudaError_t conv_mma_configure() {
+    static cudaError_t st = cudaErrorNotReady;
+    if (st == cudaErrorNotReady) {
+        const void* ks[] = {(const void*)conv_mma_kernel<9, 1>, (const void*)conv_mma_kernel<9, 2>,
+                            (const void*)conv_mma_kernel<9, 4>, (const void*)conv_mma_kernel<9, 8>,
+                            (const void*)conv_mma_kernel<1, 1>, (const void*)conv_mma_kernel<1, 2>,
+                            (const void*)conv_mma_kernel<1, 4>, (const void*)conv_mma_kernel<1, 8>};
+        st = cudaSuccess;
+        for (const void* k : ks)
+            if (st == cudaSuccess)
+                st = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CONV_MMA_SMEM_MAX);
+    }
+    return st;
+}
+
 inline dim3 ew_grid(size_t n) {
     size_t b = (n + 255) / 256;
     if (b > 148 * 32) b = 148 * 32;
@@ -64,6 +82,10 @@ struct LpcNet {
     LpcLayer out{};
     const float* wq = nullptr;  // the weights the forward pass uses (owned by the model)
     float* gw = nullptr;        // where backward accumulates the weight gradient
+    bool tensor = false;        // inference on the tensor cores (BF16 activations), not FP32 FMA
+    DBuf wre;                   // tensor-core weights of every layer (BF16 pairs in floats)
+    std::vector<size_t> wre_off;  // per layer, in BF16 elements, keyed by the layer's weight offset
+    std::vector<int> wre_key;
 
     // activations for one batch shape
     int N = 0, H = 0, W = 0;
@@ -106,6 +128,44 @@ struct LpcNet {
             gate_b.push_back(add(ch[l], hidden, 1, true));
         }
         nparams = off;
+    }
+
+    static int mma_tiles(int co) {
+        const int nt0 = (co + 7) / 8;
+        return nt0 == 1 ? 1 : nt0 == 2 ? 2 : nt0 <= 4 ? 4 : 8;
+    }
+
+    // The tensor-core kernel's copy of the forward weights (call again after they change).
+    cudaError_t prepare_tensor(cudaStream_t st) {
+        wre_off.clear();
+        wre_key.clear();
+        size_t total = 0;
+        std::vector<const LpcLayer*> all;
+        for (auto* L : {&enc_a, &enc_b, &dec_a, &dec_b, &gate_a, &gate_b})
+            for (auto& l : *L)
+                if (l.co > 0) all.push_back(&l);
+        all.push_back(&out);
+        for (auto* l : all) {
+            wre_key.push_back(l->w);
+            wre_off.push_back(total);
+            total += (size_t)mma_tiles(l->co) * 8 * l->k * l->k * conv_mma_cp(l->ci);
+        }
+        cudaError_t e = wre.alloc((total + 1) / 2 + 8);
+        if (e != cudaSuccess) return e;
+        auto* base = reinterpret_cast<unsigned short*>(wre.p);
+        for (size_t n = 0; n < all.size(); n++) {
+            const LpcLayer* l = all[n];
+            const int cnt = mma_tiles(l->co) * 8 * l->k * l->k * conv_mma_cp(l->ci);
+            conv_mma_weights_kernel<<<ew_grid(cnt), 256, 0, st>>>(wq + l->w, l->co, l->ci, l->k * l->k, mma_tiles(l->co),
+                                                                  base + wre_off[n]);
+        }
+        return cudaGetLastError();
+    }
+
+    const unsigned short* wre_of(const LpcLayer& L) const {
+        for (size_t n = 0; n < wre_key.size(); n++)
+            if (wre_key[n] == L.w) return reinterpret_cast<const unsigned short*>(wre.p) + wre_off[n];
+        return nullptr;
     }
 
     size_t max_weights() const {
@@ -178,6 +238,28 @@ struct LpcNet {
         p.W = w_of(level);
         p.N = N;
         p.act = act;
+        p.wre = tensor ? wre_of(L) : nullptr;
+        if (p.wre && L.co <= 8 * CM_NMAX) {
+            const int nt = mma_tiles(L.co);  // the instantiation's tiles
+            const size_t smem = conv_mma_smem(L.ci, 8 * nt, L.k * L.k);
+            if (smem <= CONV_MMA_SMEM_MAX) {
+                dim3 grid((p.W + CM_TX - 1) / CM_TX, (p.H + CM_TY - 1) / CM_TY, N);
+#define CONV_MMA_LAUNCH(KK_, NT_) conv_mma_kernel<KK_, NT_><<<grid, CM_NT, smem, st>>>(p)
+                if (L.k == 3) {
+                    if (nt == 1) CONV_MMA_LAUNCH(9, 1);
+                    else if (nt == 2) CONV_MMA_LAUNCH(9, 2);
+                    else if (nt <= 4) CONV_MMA_LAUNCH(9, 4);
+                    else CONV_MMA_LAUNCH(9, 8);
+                } else {
+                    if (nt == 1) CONV_MMA_LAUNCH(1, 1);
+                    else if (nt == 2) CONV_MMA_LAUNCH(1, 2);
+                    else if (nt <= 4) CONV_MMA_LAUNCH(1, 4);
+                    else CONV_MMA_LAUNCH(1, 8);
+                }
+#undef CONV_MMA_LAUNCH
+                return cudaGetLastError();
+            }
+        }
         // 32 x 32 tiles while they give every SM a few blocks, 16 x 16 below
         const int groups = N * ((L.co + CV_COB - 1) / CV_COB);
         const bool big = (size_t)((p.W + 31) / 32) * ((p.H + 31) / 32) * groups >= 4 * 148;

@@ -1576,6 +1576,32 @@ wc_status wc_lpc_forward_backward(wc_lpc* l, int32_t n, int32_t h, int32_t w, co
     return lpc_ck(cudaStreamSynchronize(st), "forward_backward");
 }
 
+wc_status wc_lpc_forward(wc_lpc* l, int32_t n, int32_t h, int32_t w, const float* x, const float* feat,
+                         int32_t tensor, float* y) {
+    if (!l || !x || !feat || !y) return set_err(WC_EINVAL, "null argument");
+    const int div = 1 << (LPC_LEVELS - 1);
+    if (n < 1 || h < div || w < div || h % div || w % div)
+        return set_err(WC_EINVAL, "batch must be >= 1 and map sides positive multiples of 8");
+    LpcModel& m = l->m;
+    LpcNet net;  // an inference instance: the model's layout and weights, its own activations
+    net.layout(m.net.ch, m.net.hidden);
+    net.wq = m.wq.p;
+    net.tensor = tensor != 0;
+    cudaStream_t st = m.st;
+    if (net.tensor) {
+        TRY(lpc_ck(conv_mma_configure(), "configure"));
+        TRY(lpc_ck(net.prepare_tensor(st), "weights"));
+    }
+    const size_t per = (size_t)n * 2 * h * w;
+    TRY(lpc_ck(net.shape(n, h, w, false), "activations"));
+    TRY(lpc_ck(cudaMemcpyAsync(net.X[0].p, x, per * sizeof(float), cudaMemcpyHostToDevice, st), "upload"));
+    TRY(lpc_ck(cudaMemcpyAsync(net.F[0].p, feat, per * sizeof(float), cudaMemcpyHostToDevice, st), "upload"));
+    TRY(lpc_ck(net.gates(st), "gates"));
+    TRY(lpc_ck(net.forward(st, false), "forward"));
+    TRY(lpc_ck(cudaMemcpyAsync(y, net.Y.p, per * sizeof(float), cudaMemcpyDeviceToHost, st), "download"));
+    return lpc_ck(cudaStreamSynchronize(st), "forward");
+}
+
 wc_status wc_lpc_harvest(wc_lpc* l, wc_solver* s) {
     if (!l || !s) return set_err(WC_EINVAL, "null argument");
     if (!s->sgn) return set_err(WC_EINVAL, "the solver has no dispersive solve to harvest");
@@ -1698,6 +1724,10 @@ wc_status wc_solver_set_lpc(wc_solver* s, wc_lpc* l) {
     s->lnet.layout(l->m.net.ch, l->m.net.hidden);
     s->lnet.wq = l->m.wq.p;
     s->lnet.gw = nullptr;
+    s->lnet.tensor = true;  // the solve applies the network on the tensor cores
+    CK(conv_mma_configure());
+    CK(s->lnet.prepare_tensor(s->stream));
+    CK(cudaStreamSynchronize(s->stream));
     CK(s->lnet.shape(1, s->lpc_hp, s->lpc_wp, false));
     if (!s->tv) {
         CK(cudaMalloc(&s->tv, s->ncell * sizeof(float2)));

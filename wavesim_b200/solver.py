@@ -66,6 +66,7 @@ EXPORTS = [
     "wc_lpc_set_rounding",
     "wc_lpc_forward_backward",
     "wc_lpc_loss_grad",
+    "wc_lpc_forward",
     "wc_lpc_harvest",
     "wc_lpc_num_systems",
     "wc_lpc_train",
@@ -142,13 +143,14 @@ def load(path: str = LIB_PATH):
     L.wc_lpc_set_rounding.argtypes = [V, C.c_int32]
     L.wc_lpc_forward_backward.argtypes = [V, C.c_int32, C.c_int32, C.c_int32, F, F, F, F, F, F]
     L.wc_lpc_loss_grad.argtypes = [V, C.c_int32, C.c_int32, C.c_int32, F, F, F, F, C.c_double, C.c_double, D, F]
+    L.wc_lpc_forward.argtypes = [V, C.c_int32, C.c_int32, C.c_int32, F, F, C.c_int32, F]
     L.wc_lpc_harvest.argtypes = [V, V]
     L.wc_lpc_num_systems.argtypes = [V]
     L.wc_lpc_num_systems.restype = C.c_uint64
     L.wc_lpc_train.argtypes = [V, C.c_uint32, C.c_uint32, C.c_uint32, C.c_float, C.c_float, C.c_uint64, D]
     L.wc_solver_set_lpc.argtypes = [V, V]
     for name in ("wc_lpc_create", "wc_lpc_set_params", "wc_lpc_get_params", "wc_lpc_set_rounding",
-                 "wc_lpc_forward_backward", "wc_lpc_loss_grad", "wc_lpc_harvest", "wc_lpc_train",
+                 "wc_lpc_forward_backward", "wc_lpc_loss_grad", "wc_lpc_forward", "wc_lpc_harvest", "wc_lpc_train",
                  "wc_solver_set_lpc"):
         getattr(L, name).restype = C.c_int
     L.wc_recorder_create.argtypes = [V, C.c_double, C.c_double, C.POINTER(V)]
@@ -397,6 +399,16 @@ class LearnedPreconditioner:
         _check(load().wc_lpc_forward_backward(self._handle, n, h, w, _fptr(x), _fptr(feat), _fptr(dy), _fptr(y),
                                               _fptr(g), _fptr(dx)))
         return y, g, dx
+
+    def forward(self, x, feat, tensor: bool = True):
+        """The network's output on [n][2][h][w] arrays: BF16 tensor-core inference (as the solver
+        applies it) or the FP32 path training uses."""
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        feat = np.ascontiguousarray(feat, dtype=np.float32)
+        n, c, h, w = x.shape
+        y = np.zeros_like(x)
+        _check(load().wc_lpc_forward(self._handle, n, h, w, _fptr(x), _fptr(feat), 1 if tensor else 0, _fptr(y)))
+        return y
 
     def loss_grad(self, c, heff, bed, e, dx: float, dy: float):
         """The training loss of patches (c, heff, bed: [n][h][w]; error fields e: [n][2][h][w])
