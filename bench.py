@@ -421,7 +421,8 @@ def run_b200(args, world, rank, local):
             spec = net.spec
             flops = spec.flops_per_cell() / spec.stride**2 * w.grid.nx * w.grid.ny
             tflops = flops / (net_ms / net_n / 1e3) / 1e12
-            roof = {"bound": "compute (FP32 CUDA-core convolutions)", "kernel": "conv_fwd_kernel chain (one network application)",
+            roof = {"bound": "tensor", "kernel": "conv_mma_kernel chain (one network application: BF16 mma.sync "
+                                                  "implicit-GEMM convolutions, FP32 accumulation)",
                     "achieved": tflops, "unit": "TFLOP/s", "flops_per_cell": spec.flops_per_cell() / spec.stride**2,
                     "avg_ms": net_ms / net_n,
                     "traffic": NETWORK_DRAM_BYTES_PER_CELL * w.grid.nx * w.grid.ny / spec.stride**2,

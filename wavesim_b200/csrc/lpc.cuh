@@ -180,11 +180,19 @@ __global__ void __launch_bounds__(CM_NT) conv_mma_kernel(ConvArgs p) {
     unsigned short* w_s = cm_smem + (size_t)EH * EW * PS;   // [8 ntiles][Kp]
     const int n = blockIdx.z;
     const int x0 = blockIdx.x * CM_TX, y0 = blockIdx.y * CM_TY;
-    for (int q = threadIdx.x; q < CP * EH * EW; q += CM_NT) {  // x fastest: coalesced reads
+    for (int q = threadIdx.x; q < ci_total * EH * EW; q += CM_NT) {  // x fastest: coalesced reads
         const int c = q / (EH * EW), r = q % (EH * EW);
-        const float v = c < ci_total ? conv_input(p, n, c, y0 + r / EW - R, x0 + r % EW - R) : 0.f;
+        const int yy = y0 + r / EW - R, xx = x0 + r % EW - R;
+        float v = 0.f;
+        if ((unsigned)yy < (unsigned)p.H && (unsigned)xx < (unsigned)p.W) {
+            if (c >= p.ca) v = __ldg(p.b + (((size_t)n * p.cb + (c - p.ca)) * p.H + yy) * p.W + xx);
+            else if (p.amode == CM_UP) v = __ldg(p.a + (((size_t)n * p.ca + c) * (p.H / 2) + yy / 2) * (p.W / 2) + xx / 2);
+            else v = conv_input(p, n, c, yy, xx);
+        }
         in_s[r * PS + c] = bf16_bits(v);
     }
+    for (int q = threadIdx.x; q < (CP - ci_total) * EH * EW; q += CM_NT)  // padding channels
+        in_s[(q % (EH * EW)) * PS + ci_total + q / (EH * EW)] = 0;
     {  // the weights, already in this kernel's order: 16-byte copies (8 tiles x Kp is a multiple of 8)
         const uint4* src = reinterpret_cast<const uint4*>(p.wre);
         uint4* dst = reinterpret_cast<uint4*>(w_s);
