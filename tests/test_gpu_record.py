@@ -93,3 +93,32 @@ def test_device_resident_steps_record_like_host_steps():
     assert oa["seconds"] == pytest.approx(ob["seconds"], rel=1e-12)
     assert np.max(np.abs(oa["eta_max"] - ob["eta_max"])) < 1e-9
     assert math.isfinite(oa["seconds"])
+
+
+def test_a_recorded_run_reads_back_in_the_reference_format(tmp_path):
+    from wavesim_b200.runio import Run, RunWriter, record_frame, record_stats
+
+    w = W.config1()
+    s0 = W.wave_train_state(w)
+    sol = w.solver(Solver)
+    sol.upload(s0)
+    rec = Recorder(sol, s0.time, w.maker.period)
+    g = w.grid
+    writer = RunWriter(str(tmp_path / "run"), "swe", g.inner(w.bed.b), g.dx, g.dy,
+                       waves={"height_m": 2 * w.maker.amplitude, "period_s": w.maker.period})
+    frames = []
+    for _ in range(4):
+        sol.step_n(150)
+        sol.synchronize()
+        t = sol.time_device()
+        record_frame(writer, sol, t)
+        frames.append((t, *sol.frame(0.0)[:2]))
+    record_stats(writer, rec, s0.time, sol.time_device())
+    writer.finish()
+    run = Run(str(tmp_path / "run"))
+    assert run.header["frame_count"] == 4 and run.header["times"] == [f[0] for f in frames]
+    for k, (t, eta, brk) in enumerate(frames):
+        assert np.array_equal(run.field("eta", k), eta) and np.array_equal(run.field("breaking", k), brk)
+    out = rec.read()
+    assert np.array_equal(run.stat("eta_max"), out["eta_max"].astype(np.float32))
+    assert run.header["stats"]["fields"][:3] == ["break_fraction", "eta_max", "eta_min"]
