@@ -348,6 +348,29 @@ wc_status wc_recorder_read(wc_recorder* r, wc_record_summary* summary, double* e
  * Returns WC_ENAN (frame still written) when the surface is not finite or more than 100 m up. */
 wc_status wc_frame(wc_solver* s, double tide, float* eta, float* breaking, double* rise);
 
+/* ---- One-way nesting: relaxation zones driven by a coarser run ---------------------------------
+ *
+ * crates/wavecore/src/forcing.rs:209-283 (Relaxation, relax_cell) and
+ * crates/wavesim/src/lib.rs:1554-1605 (Sampler), :1846-1896 (the nested step): the fine run's
+ * zone cells (where one of `zones` has a rate, at the largest rate) relax after each fine step
+ * towards the surface and velocity of the coarse run, bilinear over the wet coarse cells around
+ * the fine cell's centre and interpolated in time between two sampled coarse states. Both runs
+ * keep their states on the device. */
+typedef struct wc_nest wc_nest;
+
+/* `fine` and `coarse` are solvers of the same sea; the fine grid's origin lies at
+ * (x_offset_m, y_offset_m) in the coarse grid's frame. Both solvers must outlive the nest. */
+wc_status wc_nest_create(wc_solver* fine, wc_solver* coarse, const wc_sponge* zones, uint64_t n_zones,
+                         double x_offset_m, double y_offset_m, wc_nest** out);
+void wc_nest_destroy(wc_nest* n);
+uint64_t wc_nest_cells(const wc_nest* n);
+/* Sample the coarse run's resident state (at its device clock) into slot 0 (the state before
+ * the coarse step that brackets the fine step's end) or slot 1 (the state after it). */
+wc_status wc_nest_sample(wc_nest* n, int32_t slot);
+/* One fine step of dt on the device, then the zone's relaxation towards the targets at the
+ * step's end time (clamped to the sampled interval). Asynchronous. */
+wc_status wc_nest_step(wc_nest* n, double dt);
+
 /* Kernel launches this solver has queued since it was created (for accounting). */
 uint64_t wc_launch_count(const wc_solver* s);
 /* Human-readable text of the last error on this thread ("" if none). */

@@ -30,4 +30,4 @@ from .model import (  # noqa: F401
     linear_wave,
     manning_factor,
 )
-from .solver import Ensemble, LearnedPreconditioner, Recorder, Solver, WavecoreError  # noqa: F401
+from .solver import Ensemble, LearnedPreconditioner, Nest, Recorder, Solver, WavecoreError  # noqa: F401

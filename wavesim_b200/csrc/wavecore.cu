@@ -19,6 +19,7 @@
 #include "common.cuh"
 #include "ensemble.cuh"
 #include "lpc_host.cuh"
+#include "nest.cuh"
 #include "pcg.cuh"
 #include "record.cuh"
 #include "stage.cuh"
@@ -1986,6 +1987,159 @@ wc_status wc_frame(wc_solver* s, double tide, float* eta, float* breaking, doubl
     *rise = up;
     if (!finite || !std::isfinite(up) || up > 100.0)
         return set_err(WC_ENAN, "the surface is not finite or more than 100 m above still water");
+    return WC_OK;
+}
+
+}  // extern "C"
+
+// ---- one-way nesting: relaxation zones driven by a coarser run -------------------------------
+
+struct wc_nest {
+    wc_solver* fine = nullptr;
+    wc_solver* coarse = nullptr;
+    NestCell* cells = nullptr;
+    int n = 0;
+    double* target = nullptr;  // [2 slots][3][n]
+    double* times = nullptr;   // [2]
+    cudaEvent_t sampled = nullptr;  // the targets are written (coarse stream)
+    cudaEvent_t relaxed = nullptr;  // the targets are read (fine stream)
+    ~wc_nest() {
+        if (cells) cudaFree(cells);
+        if (target) cudaFree(target);
+        if (times) cudaFree(times);
+        if (sampled) cudaEventDestroy(sampled);
+        if (relaxed) cudaEventDestroy(relaxed);
+    }
+};
+
+namespace {
+
+// Sponge::rate (forcing.rs:180-206) at interior cell (a, b).
+double sponge_rate_host(const wc_sponge& sp, const wc_grid& g, size_t a, size_t b) {
+    const double w = (double)sp.width;
+    auto ramp = [&](size_t d) {
+        if (d < sp.width) {
+            const double f = (w - (double)d) / w;
+            return f * f;
+        }
+        return 0.0;
+    };
+    double r = 0.0;
+    if (sp.west) r = std::max(r, ramp(a));
+    if (sp.east) r = std::max(r, ramp(g.nx - 1 - a));
+    if (sp.south) r = std::max(r, ramp(b));
+    if (sp.north) r = std::max(r, ramp(g.ny - 1 - b));
+    return sp.strength * r;
+}
+
+int reflect_host(long long i, long long n) {
+    if (i >= 0 && i < n) return (int)i;
+    const long long p = 2 * n;
+    long long t = i % p;
+    if (t < 0) t += p;
+    return (int)(t < n ? t : p - 1 - t);
+}
+
+}  // namespace
+
+extern "C" {
+
+wc_status wc_nest_create(wc_solver* fine, wc_solver* coarse, const wc_sponge* zones, uint64_t n_zones,
+                         double x_offset_m, double y_offset_m, wc_nest** out) {
+    if (!out) return set_err(WC_EINVAL, "out is null");
+    *out = nullptr;
+    if (!fine || !coarse || (n_zones && !zones)) return set_err(WC_EINVAL, "null argument");
+    if (fine == coarse) return set_err(WC_EINVAL, "the fine and the coarse run must be different solvers");
+    const wc_grid& fg = fine->grid;
+    const wc_grid& cg = coarse->grid;
+    std::vector<NestCell> cells;
+    for (size_t b = 0; b < fg.ny; b++)
+        for (size_t a = 0; a < fg.nx; a++) {
+            double rate = 0.0;  // Relaxation::new: the largest of the zones' rates
+            for (uint64_t z = 0; z < n_zones; z++) rate = std::max(rate, sponge_rate_host(zones[z], fg, a, b));
+            if (!(rate > 0.0)) continue;
+            NestCell c{};
+            c.k = (int)(b * fine->g.pitch + a);
+            c.rate = rate;
+            // Sampler::new (lib.rs:1560-1588): the fine cell's centre in coarse cells
+            const double x = x_offset_m + ((double)a + 0.5) * fg.dx, y = y_offset_m + ((double)b + 0.5) * fg.dy;
+            const double cx = x / cg.dx - 0.5, cy = y / cg.dy - 0.5;
+            const double ix = std::floor(cx), iy = std::floor(cy);
+            const double wx = cx - ix, wy = cy - iy;
+            const double ws[4] = {(1.0 - wx) * (1.0 - wy), wx * (1.0 - wy), (1.0 - wx) * wy, wx * wy};
+            const int dis[4] = {0, 1, 0, 1}, djs[4] = {0, 0, 1, 1};
+            for (int e = 0; e < 4; e++) {
+                // padded index clamped to one ghost layer, read through the wall fill
+                const long long pi = std::min<long long>(std::max<long long>((long long)ix + dis[e], -1), (long long)cg.nx);
+                const long long pj = std::min<long long>(std::max<long long>((long long)iy + djs[e], -1), (long long)cg.ny);
+                const int mi = reflect_host(pi, (long long)cg.nx), mj = reflect_host(pj, (long long)cg.ny);
+                c.kc[e] = mj * coarse->g.pitch + mi;
+                c.sx[e] = (pi >= 0 && pi < (long long)cg.nx) ? 1.f : -1.f;
+                c.sy[e] = (pj >= 0 && pj < (long long)cg.ny) ? 1.f : -1.f;
+                c.w[e] = ws[e];
+            }
+            cells.push_back(c);
+        }
+    auto* nz = new wc_nest();
+    auto fail = [&](wc_status st) {
+        delete nz;
+        return st;
+    };
+    nz->fine = fine;
+    nz->coarse = coarse;
+    nz->n = (int)cells.size();
+    const size_t n = std::max<size_t>(1, cells.size());
+    if (cudaMalloc(&nz->cells, n * sizeof(NestCell)) != cudaSuccess ||
+        cudaMalloc(&nz->target, 6 * n * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&nz->times, 2 * sizeof(double)) != cudaSuccess ||
+        cudaEventCreateWithFlags(&nz->sampled, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&nz->relaxed, cudaEventDisableTiming) != cudaSuccess)
+        return fail(set_err(WC_ENOMEM, "nest allocation failed"));
+    if (!cells.empty() &&
+        (cudaMemcpy(nz->cells, cells.data(), cells.size() * sizeof(NestCell), cudaMemcpyHostToDevice) != cudaSuccess ||
+         cudaStreamSynchronize(0) != cudaSuccess))
+        return fail(set_err(WC_ECUDA, "nest set-up failed"));
+    if (cudaMemset(nz->target, 0, 6 * n * sizeof(double)) != cudaSuccess ||
+        cudaMemset(nz->times, 0, 2 * sizeof(double)) != cudaSuccess || cudaStreamSynchronize(0) != cudaSuccess)
+        return fail(set_err(WC_ECUDA, "nest set-up failed"));
+    *out = nz;
+    return WC_OK;
+}
+
+void wc_nest_destroy(wc_nest* nz) {
+    if (!nz) return;
+    cudaDeviceSynchronize();
+    delete nz;
+}
+
+uint64_t wc_nest_cells(const wc_nest* nz) { return nz ? (uint64_t)nz->n : 0; }
+
+wc_status wc_nest_sample(wc_nest* nz, int32_t slot) {
+    if (!nz) return set_err(WC_EINVAL, "null nest");
+    if (slot != 0 && slot != 1) return set_err(WC_EINVAL, "slot must be 0 (the earlier state) or 1 (the later)");
+    wc_solver* c = nz->coarse;
+    CK(cudaStreamWaitEvent(c->stream, nz->relaxed, 0));  // the last relaxation has read the slots
+    const unsigned blocks = (unsigned)std::max(1, std::min(148 * 4, (nz->n + 255) / 256));
+    nest_sample_kernel<<<blocks, 256, 0, c->stream>>>(c->q0, c->bed, nz->cells, nz->n, nz->target + (size_t)slot * 3 * nz->n,
+                                                      nz->times + slot, c->ctl);
+    c->launches++;
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(nz->sampled, c->stream));
+    return WC_OK;
+}
+
+wc_status wc_nest_step(wc_nest* nz, double dt) {
+    if (!nz) return set_err(WC_EINVAL, "null nest");
+    wc_solver* f = nz->fine;
+    CK(cudaStreamWaitEvent(f->stream, nz->sampled, 0));  // the targets come from the coarse stream
+    TRY(wc_step_device(f, dt));
+    const unsigned blocks = (unsigned)std::max(1, std::min(148 * 4, (nz->n + 255) / 256));
+    nest_relax_kernel<<<blocks, 256, 0, f->stream>>>(f->q0, f->bed, nz->cells, nz->n, nz->target,
+                                                     nz->target + 3 * (size_t)nz->n, nz->times, f->ctl);
+    f->launches++;
+    f->rate_current = false;  // the relaxed state's time-step limit is recomputed when asked
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(nz->relaxed, f->stream));
     return WC_OK;
 }
 

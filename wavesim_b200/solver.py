@@ -75,6 +75,11 @@ EXPORTS = [
     "wc_recorder_destroy",
     "wc_recorder_read",
     "wc_frame",
+    "wc_nest_create",
+    "wc_nest_destroy",
+    "wc_nest_cells",
+    "wc_nest_sample",
+    "wc_nest_step",
 ]
 
 
@@ -159,6 +164,15 @@ def load(path: str = LIB_PATH):
     L.wc_recorder_read.argtypes = [V, C.POINTER(abi.wc_record_summary), D, D, D, D, D]
     L.wc_frame.argtypes = [V, C.c_double, F, F, D]
     for name in ("wc_recorder_create", "wc_recorder_read", "wc_frame"):
+        getattr(L, name).restype = C.c_int
+    L.wc_nest_create.argtypes = [V, V, C.POINTER(abi.wc_sponge), C.c_uint64, C.c_double, C.c_double, C.POINTER(V)]
+    L.wc_nest_destroy.argtypes = [V]
+    L.wc_nest_destroy.restype = None
+    L.wc_nest_cells.argtypes = [V]
+    L.wc_nest_cells.restype = C.c_uint64
+    L.wc_nest_sample.argtypes = [V, C.c_int32]
+    L.wc_nest_step.argtypes = [V, C.c_double]
+    for name in ("wc_nest_create", "wc_nest_sample", "wc_nest_step"):
         getattr(L, name).restype = C.c_int
     L.wc_launch_count.argtypes = [V]
     L.wc_launch_count.restype = C.c_uint64
@@ -490,6 +504,59 @@ class Recorder:
         out["waves"] = int(sm.waves)
         out["unsettled"] = sm.unsettled if sm.has_unsettled else None
         return out
+
+
+class Nest:
+    """One-way nesting (`wc_nest_*`): the fine solver's relaxation zones pulled towards a coarser
+    run of the same sea, as the reference's driver does (crates/wavesim/src/lib.rs:1846-1896).
+    Both solvers keep their states on the device; `run` is the driver's loop."""
+
+    def __init__(self, fine: "Solver", coarse: "Solver", zones, x_offset_m: float = 0.0, y_offset_m: float = 0.0):
+        arr = (abi.wc_sponge * max(1, len(zones)))(*[z.to_c() for z in zones])
+        out = C.c_void_p()
+        _check(load().wc_nest_create(fine._h(), coarse._h(), arr, len(zones), float(x_offset_m), float(y_offset_m),
+                                     C.byref(out)))
+        self._handle = out
+        self.fine, self.coarse = fine, coarse
+
+    def close(self):
+        if getattr(self, "_handle", None):
+            load().wc_nest_destroy(self._handle)
+        self._handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def cells(self) -> int:
+        return int(load().wc_nest_cells(self._handle))
+
+    def sample(self, slot: int) -> None:
+        _check(load().wc_nest_sample(self._handle, int(slot)))
+
+    def step(self, dt: float) -> None:
+        _check(load().wc_nest_step(self._handle, float(dt)))
+
+    def run(self, fine_dts, coarse_dt) -> None:
+        """lib.rs:1846-1896: for each fine step, step the coarse run (by `coarse_dt(t)`, a function
+        of its time) until it brackets the step's end, sample the states around that end, then
+        take the fine step and relax its zones. Uses the device clocks of both solvers."""
+        t_fine = self.fine.time_device()
+        stepped = False
+        for dt in fine_dts:
+            end = t_fine + dt
+            while self.coarse.time_device() < end - 1e-9:
+                self.sample(0)
+                self.coarse.step_device(coarse_dt(self.coarse.time_device()))
+                stepped = True
+            if stepped:
+                self.sample(1)
+                stepped = False
+            self.step(dt)
+            t_fine = end
 
 
 class Ensemble:
