@@ -49,7 +49,9 @@ STAGE_BYTES_SWE = (36 + 52) / 2                 # stage 1 / stage 2 (RK average 
 # DRAM bytes per cell measured by ncu (one capture each; scaled to a launch by cells, and by
 # iterations for the solve): profiles/network_conv_2048x1024.md, profiles/pcg_kernel_sgn_2048x1024.md.
 NETWORK_DRAM_BYTES_PER_CELL = 1.0265e9 / (2048 * 1024)   # one application of the U-net
-PCG_DRAM_BYTES_PER_CELL_ITER = 10.52e9 / (2048 * 1024 * 57)  # one iteration of the solve
+PCG_DRAM_BYTES_PER_CELL_ITER = 10.53e9 / (2048 * 1024 * 57)  # one iteration of the solve
+STAGE_DRAM_BYTES_PER_CELL_SWE = 573.1e6 / (4096 * 4096)      # one second-order stage
+# (profiles/stage_kernel_swe_4096x4096.md)
 
 
 def workload(name: str):
@@ -442,11 +444,15 @@ def run_b200(args, world, rank, local):
             traffic = None
             if dom["kernel"].startswith("pcg_kernel"):
                 traffic = PCG_DRAM_BYTES_PER_CELL_ITER * iters_prof * cells
+            elif not w.dispersion and w.order.value == 1:
+                traffic = STAGE_DRAM_BYTES_PER_CELL_SWE * cells
             roof = {"bound": "hbm", "kernel": dom["kernel"], "achieved": achieved, "peak": peak, "unit": "GB/s",
                     "frac": achieved / peak, "peak_source": peak_kind, "algorithmic_bytes_per_cell": dom["bytes_per_cell"],
                     "avg_ms": dom["avg_ms"], "traffic": traffic,
-                    "traffic_source": "ncu DRAM bytes per cell and iteration of one solve at 2048x1024, scaled by cells "
-                                      "and iterations" if traffic else None}
+                    "traffic_source": ("ncu DRAM bytes per cell and iteration of one solve at 2048x1024, scaled by "
+                                       "cells and iterations" if dom["kernel"].startswith("pcg_kernel") else
+                                       "ncu DRAM bytes of one second-order stage at 4096x4096, scaled by cells")
+                    if traffic else None}
         line = {
             "metric": METRIC,
             "value": arm["value"],
