@@ -39,7 +39,7 @@ METRIC = "cell-steps/s (SGN on), learned-PC vs plain PCG on 1 B200 at equal resi
 UNIT = "cell-steps/s"
 L2_FLUSH_BYTES = 256 << 20
 
-# Algorithmic bytes per interior cell (FP32 state with a compensated depth; see DESIGN.md).
+# Algorithmic bytes per interior cell (FP32 state with a compensated depth).
 STAGE_BYTES_SGN = 16 + 4 + 8 + 8 + 4 + 4 + 8   # read q, b; write hn, pred, c, heff, b-vector
 SOLVE_INIT_BYTES = (8 + 4 + 4 + 8 + 8 + 8 + 8) + (8 + 8 + 4 + 4 + 8)  # r = b - A w; then q0 = A (r / diag)
 SOLVE_ITER_BYTES = (8 * 4 + 8 * 2 + 4 * 2) + 8 * 5  # read r, q, s, diag, p, w, c, heff; write p, w, s, r, q

@@ -16,8 +16,8 @@
  *
  * Differences a caller can observe, all deliberate:
  *   - the device computes in FP32 with a compensated (hi+lo) depth, FP64 reductions and FP64
- *     mass accumulation; results agree with the FP64 reference to the tolerances documented in
- *     DESIGN.md, and still water stays exactly still;
+ *     mass accumulation; results agree with the FP64 reference to the tolerances its parity tests
+ *     state, and still water stays exactly still;
  *   - ghost cells of the bed are taken from the boundary rule (mirrored at walls, wrapped when
  *     periodic in y), which is what every `Bathymetry` constructor and `with_periodic_y` produce;
  *     the ghost values the caller passes are not read;
@@ -75,11 +75,24 @@ typedef struct wc_wavemaker {
     double x, amplitude, period, angle, sigma, ramp_periods;
 } wc_wavemaker;
 
-/* crates/wavecore/src/dispersion.rs:44-74 (`Breaking`). The reference's `viscosity`
- * (followed fronts, crates/wavecore/src/eddy.rs) is not part of this build: it is `None` here. */
+/* crates/wavecore/src/eddy.rs:62-90 (`EddyViscosity`): how breaking fronts are followed from
+ * step to step, Kennedy et al.'s (2000) coefficients by default (wc_eddy_default). `initial`
+ * and `settled` are rates of rise in sqrt(g h); `duration` and `linger` are times in
+ * sqrt(h / g); `mixing` is the mixing length in depths (0 follows fronts without viscosity). */
+typedef struct wc_eddy {
+    double initial, settled, duration, mixing, linger;
+} wc_eddy;
+
+/* crates/wavecore/src/dispersion.rs:44-74 (`Breaking`). `viscosity` = 0 is the reference's
+ * `None` (the default): the switch is read afresh at every step. `viscosity` = 1 is
+ * `Some(eddy)`: breaking fronts are followed in the state's `breaking` memory, keep the switch
+ * off where they are and just behind them, and get Kennedy's eddy viscosity (eddy.rs). Only
+ * read with dispersion, as in the reference (solver.rs:509-520). */
 typedef struct wc_breaking {
     double eta_ratio_lo, eta_ratio_hi;
     double slope_lo, slope_hi;
+    int32_t viscosity;
+    wc_eddy eddy;
 } wc_breaking;
 
 /* Preconditioner of the dispersive solve. JACOBI is the reference's
@@ -129,8 +142,11 @@ typedef struct wc_solver wc_solver;
 
 /* Defaults of `Solver::new` (solver.rs:283-299): cfl 0.4, Second order, no friction, walls. */
 void wc_config_default(wc_config* cfg);
-/* `Dispersion::default()` (dispersion.rs:88-97) with `Breaking::default()` (:56-74). */
+/* `Dispersion::default()` (dispersion.rs:88-97) with `Breaking::default()` (:56-74): no
+ * followed fronts (`viscosity` = 0), `eddy` set to `EddyViscosity::default()`. */
 void wc_dispersion_default(wc_dispersion* d);
+/* `EddyViscosity::default()` (eddy.rs:81-90): 0.65, 0.15, 5, 1.2, 5. */
+void wc_eddy_default(wc_eddy* e);
 
 /* `Solver::new(grid, bed)` followed by the builders in `cfg` (solver.rs:283-429).
  * `bed_padded` holds (nx+6)*(ny+6) values; only its interior is read. Returns WC_EINVAL where
@@ -142,7 +158,9 @@ void wc_solver_destroy(wc_solver* s);
 
 /* `Solver::step(&mut State, dt)` (solver.rs:479-507) on host FP64 arrays, in place: uploads the
  * state, runs one SSP-RK2 step on the device, downloads it and advances `*time` by dt.
- * `breaking` is carried unchanged (it only changes with followed fronts, not in this build). */
+ * `breaking` is the state's breaking memory (state.rs:11-15): with followed fronts it is read
+ * and updated (its interior; ghosts are refilled by the boundary rule), otherwise carried
+ * unchanged. It may be NULL only without followed fronts. */
 wc_status wc_step(wc_solver* s, double* h, double* hu, double* hv, double* breaking,
                   double* time, double dt);
 
@@ -156,18 +174,33 @@ wc_status wc_stable_dt(wc_solver* s, const double* h, const double* hu, const do
 wc_status wc_limiting_cell(wc_solver* s, const double* h, const double* hu, const double* hv,
                            wc_limiting* out, int32_t* found);
 
-/* `Solver::breaking_indicator(&State)` (solver.rs:336-349): nx*ny values, y outer. */
+/* `Solver::breaking_indicator(&State)` (solver.rs:336-349): nx*ny values, y outer. With
+ * followed fronts the state's `breaking` memory holds the switch off where it is not 0
+ * (dispersion.rs:149-152); NULL reads as no memory. */
 wc_status wc_breaking_indicator(wc_solver* s, const double* h, const double* hu,
-                                const double* hv, double* out_interior);
+                                const double* hv, const double* breaking, double* out_interior);
+
+/* `Solver::follow_breaking` (solver.rs:509-532, private in the reference; exported for parity
+ * checks of eddy.rs): the fronts in `breaking` followed on to the state (h, hu, hv) and their
+ * eddy viscosity applied to its momentum over dt, in place, on host FP64 arrays. A no-op
+ * without followed fronts. *sub_steps (may be NULL) gets the viscous sub-steps taken. */
+wc_status wc_follow_breaking(wc_solver* s, double* h, double* hu, double* hv, double* breaking,
+                             double dt, int32_t* sub_steps);
 
 /* `Solver::dispersion_stats()` (solver.rs:391-396): *has = 0 for shallow water. */
 wc_status wc_dispersion_stats(wc_solver* s, wc_stats* out, int32_t* has);
 
 /* ---- Device-resident throughput path (no counterpart in the reference) ----------------- */
 
-/* Copy a padded FP64 host state onto the device (interior only) and set the device clock. */
+/* Copy a padded FP64 host state onto the device (interior only) and set the device clock. The
+ * breaking memory is cleared (a new state has no wave breaking, state.rs:11-15). */
 wc_status wc_state_upload(wc_solver* s, const double* h, const double* hu, const double* hv,
                           double time);
+/* The device state's breaking memory (state.rs:11-15) from / to a padded FP64 host array
+ * (interior read; ghosts written by the boundary rule). Without followed fronts the memory is
+ * not kept: upload ignores it and download writes zeros. */
+wc_status wc_breaking_upload(wc_solver* s, const double* breaking);
+wc_status wc_breaking_download(wc_solver* s, double* breaking);
 /* Copy the device state back into padded FP64 host arrays (ghosts filled by the boundary
  * rule); `time` may be NULL. */
 wc_status wc_state_download(wc_solver* s, double* h, double* hu, double* hv, double* time);
@@ -198,12 +231,13 @@ wc_status wc_set_stream(wc_solver* s, void* stream);
  * returns, per kernel kind, the launch count and the summed device milliseconds since the last
  * enable. Kinds: 0 = RK-stage stencil kernel, 1 = dispersive solve (for the learned
  * preconditioner: its vector kernels and the stage epilogue), 2 = other, 3 = the learned
- * preconditioner's network (one count per application). */
+ * preconditioner's network (one count per application), 4 = followed breaking fronts and their
+ * eddy viscosity (one launch per step). */
 typedef struct wc_kernel_time {
     uint64_t launches;
     double total_ms;
 } wc_kernel_time;
-#define WC_KERNEL_KINDS 4
+#define WC_KERNEL_KINDS 5
 wc_status wc_profile_enable(wc_solver* s, int32_t on);
 wc_status wc_profile_read(wc_solver* s, wc_kernel_time out[WC_KERNEL_KINDS]);
 

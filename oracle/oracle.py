@@ -70,6 +70,13 @@ def lib():
         L.or_dispersion_apply.argtypes = [
             C.POINTER(abi.wc_grid), C.c_int, C.POINTER(abi.wc_dispersion), D, D, D, D, D, D, D,
         ]
+        L.or_eddy_threshold.argtypes = [C.POINTER(abi.wc_eddy), C.c_double, C.c_double]
+        L.or_eddy_threshold.restype = C.c_double
+        L.or_eddy_follow.argtypes = [C.POINTER(abi.wc_grid), C.POINTER(abi.wc_eddy), D, D, D, D, D, C.c_double, D]
+        L.or_eddy_diffuse.argtypes = [C.POINTER(abi.wc_grid), C.c_int, D, D, D, D, D, C.c_double]
+        L.or_eddy_diffuse.restype = C.c_int
+        L.or_follow_breaking.argtypes = [C.c_void_p, D, D, D, D, C.c_double]
+        L.or_follow_breaking.restype = C.c_int
         L.or_volume.argtypes = [C.POINTER(abi.wc_grid), D]
         L.or_volume.restype = C.c_double
         L.or_max_abs_momentum.argtypes = [C.POINTER(abi.wc_grid), D, D]
@@ -141,6 +148,11 @@ class OracleSolver(SolverConfig):
             self._h(), abi.dptr(s.h), abi.dptr(s.hu), abi.dptr(s.hv), abi.dptr(s.breaking), abi.dptr(out)
         )
         return out
+
+    def follow_breaking(self, s: State, dt: float) -> int:
+        """solver.rs:509-532 on `s` in place; returns the viscous sub-steps taken."""
+        return lib().or_follow_breaking(self._h(), abi.dptr(s.h), abi.dptr(s.hu), abi.dptr(s.hv),
+                                        abi.dptr(s.breaking), float(dt))
 
     def dispersion_stats(self):
         st = abi.wc_stats()
@@ -222,3 +234,27 @@ def mirror_ghosts(grid, a):
 def wrap_ghosts_y(grid, a):
     g = grid.to_c()
     lib().or_wrap_ghosts_y(C.byref(g), abi.dptr(a))
+
+
+def eddy_threshold(eddy, age, h):
+    """eddy.rs:114-124."""
+    e = eddy.to_c()
+    return lib().or_eddy_threshold(C.byref(e), float(age), float(h))
+
+
+def eddy_follow(grid, eddy, s: State, phi, dt):
+    """eddy.rs:155-219 on a ghost-filled state: replaces s.breaking; returns nu (padded)."""
+    g, e = grid.to_c(), eddy.to_c()
+    nu = np.zeros(grid.cells())
+    phi = np.ascontiguousarray(phi, dtype=np.float64)
+    lib().or_eddy_follow(C.byref(g), C.byref(e), abi.dptr(s.h), abi.dptr(s.hu), abi.dptr(s.hv),
+                         abi.dptr(s.breaking), abi.dptr(phi), float(dt), abi.dptr(nu))
+    return nu
+
+
+def eddy_diffuse(grid, s: State, nu, dt, periodic=False):
+    """eddy.rs:221-302 on `s` in place; returns the sub-steps taken."""
+    g = grid.to_c()
+    nu = np.ascontiguousarray(nu, dtype=np.float64)
+    return lib().or_eddy_diffuse(C.byref(g), int(periodic), abi.dptr(s.h), abi.dptr(s.hu), abi.dptr(s.hv),
+                                 abi.dptr(s.breaking), abi.dptr(nu), float(dt))

@@ -297,9 +297,10 @@ double or_smoothstep(double lo, double hi, double x) {
     return t * t * (3.0 - 2.0 * t);
 }
 
-/* dispersion.rs:113-160; the followed-fronts branch (viscosity) is not part of this build */
-static void switch_phi(const Grid* g, const double* bed, const double* h, const wc_breaking* br,
-                       int periodic_y, double* phi) {
+/* dispersion.rs:113-160. `mem` is the state's breaking memory: with followed fronts
+ * (br->viscosity) a cell whose memory is not 0 reads breaking (:149-152). */
+static void switch_phi(const Grid* g, const double* bed, const double* h, const double* mem,
+                       const wc_breaking* br, int periodic_y, double* phi) {
     const size_t w = g->w;
     const double ix = 0.5 / g->dx, iy = 0.5 / g->dy;
 #pragma omp parallel for schedule(static) if (THREADED(g))
@@ -315,11 +316,154 @@ static void switch_phi(const Grid* g, const double* bed, const double* h, const 
             double ratio = fmax((h[k] + bed[k]) / h[k], 0.0);
             double off = fmax(or_smoothstep(br->eta_ratio_lo, br->eta_ratio_hi, ratio),
                               or_smoothstep(br->slope_lo, br->slope_hi, hypot(ex, ey)));
+            if (br->viscosity && mem && mem[k] != 0.0) off = 1.0; /* EddyViscosity::keeps_off */
             phi[k] = 1.0 - off;
         }
     }
     mirror_ghosts(g, phi);
     if (periodic_y) wrap_ghosts_y(g, phi);
+}
+
+/* ---- eddy.rs: breaking fronts followed from step to step ---------------------------------- */
+
+#define H_BREAKING_MIN 0.01 /* eddy.rs:54-56 */
+#define BREAKING_ONSET 0.8  /* eddy.rs:58-59 */
+
+/* eddy.rs:103-106 */
+static double eddy_span(const wc_eddy* e, double h) { return e->duration * sqrt(h / G); }
+
+/* eddy.rs:114-124 */
+double or_eddy_threshold(const wc_eddy* e, double age, double h) {
+    double span = eddy_span(e, h);
+    if (age >= span) return e->settled;
+    return e->initial + (e->settled - e->initial) * age / span;
+}
+
+/* f64::clamp(0, 1), which keeps NaN */
+static inline double clamp01(double x) { return x < 0.0 ? 0.0 : (x > 1.0 ? 1.0 : x); }
+
+/* eddy.rs:155-219 (`follow`). h, hu, hv and the memory `br` have their ghost cells filled; `br`
+ * is replaced by the new memory (ghosts 0, as the reference's swap leaves them) and `nu` gets
+ * the eddy viscosity (0 outside the interior). `rise` and `mem` are padded scratch. */
+static void eddy_follow(const Grid* g, const wc_eddy* e, const double* h, const double* hu,
+                        const double* hv, double* br, const double* phi, double dt, double* rise,
+                        double* mem, double* nu) {
+    const size_t w = g->w;
+    const double ix = 0.5 / g->dx, iy = 0.5 / g->dy;
+    memset(rise, 0, g->n * sizeof(double));
+#pragma omp parallel for schedule(static) if (THREADED(g))
+    for (size_t j = GH; j < g->ny + GH; j++)
+        for (size_t i = GH; i < g->nx + GH; i++) {
+            size_t k = j * w + i;
+            rise[k] = -((hu[k + 1] - hu[k - 1]) * ix + (hv[k + w] - hv[k - w]) * iy);
+        }
+    memset(mem, 0, g->n * sizeof(double));
+    memset(nu, 0, g->n * sizeof(double));
+#pragma omp parallel for schedule(static) if (THREADED(g))
+    for (size_t j = GH; j < g->ny + GH; j++)
+        for (size_t i = GH; i < g->nx + GH; i++) {
+            size_t k = j * w + i;
+            double depth = h[k];
+            if (depth < H_BREAKING_MIN) continue;
+            double c = sqrt(G * depth);
+            const size_t nb[5] = {k, k - 1, k + 1, k - w, k + w};
+            double front = 0.0;
+            for (int m = 0; m < 5; m++) front = fmax(front, br[nb[m]]);
+            int starts = depth >= H_DISPERSION_MIN && 1.0 - phi[k] >= BREAKING_ONSET && rise[k] > 0.0;
+            int goes_on = front > 0.0 && rise[k] > or_eddy_threshold(e, front, depth) * c;
+            double age = (front > 0.0 && (starts || goes_on)) ? front + dt : (starts ? dt : 0.0);
+            if (age > 0.0) {
+                double b = clamp01(rise[k] / (or_eddy_threshold(e, age, depth) * c) - 1.0);
+                mem[k] = age;
+                nu[k] = b * e->mixing * e->mixing * depth * rise[k];
+            } else if (br[k] > 0.0) {
+                mem[k] = -e->linger * sqrt(depth / G);
+            } else if (br[k] < 0.0) {
+                mem[k] = fmin(br[k] + dt, 0.0);
+            }
+        }
+    memcpy(br, mem, g->n * sizeof(double));
+}
+
+/* eddy.rs:221-302 (`diffuse`): the viscosity `nu` (0 outside the interior) applied to hu, hv over
+ * dt in explicit sub-steps, the ghost cells refilled between them. Returns the sub-steps taken.
+ * whu, whv are padded scratch. */
+static int eddy_diffuse(const Grid* g, int periodic_y, double* h, double* hu, double* hv,
+                        double* br, const double* nu, double dt, double* whu, double* whv) {
+    const size_t w = g->w;
+    /* par.rs:99-107: row maxima (f64::max, which drops NaN) folded in row order */
+    double top = 0.0;
+    for (size_t j = GH; j < GH + g->ny; j++) {
+        double m = 0.0;
+        for (size_t k = j * w + GH; k < j * w + GH + g->nx; k++) m = fmax(m, nu[k]);
+        top = max_or_nan(top, m);
+    }
+    if (top <= 0.0) return 0;
+    const double idx2 = 1.0 / (g->dx * g->dx), idy2 = 1.0 / (g->dy * g->dy);
+    const double limit = 0.5 / (top * fmax(2.0 * idx2 + idy2, idx2 + 2.0 * idy2));
+    double fsteps = fmax(ceil(dt / limit), 1.0);
+    if (fsteps > 1e9) fsteps = 1e9; /* the reference's `as usize` saturates far beyond this */
+    const int steps = (int)fsteps;
+    const double sub = dt / (double)steps;
+    const double cross = 0.25 / (g->dx * g->dy);
+    for (int step = 0; step < steps; step++) {
+        if (step > 0) fill_boundaries(g, periodic_y, h, hu, hv, br);
+#pragma omp parallel for schedule(static) if (THREADED(g))
+        for (size_t j = GH; j < g->ny + GH; j++)
+            for (size_t i = GH; i < g->nx + GH; i++) {
+                size_t k = j * w + i;
+                if (h[k] < H_BREAKING_MIN) {
+                    whu[k] = hu[k];
+                    whv[k] = hv[k];
+                    continue;
+                }
+                const size_t e = k + 1, west = k - 1, north = k + w, south = k - w;
+#define LINK(a, b) ((h[a] < H_BREAKING_MIN || h[b] < H_BREAKING_MIN) ? 0.0 : 0.5 * (nu[a] + nu[b]))
+#define WET(a) (h[a] < H_BREAKING_MIN ? 0.0 : nu[a])
+#define XX(q) ((LINK(k, e) * (q[e] - q[k]) - LINK(k, west) * (q[k] - q[west])) * idx2)
+#define YY(q) ((LINK(k, north) * (q[north] - q[k]) - LINK(k, south) * (q[k] - q[south])) * idy2)
+#define YX(q) ((WET(north) * (q[north + 1] - q[north - 1]) - WET(south) * (q[south + 1] - q[south - 1])) * cross)
+#define XY(q) ((WET(e) * (q[e + w] - q[e - w]) - WET(west) * (q[west + w] - q[west - w])) * cross)
+                whu[k] = hu[k] + sub * (XX(hu) + 0.5 * (YY(hu) + YX(hv)));
+                whv[k] = hv[k] + sub * (YY(hv) + 0.5 * (XX(hv) + XY(hu)));
+#undef LINK
+#undef WET
+#undef XX
+#undef YY
+#undef YX
+#undef XY
+            }
+        /* only the interior was written; the ghost cells are refilled before they are read */
+#pragma omp parallel for schedule(static) if (THREADED(g))
+        for (size_t j = GH; j < g->ny + GH; j++)
+            for (size_t i = GH; i < g->nx + GH; i++) {
+                size_t k = j * w + i;
+                hu[k] = whu[k];
+                hv[k] = whv[k];
+            }
+    }
+    return steps;
+}
+
+void or_eddy_follow(const wc_grid* wg, const wc_eddy* e, const double* h, const double* hu,
+                    const double* hv, double* breaking, const double* phi, double dt, double* nu) {
+    Grid g = mk_grid(wg);
+    double* rise = (double*)malloc(g.n * sizeof(double));
+    double* mem = (double*)malloc(g.n * sizeof(double));
+    eddy_follow(&g, e, h, hu, hv, breaking, phi, dt, rise, mem, nu);
+    free(rise);
+    free(mem);
+}
+
+int or_eddy_diffuse(const wc_grid* wg, int periodic_y, double* h, double* hu, double* hv,
+                    double* breaking, const double* nu, double dt) {
+    Grid g = mk_grid(wg);
+    double* whu = (double*)calloc(g.n, sizeof(double));
+    double* whv = (double*)calloc(g.n, sizeof(double));
+    int steps = eddy_diffuse(&g, periodic_y, h, hu, hv, breaking, nu, dt, whu, whv);
+    free(whu);
+    free(whv);
+    return steps;
 }
 
 /* ---- solver.rs: reconstruction and fluxes ------------------------------------------------- */
@@ -720,9 +864,11 @@ struct or_solver {
     double *rh, *rhu, *rhv;
     double *s1h, *s1hu, *s1hv, *s1br, *s2h, *s2hu, *s2hv, *s2br;
     double* rows_buf;
+    /* followed fronts (eddy.rs:92-101): rise, memory, viscosity, momentum scratch */
+    double *ed_rise, *ed_mem, *ed_nu, *ed_hu, *ed_hv;
 };
 
-static const wc_breaking k_default_breaking = {0.30, 0.55, 0.40, 0.65};
+static const wc_breaking k_default_breaking = {0.30, 0.55, 0.40, 0.65, 0, {0.65, 0.15, 5.0, 1.2, 5.0}};
 
 static const wc_breaking* breaking_config(const or_solver* s) {
     return s->has_disp ? &s->disp.breaking : &k_default_breaking;
@@ -735,8 +881,9 @@ void or_solver_destroy(or_solver* s) {
     if (s->has_disp) work_free(&s->work);
     free(s->phi);
     free(s->shallow);
-    double* arrs[] = {s->rh,   s->rhu,  s->rhv,  s->s1h, s->s1hu, s->s1hv,
-                      s->s1br, s->s2h,  s->s2hu, s->s2hv, s->s2br, s->rows_buf};
+    double* arrs[] = {s->rh,     s->rhu,     s->rhv,    s->s1h,    s->s1hu,   s->s1hv,
+                      s->s1br,   s->s2h,     s->s2hu,   s->s2hv,   s->s2br,   s->rows_buf,
+                      s->ed_rise, s->ed_mem, s->ed_nu, s->ed_hu, s->ed_hv};
     for (size_t m = 0; m < sizeof arrs / sizeof arrs[0]; m++) free(arrs[m]);
     free(s);
 }
@@ -778,6 +925,11 @@ wc_status or_solver_create(const wc_grid* wg, const double* bed, const wc_config
         if (!work_new(&s->work, g)) {
             or_solver_destroy(s);
             return fail(WC_ENOMEM, "out of memory");
+        }
+        if (s->disp.breaking.viscosity) {
+            double** ed[] = {&s->ed_rise, &s->ed_mem, &s->ed_nu, &s->ed_hu, &s->ed_hv};
+            for (size_t m = 0; m < sizeof ed / sizeof ed[0]; m++)
+                *ed[m] = (double*)calloc(g->n, sizeof(double));
         }
     }
     if (cfg->shallow_cells) {
@@ -868,11 +1020,12 @@ static void advance(const or_solver* S, const double* h, const double* hu, const
 }
 
 /* solver.rs:625-733 */
-static void rhs(or_solver* S, const double* h, const double* hu, const double* hv, double t) {
+static void rhs(or_solver* S, const double* h, const double* hu, const double* hv,
+                const double* br, double t) {
     const Grid* g = &S->g;
     const size_t w = g->w;
     if (S->order == WC_ORDER_FIFTH || S->has_disp) {
-        switch_phi(g, S->b, h, breaking_config(S), S->periodic_y, S->phi);
+        switch_phi(g, S->b, h, br, breaking_config(S), S->periodic_y, S->phi);
         if (S->shallow) {
             size_t n = 0;
             for (size_t j = GH; j < GH + g->ny; j++)
@@ -957,6 +1110,24 @@ static void damp(const or_solver* S, double* h, double* hu, double* hv, double d
     clean_dry(g, h, hu, hv);
 }
 
+/* solver.rs:509-532 (`follow_breaking`): returns the viscous sub-steps taken */
+int or_follow_breaking(or_solver* S, double* h, double* hu, double* hv, double* br, double dt) {
+    if (!S->has_disp || !S->disp.breaking.viscosity) return 0;
+    const Grid* g = &S->g;
+    fill_boundaries(g, S->periodic_y, h, hu, hv, br);
+    /* the switch as the surface alone reads it, without the fronts: where they start */
+    wc_breaking fresh = S->disp.breaking;
+    fresh.viscosity = 0;
+    switch_phi(g, S->b, h, br, &fresh, S->periodic_y, S->phi);
+    const wc_eddy* e = &S->disp.breaking.eddy;
+    eddy_follow(g, e, h, hu, hv, br, S->phi, dt, S->ed_rise, S->ed_mem, S->ed_nu);
+    int steps = 0;
+    if (e->mixing > 0.0)
+        steps = eddy_diffuse(g, S->periodic_y, h, hu, hv, br, S->ed_nu, dt, S->ed_hu, S->ed_hv);
+    clean_dry(g, h, hu, hv);
+    return steps;
+}
+
 /* solver.rs:479-507 */
 void or_step(or_solver* S, double* h, double* hu, double* hv, double* br, double* time,
              double dt) {
@@ -964,17 +1135,17 @@ void or_step(or_solver* S, double* h, double* hu, double* hv, double* br, double
     double t = *time;
     fill_boundaries(g, S->periodic_y, h, hu, hv, br);
     if (S->order == WC_ORDER_FIRST) {
-        rhs(S, h, hu, hv, t);
+        rhs(S, h, hu, hv, br, t);
         advance(S, h, hu, hv, br, dt, S->s1h, S->s1hu, S->s1hv, S->s1br);
         memcpy(h, S->s1h, g->n * sizeof(double));
         memcpy(hu, S->s1hu, g->n * sizeof(double));
         memcpy(hv, S->s1hv, g->n * sizeof(double));
         memcpy(br, S->s1br, g->n * sizeof(double));
     } else {
-        rhs(S, h, hu, hv, t);
+        rhs(S, h, hu, hv, br, t);
         advance(S, h, hu, hv, br, dt, S->s1h, S->s1hu, S->s1hv, S->s1br);
         fill_boundaries(g, S->periodic_y, S->s1h, S->s1hu, S->s1hv, S->s1br);
-        rhs(S, S->s1h, S->s1hu, S->s1hv, t + dt);
+        rhs(S, S->s1h, S->s1hu, S->s1hv, S->s1br, t + dt);
         advance(S, S->s1h, S->s1hu, S->s1hv, S->s1br, dt, S->s2h, S->s2hu, S->s2hv, S->s2br);
         const size_t n = g->n;
 #pragma omp parallel for schedule(static) if (THREADED(g))
@@ -986,6 +1157,7 @@ void or_step(or_solver* S, double* h, double* hu, double* hv, double* br, double
         clean_dry(g, h, hu, hv);
     }
     damp(S, h, hu, hv, dt);
+    or_follow_breaking(S, h, hu, hv, br, dt);
     *time = t + dt;
 }
 
@@ -1059,7 +1231,7 @@ void or_breaking_indicator(or_solver* S, const double* h, const double* hu, cons
     memcpy(fhv, hv, n * sizeof(double));
     memcpy(fbr, br, n * sizeof(double));
     fill_boundaries(g, S->periodic_y, fh, fhu, fhv, fbr);
-    switch_phi(g, S->b, fh, breaking_config(S), S->periodic_y, phi);
+    switch_phi(g, S->b, fh, fbr, breaking_config(S), S->periodic_y, phi);
     size_t m = 0;
     for (size_t j = GH; j < GH + g->ny; j++)
         for (size_t i = GH; i < GH + g->nx; i++, m++) {

@@ -6,7 +6,8 @@
  * and in the reference's loop and summation order, crates/wavecore/src/{grid,state,solver,
  * dispersion,forcing,par}.rs of mlaegn/wavesim. Parity is pinned by the reference's own
  * known-answer tests (ported under tests/), because the reference stores no numeric vectors and
- * its Rust toolchain is absent here.
+ * its Rust toolchain is absent here. The followed breaking fronts (eddy.rs) are pinned by that
+ * file's own unit tests, ported in tests/test_eddy_oracle.py.
  *
  * It shares the configuration structs of include/wavecore_c.h so that one configuration feeds
  * both the oracle and the device build.
@@ -64,6 +65,16 @@ double or_dot(const wc_grid* g, const double* ax, const double* ay, const double
 void or_dispersion_apply(const wc_grid* g, int periodic_y, const wc_dispersion* d,
                          const double* h, const double* hu, const double* hv, const double* lh,
                          double* lhu, double* lhv, const double* phi);
+/* eddy.rs: Kennedy's threshold (:114-124); `follow` (:155-219) on ghost-filled arrays,
+ * replacing `breaking` by the new memory and writing nu; `diffuse` (:221-302), returning the
+ * sub-steps; and the solver's `follow_breaking` (solver.rs:509-532). */
+double or_eddy_threshold(const wc_eddy* e, double age, double h);
+void or_eddy_follow(const wc_grid* g, const wc_eddy* e, const double* h, const double* hu,
+                    const double* hv, double* breaking, const double* phi, double dt, double* nu);
+int or_eddy_diffuse(const wc_grid* g, int periodic_y, double* h, double* hu, double* hv,
+                    double* breaking, const double* nu, double dt);
+int or_follow_breaking(or_solver* s, double* h, double* hu, double* hv, double* breaking,
+                       double dt);
 double or_volume(const wc_grid* g, const double* h);
 double or_max_abs_momentum(const wc_grid* g, const double* hu, const double* hv);
 double or_min_depth(const wc_grid* g, const double* h);

@@ -20,6 +20,7 @@ from .model import (  # noqa: F401
     Breaking,
     Dispersion,
     DispersionStats,
+    EddyViscosity,
     Grid,
     Limiting,
     LinearWave,

@@ -62,12 +62,18 @@ class wc_wavemaker(C.Structure):
     ]
 
 
+class wc_eddy(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("initial", "settled", "duration", "mixing", "linger")]
+
+
 class wc_breaking(C.Structure):
     _fields_ = [
         ("eta_ratio_lo", C.c_double),
         ("eta_ratio_hi", C.c_double),
         ("slope_lo", C.c_double),
         ("slope_hi", C.c_double),
+        ("viscosity", C.c_int32),
+        ("eddy", wc_eddy),
     ]
 
 
@@ -115,7 +121,7 @@ class wc_kernel_time(C.Structure):
     _fields_ = [("launches", C.c_uint64), ("total_ms", C.c_double)]
 
 
-KERNEL_KINDS = ("stage", "solve", "other", "network")
+KERNEL_KINDS = ("stage", "solve", "other", "network", "eddy")
 
 DPTR = C.POINTER(C.c_double)
 

@@ -150,9 +150,10 @@ __global__ void argmax64_kernel(int nx, int ny, double dx, double dy, const doub
 }
 
 // dispersion.rs:162-201: 1 - phi where the water is at least H_DISP_MIN deep, on the interior.
-// h is a device state; bed the FP32 bed.
+// h is a device state; bed the FP32 bed; mem the breaking memory of followed fronts, or null
+// (a cell whose memory is not 0 reads breaking, dispersion.rs:149-152).
 __global__ void breaking_kernel(DevGrid g, const float4* __restrict__ q, const float* __restrict__ bed,
-                                BreakingDev br, double* __restrict__ out) {
+                                BreakingDev br, const double* __restrict__ mem, double* __restrict__ out) {
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < (long long)g.nx * g.ny;
          c += (long long)gridDim.x * blockDim.x) {
         const int i = (int)(c % g.nx), j = (int)(c / g.nx);
@@ -160,6 +161,10 @@ __global__ void breaking_kernel(DevGrid g, const float4* __restrict__ q, const f
         const float h = q[k].x;
         if (h < H_DISP_MIN) {
             out[c] = 0.0;
+            continue;
+        }
+        if (mem && mem[k] != 0.0) {
+            out[c] = 1.0;
             continue;
         }
         auto eta = [&](int di, int dj) {

@@ -56,6 +56,7 @@ struct PcgArgs {
     double tol;
     long long max_iter;
     int mode;         // StageMode
+    int defer_finish; // the step's last kernel comes later (followed fronts): do not close the step
     int tiles_x, tiles_y;
     DampParams damp;
     unsigned long long timeout_ns;
@@ -456,7 +457,7 @@ __device__ __forceinline__ bool pcg_solve(const PcgArgs& a, int cta, int ncta, u
         if (rt != rt) nan_here = 1;
         else rmax = fmaxf(rmax, rt);
     }
-    if (a.mode != MODE_STAGE1) {
+    if (a.mode != MODE_STAGE1 && !a.defer_finish) {
         rmax = warp_max(rmax);
         if (nan_here) s_nan = 1;
         if ((tid & 31) == 0) s_rate[tid >> 5] = rmax;

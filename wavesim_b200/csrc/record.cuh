@@ -43,11 +43,14 @@ struct RecArrays {
     double* harm;        // [3][cells]: sums of w eta, w eta cos, w eta sin
 };
 
-// 1 - phi where the water is at least H_DISP_MIN deep (dispersion.rs:162-201).
+// 1 - phi where the water is at least H_DISP_MIN deep (dispersion.rs:162-201); with followed
+// fronts, 1 where the breaking memory `mem` (or null) is not 0 (dispersion.rs:149-152).
 __device__ __forceinline__ float breaking_off(const DevGrid& g, const float4* __restrict__ q,
-                                              const float* __restrict__ bed, const BreakingDev& br, int i, int j) {
+                                              const float* __restrict__ bed, const BreakingDev& br,
+                                              const double* __restrict__ mem, int i, int j) {
     const float h = q[j * g.pitch + i].x;
     if (h < H_DISP_MIN) return 0.f;
+    if (mem && mem[j * g.pitch + i] != 0.0) return 1.f;
     auto eta = [&](int di, int dj) {
         const Mapped m = map_cell(g, i + di, j + dj);
         return q[m.k].x + bed[m.k];
@@ -60,7 +63,8 @@ __device__ __forceinline__ float breaking_off(const DevGrid& g, const float4* __
 
 // Stage::record for every cell (lib.rs:1276-1301): a closing wave first, then this step's sample.
 __global__ void record_cells_kernel(DevGrid g, const float4* __restrict__ q, const float* __restrict__ bed,
-                                    BreakingDev br, const Ctl* __restrict__ ctl, RecDev* rd, RecArrays ra) {
+                                    BreakingDev br, const double* __restrict__ mem, const Ctl* __restrict__ ctl,
+                                    RecDev* rd, RecArrays ra) {
     const double t = ctl->t;
     const double inside = fmin(t - rd->t_last, t - rd->from);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -94,7 +98,7 @@ __global__ void record_cells_kernel(DevGrid g, const float4* __restrict__ q, con
         ra.eta_min[c] = fmin(ra.eta_min[c], eta);
         ra.wave_max[c] = fmax(ra.wave_max[c], eta);
         ra.wave_min[c] = fmin(ra.wave_min[c], eta);
-        if (breaking_off(g, q, bed, br, i, j) >= 0.8f) ra.breaking_seconds[c] += inside;
+        if (breaking_off(g, q, bed, br, mem, i, j) >= 0.8f) ra.breaking_seconds[c] += inside;
     }
 }
 

@@ -85,6 +85,7 @@ struct StageArgs {
     float4* qout;         // state written (SWE)
     const float* bed;
     const uint8_t* shallow;  // held cells (interior, pitch) or null
+    const double* mem;       // breaking memory of followed fronts (interior, pitch) or null
     BreakingDev br;
     MakerDev maker;
     DampParams damp;
@@ -292,6 +293,8 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int i0, int j0, f
                 const float off = fmaxf(smoothstep(a.br.er_lo, a.br.er_inv, ratio),
                                         smoothstep(a.br.sl_lo, a.br.sl_inv, hypotf(ex, ey)));
                 phi = 1.f - off;
+                // a front still breaking, or the water just behind it (dispersion.rs:149-152)
+                if (a.mem && a.mem[map_cell(g, i0 - ST_HALO + bx, j0 - ST_HALO + by).k] != 0.0) phi = 0.f;
             }
             if (a.shallow) {
                 const Mapped m = map_cell(g, i0 - ST_HALO + bx, j0 - ST_HALO + by);

@@ -17,6 +17,7 @@
 #include "../../include/wavecore_c.h"
 #include "aux.cuh"
 #include "common.cuh"
+#include "eddy.cuh"
 #include "ensemble.cuh"
 #include "lpc_host.cuh"
 #include "nest.cuh"
@@ -144,12 +145,23 @@ struct wc_solver {
     // Per-step statistics (wc_recorder): recorded after every step when attached.
     struct wc_recorder* rec = nullptr;
     float* frame = nullptr;  // staging of wc_frame: eta and the breaking indicator, FP32
+    // Followed breaking fronts (Breaking::viscosity, eddy.rs): the memory, the step's viscosity,
+    // the sub-steps' momentum banks and the cooperative kernel's barrier state.
+    int eddy_on = 0;
+    EddyParams eddy{};
+    double *mem = nullptr, *mem_new = nullptr;
+    float* nu = nullptr;
+    float2 *mb0 = nullptr, *mb1 = nullptr;
+    double* ed_part = nullptr;
+    unsigned* ed_bar = nullptr;
+    int* ed_sub = nullptr;
+    int ed_blocks = 0;
 
     ~wc_solver();
     void free_all() {
         void* bufs[] = {q0, q1, bed, prof, ycs, shallow, hn, pred, bv, w, r, p0, p1, ap, diag, cc, heff,
                         part, bar, ctl, st_h, st_hu, st_hv, r64, diag_bands, diag_done, diag_out, tv, fsc, fpart,
-                        r2, s_a, s_b, q_a, q_b, frame};
+                        r2, s_a, s_b, q_a, q_b, frame, mem, mem_new, nu, mb0, mb1, ed_part, ed_bar, ed_sub};
         for (void* b : bufs)
             if (b) cudaFree(b);
         if (done_host) cudaFreeHost(done_host);
@@ -252,6 +264,7 @@ StageArgs stage_args(const wc_solver* s, const float4* qin, const float4* qold, 
     a.qout = qout;
     a.bed = s->bed;
     a.shallow = s->shallow;
+    a.mem = s->eddy_on ? s->mem : nullptr;
     a.br = s->br;
     a.maker.on = s->has_maker;
     a.maker.omega = s->drive.omega;
@@ -326,6 +339,7 @@ PcgArgs pcg_args(const wc_solver* s, int mode, const float4* qold, float4* qout,
     a.tol = s->disp.tolerance;
     a.max_iter = (long long)s->disp.max_iterations;
     a.mode = mode;
+    a.defer_finish = s->eddy_on;
     a.tiles_x = s->pcg_tiles_x;
     a.tiles_y = s->pcg_tiles_y;
     a.damp = s->damp;
@@ -505,22 +519,59 @@ wc_status launch_solve(wc_solver* s, int mode, const float4* qold, float4* qout)
 // One SSP-RK2 step (solver.rs:479-507) of size ctl->dt on the device-resident state q0.
 wc_status enqueue_record(wc_solver* s);
 
+// Followed fronts and their eddy viscosity on the resident state (solver.rs:509-532): one
+// cooperative launch, so that its grid barriers cannot deadlock. With `finish` it is the step's
+// last kernel and closes the step; `sub_out` (device) receives the sub-steps taken.
+wc_status launch_eddy(wc_solver* s, int finish, int* sub_out) {
+    EddyArgs a{};
+    a.g = s->g;
+    a.q = s->q0;
+    a.bed = s->bed;
+    a.mem = s->mem;
+    a.mem_new = s->mem_new;
+    a.nu = s->nu;
+    a.mb[0] = s->mb0;
+    a.mb[1] = s->mb1;
+    a.part = s->ed_part;
+    a.cnt = s->ed_bar;
+    a.ctl = s->ctl;
+    a.sub_out = sub_out;
+    a.e = s->eddy;
+    a.finish = finish;
+    a.timeout_ns = BARRIER_TIMEOUT_NS;
+    CK(cudaMemsetAsync(s->ed_bar, 0, 2 * sizeof(unsigned), s->stream));
+    ProfScope ps(s, 4);
+    cudaLaunchConfig_t lc{};
+    lc.gridDim = dim3(s->ed_blocks);
+    lc.blockDim = dim3(ED_NT);
+    lc.dynamicSmemBytes = 0;
+    lc.stream = s->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    lc.attrs = attr;
+    lc.numAttrs = 1;
+    CK(cudaLaunchKernelEx(&lc, eddy_kernel, a));
+    s->launches++;
+    return WC_OK;
+}
+
 wc_status enqueue_step_kernels(wc_solver* s) {
     if (s->order == WC_ORDER_FIRST) {
         TRY(launch_stage(s, MODE_FIRST, s->q0, s->q0, s->q1, false));
         if (s->sgn) TRY(launch_solve(s, MODE_FIRST, s->q0, s->q1));
         CK(cudaMemcpyAsync(s->q0, s->q1, s->ncell * sizeof(float4), cudaMemcpyDeviceToDevice, s->stream));
-        return WC_OK;
-    }
-    if (!s->sgn) {
+    } else if (!s->sgn) {
         TRY(launch_stage(s, MODE_STAGE1, s->q0, s->q0, s->q1, false));
         TRY(launch_stage(s, MODE_STAGE2, s->q1, s->q0, s->q0, true));
-        return WC_OK;
+    } else {
+        TRY(launch_stage(s, MODE_STAGE1, s->q0, s->q0, s->q1, false));
+        TRY(launch_solve(s, MODE_STAGE1, s->q0, s->q1));
+        TRY(launch_stage(s, MODE_STAGE1, s->q1, s->q0, s->q1, true));
+        TRY(launch_solve(s, MODE_STAGE2, s->q0, s->q0));
     }
-    TRY(launch_stage(s, MODE_STAGE1, s->q0, s->q0, s->q1, false));
-    TRY(launch_solve(s, MODE_STAGE1, s->q0, s->q1));
-    TRY(launch_stage(s, MODE_STAGE1, s->q1, s->q0, s->q1, true));
-    TRY(launch_solve(s, MODE_STAGE2, s->q0, s->q0));
+    // solver.rs:505: the fronts follow the damped state, and close the step
+    if (s->eddy_on) TRY(launch_eddy(s, 1, nullptr));
     return WC_OK;
 }
 
@@ -571,6 +622,8 @@ wc_status status_of(wc_solver* s) {
     if (s->ctl_host->error & ERR_TIMEOUT)
         return set_err(WC_ETIMEOUT, "a grid barrier of the dispersive solve timed out");
     if (s->ctl_host->error & ERR_NAN) return set_err(WC_ENAN, "the state holds a NaN");
+    if (s->ctl_host->error & ERR_EDDY)
+        return set_err(WC_EUNSUPPORTED, "the eddy viscosity needed more than 65536 sub-steps; it was not applied");
     return WC_OK;
 }
 
@@ -625,6 +678,16 @@ void wc_dispersion_default(wc_dispersion* d) {
     d->tolerance = 1e-4;
     d->max_iterations = 200;
     d->preconditioner = WC_PC_JACOBI;
+    d->breaking.viscosity = 0;
+    wc_eddy_default(&d->breaking.eddy);
+}
+
+void wc_eddy_default(wc_eddy* e) {
+    e->initial = 0.65;
+    e->settled = 0.15;
+    e->duration = 5.0;
+    e->mixing = 1.2;
+    e->linger = 5.0;
 }
 
 const char* wc_last_error(void) { return g_err.c_str(); }
@@ -699,6 +762,10 @@ wc_status wc_solver_create(const wc_grid* grid, const double* bed_padded, const 
     s->br.er_inv = (float)(1.0 / (b.eta_ratio_hi - b.eta_ratio_lo));
     s->br.sl_lo = (float)b.slope_lo;
     s->br.sl_inv = (float)(1.0 / (b.slope_hi - b.slope_lo));
+    // follow_breaking reads the viscosity of the dispersion only (solver.rs:512-518)
+    s->eddy_on = (s->sgn && b.viscosity) ? 1 : 0;
+    s->eddy = EddyParams{b.eddy.initial, b.eddy.settled, b.eddy.duration, b.eddy.mixing, b.eddy.linger,
+                         b.eta_ratio_lo, b.eta_ratio_hi, b.slope_lo, b.slope_hi};
     s->damp.nsp = (int)cfg->n_sponges;
     s->damp.manning = (float)cfg->manning;
     for (int m = 0; m < s->damp.nsp; m++) {
@@ -830,6 +897,23 @@ wc_status wc_solver_create(const wc_grid* grid, const double* bed_padded, const 
         ALLOC(s->part, 8 * (size_t)s->pcg_blocks);
         ALLOC(s->bar, 2);
     }
+    if (s->eddy_on) {
+        ALLOC(s->mem, s->ncell);
+        ALLOC(s->mem_new, s->ncell);
+        ALLOC(s->nu, s->ncell);
+        ALLOC(s->mb0, s->ncell);
+        ALLOC(s->mb1, s->ncell);
+        ALLOC(s->ed_bar, 2);
+        ALLOC(s->ed_sub, 1);
+        int dev = 0, sms = 0, occ = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, eddy_kernel, ED_NT, 0) != cudaSuccess || occ < 1)
+            return fail(set_err(WC_ECUDA, "occupancy query for the eddy kernel failed"));
+        const size_t need = ((size_t)nx * ny + ED_NT - 1) / ED_NT;
+        s->ed_blocks = (int)std::max<size_t>(1, std::min<size_t>(need, (size_t)sms * std::min(occ, 4)));
+        ALLOC(s->ed_part, 2 * (size_t)s->ed_blocks);
+    }
 #undef ALLOC
     if (cudaMallocHost(&s->ctl_host, sizeof(Ctl)) != cudaSuccess)
         return fail(set_err(WC_ENOMEM, "cudaMallocHost failed"));
@@ -895,6 +979,7 @@ wc_status wc_state_upload(wc_solver* s, const double* h, const double* hu, const
     upload_kernel<<<aux_grid(s->ncell), AUX_NT, 0, s->stream>>>(s->g, s->st_h, s->st_hu, s->st_hv, s->q0);
     s->launches++;
     s->rate_current = false;
+    if (s->eddy_on) CK(cudaMemsetAsync(s->mem, 0, s->ncell * sizeof(double), s->stream));
     CK(cudaGetLastError());
     // The clock; a new state clears the error bits.
     TRY(read_ctl(s));
@@ -918,6 +1003,52 @@ wc_status wc_state_download(wc_solver* s, double* h, double* hu, double* hv, dou
     CK(cudaMemcpyAsync(hv, s->st_hv, bytes, cudaMemcpyDeviceToHost, s->stream));
     TRY(read_ctl(s));
     if (time) *time = s->ctl_host->t;
+    return WC_OK;
+}
+
+wc_status wc_breaking_upload(wc_solver* s, const double* breaking) {
+    if (!s || !breaking) return set_err(WC_EINVAL, "null argument");
+    if (!s->eddy_on) return WC_OK;
+    CK(cudaMemcpyAsync(s->st_h, breaking, s->npad * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+    pack_f64_kernel<<<aux_grid(s->ncell), AUX_NT, 0, s->stream>>>(s->g, s->st_h, s->mem);
+    s->launches++;
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(s->stream));
+    return WC_OK;
+}
+
+wc_status wc_breaking_download(wc_solver* s, double* breaking) {
+    if (!s || !breaking) return set_err(WC_EINVAL, "null argument");
+    if (!s->eddy_on) {
+        std::memset(breaking, 0, s->npad * sizeof(double));
+        return WC_OK;
+    }
+    unpack_f64_kernel<<<aux_grid(s->npad), AUX_NT, 0, s->stream>>>(s->g, s->mem, s->st_h);
+    s->launches++;
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(breaking, s->st_h, s->npad * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return WC_OK;
+}
+
+wc_status wc_follow_breaking(wc_solver* s, double* h, double* hu, double* hv, double* breaking, double dt,
+                             int32_t* sub_steps) {
+    if (!s || !h || !hu || !hv || !breaking) return set_err(WC_EINVAL, "null argument");
+    if (sub_steps) *sub_steps = 0;
+    if (!s->eddy_on) return WC_OK;
+    TRY(wc_state_upload(s, h, hu, hv, 0.0));
+    TRY(wc_breaking_upload(s, breaking));
+    set_dt_kernel<<<1, 1, 0, s->stream>>>(s->ctl, dt);
+    s->launches++;
+    CK(cudaMemsetAsync(s->ed_sub, 0, sizeof(int), s->stream));
+    TRY(launch_eddy(s, 0, s->ed_sub));
+    TRY(status_of(s));
+    TRY(wc_state_download(s, h, hu, hv, nullptr));
+    TRY(wc_breaking_download(s, breaking));
+    int n = 0;
+    CK(cudaMemcpyAsync(&n, s->ed_sub, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    if (sub_steps) *sub_steps = n;
     return WC_OK;
 }
 
@@ -955,11 +1086,14 @@ wc_status wc_synchronize(wc_solver* s) {
 wc_status wc_step(wc_solver* s, double* h, double* hu, double* hv, double* breaking, double* time,
                   double dt) {
     if (!s || !h || !hu || !hv || !time) return set_err(WC_EINVAL, "null argument");
+    if (s->eddy_on && !breaking) return set_err(WC_EINVAL, "followed fronts need the state's breaking memory");
     TRY(wc_state_upload(s, h, hu, hv, *time));
+    if (s->eddy_on) TRY(wc_breaking_upload(s, breaking));
     TRY(wc_step_device(s, dt));
     TRY(status_of(s));
     TRY(wc_state_download(s, h, hu, hv, nullptr));
-    if (breaking) fill_scalar_ghosts(s->grid, s->g.periodic != 0, breaking);
+    if (s->eddy_on) TRY(wc_breaking_download(s, breaking));
+    else if (breaking) fill_scalar_ghosts(s->grid, s->g.periodic != 0, breaking);
     // `s.time = t + dt` (solver.rs:506)
     *time = *time + dt;
     if (s->ctl_host->unconverged != s->seen_unconverged) {
@@ -1028,12 +1162,20 @@ wc_status wc_limiting_cell(wc_solver* s, const double* h, const double* hu, cons
 }
 
 wc_status wc_breaking_indicator(wc_solver* s, const double* h, const double* hu, const double* hv,
-                                double* out_interior) {
+                                const double* breaking, double* out_interior) {
     if (!s || !h || !hu || !hv || !out_interior) return set_err(WC_EINVAL, "null argument");
     TRY(stage_host(s, h, hu, hv));
     upload_kernel<<<aux_grid(s->ncell), AUX_NT, 0, s->stream>>>(s->g, s->st_h, s->st_hu, s->st_hv, s->q1);
-    breaking_kernel<<<aux_grid(s->ncell), AUX_NT, 0, s->stream>>>(s->g, s->q1, s->bed, s->br, s->st_h);
-    s->launches += 2;
+    s->launches++;
+    const double* mem = nullptr;
+    if (s->eddy_on && breaking) {  // the memory into scratch: the resident state's stays as it is
+        CK(cudaMemcpyAsync(s->st_hu, breaking, s->npad * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+        pack_f64_kernel<<<aux_grid(s->ncell), AUX_NT, 0, s->stream>>>(s->g, s->st_hu, s->mem_new);
+        s->launches++;
+        mem = s->mem_new;
+    }
+    breaking_kernel<<<aux_grid(s->ncell), AUX_NT, 0, s->stream>>>(s->g, s->q1, s->bed, s->br, mem, s->st_h);
+    s->launches++;
     CK(cudaMemcpyAsync(out_interior, s->st_h, s->grid.nx * s->grid.ny * sizeof(double),
                        cudaMemcpyDeviceToHost, s->stream));
     CK(cudaStreamSynchronize(s->stream));
@@ -1351,9 +1493,12 @@ wc_status wc_ensemble_create(uint64_t n, const wc_grid* grids, const double* con
     if (!out) return set_err(WC_EINVAL, "out is null");
     *out = nullptr;
     if (n == 0 || !grids || !beds || !cfgs) return set_err(WC_EINVAL, "an ensemble needs members");
-    for (uint64_t m = 0; m < n; m++)
+    for (uint64_t m = 0; m < n; m++) {
         if (cfgs[m].order == WC_ORDER_FIRST)
             return set_err(WC_EUNSUPPORTED, "ensemble members run second or fifth order (SSP-RK2)");
+        if (cfgs[m].dispersion && cfgs[m].dispersion->breaking.viscosity)
+            return set_err(WC_EUNSUPPORTED, "ensemble members do not follow breaking fronts (Breaking::viscosity)");
+    }
     wc_ensemble* e = new wc_ensemble();
     auto fail = [&](wc_status st) {
         delete e;
@@ -1775,7 +1920,8 @@ wc_status enqueue_record(wc_solver* s) {
     wc_recorder* r = s->rec;
     const size_t cells = r->cells;
     const unsigned blocks = (unsigned)std::min<size_t>(148 * 8, (cells + 255) / 256);
-    record_cells_kernel<<<blocks, 256, 0, s->stream>>>(s->g, s->q0, s->bed, s->br, s->ctl, r->rd, r->ra);
+    record_cells_kernel<<<blocks, 256, 0, s->stream>>>(s->g, s->q0, s->bed, s->br, s->eddy_on ? s->mem : nullptr,
+                                                       s->ctl, r->rd, r->ra);
     record_finish_kernel<<<1, 32, 0, s->stream>>>(s->ctl, r->rd);
     s->launches += 2;
     CK(cudaGetLastError());
@@ -1788,14 +1934,15 @@ __global__ void fill_kernel(double* a, size_t n, double v) {
 
 // eta = h + b and the breaking indicator of the resident state, FP32, interior row-major.
 __global__ void frame_kernel(DevGrid g, const float4* __restrict__ q, const float* __restrict__ bed, BreakingDev br,
-                             float* __restrict__ eta, float* __restrict__ brk, float* __restrict__ depth) {
+                             const double* __restrict__ mem, float* __restrict__ eta, float* __restrict__ brk,
+                             float* __restrict__ depth) {
     const size_t cells = (size_t)g.nx * g.ny;
     for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < cells; c += (size_t)gridDim.x * blockDim.x) {
         const int i = (int)(c % g.nx), j = (int)(c / g.nx);
         const int k = j * g.pitch + i;
         const double h = depth64(q[k]);
         eta[c] = (float)(h + (double)bed[k]);
-        brk[c] = breaking_off(g, q, bed, br, i, j);
+        brk[c] = breaking_off(g, q, bed, br, mem, i, j);
         depth[c] = (float)h;
     }
 }
@@ -1968,7 +2115,8 @@ wc_status wc_frame(wc_solver* s, double tide, float* eta, float* breaking, doubl
         CK(cudaMalloc(&s->frame, 3 * n * sizeof(float)));
     }
     const unsigned blocks = (unsigned)std::min<size_t>(148 * 8, (n + 255) / 256);
-    frame_kernel<<<blocks, 256, 0, s->stream>>>(s->g, s->q0, s->bed, s->br, s->frame, s->frame + n, s->frame + 2 * n);
+    frame_kernel<<<blocks, 256, 0, s->stream>>>(s->g, s->q0, s->bed, s->br, s->eddy_on ? s->mem : nullptr, s->frame,
+                                                s->frame + n, s->frame + 2 * n);
     s->launches++;
     CK(cudaGetLastError());
     std::vector<float> depth(n);

@@ -280,15 +280,35 @@ class WaveMaker:
 
 
 @dataclass
+class EddyViscosity:
+    """eddy.rs:62-90: how breaking fronts are followed, Kennedy et al.'s (2000) coefficients by
+    default. `initial`, `settled`: rates of rise in sqrt(g h); `duration`, `linger`: times in
+    sqrt(h / g); `mixing`: the mixing length in depths (0 follows fronts without viscosity)."""
+
+    initial: float = 0.65
+    settled: float = 0.15
+    duration: float = 5.0
+    mixing: float = 1.2
+    linger: float = 5.0
+
+    def to_c(self) -> abi.wc_eddy:
+        return abi.wc_eddy(float(self.initial), float(self.settled), float(self.duration), float(self.mixing),
+                           float(self.linger))
+
+
+@dataclass
 class Breaking:
-    """dispersion.rs:44-74. Followed fronts (`viscosity`) are not part of this build."""
+    """dispersion.rs:44-74. `viscosity` None reads the switch afresh every step (the default);
+    an EddyViscosity follows breaking fronts in the state's breaking memory (eddy.rs)."""
 
     eta_ratio: tuple = (0.30, 0.55)
     slope: tuple = (0.40, 0.65)
+    viscosity: Optional[EddyViscosity] = None
 
     def to_c(self) -> abi.wc_breaking:
         return abi.wc_breaking(
-            float(self.eta_ratio[0]), float(self.eta_ratio[1]), float(self.slope[0]), float(self.slope[1])
+            float(self.eta_ratio[0]), float(self.eta_ratio[1]), float(self.slope[0]), float(self.slope[1]),
+            1 if self.viscosity is not None else 0, (self.viscosity or EddyViscosity()).to_c(),
         )
 
 

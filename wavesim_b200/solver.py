@@ -28,6 +28,7 @@ _lib = None
 EXPORTS = [
     "wc_config_default",
     "wc_dispersion_default",
+    "wc_eddy_default",
     "wc_solver_create",
     "wc_solver_destroy",
     "wc_step",
@@ -37,6 +38,9 @@ EXPORTS = [
     "wc_dispersion_stats",
     "wc_state_upload",
     "wc_state_download",
+    "wc_breaking_upload",
+    "wc_breaking_download",
+    "wc_follow_breaking",
     "wc_step_device",
     "wc_step_n",
     "wc_stable_dt_device",
@@ -108,7 +112,12 @@ def load(path: str = LIB_PATH):
     L.wc_step.argtypes = [V, D, D, D, D, D, C.c_double]
     L.wc_stable_dt.argtypes = [V, D, D, D, D]
     L.wc_limiting_cell.argtypes = [V, D, D, D, C.POINTER(abi.wc_limiting), C.POINTER(C.c_int32)]
-    L.wc_breaking_indicator.argtypes = [V, D, D, D, D]
+    L.wc_breaking_indicator.argtypes = [V, D, D, D, D, D]
+    L.wc_eddy_default.argtypes = [C.POINTER(abi.wc_eddy)]
+    L.wc_eddy_default.restype = None
+    L.wc_breaking_upload.argtypes = [V, D]
+    L.wc_breaking_download.argtypes = [V, D]
+    L.wc_follow_breaking.argtypes = [V, D, D, D, D, C.c_double, C.POINTER(C.c_int32)]
     L.wc_dispersion_stats.argtypes = [V, C.POINTER(abi.wc_stats), C.POINTER(C.c_int32)]
     L.wc_state_upload.argtypes = [V, D, D, D, C.c_double]
     L.wc_state_download.argtypes = [V, D, D, D, D]
@@ -181,7 +190,8 @@ def load(path: str = LIB_PATH):
         "wc_solver_create", "wc_step", "wc_stable_dt", "wc_limiting_cell", "wc_breaking_indicator",
         "wc_dispersion_stats", "wc_state_upload", "wc_state_download", "wc_step_device", "wc_step_n",
         "wc_stable_dt_device", "wc_diagnostics_device", "wc_time_device", "wc_synchronize",
-        "wc_set_stream", "wc_profile_enable", "wc_profile_read",
+        "wc_set_stream", "wc_profile_enable", "wc_profile_read", "wc_breaking_upload", "wc_breaking_download",
+        "wc_follow_breaking",
     ):
         getattr(L, name).restype = C.c_int
     L.wc_config_default.restype = None
@@ -272,8 +282,18 @@ class Solver(SolverConfig):
     def breaking_indicator(self, s: State) -> np.ndarray:
         """solver.rs:336-349: nx*ny values, y outer."""
         out = np.zeros(self.grid.nx * self.grid.ny)
-        _check(load().wc_breaking_indicator(self._h(), abi.dptr(s.h), abi.dptr(s.hu), abi.dptr(s.hv), abi.dptr(out)))
+        _check(load().wc_breaking_indicator(self._h(), abi.dptr(s.h), abi.dptr(s.hu), abi.dptr(s.hv),
+                                            abi.dptr(s.breaking), abi.dptr(out)))
         return out
+
+    def follow_breaking(self, s: State, dt: float) -> int:
+        """solver.rs:509-532 (private in the reference, exported for parity checks of eddy.rs):
+        the fronts in s.breaking followed on to the state and their eddy viscosity applied over
+        dt, in place. Returns the viscous sub-steps taken; a no-op without followed fronts."""
+        n = C.c_int32()
+        _check(load().wc_follow_breaking(self._h(), abi.dptr(s.h), abi.dptr(s.hu), abi.dptr(s.hv),
+                                         abi.dptr(s.breaking), float(dt), C.byref(n)))
+        return n.value
 
     def dispersion_stats(self):
         """solver.rs:391-396."""
@@ -287,12 +307,23 @@ class Solver(SolverConfig):
     # ---- the device-resident throughput path --------------------------------------------
 
     def upload(self, s: State) -> None:
+        """The state onto the device, its breaking memory included (kept only with followed
+        fronts)."""
         _check(load().wc_state_upload(self._h(), abi.dptr(s.h), abi.dptr(s.hu), abi.dptr(s.hv), float(s.time)))
+        _check(load().wc_breaking_upload(self._h(), abi.dptr(s.breaking)))
 
     def download(self, s: State) -> None:
         t = C.c_double()
         _check(load().wc_state_download(self._h(), abi.dptr(s.h), abi.dptr(s.hu), abi.dptr(s.hv), C.byref(t)))
+        if self.follows_fronts:  # otherwise the memory is carried unchanged, as a step does
+            _check(load().wc_breaking_download(self._h(), abi.dptr(s.breaking)))
         s.time = t.value
+
+    @property
+    def follows_fronts(self) -> bool:
+        """Breaking::viscosity is set (and read: only with dispersion, solver.rs:512-518)."""
+        d = self.dispersion()
+        return d is not None and d.breaking.viscosity is not None
 
     def step_device(self, dt: float) -> None:
         _check(load().wc_step_device(self._h(), float(dt)))
