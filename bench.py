@@ -268,6 +268,8 @@ def measure_arm(w, args, world, stream, flush, net=None):
     sol.set_stream(stream.cuda_stream)
     if net is not None:
         sol.set_preconditioner(net)
+    if args.direct:
+        sol.profile(True)
     s0 = W.wave_train_state(w)
     sol.upload(s0)
     sol.step_n(args.warmup)  # warm-up: adaptive steps on the device
@@ -524,6 +526,9 @@ def main():
     ap.add_argument("--eta-steps", type=int, default=10)
     ap.add_argument("--cpu-steps", type=int, default=40)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--direct", action="store_true",
+                    help="launch every kernel directly, no step graph (for profilers: a graph with a "
+                         "conditional node hides its kernels from ncu)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")

@@ -250,6 +250,206 @@ __global__ void __launch_bounds__(CM_NT) conv_mma_kernel(ConvArgs p) {
     }
 }
 
+// ---- the solver's inference path: channels-innermost BF16 activations ----------------------
+//
+// The same implicit GEMM as conv_mma_kernel on activations stored NHWC in BF16 (a pixel's
+// channels contiguous, channel stride = the channel count, 2 or a multiple of 8): the staging
+// moves 16-byte groups of 8 channels (one load and one shared store each, instead of one scalar
+// load per element from NCHW FP32), a pooled input is the mean of four such groups, and the
+// epilogue writes each thread's channel pairs as 32-bit words, contiguous across the warp. The
+// numerics are those of conv_mma_kernel: every input is a BF16 number, products accumulate in
+// FP32, and the output is rounded to BF16 once (the network's last layer writes FP32).
+struct ConvH {
+    const unsigned short* a;  // ca channels, NHWC; CM_POOL: at 2H x 2W (2x2 mean), CM_UP: at H/2 x W/2
+    int ca, amode;
+    const unsigned short* b;  // cb channels at H x W (concatenated after a), or null
+    int cb;
+    const unsigned short* wre;  // weights, BF16, [8 ntiles][k k CP] (conv_mma_weights_kernel)
+    const float* bias;          // [co] or null
+    const unsigned short* gate; // co channels, NHWC, or null: y = act(conv + bias) * gate
+    unsigned short* y;          // co channels, NHWC BF16 ...
+    float* yf;                  // ... or FP32 (non-null: the network's output)
+    int co, H, W, N, act;
+};
+
+__host__ __device__ inline int conv_h_ps(int cp) { return cp + 8; }  // pixel stride in halves: 16-byte rows
+
+__host__ __device__ inline size_t conv_h_smem(int ci, int co, int kk) {
+    const int r = kk == 9 ? 1 : 0, cp = conv_mma_cp(ci);
+    return ((size_t)(CM_TY + 2 * r) * (CM_TX + 2 * r) * conv_h_ps(cp) + (size_t)((co + 7) / 8) * 8 * kk * cp) * 2;
+}
+
+__device__ __forceinline__ float bf16_lo(unsigned v) { return __uint_as_float(v << 16); }
+__device__ __forceinline__ float bf16_hi(unsigned v) { return __uint_as_float(v & 0xFFFF0000u); }
+__device__ __forceinline__ unsigned bf16_pack(float lo, float hi) {
+    return (unsigned)bf16_bits(lo) | ((unsigned)bf16_bits(hi) << 16);
+}
+// the mean of four groups of 8 BF16 channels, in conv_input's order, rounded to BF16
+__device__ __forceinline__ unsigned pool_word(unsigned a, unsigned b, unsigned c, unsigned d) {
+    const float lo = 0.25f * ((bf16_lo(a) + bf16_lo(b)) + (bf16_lo(c) + bf16_lo(d)));
+    const float hi = 0.25f * ((bf16_hi(a) + bf16_hi(b)) + (bf16_hi(c) + bf16_hi(d)));
+    return bf16_pack(lo, hi);
+}
+
+template <int KK, int NTL>
+__global__ void __launch_bounds__(CM_NT) conv_h_kernel(ConvH p) {
+    constexpr int R = KK == 9 ? 1 : 0, EW = CM_TX + 2 * R, EH = CM_TY + 2 * R;
+    extern __shared__ __align__(16) unsigned short cm_smem[];
+    const int ci_total = p.ca + p.cb;
+    const int CP = conv_mma_cp(ci_total), PS = conv_h_ps(CP), Kp = KK * CP;
+    unsigned short* in_s = cm_smem;                         // [EH][EW][PS]
+    unsigned short* w_s = cm_smem + (size_t)EH * EW * PS;   // [8 NTL][Kp]
+    const int n = blockIdx.z;
+    const int x0 = blockIdx.x * CM_TX, y0 = blockIdx.y * CM_TY;
+    // staging: unit = (pixel of the halo box, group of 8 channels), groups of a pixel adjacent
+    const int groups = CP / 8;
+    for (int q = threadIdx.x; q < EH * EW * groups; q += CM_NT) {
+        const int r = q / groups, gi = q - r * groups, c0 = gi * 8;
+        const int yy = y0 + r / EW - R, xx = x0 + r % EW - R;
+        uint4 v = make_uint4(0u, 0u, 0u, 0u);
+        if ((unsigned)yy < (unsigned)p.H && (unsigned)xx < (unsigned)p.W && c0 < ci_total) {
+            if (c0 >= p.ca) {
+                v = __ldg(reinterpret_cast<const uint4*>(p.b + (((size_t)n * p.H + yy) * p.W + xx) * p.cb + (c0 - p.ca)));
+            } else if (p.ca == 2) {  // a two-channel input: one word, zeros after it
+                size_t at;
+                if (p.amode == CM_POOL) {
+                    const size_t W2 = 2 * (size_t)p.W;
+                    at = (((size_t)n * 2 * p.H + 2 * yy) * W2 + 2 * xx);
+                    const unsigned* w = reinterpret_cast<const unsigned*>(p.a);
+                    v.x = pool_word(__ldg(w + at), __ldg(w + at + 1), __ldg(w + at + W2), __ldg(w + at + W2 + 1));
+                } else {
+                    at = p.amode == CM_UP ? (((size_t)n * (p.H / 2) + yy / 2) * (p.W / 2) + xx / 2)
+                                          : (((size_t)n * p.H + yy) * p.W + xx);
+                    v.x = __ldg(reinterpret_cast<const unsigned*>(p.a) + at);
+                }
+            } else if (p.amode == CM_POOL) {
+                const size_t W2 = 2 * (size_t)p.W;
+                const size_t at = (((size_t)n * 2 * p.H + 2 * yy) * W2 + 2 * xx) * p.ca + c0;
+                const uint4 a0 = __ldg(reinterpret_cast<const uint4*>(p.a + at));
+                const uint4 a1 = __ldg(reinterpret_cast<const uint4*>(p.a + at + p.ca));
+                const uint4 a2 = __ldg(reinterpret_cast<const uint4*>(p.a + at + W2 * p.ca));
+                const uint4 a3 = __ldg(reinterpret_cast<const uint4*>(p.a + at + (W2 + 1) * p.ca));
+                v = make_uint4(pool_word(a0.x, a1.x, a2.x, a3.x), pool_word(a0.y, a1.y, a2.y, a3.y),
+                               pool_word(a0.z, a1.z, a2.z, a3.z), pool_word(a0.w, a1.w, a2.w, a3.w));
+            } else {
+                const size_t at = p.amode == CM_UP ? (((size_t)n * (p.H / 2) + yy / 2) * (p.W / 2) + xx / 2)
+                                                   : (((size_t)n * p.H + yy) * p.W + xx);
+                v = __ldg(reinterpret_cast<const uint4*>(p.a + at * p.ca + c0));
+            }
+        }
+        *reinterpret_cast<uint4*>(in_s + (size_t)r * PS + c0) = v;
+    }
+    {  // the weights, already in this kernel's order: 16-byte copies
+        const uint4* src = reinterpret_cast<const uint4*>(p.wre);
+        uint4* dst = reinterpret_cast<uint4*>(w_s);
+        for (int q = threadIdx.x; q < NTL * Kp; q += CM_NT) dst[q] = __ldg(src + q);
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int grp = lane >> 2, tig = lane & 3;
+    float acc[2][NTL][4];
+#pragma unroll
+    for (int r = 0; r < 2; r++)
+#pragma unroll
+        for (int t = 0; t < NTL; t++)
+#pragma unroll
+            for (int e = 0; e < 4; e++) acc[r][t][e] = 0.f;
+    for (int kb = 0; kb < Kp; kb += 16) {
+        const int tap = kb / CP, c0 = kb - tap * CP + tig * 2;
+        const int dy = KK == 9 ? tap / 3 : 0, dx = KK == 9 ? tap - 3 * (tap / 3) : 0;
+        unsigned b[NTL][2];
+#pragma unroll
+        for (int t = 0; t < NTL; t++) {
+            const unsigned* wrow = reinterpret_cast<const unsigned*>(w_s + (size_t)(t * 8 + grp) * Kp + kb + tig * 2);
+            b[t][0] = wrow[0];
+            b[t][1] = wrow[4];
+        }
+#pragma unroll
+        for (int r = 0; r < 2; r++) {
+            const int row = warp * 2 + r + dy;
+            const unsigned* lo = reinterpret_cast<const unsigned*>(in_s + ((size_t)row * EW + grp + dx) * PS + c0);
+            const unsigned* hi = reinterpret_cast<const unsigned*>(in_s + ((size_t)row * EW + grp + 8 + dx) * PS + c0);
+            const unsigned a[4] = {lo[0], hi[0], lo[4], hi[4]};
+#pragma unroll
+            for (int t = 0; t < NTL; t++) mma_bf16_16816(acc[r][t], a, b[t]);
+        }
+    }
+    // D[pixel][channel]: pixels grp and grp + 8 of the warp's rows, channels t * 8 + tig * 2 + {0, 1}
+#pragma unroll
+    for (int r = 0; r < 2; r++) {
+        const int y = y0 + warp * 2 + r;
+#pragma unroll
+        for (int t = 0; t < NTL; t++) {
+#pragma unroll
+            for (int half = 0; half < 2; half++) {
+                const int x = x0 + grp + 8 * half;
+                const int co = t * 8 + tig * 2;
+                if (x >= p.W || y >= p.H || co >= p.co) continue;
+                float v0 = acc[r][t][2 * half] + (p.bias ? p.bias[co] : 0.f);
+                float v1 = acc[r][t][2 * half + 1] + (p.bias ? p.bias[co + 1] : 0.f);
+                if (p.act == ACT_RELU) {
+                    v0 = fmaxf(v0, 0.f);
+                    v1 = fmaxf(v1, 0.f);
+                } else if (p.act == ACT_SIG2) {
+                    v0 = 2.f / (1.f + expf(-v0));
+                    v1 = 2.f / (1.f + expf(-v1));
+                }
+                const size_t at = (((size_t)n * p.H + y) * p.W + x) * p.co + co;
+                if (p.gate) {
+                    const unsigned gw = __ldg(reinterpret_cast<const unsigned*>(p.gate + at));
+                    v0 *= bf16_lo(gw);
+                    v1 *= bf16_hi(gw);
+                }
+                if (p.yf) *reinterpret_cast<float2*>(p.yf + at) = make_float2(v0, v1);
+                else *reinterpret_cast<unsigned*>(p.y + at) = bf16_pack(v0, v1);
+            }
+        }
+    }
+}
+
+// NCHW FP32 maps -> NHWC BF16 (c channels, 2 or a multiple of 2).
+__global__ void to_h_kernel(const float* __restrict__ x, int N, int C, int H, int W, unsigned short* __restrict__ y) {
+    const size_t plane = (size_t)H * W, total = (size_t)N * plane * (C / 2);
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
+        const size_t pix = q / (C / 2);
+        const int c = 2 * (int)(q % (C / 2));
+        const size_t n = pix / plane, r = pix % plane;
+        const float* s = x + (n * C + c) * plane + r;
+        reinterpret_cast<unsigned*>(y)[q] = bf16_pack(s[0], s[plane]);
+    }
+}
+
+// NHWC FP32 two-channel output -> NCHW planes.
+__global__ void from_h_kernel(const float* __restrict__ y, int N, int H, int W, float* __restrict__ out) {
+    const size_t plane = (size_t)H * W, total = (size_t)N * plane;
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
+        const size_t n = q / plane, r = q % plane;
+        const float2 v = reinterpret_cast<const float2*>(y)[q];
+        out[n * 2 * plane + r] = v.x;
+        out[(n * 2 + 1) * plane + r] = v.y;
+    }
+}
+
+// The features of level l (the 2^l x 2^l block means of the level-0 NCHW FP32 features), NHWC BF16.
+__global__ void features_h_kernel(const float* __restrict__ f0, int N, int H0, int W0, int l,
+                                  unsigned short* __restrict__ fl) {
+    const int S = 1 << l, H = H0 >> l, W = W0 >> l;
+    const size_t plane0 = (size_t)H0 * W0, total = (size_t)N * H * W;
+    const float inv = 1.f / (float)(S * S);
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
+        const size_t n = q / ((size_t)H * W);
+        const int r = (int)(q % ((size_t)H * W)), yy = r / W, xx = r % W;
+        float a = 0.f, b = 0.f;
+        for (int u = 0; u < S; u++)
+            for (int v = 0; v < S; v++) {
+                const size_t k = (size_t)(yy * S + u) * W0 + (xx * S + v);
+                a += f0[n * 2 * plane0 + k];
+                b += f0[(n * 2 + 1) * plane0 + k];
+            }
+        reinterpret_cast<unsigned*>(fl)[q] = bf16_pack(a * inv, b * inv);
+    }
+}
+
 // dw[co][ci][t] = sum over samples and pixels of dy[co] * x[ci] shifted by tap t; one block per
 // (co, ci) pair. x is the concatenation of xa (ca channels) and xb, both at H x W.
 template <int K>
@@ -744,9 +944,9 @@ __global__ void lpc_jacobi_kernel(DevGrid g, const float2* r, const float2* d, f
 }
 
 // the network input: (r - t) / diag, as 2 planes of Hp x Wp (the S x S block means; zero
-// outside the interior)
+// outside the interior), or with `xh` as one NHWC BF16 pair per pixel
 __global__ void lpc_input_kernel(DevGrid g, const float2* r, const float2* t, const float2* d, float* x, int Hp, int Wp,
-                                 int S, const FcgScalars* sc) {
+                                 int S, const FcgScalars* sc, unsigned* xh = nullptr) {
     if (sc->done) return;
     const size_t plane = (size_t)Hp * Wp;
     const float inv = 1.f / (float)(S * S);
@@ -763,14 +963,19 @@ __global__ void lpc_input_kernel(DevGrid g, const float2* r, const float2* t, co
                     vy += (rr.y - tt.y) / dd.y;
                 }
             }
-        x[q] = vx * inv;
-        x[plane + q] = vy * inv;
+        if (xh) {
+            xh[q] = bf16_pack(vx * inv, vy * inv);
+        } else {
+            x[q] = vx * inv;
+            x[plane + q] = vy * inv;
+        }
     }
 }
 
-// z2 = z1 + mask * y (network output planes, read at the cell's block)
+// z2 = z1 + mask * y (network output planes, or with `nhwc` pairs per pixel, read at the
+// cell's block)
 __global__ void lpc_correct_kernel(DevGrid g, const float2* z1, const float* y, const float* heff, float2* z2, int Hp,
-                                   int Wp, int S, const FcgScalars* sc) {
+                                   int Wp, int S, const FcgScalars* sc, int nhwc = 0) {
     if (sc->done) return;
     const size_t plane = (size_t)Hp * Wp;
     const int n = g.nx * g.ny;
@@ -780,7 +985,8 @@ __global__ void lpc_correct_kernel(DevGrid g, const float2* z1, const float* y, 
         const float m = heff[k] >= H_DISP_MIN ? 1.f : 0.f;
         const size_t q = (size_t)(j / S) * Wp + i / S;
         const float2 a = z1[k];
-        z2[k] = make_float2(a.x + m * y[q], a.y + m * y[plane + q]);
+        const float2 v = nhwc ? reinterpret_cast<const float2*>(y)[q] : make_float2(y[q], y[plane + q]);
+        z2[k] = make_float2(a.x + m * v.x, a.y + m * v.y);
     }
 }
 

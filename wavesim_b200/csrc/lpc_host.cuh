@@ -37,7 +37,11 @@ inline cudaError_t conv_mma_configure() {
         const void* ks[] = {(const void*)conv_mma_kernel<9, 1>, (const void*)conv_mma_kernel<9, 2>,
                             (const void*)conv_mma_kernel<9, 4>, (const void*)conv_mma_kernel<9, 8>,
                             (const void*)conv_mma_kernel<1, 1>, (const void*)conv_mma_kernel<1, 2>,
-                            (const void*)conv_mma_kernel<1, 4>, (const void*)conv_mma_kernel<1, 8>};
+                            (const void*)conv_mma_kernel<1, 4>, (const void*)conv_mma_kernel<1, 8>,
+                            (const void*)conv_h_kernel<9, 1>,   (const void*)conv_h_kernel<9, 2>,
+                            (const void*)conv_h_kernel<9, 4>,   (const void*)conv_h_kernel<9, 8>,
+                            (const void*)conv_h_kernel<1, 1>,   (const void*)conv_h_kernel<1, 2>,
+                            (const void*)conv_h_kernel<1, 4>,   (const void*)conv_h_kernel<1, 8>};
         st = cudaSuccess;
         for (const void* k : ks)
             if (st == cudaSuccess)
@@ -86,6 +90,12 @@ struct LpcNet {
     DBuf wre;                   // tensor-core weights of every layer (BF16 pairs in floats)
     std::vector<size_t> wre_off;  // per layer, in BF16 elements, keyed by the layer's weight offset
     std::vector<int> wre_key;
+
+    // Inference on NHWC BF16 activations (conv_h_kernel): every channel count a multiple of 8
+    // and every layer's tile within the shared-memory limit; set by configure_nhwc.
+    bool nhwc = false;
+    DBuf Xh, Yh, Fh[LPC_LEVELS], HIDh[LPC_LEVELS], Gh[LPC_LEVELS], Ah[LPC_LEVELS], Eh[LPC_LEVELS],
+        DAh[LPC_LEVELS], Dh[LPC_LEVELS];
 
     // activations for one batch shape
     int N = 0, H = 0, W = 0;
@@ -168,6 +178,18 @@ struct LpcNet {
         return nullptr;
     }
 
+    bool configure_nhwc() {
+        nhwc = false;
+        if (!tensor || hidden % 8) return false;
+        for (int l = 0; l < LPC_LEVELS; l++)
+            if (ch[l] % 8 || ch[l] > 8 * CM_NMAX) return false;
+        for (auto* L : {&enc_a, &enc_b, &dec_a, &dec_b, &gate_a, &gate_b})
+            for (auto& l : *L)
+                if (l.co > 0 && conv_h_smem(l.ci, 8 * mma_tiles(l.co), l.k * l.k) > CONV_MMA_SMEM_MAX) return false;
+        nhwc = true;
+        return true;
+    }
+
     size_t max_weights() const {
         size_t maxw = 0;
         for (auto* L : {&enc_a, &enc_b, &dec_a, &dec_b, &gate_a, &gate_b})
@@ -210,6 +232,22 @@ struct LpcNet {
             }
         }
         A_(Y, sz(0, 2));
+        if (nhwc && !training) {  // BF16 halves, two per float of the buffer
+            auto H_ = [&](DBuf& b, size_t halves) { A_(b, (halves + 1) / 2); };
+            H_(Xh, sz(0, 2));
+            A_(Yh, sz(0, 2));
+            for (int l = 0; l < LPC_LEVELS; l++) {
+                H_(Fh[l], sz(l, 2));
+                H_(HIDh[l], sz(l, hidden));
+                H_(Gh[l], sz(l, ch[l]));
+                H_(Ah[l], sz(l, ch[l]));
+                H_(Eh[l], sz(l, ch[l]));
+                if (l < LPC_LEVELS - 1) {
+                    H_(DAh[l], sz(l, ch[l]));
+                    H_(Dh[l], sz(l, ch[l]));
+                }
+            }
+        }
         if (training) {
             size_t big = 0;
             for (int l = 0; l < LPC_LEVELS; l++) big = std::max(big, sz(l, ch[l] + (l + 1 < LPC_LEVELS ? ch[l + 1] : 0) + hidden + 2));
@@ -273,6 +311,81 @@ struct LpcNet {
             else conv_fwd_kernel<1, 1><<<grid, CV_TH * CV_TH, 0, st>>>(p);
         }
         return cudaGetLastError();
+    }
+
+    static const unsigned short* hp(const DBuf& b) { return reinterpret_cast<const unsigned short*>(b.p); }
+    static unsigned short* hp(DBuf& b) { return reinterpret_cast<unsigned short*>(b.p); }
+
+    // One convolution on NHWC BF16 activations (conv_h_kernel); yf: FP32 output instead of y.
+    cudaError_t conv_h(const unsigned short* a, int ca, int amode, const unsigned short* b, int cb, const LpcLayer& L,
+                       const unsigned short* gate, unsigned short* y, float* yf, int level, int act,
+                       cudaStream_t st) const {
+        ConvH p{};
+        p.a = a;
+        p.ca = ca;
+        p.amode = amode;
+        p.b = b;
+        p.cb = cb;
+        p.wre = wre_of(L);
+        p.bias = L.b >= 0 ? wq + L.b : nullptr;
+        p.gate = gate;
+        p.y = y;
+        p.yf = yf;
+        p.co = L.co;
+        p.H = h_of(level);
+        p.W = w_of(level);
+        p.N = N;
+        p.act = act;
+        const int nt = mma_tiles(L.co);
+        const size_t smem = conv_h_smem(L.ci, 8 * nt, L.k * L.k);
+        dim3 grid((p.W + CM_TX - 1) / CM_TX, (p.H + CM_TY - 1) / CM_TY, N);
+#define CONV_H_LAUNCH(KK_, NT_) conv_h_kernel<KK_, NT_><<<grid, CM_NT, smem, st>>>(p)
+        if (L.k == 3) {
+            if (nt == 1) CONV_H_LAUNCH(9, 1);
+            else if (nt == 2) CONV_H_LAUNCH(9, 2);
+            else if (nt <= 4) CONV_H_LAUNCH(9, 4);
+            else CONV_H_LAUNCH(9, 8);
+        } else {
+            if (nt == 1) CONV_H_LAUNCH(1, 1);
+            else if (nt == 2) CONV_H_LAUNCH(1, 2);
+            else if (nt <= 4) CONV_H_LAUNCH(1, 4);
+            else CONV_H_LAUNCH(1, 8);
+        }
+#undef CONV_H_LAUNCH
+        return cudaGetLastError();
+    }
+
+    // The gates on NHWC BF16 from the level-0 features F[0] (NCHW FP32): 3 launches a level.
+    cudaError_t gates_h(cudaStream_t st) {
+        cudaError_t e = cudaSuccess;
+        for (int l = 0; l < LPC_LEVELS && e == cudaSuccess; l++) {
+            features_h_kernel<<<ew_grid(sz(l, 1)), 256, 0, st>>>(F[0].p, N, H, W, l, hp(Fh[l]));
+            e = conv_h(hp(Fh[l]), 2, CM_DIRECT, nullptr, 0, gate_a[l], nullptr, hp(HIDh[l]), nullptr, l, ACT_RELU, st);
+            if (e == cudaSuccess)
+                e = conv_h(hp(HIDh[l]), hidden, CM_DIRECT, nullptr, 0, gate_b[l], nullptr, hp(Gh[l]), nullptr, l, ACT_SIG2, st);
+        }
+        return e;
+    }
+
+    // Yh = N(Xh) on NHWC BF16 activations with the gates already in Gh: the launches of forward().
+    cudaError_t forward_h(cudaStream_t st) {
+        cudaError_t e = cudaSuccess;
+        for (int l = 0; l < LPC_LEVELS && e == cudaSuccess; l++) {
+            const int cin = l == 0 ? 2 : ch[l - 1];
+            const unsigned short* in = l == 0 ? hp(Xh) : hp(Eh[l - 1]);
+            e = conv_h(in, cin, l == 0 ? CM_DIRECT : CM_POOL, nullptr, 0, enc_a[l], nullptr, hp(Ah[l]), nullptr, l,
+                       ACT_NONE, st);
+            if (e == cudaSuccess)
+                e = conv_h(hp(Ah[l]), ch[l], CM_DIRECT, nullptr, 0, enc_b[l], hp(Gh[l]), hp(Eh[l]), nullptr, l, ACT_NONE, st);
+        }
+        for (int l = LPC_LEVELS - 2; l >= 0 && e == cudaSuccess; l--) {
+            const unsigned short* below = (l == LPC_LEVELS - 2) ? hp(Eh[l + 1]) : hp(Dh[l + 1]);
+            e = conv_h(below, ch[l + 1], CM_UP, hp(Eh[l]), ch[l], dec_a[l], nullptr, hp(DAh[l]), nullptr, l, ACT_NONE, st);
+            if (e == cudaSuccess)
+                e = conv_h(hp(DAh[l]), ch[l], CM_DIRECT, nullptr, 0, dec_b[l], hp(Gh[l]), hp(Dh[l]), nullptr, l, ACT_NONE, st);
+        }
+        if (e == cudaSuccess) e = conv_h(hp(Dh[0]), ch[0], CM_DIRECT, nullptr, 0, out, nullptr, nullptr, Yh.p, 0, ACT_NONE, st);
+        return e;
     }
 
     // Gates of every level from the features F[0] (h / H0, b / H0): constant within a solve.

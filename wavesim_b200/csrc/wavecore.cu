@@ -410,8 +410,13 @@ wc_status fcg_pre(wc_solver* s, cudaStream_t st, cudaGraphConditionalHandle h, i
     const size_t plane = (size_t)s->lpc_hp * s->lpc_wp;
     FCG_LAUNCH(lpc_features_kernel<<<ew_grid(plane), 256, 0, st>>>(s->g, s->heff, s->bed, s->lnet.F[0].p, s->lpc_hp,
                                                                    s->lpc_wp, s->lpc->stride));
-    CK(s->lnet.gates(st));
-    s->launches += 2 * LPC_LEVELS + (LPC_LEVELS - 1);
+    if (s->lnet.nhwc) {
+        CK(s->lnet.gates_h(st));
+        s->launches += 3 * LPC_LEVELS;
+    } else {
+        CK(s->lnet.gates(st));
+        s->launches += 2 * LPC_LEVELS + (LPC_LEVELS - 1);
+    }
     return WC_OK;
 }
 
@@ -427,16 +432,19 @@ wc_status fcg_body(wc_solver* s, cudaStream_t st, cudaGraphConditionalHandle h, 
         ProfScope ps(s, 1);
         FCG_LAUNCH(lpc_jacobi_kernel<<<nb, 256, 0, st>>>(g, s->r, s->diag, z, LPC_OMEGA, sc));
         FCG_LAUNCH(fcg_matvec_kernel<<<nb, 256, 0, st>>>(g, z, s->cc, s->heff, s->tv, sc));
+        unsigned* xh = s->lnet.nhwc ? reinterpret_cast<unsigned*>(s->lnet.Xh.p) : nullptr;
         FCG_LAUNCH(lpc_input_kernel<<<ew_grid(plane), 256, 0, st>>>(g, s->r, s->tv, s->diag, s->lnet.X[0].p, hp, wp,
-                                                                    s->lpc->stride, sc));
+                                                                    s->lpc->stride, sc, xh));
     }
     {
         ProfScope ps(s, 3);
-        CK(s->lnet.forward(st, false));
+        CK(s->lnet.nhwc ? s->lnet.forward_h(st) : s->lnet.forward(st, false));
         s->launches += 2 * LPC_LEVELS + 2 * (LPC_LEVELS - 1) + 1;
     }
     ProfScope ps(s, 1);
-    FCG_LAUNCH(lpc_correct_kernel<<<nb, 256, 0, st>>>(g, z, s->lnet.Y.p, s->heff, z, hp, wp, s->lpc->stride, sc));
+    const float* y = s->lnet.nhwc ? s->lnet.Yh.p : s->lnet.Y.p;
+    FCG_LAUNCH(lpc_correct_kernel<<<nb, 256, 0, st>>>(g, z, y, s->heff, z, hp, wp, s->lpc->stride, sc,
+                                                      s->lnet.nhwc ? 1 : 0));
     FCG_LAUNCH(fcg_matvec_kernel<<<nb, 256, 0, st>>>(g, z, s->cc, s->heff, s->tv, sc));
     FCG_LAUNCH(lpc_post_kernel<<<nb, 256, 0, st>>>(g, z, s->r, s->tv, s->diag, z, LPC_OMEGA, sc));
     TRY(fcg_dots(s, st, FCG_BETA, z, q, nullptr, nullptr, h, 0));
@@ -1733,6 +1741,7 @@ wc_status wc_lpc_forward(wc_lpc* l, int32_t n, int32_t h, int32_t w, const float
     net.layout(m.net.ch, m.net.hidden);
     net.wq = m.wq.p;
     net.tensor = tensor != 0;
+    net.configure_nhwc();
     cudaStream_t st = m.st;
     if (net.tensor) {
         TRY(lpc_ck(conv_mma_configure(), "configure"));
@@ -1742,8 +1751,16 @@ wc_status wc_lpc_forward(wc_lpc* l, int32_t n, int32_t h, int32_t w, const float
     TRY(lpc_ck(net.shape(n, h, w, false), "activations"));
     TRY(lpc_ck(cudaMemcpyAsync(net.X[0].p, x, per * sizeof(float), cudaMemcpyHostToDevice, st), "upload"));
     TRY(lpc_ck(cudaMemcpyAsync(net.F[0].p, feat, per * sizeof(float), cudaMemcpyHostToDevice, st), "upload"));
-    TRY(lpc_ck(net.gates(st), "gates"));
-    TRY(lpc_ck(net.forward(st, false), "forward"));
+    if (net.nhwc) {  // the solver's path: NHWC BF16 activations
+        to_h_kernel<<<ew_grid(per / 2), 256, 0, st>>>(net.X[0].p, n, 2, h, w, LpcNet::hp(net.Xh));
+        TRY(lpc_ck(net.gates_h(st), "gates"));
+        TRY(lpc_ck(net.forward_h(st), "forward"));
+        from_h_kernel<<<ew_grid(per / 2), 256, 0, st>>>(net.Yh.p, n, h, w, net.Y.p);
+        TRY(lpc_ck(cudaGetLastError(), "forward"));
+    } else {
+        TRY(lpc_ck(net.gates(st), "gates"));
+        TRY(lpc_ck(net.forward(st, false), "forward"));
+    }
     TRY(lpc_ck(cudaMemcpyAsync(y, net.Y.p, per * sizeof(float), cudaMemcpyDeviceToHost, st), "download"));
     return lpc_ck(cudaStreamSynchronize(st), "forward");
 }
@@ -1871,6 +1888,7 @@ wc_status wc_solver_set_lpc(wc_solver* s, wc_lpc* l) {
     s->lnet.wq = l->m.wq.p;
     s->lnet.gw = nullptr;
     s->lnet.tensor = true;  // the solve applies the network on the tensor cores
+    s->lnet.configure_nhwc();
     CK(conv_mma_configure());
     CK(s->lnet.prepare_tensor(s->stream));
     CK(cudaStreamSynchronize(s->stream));
