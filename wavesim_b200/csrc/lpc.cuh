@@ -6,6 +6,8 @@
 // arithmetic is BF16 weights with FP32 accumulation). Zero padding at tensor edges.
 #pragma once
 
+#include <cuda_bf16.h>
+
 #include "common.cuh"
 
 namespace wcb {
@@ -274,15 +276,11 @@ struct ConvH {
 
 __host__ __device__ inline int conv_h_ps(int cp) { return cp + 8; }  // pixel stride in halves: 16-byte rows
 
-__host__ __device__ inline size_t conv_h_smem(int ci, int co, int kk) {
-    const int r = kk == 9 ? 1 : 0, cp = conv_mma_cp(ci);
-    return ((size_t)(CM_TY + 2 * r) * (CM_TX + 2 * r) * conv_h_ps(cp) + (size_t)((co + 7) / 8) * 8 * kk * cp) * 2;
-}
-
 __device__ __forceinline__ float bf16_lo(unsigned v) { return __uint_as_float(v << 16); }
 __device__ __forceinline__ float bf16_hi(unsigned v) { return __uint_as_float(v & 0xFFFF0000u); }
-__device__ __forceinline__ unsigned bf16_pack(float lo, float hi) {
-    return (unsigned)bf16_bits(lo) | ((unsigned)bf16_bits(hi) << 16);
+__device__ __forceinline__ unsigned bf16_pack(float lo, float hi) {  // cvt.rn.bf16x2.f32: nearest, ties to even
+    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const unsigned*>(&v);
 }
 // the mean of four groups of 8 BF16 channels, in conv_input's order, rounded to BF16
 __device__ __forceinline__ unsigned pool_word(unsigned a, unsigned b, unsigned c, unsigned d) {
@@ -291,102 +289,155 @@ __device__ __forceinline__ unsigned pool_word(unsigned a, unsigned b, unsigned c
     return bf16_pack(lo, hi);
 }
 
-template <int KK, int NTL>
-__global__ void __launch_bounds__(CM_NT) conv_h_kernel(ConvH p) {
-    constexpr int R = KK == 9 ? 1 : 0, EW = CM_TX + 2 * R, EH = CM_TY + 2 * R;
+// 16-byte global -> shared copy that does not hold a register (src_bytes 0: zero fill)
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int src_bytes) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+// Four 8x8 BF16 matrices from shared memory, one 16-byte row address per lane
+__device__ __forceinline__ void ldmatrix_x4(unsigned* r, const void* row) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(row);
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(sa));
+}
+
+// Rows of 16 pixels per warp: taller tiles for the thin layers (fewer halo cells and less fixed
+// work per pixel), two rows where the output has four or more tiles of 8 channels.
+__host__ __device__ constexpr int conv_h_rows(int ntl) { return ntl <= 2 ? 4 : 2; }
+
+// Shared memory of the channels-innermost convolution (bytes): the input box, the weights.
+__host__ __device__ inline size_t conv_h_smem2(int ci, int co, int kk) {
+    const int r = kk == 9 ? 1 : 0, cp = conv_mma_cp(ci), ntl = (co + 7) / 8;
+    const int th = 8 * conv_h_rows(ntl);
+    const size_t box = (size_t)(th + 2 * r) * (CM_TX + 2 * r) * conv_h_ps(cp);
+    return (box + (size_t)ntl * 8 * kk * cp) * 2;
+}
+
+// KK taps (9 or 1), NTL tiles of 8 output channels, CP input channels padded to 16: all index
+// arithmetic is compile-time and 32-bit (a map of up to 2^31 values). A block computes a tile of
+// 16 x (8 RW) pixels, each warp RW rows of 16; its halo box is staged with cp.async (pooled
+// inputs through registers), A fragments are read with ldmatrix, and values are rounded to BF16
+// by the hardware conversion (round to nearest even, as bf16_bits).
+template <int KK, int NTL, int CP>
+__global__ void __launch_bounds__(CM_NT, 2) conv_h_kernel(ConvH p) {
+    constexpr int RW = conv_h_rows(NTL), TH = 8 * RW;
+    constexpr int R = KK == 9 ? 1 : 0, EW = CM_TX + 2 * R, EH = TH + 2 * R;
+    constexpr int PS = CP + 8, KP = KK * CP, GROUPS = CP / 8, UNITS = EH * EW * GROUPS;
+    constexpr int PER = (UNITS + CM_NT - 1) / CM_NT;
     extern __shared__ __align__(16) unsigned short cm_smem[];
+    unsigned short* in_s = cm_smem;             // [EH][EW][PS]
+    unsigned short* w_s = cm_smem + EH * EW * PS;  // [8 NTL][KP]
     const int ci_total = p.ca + p.cb;
-    const int CP = conv_mma_cp(ci_total), PS = conv_h_ps(CP), Kp = KK * CP;
-    unsigned short* in_s = cm_smem;                         // [EH][EW][PS]
-    unsigned short* w_s = cm_smem + (size_t)EH * EW * PS;   // [8 NTL][Kp]
     const int n = blockIdx.z;
-    const int x0 = blockIdx.x * CM_TX, y0 = blockIdx.y * CM_TY;
-    // staging: unit = (pixel of the halo box, group of 8 channels), groups of a pixel adjacent
-    const int groups = CP / 8;
-    for (int q = threadIdx.x; q < EH * EW * groups; q += CM_NT) {
-        const int r = q / groups, gi = q - r * groups, c0 = gi * 8;
-        const int yy = y0 + r / EW - R, xx = x0 + r % EW - R;
-        uint4 v = make_uint4(0u, 0u, 0u, 0u);
-        if ((unsigned)yy < (unsigned)p.H && (unsigned)xx < (unsigned)p.W && c0 < ci_total) {
-            if (c0 >= p.ca) {
-                v = __ldg(reinterpret_cast<const uint4*>(p.b + (((size_t)n * p.H + yy) * p.W + xx) * p.cb + (c0 - p.ca)));
-            } else if (p.ca == 2) {  // a two-channel input: one word, zeros after it
-                size_t at;
-                if (p.amode == CM_POOL) {
-                    const size_t W2 = 2 * (size_t)p.W;
-                    at = (((size_t)n * 2 * p.H + 2 * yy) * W2 + 2 * xx);
-                    const unsigned* w = reinterpret_cast<const unsigned*>(p.a);
-                    v.x = pool_word(__ldg(w + at), __ldg(w + at + 1), __ldg(w + at + W2), __ldg(w + at + W2 + 1));
-                } else {
-                    at = p.amode == CM_UP ? (((size_t)n * (p.H / 2) + yy / 2) * (p.W / 2) + xx / 2)
-                                          : (((size_t)n * p.H + yy) * p.W + xx);
-                    v.x = __ldg(reinterpret_cast<const unsigned*>(p.a) + at);
-                }
-            } else if (p.amode == CM_POOL) {
-                const size_t W2 = 2 * (size_t)p.W;
-                const size_t at = (((size_t)n * 2 * p.H + 2 * yy) * W2 + 2 * xx) * p.ca + c0;
-                const uint4 a0 = __ldg(reinterpret_cast<const uint4*>(p.a + at));
-                const uint4 a1 = __ldg(reinterpret_cast<const uint4*>(p.a + at + p.ca));
-                const uint4 a2 = __ldg(reinterpret_cast<const uint4*>(p.a + at + W2 * p.ca));
-                const uint4 a3 = __ldg(reinterpret_cast<const uint4*>(p.a + at + (W2 + 1) * p.ca));
-                v = make_uint4(pool_word(a0.x, a1.x, a2.x, a3.x), pool_word(a0.y, a1.y, a2.y, a3.y),
-                               pool_word(a0.z, a1.z, a2.z, a3.z), pool_word(a0.w, a1.w, a2.w, a3.w));
-            } else {
-                const size_t at = p.amode == CM_UP ? (((size_t)n * (p.H / 2) + yy / 2) * (p.W / 2) + xx / 2)
-                                                   : (((size_t)n * p.H + yy) * p.W + xx);
-                v = __ldg(reinterpret_cast<const uint4*>(p.a + at * p.ca + c0));
-            }
-        }
-        *reinterpret_cast<uint4*>(in_s + (size_t)r * PS + c0) = v;
-    }
-    {  // the weights, already in this kernel's order: 16-byte copies
+    const int x0 = blockIdx.x * CM_TX, y0 = blockIdx.y * TH;
+    const bool two = p.ca == 2;
+    {
         const uint4* src = reinterpret_cast<const uint4*>(p.wre);
         uint4* dst = reinterpret_cast<uint4*>(w_s);
-        for (int q = threadIdx.x; q < NTL * Kp; q += CM_NT) dst[q] = __ldg(src + q);
+        for (int q = threadIdx.x; q < NTL * KP; q += CM_NT) cp_async16(dst + q, src + q, 16);
     }
+    const int Hs = p.amode == CM_POOL ? 2 * p.H : p.amode == CM_UP ? p.H / 2 : p.H;  // a's map
+    const int Ws = p.amode == CM_POOL ? 2 * p.W : p.amode == CM_UP ? p.W / 2 : p.W;
+    const int abase = n * Hs * Ws, bbase = n * p.H * p.W;
+#pragma unroll 4
+    for (int u = 0; u < PER; u++) {
+        const int q = threadIdx.x + u * CM_NT;
+        if (UNITS % CM_NT != 0 && q >= UNITS) break;
+        const int r = q / GROUPS, c0 = (q % GROUPS) * 8;
+        const int yy = y0 + r / EW - R, xx = x0 + r % EW - R;
+        unsigned short* dst = in_s + r * PS + c0;
+        const bool inside = (unsigned)yy < (unsigned)p.H && (unsigned)xx < (unsigned)p.W && c0 < ci_total;
+        if (inside && c0 < p.ca && (p.amode == CM_POOL || two)) {
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (p.amode == CM_POOL) {
+                const int at = abase + (2 * yy) * Ws + 2 * xx;
+                if (two) {
+                    const unsigned* w = reinterpret_cast<const unsigned*>(p.a);
+                    v.x = pool_word(__ldg(w + at), __ldg(w + at + 1), __ldg(w + at + Ws), __ldg(w + at + Ws + 1));
+                } else {
+                    const uint4* w = reinterpret_cast<const uint4*>(p.a);
+                    const int g = p.ca / 8, o = c0 / 8;
+                    const uint4 a0 = __ldg(w + at * g + o), a1 = __ldg(w + (at + 1) * g + o);
+                    const uint4 a2 = __ldg(w + (at + Ws) * g + o), a3 = __ldg(w + (at + Ws + 1) * g + o);
+                    v = make_uint4(pool_word(a0.x, a1.x, a2.x, a3.x), pool_word(a0.y, a1.y, a2.y, a3.y),
+                                   pool_word(a0.z, a1.z, a2.z, a3.z), pool_word(a0.w, a1.w, a2.w, a3.w));
+                }
+            } else {
+                const int at = abase + (p.amode == CM_UP ? (yy / 2) * Ws + xx / 2 : yy * Ws + xx);
+                v.x = __ldg(reinterpret_cast<const unsigned*>(p.a) + at);
+            }
+            *reinterpret_cast<uint4*>(dst) = v;
+        } else {
+            const unsigned short* src = p.a;  // a valid address when nothing is read
+            if (inside) {
+                if (c0 >= p.ca) src = p.b + (bbase + yy * p.W + xx) * p.cb + (c0 - p.ca);
+                else src = p.a + (abase + (p.amode == CM_UP ? (yy / 2) * Ws + xx / 2 : yy * Ws + xx)) * p.ca + c0;
+            }
+            cp_async16(dst, src, inside ? 16 : 0);
+        }
+    }
+    cp_async_wait_all();
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int grp = lane >> 2, tig = lane & 3;
-    float acc[2][NTL][4];
+    const int lpix = (lane & 7) + ((lane >> 3) & 1) * 8, lk = (lane >> 4) * 8;  // ldmatrix row of this lane
+    float acc[RW][NTL][4];
 #pragma unroll
-    for (int r = 0; r < 2; r++)
+    for (int r = 0; r < RW; r++)
 #pragma unroll
         for (int t = 0; t < NTL; t++)
 #pragma unroll
             for (int e = 0; e < 4; e++) acc[r][t][e] = 0.f;
-    for (int kb = 0; kb < Kp; kb += 16) {
-        const int tap = kb / CP, c0 = kb - tap * CP + tig * 2;
-        const int dy = KK == 9 ? tap / 3 : 0, dx = KK == 9 ? tap - 3 * (tap / 3) : 0;
-        unsigned b[NTL][2];
+#pragma unroll 3
+    for (int tap = 0; tap < KK; tap++) {
+        const int dy = KK == 9 ? tap / 3 : 0, dx = KK == 9 ? tap % 3 : 0;
 #pragma unroll
-        for (int t = 0; t < NTL; t++) {
-            const unsigned* wrow = reinterpret_cast<const unsigned*>(w_s + (size_t)(t * 8 + grp) * Kp + kb + tig * 2);
-            b[t][0] = wrow[0];
-            b[t][1] = wrow[4];
-        }
+        for (int cb = 0; cb < CP; cb += 16) {
+            const int kb = tap * CP + cb;
+            unsigned b[NTL][2];
 #pragma unroll
-        for (int r = 0; r < 2; r++) {
-            const int row = warp * 2 + r + dy;
-            const unsigned* lo = reinterpret_cast<const unsigned*>(in_s + ((size_t)row * EW + grp + dx) * PS + c0);
-            const unsigned* hi = reinterpret_cast<const unsigned*>(in_s + ((size_t)row * EW + grp + 8 + dx) * PS + c0);
-            const unsigned a[4] = {lo[0], hi[0], lo[4], hi[4]};
+            for (int t = 0; t < NTL; t++) {
+                const unsigned* wrow = reinterpret_cast<const unsigned*>(w_s + (t * 8 + grp) * KP + kb + tig * 2);
+                b[t][0] = wrow[0];
+                b[t][1] = wrow[4];
+            }
 #pragma unroll
-            for (int t = 0; t < NTL; t++) mma_bf16_16816(acc[r][t], a, b[t]);
+            for (int r = 0; r < RW; r++) {
+                unsigned a[4];
+                ldmatrix_x4(a, in_s + ((warp * RW + r + dy) * EW + lpix + dx) * PS + cb + lk);
+#pragma unroll
+                for (int t = 0; t < NTL; t++) mma_bf16_16816(acc[r][t], a, b[t]);
+            }
         }
     }
     // D[pixel][channel]: pixels grp and grp + 8 of the warp's rows, channels t * 8 + tig * 2 + {0, 1}
+    float bias[NTL][2];
 #pragma unroll
-    for (int r = 0; r < 2; r++) {
-        const int y = y0 + warp * 2 + r;
+    for (int t = 0; t < NTL; t++) {
+        const int co = t * 8 + tig * 2;
+        bias[t][0] = p.bias && co < p.co ? __ldg(p.bias + co) : 0.f;
+        bias[t][1] = p.bias && co < p.co ? __ldg(p.bias + co + 1) : 0.f;
+    }
 #pragma unroll
-        for (int t = 0; t < NTL; t++) {
+    for (int r = 0; r < RW; r++) {
+        const int y = y0 + warp * RW + r;
+        if (y >= p.H) continue;
+        const int row = (n * p.H + y) * p.W;
 #pragma unroll
-            for (int half = 0; half < 2; half++) {
-                const int x = x0 + grp + 8 * half;
+        for (int half = 0; half < 2; half++) {
+            const int x = x0 + grp + 8 * half;
+            if (x >= p.W) continue;
+            const int pix = (row + x) * p.co;
+#pragma unroll
+            for (int t = 0; t < NTL; t++) {
                 const int co = t * 8 + tig * 2;
-                if (x >= p.W || y >= p.H || co >= p.co) continue;
-                float v0 = acc[r][t][2 * half] + (p.bias ? p.bias[co] : 0.f);
-                float v1 = acc[r][t][2 * half + 1] + (p.bias ? p.bias[co + 1] : 0.f);
+                if (co >= p.co) continue;
+                float v0 = acc[r][t][2 * half] + bias[t][0];
+                float v1 = acc[r][t][2 * half + 1] + bias[t][1];
                 if (p.act == ACT_RELU) {
                     v0 = fmaxf(v0, 0.f);
                     v1 = fmaxf(v1, 0.f);
@@ -394,14 +445,13 @@ __global__ void __launch_bounds__(CM_NT) conv_h_kernel(ConvH p) {
                     v0 = 2.f / (1.f + expf(-v0));
                     v1 = 2.f / (1.f + expf(-v1));
                 }
-                const size_t at = (((size_t)n * p.H + y) * p.W + x) * p.co + co;
                 if (p.gate) {
-                    const unsigned gw = __ldg(reinterpret_cast<const unsigned*>(p.gate + at));
+                    const unsigned gw = __ldg(reinterpret_cast<const unsigned*>(p.gate + pix + co));
                     v0 *= bf16_lo(gw);
                     v1 *= bf16_hi(gw);
                 }
-                if (p.yf) *reinterpret_cast<float2*>(p.yf + at) = make_float2(v0, v1);
-                else *reinterpret_cast<unsigned*>(p.y + at) = bf16_pack(v0, v1);
+                if (p.yf) *reinterpret_cast<float2*>(p.yf + pix + co) = make_float2(v0, v1);
+                else *reinterpret_cast<unsigned*>(p.y + pix + co) = bf16_pack(v0, v1);
             }
         }
     }

@@ -8,6 +8,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <string>
 #include <vector>
 
@@ -31,6 +32,14 @@ struct LpcLayer {
 constexpr size_t CONV_MMA_SMEM_MAX = 160 * 1024;
 
 // The tensor-core convolution's shared-memory limit, set once per process before any capture.
+// Every instantiation of the channels-innermost convolution: taps x output tiles x padded inputs.
+#define CONV_H_FOR_ALL(X)                                                                          \
+    X(9, 1, 16) X(9, 1, 32) X(9, 1, 48) X(9, 1, 64) X(9, 2, 16) X(9, 2, 32) X(9, 2, 48) X(9, 2, 64) \
+    X(9, 4, 16) X(9, 4, 32) X(9, 4, 48) X(9, 4, 64) X(9, 8, 16) X(9, 8, 32) X(9, 8, 48) X(9, 8, 64) \
+    X(1, 1, 16) X(1, 1, 32) X(1, 1, 48) X(1, 1, 64) X(1, 2, 16) X(1, 2, 32) X(1, 2, 48) X(1, 2, 64) \
+    X(1, 4, 16) X(1, 4, 32) X(1, 4, 48) X(1, 4, 64) X(1, 8, 16) X(1, 8, 32) X(1, 8, 48) X(1, 8, 64)
+constexpr int CONV_H_CP_MAX = 64;
+
 inline cudaError_t conv_mma_configure() {
     static cudaError_t st = cudaErrorNotReady;
     if (st == cudaErrorNotReady) {
@@ -38,10 +47,10 @@ inline cudaError_t conv_mma_configure() {
                             (const void*)conv_mma_kernel<9, 4>, (const void*)conv_mma_kernel<9, 8>,
                             (const void*)conv_mma_kernel<1, 1>, (const void*)conv_mma_kernel<1, 2>,
                             (const void*)conv_mma_kernel<1, 4>, (const void*)conv_mma_kernel<1, 8>,
-                            (const void*)conv_h_kernel<9, 1>,   (const void*)conv_h_kernel<9, 2>,
-                            (const void*)conv_h_kernel<9, 4>,   (const void*)conv_h_kernel<9, 8>,
-                            (const void*)conv_h_kernel<1, 1>,   (const void*)conv_h_kernel<1, 2>,
-                            (const void*)conv_h_kernel<1, 4>,   (const void*)conv_h_kernel<1, 8>};
+#define CONV_H_PTR(KK_, NT_, CP_) (const void*)conv_h_kernel<KK_, NT_, CP_>,
+                            CONV_H_FOR_ALL(CONV_H_PTR)
+#undef CONV_H_PTR
+        };
         st = cudaSuccess;
         for (const void* k : ks)
             if (st == cudaSuccess)
@@ -185,7 +194,9 @@ struct LpcNet {
             if (ch[l] % 8 || ch[l] > 8 * CM_NMAX) return false;
         for (auto* L : {&enc_a, &enc_b, &dec_a, &dec_b, &gate_a, &gate_b})
             for (auto& l : *L)
-                if (l.co > 0 && conv_h_smem(l.ci, 8 * mma_tiles(l.co), l.k * l.k) > CONV_MMA_SMEM_MAX) return false;
+                if (l.co > 0 && (conv_mma_cp(l.ci) > CONV_H_CP_MAX ||
+                                 conv_h_smem2(l.ci, 8 * mma_tiles(l.co), l.k * l.k) > CONV_MMA_SMEM_MAX))
+                    return false;
         nhwc = true;
         return true;
     }
@@ -337,21 +348,19 @@ struct LpcNet {
         p.N = N;
         p.act = act;
         const int nt = mma_tiles(L.co);
-        const size_t smem = conv_h_smem(L.ci, 8 * nt, L.k * L.k);
-        dim3 grid((p.W + CM_TX - 1) / CM_TX, (p.H + CM_TY - 1) / CM_TY, N);
-#define CONV_H_LAUNCH(KK_, NT_) conv_h_kernel<KK_, NT_><<<grid, CM_NT, smem, st>>>(p)
-        if (L.k == 3) {
-            if (nt == 1) CONV_H_LAUNCH(9, 1);
-            else if (nt == 2) CONV_H_LAUNCH(9, 2);
-            else if (nt <= 4) CONV_H_LAUNCH(9, 4);
-            else CONV_H_LAUNCH(9, 8);
-        } else {
-            if (nt == 1) CONV_H_LAUNCH(1, 1);
-            else if (nt == 2) CONV_H_LAUNCH(1, 2);
-            else if (nt <= 4) CONV_H_LAUNCH(1, 4);
-            else CONV_H_LAUNCH(1, 8);
+        const size_t smem = conv_h_smem2(L.ci, 8 * nt, L.k * L.k);
+        const int th = 8 * conv_h_rows(nt);
+        dim3 grid((p.W + CM_TX - 1) / CM_TX, (p.H + th - 1) / th, N);
+        const int kk = L.k * L.k, cp = conv_mma_cp(L.ci);
+        bool launched = false;
+#define CONV_H_LAUNCH(KK_, NT_, CP_)                                          \
+        if (!launched && kk == KK_ && nt == NT_ && cp == CP_) {                 \
+            conv_h_kernel<KK_, NT_, CP_><<<grid, CM_NT, smem, st>>>(p);        \
+            launched = true;                                                   \
         }
+        CONV_H_FOR_ALL(CONV_H_LAUNCH)
 #undef CONV_H_LAUNCH
+        if (!launched) return cudaErrorInvalidConfiguration;
         return cudaGetLastError();
     }
 
