@@ -233,7 +233,9 @@ def test_learned_solve_counts_its_iteration_kernels():
     st = sol.dispersion_stats()
     n1 = sol.launch_count()
     assert st.iterations > 0
-    assert n1 - n0 > 30 * st.iterations  # every iteration is ~30 kernels of the device library
+    # every iteration is 22 kernels of the device library: four passes over the cells, three
+    # scalar kernels and the network's fifteen convolutions
+    assert n1 - n0 >= 22 * st.iterations
     assert math.isfinite(sol.time_device())
 
 

@@ -91,6 +91,7 @@ struct FcgScalars {
 
 struct Mapped {
     int k;        // linear index of the source cell
+    int i, j;     // its interior coordinates
     float sx, sy; // sign of the x- and y-normal vector components
 };
 
@@ -100,6 +101,8 @@ __device__ __forceinline__ Mapped map_cell(const DevGrid& g, int i, int j) {
     const int mi = reflect_idx(i, g.nx);
     const int mj = g.periodic ? wrap_idx(j, g.ny) : reflect_idx(j, g.ny);
     m.k = mj * g.pitch + mi;
+    m.i = mi;
+    m.j = mj;
     m.sx = ((unsigned)i < (unsigned)g.nx) ? 1.f : -1.f;
     m.sy = (g.periodic || (unsigned)j < (unsigned)g.ny) ? 1.f : -1.f;
     return m;

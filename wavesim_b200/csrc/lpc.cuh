@@ -271,6 +271,7 @@ struct ConvH {
     const unsigned short* gate; // co channels, NHWC, or null: y = act(conv + bias) * gate
     unsigned short* y;          // co channels, NHWC BF16 ...
     float* yf;                  // ... or FP32 (non-null: the network's output)
+    const int* done;            // or null: the solve this application serves has ended, skip it
     int co, H, W, N, act;
 };
 
@@ -324,6 +325,7 @@ __host__ __device__ inline size_t conv_h_smem2(int ci, int co, int kk) {
 // by the hardware conversion (round to nearest even, as bf16_bits).
 template <int KK, int NTL, int CP>
 __global__ void __launch_bounds__(CM_NT, 2) conv_h_kernel(ConvH p) {
+    if (p.done && *p.done) return;
     constexpr int RW = conv_h_rows(NTL), TH = 8 * RW;
     constexpr int R = KK == 9 ? 1 : 0, EW = CM_TX + 2 * R, EH = TH + 2 * R;
     constexpr int PS = CP + 8, KP = KK * CP, GROUPS = CP / 8, UNITS = EH * EW * GROUPS;
@@ -844,7 +846,7 @@ __global__ void fcg_matvec_kernel(DevGrid g, const float2* __restrict__ v, const
     }
 }
 
-// The Jacobi diagonal (dispersion.rs:441-457) and the warm start masked (:480-490).
+// The inverse of the Jacobi diagonal (dispersion.rs:441-457) and the warm start masked (:480-490).
 __global__ void fcg_setup_kernel(DevGrid g, const float* __restrict__ cc, const float* __restrict__ heff,
                                  float2* __restrict__ diag, float2* __restrict__ w) {
     const int n = g.nx * g.ny;
@@ -855,12 +857,12 @@ __global__ void fcg_setup_kernel(DevGrid g, const float* __restrict__ cc, const 
         float2 d = make_float2(1.f, 1.f);
         if (he >= H_DISP_MIN) {
             auto C = [&](int a, int b) { return cc[map_cell(g, a, b).k]; };
-            d.x = he + (C(i + 1, j) + C(i - 1, j)) * 0.25f / (g.dx * g.dx);
-            d.y = he + (C(i, j + 1) + C(i, j - 1)) * 0.25f / (g.dy * g.dy);
+            d.x = 1.f / (he + (C(i + 1, j) + C(i - 1, j)) * 0.25f / (g.dx * g.dx));
+            d.y = 1.f / (he + (C(i, j + 1) + C(i, j - 1)) * 0.25f / (g.dy * g.dy));
         } else {
             w[k] = make_float2(0.f, 0.f);
         }
-        diag[k] = d;
+        diag[k] = d;  // inverted: the passes multiply
     }
 }
 
@@ -938,38 +940,6 @@ __global__ void fcg_scalars_kernel(const double* part, int nblocks, FcgScalars* 
     if (cond && (step == FCG_INIT || step == FCG_RESID)) cudaGraphSetConditional(handle, sc->done ? 0u : 1u);
 }
 
-// w += alpha p, r -= alpha q
-__global__ void fcg_update_kernel(DevGrid g, float2* w, float2* r, const float2* p, const float2* q, const FcgScalars* sc) {
-    if (sc->done) return;
-    const float a = (float)sc->alpha;
-    const int n = g.nx * g.ny;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
-        const int k = (c / g.nx) * g.pitch + c % g.nx;
-        float2 ww = w[k], rr = r[k];
-        const float2 pp = p[k], qq = q[k];
-        ww.x += a * pp.x;
-        ww.y += a * pp.y;
-        rr.x -= a * qq.x;
-        rr.y -= a * qq.y;
-        w[k] = ww;
-        r[k] = rr;
-    }
-}
-
-// p = z + beta p (the first direction: p = z)
-__global__ void fcg_direction_kernel(DevGrid g, float2* p, const float2* z, const FcgScalars* sc) {
-    if (sc->done) return;
-    const bool first = sc->iterations == 0;
-    const float b = first ? 0.f : (float)sc->beta;
-    const int n = g.nx * g.ny;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
-        const int k = (c / g.nx) * g.pitch + c % g.nx;
-        const float2 zz = z[k];
-        const float2 pp = first ? make_float2(0.f, 0.f) : p[k];
-        p[k] = make_float2(zz.x + b * pp.x, zz.y + b * pp.y);
-    }
-}
-
 // r = b - t (the initial residual)
 __global__ void fcg_residual_kernel(DevGrid g, const float2* b, const float2* t, float2* r) {
     const int n = g.nx * g.ny;
@@ -980,38 +950,61 @@ __global__ void fcg_residual_kernel(DevGrid g, const float2* b, const float2* t,
     }
 }
 
-// Preconditioner pieces. Network tensors are 2 planes of Hp x Wp (the interior, zero-padded to a
-// multiple of 8).
-// z1 = omega r / diag
-__global__ void lpc_jacobi_kernel(DevGrid g, const float2* r, const float2* d, float2* z, float omega, const FcgScalars* sc) {
-    if (sc->done) return;
-    const int n = g.nx * g.ny;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
-        const int k = (c / g.nx) * g.pitch + c % g.nx;
-        const float2 rr = r[k], dd = d[k];
-        z[k] = make_float2(omega * rr.x / dd.x, omega * rr.y / dd.y);
-    }
+// ---- the iteration as four passes -------------------------------------------------------
+//
+// One flexible-CG iteration touches every cell four times instead of once per vector operation:
+//   pre   z1 = w r / D, and the network's input (r - A z1) / D        (A z1 from z1 of the stencil)
+//   post  z = z2 + w (r - A z2) / D with z2 = z1 + m y, and <z, q>     (A z2 likewise)
+//   dir   p = z + beta p, q = A p, <p, q>, <r, p>                       (p from the other bank)
+//   upd   w += alpha p, r -= alpha q, <r, r>
+// A vector at a stencil neighbour is recomputed from the inputs it is made of, so no pass waits
+// for another's output of the same iteration. Dot partials use the fixed partition of
+// fcg_dot_partial_kernel (grid-stride over cells, block_sum3), so runs are reproducible.
+
+// A v at interior cell (i, j) (dispersion.rs:269-317), v given at any padded position by V(a, b)
+// with its wall-normal components already sign-flipped.
+template <typename VF>
+__device__ __forceinline__ float2 apply_a(const DevGrid& g, int i, int j, const float* __restrict__ cc,
+                                          const float* __restrict__ heff, VF V) {
+    auto F = [&](int a, int b) {
+        const Mapped m = map_cell(g, a, b);
+        return cc[m.k] * ((V(a + 1, b).x - V(a - 1, b).x) * g.ix + (V(a, b + 1).y - V(a, b - 1).y) * g.iy);
+    };
+    const float he = heff[j * g.pitch + i];
+    const float mask = he >= H_DISP_MIN ? 1.f : 0.f;
+    const float2 own = V(i, j);
+    return make_float2(mask * (he * own.x - (F(i + 1, j) - F(i - 1, j)) * g.ix),
+                       mask * (he * own.y - (F(i, j + 1) - F(i, j - 1)) * g.iy));
 }
 
-// the network input: (r - t) / diag, as 2 planes of Hp x Wp (the S x S block means; zero
-// outside the interior), or with `xh` as one NHWC BF16 pair per pixel
-__global__ void lpc_input_kernel(DevGrid g, const float2* r, const float2* t, const float2* d, float* x, int Hp, int Wp,
-                                 int S, const FcgScalars* sc, unsigned* xh = nullptr) {
+// pre: per network pixel (S x S cells): z1 of its cells, and the block mean of (r - A z1) / D as
+// the network input (NHWC BF16 pairs in xh, else 2 planes in x); zero outside the interior. d
+// holds the inverse diagonal.
+__global__ void fcg_pre_kernel(DevGrid g, const float2* __restrict__ r, const float2* __restrict__ d,
+                               const float* __restrict__ cc, const float* __restrict__ heff, float2* __restrict__ z1,
+                               float omega, float* __restrict__ x, unsigned* __restrict__ xh, int Hp, int Wp, int S,
+                               const FcgScalars* __restrict__ sc) {
     if (sc->done) return;
     const size_t plane = (size_t)Hp * Wp;
     const float inv = 1.f / (float)(S * S);
+    auto Z = [&](int a, int b) {  // d holds the inverse diagonal
+        const Mapped m = map_cell(g, a, b);
+        const float2 rr = r[m.k], dd = d[m.k];
+        return make_float2(omega * rr.x * dd.x * m.sx, omega * rr.y * dd.y * m.sy);
+    };
     for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < plane; q += (size_t)gridDim.x * blockDim.x) {
         const int i0 = (int)(q % Wp) * S, j0 = (int)(q / Wp) * S;
         float vx = 0.f, vy = 0.f;
         for (int a = 0; a < S; a++)
             for (int b = 0; b < S; b++) {
                 const int i = i0 + b, j = j0 + a;
-                if (i < g.nx && j < g.ny) {
-                    const int k = j * g.pitch + i;
-                    const float2 rr = r[k], tt = t[k], dd = d[k];
-                    vx += (rr.x - tt.x) / dd.x;
-                    vy += (rr.y - tt.y) / dd.y;
-                }
+                if (i >= g.nx || j >= g.ny) continue;
+                const int k = j * g.pitch + i;
+                const float2 t = apply_a(g, i, j, cc, heff, Z);
+                const float2 rr = r[k], dd = d[k];
+                z1[k] = make_float2(omega * rr.x * dd.x, omega * rr.y * dd.y);
+                vx += (rr.x - t.x) * dd.x;
+                vy += (rr.y - t.y) * dd.y;
             }
         if (xh) {
             xh[q] = bf16_pack(vx * inv, vy * inv);
@@ -1022,33 +1015,103 @@ __global__ void lpc_input_kernel(DevGrid g, const float2* r, const float2* t, co
     }
 }
 
-// z2 = z1 + mask * y (network output planes, or with `nhwc` pairs per pixel, read at the
-// cell's block)
-__global__ void lpc_correct_kernel(DevGrid g, const float2* z1, const float* y, const float* heff, float2* z2, int Hp,
-                                   int Wp, int S, const FcgScalars* sc, int nhwc = 0) {
+// post: z = z2 + w (r - A z2) / D with z2 = z1 + m y (y: the network's output at the cell's
+// block of 2^lgS cells a side, NHWC pairs or planes); partial <z, q> for beta. d holds the
+// inverse diagonal.
+__global__ void fcg_post_kernel(DevGrid g, const float2* __restrict__ z1, const float* __restrict__ y, int nhwc,
+                                const float2* __restrict__ r, const float2* __restrict__ d, const float* __restrict__ cc,
+                                const float* __restrict__ heff, float2* __restrict__ z, const float2* __restrict__ qv,
+                                float omega, int Hp, int Wp, int lgS, double* __restrict__ part,
+                                const FcgScalars* __restrict__ sc) {
     if (sc->done) return;
     const size_t plane = (size_t)Hp * Wp;
+    auto Z2 = [&](int a, int b) {
+        const Mapped m = map_cell(g, a, b);
+        const int q = (m.j >> lgS) * Wp + (m.i >> lgS);
+        const float2 yv = nhwc ? reinterpret_cast<const float2*>(y)[q] : make_float2(y[q], y[plane + q]);
+        const float mk = heff[m.k] >= H_DISP_MIN ? 1.f : 0.f;
+        const float2 a1 = z1[m.k];
+        return make_float2((a1.x + mk * yv.x) * m.sx, (a1.y + mk * yv.y) * m.sy);
+    };
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
     const int n = g.nx * g.ny;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
-        const int i = c % g.nx, j = c / g.nx;
-        const int k = j * g.pitch + i;
-        const float m = heff[k] >= H_DISP_MIN ? 1.f : 0.f;
-        const size_t q = (size_t)(j / S) * Wp + i / S;
-        const float2 a = z1[k];
-        const float2 v = nhwc ? reinterpret_cast<const float2*>(y)[q] : make_float2(y[q], y[plane + q]);
-        z2[k] = make_float2(a.x + m * v.x, a.y + m * v.y);
+        const int i = c % g.nx, j = c / g.nx, k = j * g.pitch + i;
+        const float2 t = apply_a(g, i, j, cc, heff, Z2);
+        const float2 a2 = Z2(i, j), rr = r[k], dd = d[k];
+        const float2 zz = make_float2(a2.x + omega * (rr.x - t.x) * dd.x, a2.y + omega * (rr.y - t.y) * dd.y);
+        z[k] = zz;
+        const float2 qq = qv[k];
+        s0 += (double)zz.x * qq.x + (double)zz.y * qq.y;
+    }
+    __shared__ double red[100];
+    block_sum3<256>(s0, s1, s2, red);
+    if (threadIdx.x == 0) {
+        part[3 * blockIdx.x] = s0;
+        part[3 * blockIdx.x + 1] = 0.0;
+        part[3 * blockIdx.x + 2] = 0.0;
     }
 }
 
-// z = z2 + omega (r - t) / diag
-__global__ void lpc_post_kernel(DevGrid g, const float2* z2, const float2* r, const float2* t, const float2* d, float2* z,
-                                float omega, const FcgScalars* sc) {
+// dir: p = z + beta p_old (the first direction: p = z), q = A p; partials <p, q>, <r, p>.
+__global__ void fcg_dir_kernel(DevGrid g, const float2* __restrict__ z, const float2* __restrict__ p_old,
+                               float2* __restrict__ p_new, const float* __restrict__ cc, const float* __restrict__ heff,
+                               float2* __restrict__ qv, const float2* __restrict__ r, double* __restrict__ part,
+                               const FcgScalars* __restrict__ sc) {
     if (sc->done) return;
+    const bool first = sc->iterations == 0;
+    const float beta = first ? 0.f : (float)sc->beta;
+    auto P = [&](int a, int b) {
+        const Mapped m = map_cell(g, a, b);
+        const float2 zz = z[m.k];
+        const float2 pp = first ? make_float2(0.f, 0.f) : p_old[m.k];
+        return make_float2((zz.x + beta * pp.x) * m.sx, (zz.y + beta * pp.y) * m.sy);
+    };
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    const int n = g.nx * g.ny;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        const int i = c % g.nx, j = c / g.nx, k = j * g.pitch + i;
+        const float2 qq = apply_a(g, i, j, cc, heff, P);
+        const float2 pp = P(i, j), rr = r[k];
+        p_new[k] = pp;
+        qv[k] = qq;
+        s0 += (double)pp.x * qq.x + (double)pp.y * qq.y;
+        s1 += (double)rr.x * pp.x + (double)rr.y * pp.y;
+    }
+    __shared__ double red[100];
+    block_sum3<256>(s0, s1, s2, red);
+    if (threadIdx.x == 0) {
+        part[3 * blockIdx.x] = s0;
+        part[3 * blockIdx.x + 1] = s1;
+        part[3 * blockIdx.x + 2] = 0.0;
+    }
+}
+
+// upd: w += alpha p, r -= alpha q; partial <r, r>.
+__global__ void fcg_upd_kernel(DevGrid g, float2* __restrict__ w, float2* __restrict__ r, const float2* __restrict__ p,
+                               const float2* __restrict__ qv, double* __restrict__ part, const FcgScalars* __restrict__ sc) {
+    if (sc->done) return;
+    const float a = (float)sc->alpha;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
     const int n = g.nx * g.ny;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
         const int k = (c / g.nx) * g.pitch + c % g.nx;
-        const float2 a = z2[k], rr = r[k], tt = t[k], dd = d[k];
-        z[k] = make_float2(a.x + omega * (rr.x - tt.x) / dd.x, a.y + omega * (rr.y - tt.y) / dd.y);
+        float2 ww = w[k], rr = r[k];
+        const float2 pp = p[k], qq = qv[k];
+        ww.x += a * pp.x;
+        ww.y += a * pp.y;
+        rr.x -= a * qq.x;
+        rr.y -= a * qq.y;
+        w[k] = ww;
+        r[k] = rr;
+        s0 += (double)rr.x * rr.x + (double)rr.y * rr.y;
+    }
+    __shared__ double red[100];
+    block_sum3<256>(s0, s1, s2, red);
+    if (threadIdx.x == 0) {
+        part[3 * blockIdx.x] = s0;
+        part[3 * blockIdx.x + 1] = 0.0;
+        part[3 * blockIdx.x + 2] = 0.0;
     }
 }
 

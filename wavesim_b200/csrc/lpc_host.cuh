@@ -103,6 +103,7 @@ struct LpcNet {
     // Inference on NHWC BF16 activations (conv_h_kernel): every channel count a multiple of 8
     // and every layer's tile within the shared-memory limit; set by configure_nhwc.
     bool nhwc = false;
+    const int* done = nullptr;  // the flexible CG's end flag: applications after it are skipped
     DBuf Xh, Yh, Fh[LPC_LEVELS], HIDh[LPC_LEVELS], Gh[LPC_LEVELS], Ah[LPC_LEVELS], Eh[LPC_LEVELS],
         DAh[LPC_LEVELS], Dh[LPC_LEVELS];
 
@@ -342,6 +343,7 @@ struct LpcNet {
         p.gate = gate;
         p.y = y;
         p.yf = yf;
+        p.done = done;
         p.co = L.co;
         p.H = h_of(level);
         p.W = w_of(level);

@@ -420,39 +420,48 @@ wc_status fcg_pre(wc_solver* s, cudaStream_t st, cudaGraphConditionalHandle h, i
     return WC_OK;
 }
 
-// One iteration: z = M r, p = z + beta p, q = A p, alpha, w and r, the residual norm.
-wc_status fcg_body(wc_solver* s, cudaStream_t st, cudaGraphConditionalHandle h, int cond) {
+// the scalars kernel at `step`, over the partials the last pass left in fpart
+wc_status fcg_scalars(wc_solver* s, cudaStream_t st, int step, cudaGraphConditionalHandle h, int cond) {
+    FCG_LAUNCH(fcg_scalars_kernel<<<1, 256, 0, st>>>(s->fpart, fcg_blocks(s), s->fsc, step, s->disp.tolerance,
+                                                     (long long)s->disp.max_iterations, h, cond));
+    return WC_OK;
+}
+
+// One iteration in four passes over the cells (lpc.cuh): z = M r (pre, the network, post),
+// p = z + beta p and q = A p (dir), w and r (upd), with the scalars kernel after each dot.
+// Directions alternate between two banks by `parity`: dir reads the previous one at stencil
+// neighbours while it writes the new one.
+wc_status fcg_body(wc_solver* s, cudaStream_t st, cudaGraphConditionalHandle h, int cond, int parity) {
     const DevGrid& g = s->g;
     const int nb = fcg_blocks(s);
     FcgScalars* sc = s->fsc;
-    float2 *z = s->p1, *p = s->p0, *q = s->ap;
-    const int hp = s->lpc_hp, wp = s->lpc_wp;
+    float2 *z1 = s->tv, *z = s->p1, *q = s->ap;
+    float2* p_old = parity ? s->r2 : s->p0;
+    float2* p_new = parity ? s->p0 : s->r2;
+    const int hp = s->lpc_hp, wp = s->lpc_wp, S = s->lpc->stride;
     const size_t plane = (size_t)hp * wp;
+    const bool nhwc = s->lnet.nhwc;
     {
         ProfScope ps(s, 1);
-        FCG_LAUNCH(lpc_jacobi_kernel<<<nb, 256, 0, st>>>(g, s->r, s->diag, z, LPC_OMEGA, sc));
-        FCG_LAUNCH(fcg_matvec_kernel<<<nb, 256, 0, st>>>(g, z, s->cc, s->heff, s->tv, sc));
-        unsigned* xh = s->lnet.nhwc ? reinterpret_cast<unsigned*>(s->lnet.Xh.p) : nullptr;
-        FCG_LAUNCH(lpc_input_kernel<<<ew_grid(plane), 256, 0, st>>>(g, s->r, s->tv, s->diag, s->lnet.X[0].p, hp, wp,
-                                                                    s->lpc->stride, sc, xh));
+        unsigned* xh = nhwc ? reinterpret_cast<unsigned*>(s->lnet.Xh.p) : nullptr;
+        FCG_LAUNCH(fcg_pre_kernel<<<ew_grid(plane), 256, 0, st>>>(g, s->r, s->diag, s->cc, s->heff, z1, LPC_OMEGA,
+                                                                  s->lnet.X[0].p, xh, hp, wp, S, sc));
     }
     {
         ProfScope ps(s, 3);
-        CK(s->lnet.nhwc ? s->lnet.forward_h(st) : s->lnet.forward(st, false));
+        CK(nhwc ? s->lnet.forward_h(st) : s->lnet.forward(st, false));
         s->launches += 2 * LPC_LEVELS + 2 * (LPC_LEVELS - 1) + 1;
     }
     ProfScope ps(s, 1);
-    const float* y = s->lnet.nhwc ? s->lnet.Yh.p : s->lnet.Y.p;
-    FCG_LAUNCH(lpc_correct_kernel<<<nb, 256, 0, st>>>(g, z, y, s->heff, z, hp, wp, s->lpc->stride, sc,
-                                                      s->lnet.nhwc ? 1 : 0));
-    FCG_LAUNCH(fcg_matvec_kernel<<<nb, 256, 0, st>>>(g, z, s->cc, s->heff, s->tv, sc));
-    FCG_LAUNCH(lpc_post_kernel<<<nb, 256, 0, st>>>(g, z, s->r, s->tv, s->diag, z, LPC_OMEGA, sc));
-    TRY(fcg_dots(s, st, FCG_BETA, z, q, nullptr, nullptr, h, 0));
-    FCG_LAUNCH(fcg_direction_kernel<<<nb, 256, 0, st>>>(g, p, z, sc));
-    FCG_LAUNCH(fcg_matvec_kernel<<<nb, 256, 0, st>>>(g, p, s->cc, s->heff, q, sc));
-    TRY(fcg_dots(s, st, FCG_ALPHA, p, q, s->r, p, h, 0));
-    FCG_LAUNCH(fcg_update_kernel<<<nb, 256, 0, st>>>(g, s->w, s->r, p, q, sc));
-    TRY(fcg_dots(s, st, FCG_RESID, s->r, s->r, nullptr, nullptr, h, cond));
+    const float* y = nhwc ? s->lnet.Yh.p : s->lnet.Y.p;
+    const int lgS = S == 1 ? 0 : S == 2 ? 1 : S == 4 ? 2 : 3;
+    FCG_LAUNCH(fcg_post_kernel<<<nb, 256, 0, st>>>(g, z1, y, nhwc ? 1 : 0, s->r, s->diag, s->cc, s->heff, z, q,
+                                                   LPC_OMEGA, hp, wp, lgS, s->fpart, sc));
+    TRY(fcg_scalars(s, st, FCG_BETA, h, 0));
+    FCG_LAUNCH(fcg_dir_kernel<<<nb, 256, 0, st>>>(g, z, p_old, p_new, s->cc, s->heff, q, s->r, s->fpart, sc));
+    TRY(fcg_scalars(s, st, FCG_ALPHA, h, 0));
+    FCG_LAUNCH(fcg_upd_kernel<<<nb, 256, 0, st>>>(g, s->w, s->r, p_new, q, s->fpart, sc));
+    TRY(fcg_scalars(s, st, FCG_RESID, h, cond));
     return WC_OK;
 }
 
@@ -488,10 +497,13 @@ wc_status launch_fcg(wc_solver* s, int mode, const float4* qold, float4* qout) {
             cudaGraph_t body = np.conditional.phGraph_out[0];
             CK(cudaStreamBeginCaptureToGraph(s->body_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
             const unsigned long long before = s->launches;
-            const wc_status bs = fcg_body(s, s->body_stream, h, 1);
+            // two iterations per body, so that the direction banks alternate (the second returns
+            // at once when the first converged)
+            wc_status bs = fcg_body(s, s->body_stream, h, 1, 0);
+            if (bs == WC_OK) bs = fcg_body(s, s->body_stream, h, 1, 1);
             cudaGraph_t captured = nullptr;
             const cudaError_t e = cudaStreamEndCapture(s->body_stream, &captured);
-            s->fcg_body_launches = s->launches - before;
+            s->fcg_body_launches = (s->launches - before) / 2;
             s->launches = before;  // body launches are counted per executed iteration
             if (bs != WC_OK) return bs;
             CK(e);
@@ -502,7 +514,7 @@ wc_status launch_fcg(wc_solver* s, int mode, const float4* qold, float4* qout) {
             for (long long k = 0; k < max_it;) {
                 const long long chunk = std::min<long long>(4, max_it - k);
                 const unsigned long long before = s->launches;
-                for (long long c = 0; c < chunk; c++) TRY(fcg_body(s, st, 0, 0));
+                for (long long c = 0; c < chunk; c++) TRY(fcg_body(s, st, 0, 0, (int)((k + c) & 1)));
                 s->fcg_body_launches = (s->launches - before) / (unsigned long long)chunk;
                 s->launches = before;
                 k += chunk;
@@ -1903,6 +1915,7 @@ wc_status wc_solver_set_lpc(wc_solver* s, wc_lpc* l) {
         CK(cudaMallocHost(&s->done_host, sizeof(int)));
         CK(cudaStreamCreateWithFlags(&s->body_stream, cudaStreamNonBlocking));
     }
+    s->lnet.done = &s->fsc->done;
     // training and inference may run on different streams: the weights are final from here
     CK(cudaStreamSynchronize(l->m.st));
     s->lpc = &l->m;
