@@ -48,15 +48,33 @@ STAGE_BYTES_SWE = (36 + 52) / 2                 # stage 1 / stage 2 (RK average 
 
 # DRAM bytes per cell measured by ncu (one capture each; scaled to a launch by cells, and by
 # iterations for the solve): profiles/network_conv_2048x1024.md, profiles/pcg_kernel_sgn_2048x1024.md.
-NETWORK_DRAM_BYTES_PER_CELL = 1.0265e9 / (2048 * 1024)   # one application of the U-net
+NETWORK_DRAM_BYTES_PER_CELL = 448.2e6 / (2048 * 1024)    # one application of the U-net
 PCG_DRAM_BYTES_PER_CELL_ITER = 10.53e9 / (2048 * 1024 * 57)  # one iteration of the solve
 STAGE_DRAM_BYTES_PER_CELL_SWE = 573.1e6 / (4096 * 4096)      # one second-order stage
 # (profiles/stage_kernel_swe_4096x4096.md)
 
 
-def workload(name: str):
-    return {"config1": W.config1, "config2": W.config2, "config3": W.config3, "config5": W.config5,
-            "swe4096": W.swe_large}[name]()
+def workload(name: str, eddy: bool = False):
+    """The named workload; with `eddy`, its dispersive model follows breaking fronts with Kennedy's
+    eddy viscosity (Breaking::viscosity, crates/wavecore/src/eddy.rs)."""
+    w = {"config1": W.config1, "config2": W.config2, "config3": W.config3, "config5": W.config5,
+         "swe4096": W.swe_large}[name]()
+    if eddy:
+        if w.dispersion is None:
+            raise SystemExit("--eddy needs a dispersive workload: followed fronts exist only with dispersion")
+        from dataclasses import replace
+
+        from wavesim_b200 import EddyViscosity
+        w.dispersion = replace(w.dispersion, breaking=replace(w.dispersion.breaking, viscosity=EddyViscosity()))
+        w.meta["followed_fronts"] = "Kennedy eddy viscosity (EddyViscosity::default)"
+    return w
+
+# Algorithmic bytes per cell of the eddy kernel: follow reads the state (16), bed (4) and memory
+# (8) and writes the new memory (8), nu (4) and the momentum bank (8); each viscous sub-step reads
+# the depth (8), nu (4) and a bank (8) and writes a bank or the momentum (8); the finish moves
+# the memory (16).
+EDDY_BYTES = 48 + 16
+EDDY_SUBSTEP_BYTES = 28
 
 
 def run_ensemble(args, world, rank, local):
@@ -218,7 +236,7 @@ def run_reference(args, world, rank):
         return
     from oracle.oracle import OracleSolver, set_threads
 
-    w = workload(args.workload)
+    w = workload(args.workload, args.eddy)
     threads = set_threads(0)
     sol = w.solver(OracleSolver)
     s = W.wave_train_state(w)
@@ -388,7 +406,7 @@ def run_b200(args, world, rank, local):
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
-    w = workload(args.workload)
+    w = workload(args.workload, args.eddy)
     stream = torch.cuda.Stream()  # a real stream handle: the solvers and the events share it
     torch.cuda.set_stream(stream)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
@@ -422,17 +440,22 @@ def run_b200(args, world, rank, local):
         peak, peak_kind = measured_peaks()
         iters_prof = arm["iterations_per_solve_profiled"]
         if learned and net_ms >= max(solve_ms, stage_ms):
+            # One network application: 18 kFLOP and 325 B per cell of its finest level, 56 FLOP/B,
+            # below the B200's ridge point (about 220 FLOP/B), so its roof is HBM bandwidth.
             spec = net.spec
-            flops = spec.flops_per_cell() / spec.stride**2 * w.grid.nx * w.grid.ny
-            tflops = flops / (net_ms / net_n / 1e3) / 1e12
-            roof = {"bound": "tensor", "kernel": "conv_mma_kernel chain (one network application: BF16 mma.sync "
-                                                  "implicit-GEMM convolutions, FP32 accumulation)",
-                    "achieved": tflops, "unit": "TFLOP/s", "flops_per_cell": spec.flops_per_cell() / spec.stride**2,
-                    "avg_ms": net_ms / net_n,
-                    "traffic": NETWORK_DRAM_BYTES_PER_CELL * w.grid.nx * w.grid.ny / spec.stride**2,
-                    "traffic_source": "ncu DRAM bytes of one application at 2048x1024, scaled by cells"}
+            ncell = w.grid.nx * w.grid.ny / spec.stride**2
+            avg_ms = net_ms / net_n
+            tflops = spec.flops_per_cell() * ncell / (avg_ms / 1e3) / 1e12
+            gbs = spec.bytes_per_cell() * ncell / (avg_ms / 1e3) / 1e9
             bf16 = peak_tensor()
-            roof.update({"peak": bf16[0], "frac": tflops / bf16[0], "peak_source": bf16[1]})
+            roof = {"bound": "hbm", "kernel": "conv_h_kernel chain (one network application: channels-innermost BF16 "
+                                              "mma.sync implicit-GEMM convolutions, FP32 accumulation)",
+                    "achieved": gbs, "unit": "GB/s", "peak": peak, "frac": gbs / peak, "peak_source": peak_kind,
+                    "algorithmic_bytes_per_cell": spec.bytes_per_cell(), "flops_per_cell": spec.flops_per_cell(),
+                    "avg_ms": avg_ms, "tensor_tflops": tflops, "tensor_frac": tflops / bf16[0],
+                    "tensor_peak_source": bf16[1],
+                    "traffic": NETWORK_DRAM_BYTES_PER_CELL * ncell,
+                    "traffic_source": "ncu DRAM bytes of one application at 2048x1024, scaled by cells"}
         else:
             if solve_n and solve_ms >= stage_ms:
                 per_cell = SOLVE_INIT_BYTES + SOLVE_ITER_BYTES * iters_prof + SOLVE_FINISH_BYTES
@@ -483,12 +506,21 @@ def run_b200(args, world, rank, local):
             "roofline": roof,
             "kernel_ms_per_step": {"stage": stage_ms / args.steps, "solve": solve_ms / args.steps,
                                    "network": net_ms / args.steps, "other": prof["other"][1] / args.steps,
+                                   "eddy": prof.get("eddy", (0, 0.0))[1] / args.steps,
                                    "source": "profiled pass of the same number of steps after the timed pass "
                                              "(direct launches; the learned solve syncs with the host every 4 iterations there)"},
             "e2e": arm["e2e"],
             "gpu_launches": arm["launches"],
             "clocks": arm["clocks"],
         }
+        if args.eddy and prof.get("eddy", (0, 0.0))[0]:
+            en, ems = prof["eddy"]
+            total = sum(v[1] for v in prof.values())
+            per = EDDY_BYTES + EDDY_SUBSTEP_BYTES  # at least one viscous sub-step when a front breaks
+            line["eddy_kernel"] = {"kernel": "eddy_kernel (fronts, viscosity sub-steps, finish; cooperative)",
+                                   "launches": en, "avg_ms": ems / en, "share_of_kernel_time": ems / total,
+                                   "bytes_per_cell_one_substep": per,
+                                   "achieved_gbs_one_substep": per * cells / (ems / en / 1e3) / 1e9, "peak": peak}
         if learned:
             line["plain_pcg"] = {
                 "value": plain["value"], "ms_per_step": plain["ms_per_step"],
@@ -526,6 +558,8 @@ def main():
     ap.add_argument("--eta-steps", type=int, default=10)
     ap.add_argument("--cpu-steps", type=int, default=40)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--eddy", action="store_true",
+                    help="follow breaking fronts with Kennedy's eddy viscosity (dispersive workloads)")
     ap.add_argument("--direct", action="store_true",
                     help="launch every kernel directly, no step graph (for profilers: a graph with a "
                          "conditional node hides its kernels from ncu)")

@@ -92,6 +92,25 @@ class UNetSpec:
             f += 2.0 * co * ci * k * k / (4.0 ** level)
         return f
 
+    def bytes_per_cell(self) -> float:
+        """Algorithmic DRAM bytes of one application per cell of the finest level, for the
+        device's channels-innermost BF16 activations: every convolution reads each of its inputs
+        and its gate once and writes its output once (a pooled input is read at the finer level,
+        an upsampled one at the coarser); the input is 2 BF16 channels, the output 2 FP32."""
+        c, L, b = self.channels, self.levels, 2.0
+        per = [0.0] * L  # bytes per pixel of level l
+        for l in range(L):
+            cin = self.in_ch if l == 0 else c[l - 1]
+            src = b * cin * (4.0 if l > 0 else 1.0)  # enc_a reads its input (pooled: 4 finer pixels)
+            per[l] += src + b * c[l]                 # ... and writes A
+            per[l] += 3 * b * c[l]                   # enc_b: A and the gate in, E out
+        for l in range(L - 2, -1, -1):
+            below = b * c[l + 1] / 4.0               # the upsampled map, read once at its level
+            per[l] += below + b * c[l] + b * c[l]    # dec_a: up(below), E in, DA out
+            per[l] += 3 * b * c[l]                   # dec_b: DA and the gate in, D out
+        per[0] += b * c[0] + 4.0 * self.out_ch       # out: D in, FP32 output
+        return sum(v / 4.0 ** l for l, v in enumerate(per))
+
 
 def init_params(spec: UNetSpec, seed: int = 0) -> np.ndarray:
     """Scaled normal weights, zero biases, a zero output layer (the network starts at zero)."""
