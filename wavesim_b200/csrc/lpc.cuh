@@ -1015,37 +1015,116 @@ __global__ void fcg_pre_kernel(DevGrid g, const float2* __restrict__ r, const fl
     }
 }
 
-// post: z = z2 + w (r - A z2) / D with z2 = z1 + m y (y: the network's output at the cell's
-// block of 2^lgS cells a side, NHWC pairs or planes); partial <z, q> for beta. d holds the
-// inverse diagonal.
-__global__ void fcg_post_kernel(DevGrid g, const float2* __restrict__ z1, const float* __restrict__ y, int nhwc,
-                                const float2* __restrict__ r, const float2* __restrict__ d, const float* __restrict__ cc,
-                                const float* __restrict__ heff, float2* __restrict__ z, const float2* __restrict__ qv,
-                                float omega, int Hp, int Wp, int lgS, double* __restrict__ part,
-                                const FcgScalars* __restrict__ sc) {
-    if (sc->done) return;
-    const size_t plane = (size_t)Hp * Wp;
-    auto Z2 = [&](int a, int b) {
-        const Mapped m = map_cell(g, a, b);
-        const int q = (m.j >> lgS) * Wp + (m.i >> lgS);
-        const float2 yv = nhwc ? reinterpret_cast<const float2*>(y)[q] : make_float2(y[q], y[plane + q]);
-        const float mk = heff[m.k] >= H_DISP_MIN ? 1.f : 0.f;
-        const float2 a1 = z1[m.k];
-        return make_float2((a1.x + mk * yv.x) * m.sx, (a1.y + mk * yv.y) * m.sy);
+// The same passes on 32 x 8-cell tiles through shared memory: the derived vector is formed once
+// per cell of the tile's box (halo 2, wall-normal signs applied), c once per cell of its halo-1
+// box, and A v of every own cell read from there. A block walks tiles b, b + nb, ... (a fixed
+// partition, so the dots stay reproducible).
+constexpr int FT_X = 32, FT_Y = 8, FT_NT = FT_X * FT_Y;
+constexpr int FB_W = FT_X + 4, FB_H = FT_Y + 4, FB_N = FB_W * FB_H;
+constexpr int FC_W = FT_X + 2, FC_H = FT_Y + 2, FC_N = FC_W * FC_H;
+
+struct FcgTile {
+    float2 v[FB_N];
+    float c[FC_N];
+};
+
+// box of VF(mapped cell) (the unsigned vector there) and of c; ends with a barrier
+template <typename VF>
+__device__ __forceinline__ void fcg_tile_stage(const DevGrid& g, int i0, int j0, const float* __restrict__ cc,
+                                               FcgTile& sm, VF vf) {
+    __syncthreads();  // the previous tile's box is read
+    for (int q = threadIdx.x; q < FB_N; q += FT_NT) {
+        const Mapped m = map_cell(g, i0 - 2 + q % FB_W, j0 - 2 + q / FB_W);
+        const float2 v = vf(m);
+        sm.v[q] = make_float2(v.x * m.sx, v.y * m.sy);
+    }
+    for (int q = threadIdx.x; q < FC_N; q += FT_NT) sm.c[q] = cc[map_cell(g, i0 - 1 + q % FC_W, j0 - 1 + q / FC_W).k];
+    __syncthreads();
+}
+
+// A v at the own cell (tx, ty) of the staged tile (apply_a's arithmetic)
+__device__ __forceinline__ float2 fcg_tile_apply(const DevGrid& g, const FcgTile& sm, int tx, int ty, float he) {
+    auto V = [&](int a, int b) { return sm.v[(ty + 2 + b) * FB_W + tx + 2 + a]; };
+    auto F = [&](int a, int b) {
+        return sm.c[(ty + 1 + b) * FC_W + tx + 1 + a] *
+               ((V(a + 1, b).x - V(a - 1, b).x) * g.ix + (V(a, b + 1).y - V(a, b - 1).y) * g.iy);
     };
+    const float mask = he >= H_DISP_MIN ? 1.f : 0.f;
+    const float2 own = V(0, 0);
+    return make_float2(mask * (he * own.x - (F(1, 0) - F(-1, 0)) * g.ix), mask * (he * own.y - (F(0, 1) - F(0, -1)) * g.iy));
+}
+
+// pre on tiles, network on the solver's grid (stride 1): z1 and (r - A z1) / D as the input
+__global__ void __launch_bounds__(FT_NT) fcg_pre_tile_kernel(DevGrid g, const float2* __restrict__ r,
+                                                             const float2* __restrict__ d, const float* __restrict__ cc,
+                                                             const float* __restrict__ heff, float2* __restrict__ z1,
+                                                             float omega, float* __restrict__ x,
+                                                             unsigned* __restrict__ xh, int Hp, int Wp,
+                                                             const FcgScalars* __restrict__ sc) {
+    if (sc->done) return;
+    __shared__ FcgTile sm;
+    const int tx = threadIdx.x % FT_X, ty = threadIdx.x / FT_X;
+    const int ntx = (g.nx + FT_X - 1) / FT_X, ntiles = ntx * ((g.ny + FT_Y - 1) / FT_Y);
+    const size_t plane = (size_t)Hp * Wp;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int i0 = (t % ntx) * FT_X, j0 = (t / ntx) * FT_Y;
+        fcg_tile_stage(g, i0, j0, cc, sm, [&](const Mapped& m) {
+            const float2 rr = r[m.k], dd = d[m.k];
+            return make_float2(omega * rr.x * dd.x, omega * rr.y * dd.y);
+        });
+        const int i = i0 + tx, j = j0 + ty;
+        if (i >= g.nx || j >= g.ny) continue;
+        const int k = j * g.pitch + i;
+        const float2 tv = fcg_tile_apply(g, sm, tx, ty, heff[k]);
+        const float2 rr = r[k], dd = d[k];
+        z1[k] = make_float2(omega * rr.x * dd.x, omega * rr.y * dd.y);
+        const float vx = (rr.x - tv.x) * dd.x, vy = (rr.y - tv.y) * dd.y;
+        const size_t q = (size_t)j * Wp + i;
+        if (xh) {
+            xh[q] = bf16_pack(vx, vy);
+        } else {
+            x[q] = vx;
+            x[plane + q] = vy;
+        }
+    }
+}
+
+// post on tiles: z = z2 + w (r - A z2) / D, z2 = z1 + m y; partial <z, q>
+__global__ void __launch_bounds__(FT_NT) fcg_post_tile_kernel(DevGrid g, const float2* __restrict__ z1,
+                                                              const float* __restrict__ y, int nhwc,
+                                                              const float2* __restrict__ r, const float2* __restrict__ d,
+                                                              const float* __restrict__ cc, const float* __restrict__ heff,
+                                                              float2* __restrict__ z, const float2* __restrict__ qv,
+                                                              float omega, int Hp, int Wp, int lgS,
+                                                              double* __restrict__ part,
+                                                              const FcgScalars* __restrict__ sc) {
+    if (sc->done) return;
+    __shared__ FcgTile sm;
+    const int tx = threadIdx.x % FT_X, ty = threadIdx.x / FT_X;
+    const int ntx = (g.nx + FT_X - 1) / FT_X, ntiles = ntx * ((g.ny + FT_Y - 1) / FT_Y);
+    const size_t plane = (size_t)Hp * Wp;
     double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-    const int n = g.nx * g.ny;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
-        const int i = c % g.nx, j = c / g.nx, k = j * g.pitch + i;
-        const float2 t = apply_a(g, i, j, cc, heff, Z2);
-        const float2 a2 = Z2(i, j), rr = r[k], dd = d[k];
-        const float2 zz = make_float2(a2.x + omega * (rr.x - t.x) * dd.x, a2.y + omega * (rr.y - t.y) * dd.y);
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int i0 = (t % ntx) * FT_X, j0 = (t / ntx) * FT_Y;
+        fcg_tile_stage(g, i0, j0, cc, sm, [&](const Mapped& m) {
+            const int q = (m.j >> lgS) * Wp + (m.i >> lgS);
+            const float2 yv = nhwc ? reinterpret_cast<const float2*>(y)[q] : make_float2(y[q], y[plane + q]);
+            const float mk = heff[m.k] >= H_DISP_MIN ? 1.f : 0.f;
+            const float2 a1 = z1[m.k];
+            return make_float2(a1.x + mk * yv.x, a1.y + mk * yv.y);
+        });
+        const int i = i0 + tx, j = j0 + ty;
+        if (i >= g.nx || j >= g.ny) continue;
+        const int k = j * g.pitch + i;
+        const float2 tv = fcg_tile_apply(g, sm, tx, ty, heff[k]);
+        const float2 a2 = sm.v[(ty + 2) * FB_W + tx + 2], rr = r[k], dd = d[k];
+        const float2 zz = make_float2(a2.x + omega * (rr.x - tv.x) * dd.x, a2.y + omega * (rr.y - tv.y) * dd.y);
         z[k] = zz;
         const float2 qq = qv[k];
         s0 += (double)zz.x * qq.x + (double)zz.y * qq.y;
     }
     __shared__ double red[100];
-    block_sum3<256>(s0, s1, s2, red);
+    block_sum3<FT_NT>(s0, s1, s2, red);
     if (threadIdx.x == 0) {
         part[3 * blockIdx.x] = s0;
         part[3 * blockIdx.x + 1] = 0.0;
@@ -1053,33 +1132,39 @@ __global__ void fcg_post_kernel(DevGrid g, const float2* __restrict__ z1, const 
     }
 }
 
-// dir: p = z + beta p_old (the first direction: p = z), q = A p; partials <p, q>, <r, p>.
-__global__ void fcg_dir_kernel(DevGrid g, const float2* __restrict__ z, const float2* __restrict__ p_old,
-                               float2* __restrict__ p_new, const float* __restrict__ cc, const float* __restrict__ heff,
-                               float2* __restrict__ qv, const float2* __restrict__ r, double* __restrict__ part,
-                               const FcgScalars* __restrict__ sc) {
+// dir on tiles: p = z + beta p_old (first: p = z), q = A p; partials <p, q>, <r, p>
+__global__ void __launch_bounds__(FT_NT) fcg_dir_tile_kernel(DevGrid g, const float2* __restrict__ z,
+                                                             const float2* __restrict__ p_old,
+                                                             float2* __restrict__ p_new, const float* __restrict__ cc,
+                                                             const float* __restrict__ heff, float2* __restrict__ qv,
+                                                             const float2* __restrict__ r, double* __restrict__ part,
+                                                             const FcgScalars* __restrict__ sc) {
     if (sc->done) return;
+    __shared__ FcgTile sm;
     const bool first = sc->iterations == 0;
     const float beta = first ? 0.f : (float)sc->beta;
-    auto P = [&](int a, int b) {
-        const Mapped m = map_cell(g, a, b);
-        const float2 zz = z[m.k];
-        const float2 pp = first ? make_float2(0.f, 0.f) : p_old[m.k];
-        return make_float2((zz.x + beta * pp.x) * m.sx, (zz.y + beta * pp.y) * m.sy);
-    };
+    const int tx = threadIdx.x % FT_X, ty = threadIdx.x / FT_X;
+    const int ntx = (g.nx + FT_X - 1) / FT_X, ntiles = ntx * ((g.ny + FT_Y - 1) / FT_Y);
     double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-    const int n = g.nx * g.ny;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
-        const int i = c % g.nx, j = c / g.nx, k = j * g.pitch + i;
-        const float2 qq = apply_a(g, i, j, cc, heff, P);
-        const float2 pp = P(i, j), rr = r[k];
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int i0 = (t % ntx) * FT_X, j0 = (t / ntx) * FT_Y;
+        fcg_tile_stage(g, i0, j0, cc, sm, [&](const Mapped& m) {
+            const float2 zz = z[m.k];
+            const float2 pp = first ? make_float2(0.f, 0.f) : p_old[m.k];
+            return make_float2(zz.x + beta * pp.x, zz.y + beta * pp.y);
+        });
+        const int i = i0 + tx, j = j0 + ty;
+        if (i >= g.nx || j >= g.ny) continue;
+        const int k = j * g.pitch + i;
+        const float2 qq = fcg_tile_apply(g, sm, tx, ty, heff[k]);
+        const float2 pp = sm.v[(ty + 2) * FB_W + tx + 2], rr = r[k];
         p_new[k] = pp;
         qv[k] = qq;
         s0 += (double)pp.x * qq.x + (double)pp.y * qq.y;
         s1 += (double)rr.x * pp.x + (double)rr.y * pp.y;
     }
     __shared__ double red[100];
-    block_sum3<256>(s0, s1, s2, red);
+    block_sum3<FT_NT>(s0, s1, s2, red);
     if (threadIdx.x == 0) {
         part[3 * blockIdx.x] = s0;
         part[3 * blockIdx.x + 1] = s1;

@@ -420,11 +420,17 @@ wc_status fcg_pre(wc_solver* s, cudaStream_t st, cudaGraphConditionalHandle h, i
     return WC_OK;
 }
 
-// the scalars kernel at `step`, over the partials the last pass left in fpart
-wc_status fcg_scalars(wc_solver* s, cudaStream_t st, int step, cudaGraphConditionalHandle h, int cond) {
-    FCG_LAUNCH(fcg_scalars_kernel<<<1, 256, 0, st>>>(s->fpart, fcg_blocks(s), s->fsc, step, s->disp.tolerance,
+// the scalars kernel at `step`, over the partials of the `nblocks` blocks of the last pass
+wc_status fcg_scalars(wc_solver* s, cudaStream_t st, int step, int nblocks, cudaGraphConditionalHandle h, int cond) {
+    FCG_LAUNCH(fcg_scalars_kernel<<<1, 256, 0, st>>>(s->fpart, nblocks, s->fsc, step, s->disp.tolerance,
                                                      (long long)s->disp.max_iterations, h, cond));
     return WC_OK;
+}
+
+// blocks of the tiled passes: every tile of 32 x 8 cells once, at most FCG_BLOCKS blocks
+int fcg_tile_blocks(const wc_solver* s) {
+    const long long tiles = (long long)((s->grid.nx + FT_X - 1) / FT_X) * (long long)((s->grid.ny + FT_Y - 1) / FT_Y);
+    return (int)std::max<long long>(1, std::min<long long>(FCG_BLOCKS, tiles));
 }
 
 // One iteration in four passes over the cells (lpc.cuh): z = M r (pre, the network, post),
@@ -433,7 +439,7 @@ wc_status fcg_scalars(wc_solver* s, cudaStream_t st, int step, cudaGraphConditio
 // neighbours while it writes the new one.
 wc_status fcg_body(wc_solver* s, cudaStream_t st, cudaGraphConditionalHandle h, int cond, int parity) {
     const DevGrid& g = s->g;
-    const int nb = fcg_blocks(s);
+    const int nb = fcg_blocks(s), nt = fcg_tile_blocks(s);
     FcgScalars* sc = s->fsc;
     float2 *z1 = s->tv, *z = s->p1, *q = s->ap;
     float2* p_old = parity ? s->r2 : s->p0;
@@ -444,8 +450,12 @@ wc_status fcg_body(wc_solver* s, cudaStream_t st, cudaGraphConditionalHandle h, 
     {
         ProfScope ps(s, 1);
         unsigned* xh = nhwc ? reinterpret_cast<unsigned*>(s->lnet.Xh.p) : nullptr;
-        FCG_LAUNCH(fcg_pre_kernel<<<ew_grid(plane), 256, 0, st>>>(g, s->r, s->diag, s->cc, s->heff, z1, LPC_OMEGA,
-                                                                  s->lnet.X[0].p, xh, hp, wp, S, sc));
+        if (S == 1)
+            FCG_LAUNCH(fcg_pre_tile_kernel<<<nt, FT_NT, 0, st>>>(g, s->r, s->diag, s->cc, s->heff, z1, LPC_OMEGA,
+                                                                 s->lnet.X[0].p, xh, hp, wp, sc));
+        else
+            FCG_LAUNCH(fcg_pre_kernel<<<ew_grid(plane), 256, 0, st>>>(g, s->r, s->diag, s->cc, s->heff, z1, LPC_OMEGA,
+                                                                      s->lnet.X[0].p, xh, hp, wp, S, sc));
     }
     {
         ProfScope ps(s, 3);
@@ -455,13 +465,13 @@ wc_status fcg_body(wc_solver* s, cudaStream_t st, cudaGraphConditionalHandle h, 
     ProfScope ps(s, 1);
     const float* y = nhwc ? s->lnet.Yh.p : s->lnet.Y.p;
     const int lgS = S == 1 ? 0 : S == 2 ? 1 : S == 4 ? 2 : 3;
-    FCG_LAUNCH(fcg_post_kernel<<<nb, 256, 0, st>>>(g, z1, y, nhwc ? 1 : 0, s->r, s->diag, s->cc, s->heff, z, q,
-                                                   LPC_OMEGA, hp, wp, lgS, s->fpart, sc));
-    TRY(fcg_scalars(s, st, FCG_BETA, h, 0));
-    FCG_LAUNCH(fcg_dir_kernel<<<nb, 256, 0, st>>>(g, z, p_old, p_new, s->cc, s->heff, q, s->r, s->fpart, sc));
-    TRY(fcg_scalars(s, st, FCG_ALPHA, h, 0));
+    FCG_LAUNCH(fcg_post_tile_kernel<<<nt, FT_NT, 0, st>>>(g, z1, y, nhwc ? 1 : 0, s->r, s->diag, s->cc, s->heff, z, q,
+                                                          LPC_OMEGA, hp, wp, lgS, s->fpart, sc));
+    TRY(fcg_scalars(s, st, FCG_BETA, nt, h, 0));
+    FCG_LAUNCH(fcg_dir_tile_kernel<<<nt, FT_NT, 0, st>>>(g, z, p_old, p_new, s->cc, s->heff, q, s->r, s->fpart, sc));
+    TRY(fcg_scalars(s, st, FCG_ALPHA, nt, h, 0));
     FCG_LAUNCH(fcg_upd_kernel<<<nb, 256, 0, st>>>(g, s->w, s->r, p_new, q, s->fpart, sc));
-    TRY(fcg_scalars(s, st, FCG_RESID, h, cond));
+    TRY(fcg_scalars(s, st, FCG_RESID, nb, h, cond));
     return WC_OK;
 }
 
