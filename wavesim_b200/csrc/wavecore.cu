@@ -376,6 +376,7 @@ wc_status launch_pcg(wc_solver* s, int mode, const float4* qold, float4* qout, c
 // residual kernel sets, so the loop runs on the device without the host.
 
 constexpr int FCG_BLOCKS = 148 * 4;
+constexpr int FCG_TILE_BLOCKS = 148 * 8;  // the tiled passes: 32 registers, 5.6 KB shared: 8 blocks per SM
 
 int fcg_blocks(const wc_solver* s) {
     const size_t n = (size_t)s->grid.nx * s->grid.ny;
@@ -427,10 +428,10 @@ wc_status fcg_scalars(wc_solver* s, cudaStream_t st, int step, int nblocks, cuda
     return WC_OK;
 }
 
-// blocks of the tiled passes: every tile of 32 x 8 cells once, at most FCG_BLOCKS blocks
+// blocks of the tiled passes: every tile of 32 x 8 cells once, at most FCG_TILE_BLOCKS blocks
 int fcg_tile_blocks(const wc_solver* s) {
     const long long tiles = (long long)((s->grid.nx + FT_X - 1) / FT_X) * (long long)((s->grid.ny + FT_Y - 1) / FT_Y);
-    return (int)std::max<long long>(1, std::min<long long>(FCG_BLOCKS, tiles));
+    return (int)std::max<long long>(1, std::min<long long>(FCG_TILE_BLOCKS, tiles));
 }
 
 // One iteration in four passes over the cells (lpc.cuh): z = M r (pre, the network, post),
@@ -1921,7 +1922,7 @@ wc_status wc_solver_set_lpc(wc_solver* s, wc_lpc* l) {
         CK(cudaMalloc(&s->fsc, sizeof(FcgScalars)));
         CK(cudaMemset(s->fsc, 0, sizeof(FcgScalars)));
         CK(cudaStreamSynchronize(0));
-        CK(cudaMalloc(&s->fpart, 3 * FCG_BLOCKS * sizeof(double)));
+        CK(cudaMalloc(&s->fpart, 3 * std::max(FCG_BLOCKS, FCG_TILE_BLOCKS) * sizeof(double)));
         CK(cudaMallocHost(&s->done_host, sizeof(int)));
         CK(cudaStreamCreateWithFlags(&s->body_stream, cudaStreamNonBlocking));
     }
