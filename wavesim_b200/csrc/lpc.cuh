@@ -310,12 +310,13 @@ __device__ __forceinline__ void ldmatrix_x4(unsigned* r, const void* row) {
 // work per pixel), two rows where the output has four or more tiles of 8 channels.
 __host__ __device__ constexpr int conv_h_rows(int ntl) { return ntl <= 2 ? 4 : 2; }
 
-// Shared memory of the channels-innermost convolution (bytes): the input box, the weights.
-__host__ __device__ inline size_t conv_h_smem2(int ci, int co, int kk) {
+// Shared memory of the channels-innermost convolution (bytes): the input box, the weights and,
+// for a gated layer, the gate tile ([pixel][co]).
+__host__ __device__ inline size_t conv_h_smem2(int ci, int co, int kk, bool gated) {
     const int r = kk == 9 ? 1 : 0, cp = conv_mma_cp(ci), ntl = (co + 7) / 8;
     const int th = 8 * conv_h_rows(ntl);
     const size_t box = (size_t)(th + 2 * r) * (CM_TX + 2 * r) * conv_h_ps(cp);
-    return (box + (size_t)ntl * 8 * kk * cp) * 2;
+    return (box + (size_t)ntl * 8 * kk * cp + (gated ? (size_t)th * CM_TX * ntl * 8 : 0)) * 2;
 }
 
 // KK taps (9 or 1), NTL tiles of 8 output channels, CP input channels padded to 16: all index
@@ -333,6 +334,7 @@ __global__ void __launch_bounds__(CM_NT, 2) conv_h_kernel(ConvH p) {
     extern __shared__ __align__(16) unsigned short cm_smem[];
     unsigned short* in_s = cm_smem;             // [EH][EW][PS]
     unsigned short* w_s = cm_smem + EH * EW * PS;  // [8 NTL][KP]
+    unsigned short* g_s = w_s + 8 * NTL * KP;      // gated layers: [TH][16][co]
     const int ci_total = p.ca + p.cb;
     const int n = blockIdx.z;
     const int x0 = blockIdx.x * CM_TX, y0 = blockIdx.y * TH;
@@ -341,6 +343,15 @@ __global__ void __launch_bounds__(CM_NT, 2) conv_h_kernel(ConvH p) {
         const uint4* src = reinterpret_cast<const uint4*>(p.wre);
         uint4* dst = reinterpret_cast<uint4*>(w_s);
         for (int q = threadIdx.x; q < NTL * KP; q += CM_NT) cp_async16(dst + q, src + q, 16);
+    }
+    if (p.gate) {  // the tile's gate, in flight with the input box
+        const int gg = p.co / 8;
+        for (int q = threadIdx.x; q < TH * CM_TX * gg; q += CM_NT) {
+            const int pix = q / gg, c0 = (q - pix * gg) * 8;
+            const int y = y0 + pix / CM_TX, x = x0 + pix % CM_TX;
+            const bool in = y < p.H && x < p.W;
+            cp_async16(g_s + pix * p.co + c0, in ? p.gate + ((n * p.H + y) * p.W + x) * p.co + c0 : p.gate, in ? 16 : 0);
+        }
     }
     const int Hs = p.amode == CM_POOL ? 2 * p.H : p.amode == CM_UP ? p.H / 2 : p.H;  // a's map
     const int Ws = p.amode == CM_POOL ? 2 * p.W : p.amode == CM_UP ? p.W / 2 : p.W;
@@ -448,7 +459,8 @@ __global__ void __launch_bounds__(CM_NT, 2) conv_h_kernel(ConvH p) {
                     v1 = 2.f / (1.f + expf(-v1));
                 }
                 if (p.gate) {
-                    const unsigned gw = __ldg(reinterpret_cast<const unsigned*>(p.gate + pix + co));
+                    const int lp = (warp * RW + r) * CM_TX + grp + 8 * half;
+                    const unsigned gw = *reinterpret_cast<const unsigned*>(g_s + lp * p.co + co);
                     v0 *= bf16_lo(gw);
                     v1 *= bf16_hi(gw);
                 }

@@ -196,7 +196,7 @@ struct LpcNet {
         for (auto* L : {&enc_a, &enc_b, &dec_a, &dec_b, &gate_a, &gate_b})
             for (auto& l : *L)
                 if (l.co > 0 && (conv_mma_cp(l.ci) > CONV_H_CP_MAX ||
-                                 conv_h_smem2(l.ci, 8 * mma_tiles(l.co), l.k * l.k) > CONV_MMA_SMEM_MAX))
+                                 conv_h_smem2(l.ci, 8 * mma_tiles(l.co), l.k * l.k, true) > CONV_MMA_SMEM_MAX))
                     return false;
         nhwc = true;
         return true;
@@ -350,7 +350,7 @@ struct LpcNet {
         p.N = N;
         p.act = act;
         const int nt = mma_tiles(L.co);
-        const size_t smem = conv_h_smem2(L.ci, 8 * nt, L.k * L.k);
+        const size_t smem = conv_h_smem2(L.ci, 8 * nt, L.k * L.k, gate != nullptr);
         const int th = 8 * conv_h_rows(nt);
         dim3 grid((p.W + CM_TX - 1) / CM_TX, (p.H + th - 1) / th, N);
         const int kk = L.k * L.k, cp = conv_mma_cp(L.ci);
