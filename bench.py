@@ -552,7 +552,7 @@ def main():
     ap.add_argument("--workload", default="config3", choices=["config1", "config2", "config3", "config4", "config5", "swe4096"])
     ap.add_argument("--pc", default="learned", choices=["learned", "jacobi"],
                     help="learned: time the learned preconditioner and plain PCG side by side (SGN workloads)")
-    ap.add_argument("--train-steps", type=int, default=3000)
+    ap.add_argument("--train-steps", type=int, default=20000)
     ap.add_argument("--lpc-stride", type=int, default=1, choices=[1, 2, 4])
     ap.add_argument("--lpc-channels", default="8,16,32,32")
     ap.add_argument("--eta-steps", type=int, default=10)

@@ -7,7 +7,7 @@ the network (`LearnedPreconditioner.harvest`). Training then takes Adam steps on
 random patches of those systems with random error fields (`LearnedPreconditioner.train`): every
 kernel involved is the library's own.
 
-    python -m wavesim_b200.train_lpc --out lpc_dx2.npy [--steps 3000]
+    python -m wavesim_b200.train_lpc --out lpc_dx2.npy [--steps 20000]
 """
 from __future__ import annotations
 
@@ -45,7 +45,7 @@ def harvest_runs(net: LearnedPreconditioner, runs: int = 8, nx: int = 512, ny: i
             "seconds": time.perf_counter() - t0}
 
 
-def train(net: LearnedPreconditioner, steps: int = 3000, batch: int = 16, patch: int = 0, lr: float = 2e-3,
+def train(net: LearnedPreconditioner, steps: int = 20000, batch: int = 16, patch: int = 0, lr: float = 2e-3,
           seed: int = 0) -> dict:
     """Adam with the learning rate dropped by 4 for the last quarter; returns the loss record."""
     t0 = time.perf_counter()
@@ -60,7 +60,7 @@ def train(net: LearnedPreconditioner, steps: int = 3000, batch: int = 16, patch:
             "seconds": time.perf_counter() - t0}
 
 
-def trained_network(dx: float = 2.0, steps: int = 3000, seed: int = 0, spec: UNetSpec | None = None):
+def trained_network(dx: float = 2.0, steps: int = 20000, seed: int = 0, spec: UNetSpec | None = None):
     """A network harvested and trained from scratch on this GPU; returns (network, record)."""
     net = LearnedPreconditioner(spec or UNetSpec(), seed=seed)
     h = harvest_runs(net, dx=dx, seed=seed)
@@ -71,7 +71,7 @@ def trained_network(dx: float = 2.0, steps: int = 3000, seed: int = 0, spec: UNe
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", required=True)
-    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--steps", type=int, default=20000)
     ap.add_argument("--dx", type=float, default=2.0)
     ap.add_argument("--seed", type=int, default=0)
     a = ap.parse_args()
