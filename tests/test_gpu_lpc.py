@@ -233,9 +233,10 @@ def test_learned_solve_counts_its_iteration_kernels():
     st = sol.dispersion_stats()
     n1 = sol.launch_count()
     assert st.iterations > 0
-    # every iteration is 22 kernels of the device library: four passes over the cells, three
-    # scalar kernels and the network's fifteen convolutions
-    assert n1 - n0 >= 22 * st.iterations
+    # every iteration is 21 kernels of the device library: four passes over the cells, three
+    # scalar kernels and the network's fourteen convolutions (the 1x1 output layer rides in the
+    # last one's epilogue)
+    assert n1 - n0 >= 21 * st.iterations
     assert math.isfinite(sol.time_device())
 
 

@@ -272,6 +272,8 @@ struct ConvH {
     unsigned short* y;          // co channels, NHWC BF16 ...
     float* yf;                  // ... or FP32 (non-null: the network's output)
     const int* done;            // or null: the solve this application serves has ended, skip it
+    const float* out_w;         // or null: an 8-channel layer followed by the 2 x 8 1x1 output layer,
+                                // applied in the epilogue; yf then gets its FP32 output
     int co, H, W, N, act;
 };
 
@@ -434,6 +436,41 @@ __global__ void __launch_bounds__(CM_NT, 2) conv_h_kernel(ConvH p) {
         const int co = t * 8 + tig * 2;
         bias[t][0] = p.bias && co < p.co ? __ldg(p.bias + co) : 0.f;
         bias[t][1] = p.bias && co < p.co ? __ldg(p.bias + co + 1) : 0.f;
+    }
+    if constexpr (NTL == 1) {
+        if (p.out_w) {  // the output layer on this layer's 8 gated channels: a dot over the lane quad
+            const int co = tig * 2;
+            const float w00 = __ldg(p.out_w + co), w01 = __ldg(p.out_w + co + 1);
+            const float w10 = __ldg(p.out_w + 8 + co), w11 = __ldg(p.out_w + 8 + co + 1);
+#pragma unroll
+            for (int r = 0; r < RW; r++) {
+                const int y = y0 + warp * RW + r;
+#pragma unroll
+                for (int half = 0; half < 2; half++) {
+                    const int x = x0 + grp + 8 * half;
+                    float v0 = acc[r][0][2 * half] + bias[0][0];
+                    float v1 = acc[r][0][2 * half + 1] + bias[0][1];
+                    if (p.act == ACT_RELU) {
+                        v0 = fmaxf(v0, 0.f);
+                        v1 = fmaxf(v1, 0.f);
+                    }
+                    if (p.gate) {  // the gate tile covers every pixel of the tile (zero outside)
+                        const int lp = (warp * RW + r) * CM_TX + grp + 8 * half;
+                        const unsigned gw = *reinterpret_cast<const unsigned*>(g_s + lp * p.co + co);
+                        v0 *= bf16_lo(gw);
+                        v1 *= bf16_hi(gw);
+                    }
+                    float o0 = w00 * v0 + w01 * v1, o1 = w10 * v0 + w11 * v1;
+                    o0 += __shfl_xor_sync(0xffffffffu, o0, 1);
+                    o1 += __shfl_xor_sync(0xffffffffu, o1, 1);
+                    o0 += __shfl_xor_sync(0xffffffffu, o0, 2);
+                    o1 += __shfl_xor_sync(0xffffffffu, o1, 2);
+                    if (tig == 0 && y < p.H && x < p.W)
+                        *reinterpret_cast<float2*>(p.yf + ((n * p.H + y) * p.W + x) * 2) = make_float2(o0, o1);
+                }
+            }
+            return;
+        }
     }
 #pragma unroll
     for (int r = 0; r < RW; r++) {

@@ -331,7 +331,7 @@ struct LpcNet {
     // One convolution on NHWC BF16 activations (conv_h_kernel); yf: FP32 output instead of y.
     cudaError_t conv_h(const unsigned short* a, int ca, int amode, const unsigned short* b, int cb, const LpcLayer& L,
                        const unsigned short* gate, unsigned short* y, float* yf, int level, int act,
-                       cudaStream_t st) const {
+                       cudaStream_t st, const float* out_w = nullptr) const {
         ConvH p{};
         p.a = a;
         p.ca = ca;
@@ -344,6 +344,7 @@ struct LpcNet {
         p.y = y;
         p.yf = yf;
         p.done = done;
+        p.out_w = out_w;
         p.co = L.co;
         p.H = h_of(level);
         p.W = w_of(level);
@@ -378,7 +379,13 @@ struct LpcNet {
         return e;
     }
 
-    // Yh = N(Xh) on NHWC BF16 activations with the gates already in Gh: the launches of forward().
+    // The output layer rides in dec_b[0]'s epilogue when that layer has one tile of 8 channels.
+    bool fused_out() const { return ch[0] == 8 && out.co == 2 && out.k == 1; }
+    // launches of forward_h()
+    int forward_h_launches() const { return 2 * LPC_LEVELS + 2 * (LPC_LEVELS - 1) + (fused_out() ? 0 : 1); }
+
+    // Yh = N(Xh) on NHWC BF16 activations with the gates already in Gh: the launches of forward()
+    // (the output layer fused into the last when fused_out()).
     cudaError_t forward_h(cudaStream_t st) {
         cudaError_t e = cudaSuccess;
         for (int l = 0; l < LPC_LEVELS && e == cudaSuccess; l++) {
@@ -392,10 +399,15 @@ struct LpcNet {
         for (int l = LPC_LEVELS - 2; l >= 0 && e == cudaSuccess; l--) {
             const unsigned short* below = (l == LPC_LEVELS - 2) ? hp(Eh[l + 1]) : hp(Dh[l + 1]);
             e = conv_h(below, ch[l + 1], CM_UP, hp(Eh[l]), ch[l], dec_a[l], nullptr, hp(DAh[l]), nullptr, l, ACT_NONE, st);
-            if (e == cudaSuccess)
+            if (e != cudaSuccess) break;
+            if (l == 0 && fused_out())  // dec_b[0] with the 1x1 output layer in its epilogue
+                e = conv_h(hp(DAh[0]), ch[0], CM_DIRECT, nullptr, 0, dec_b[0], hp(Gh[0]), nullptr, Yh.p, 0, ACT_NONE, st,
+                           wq + out.w);
+            else
                 e = conv_h(hp(DAh[l]), ch[l], CM_DIRECT, nullptr, 0, dec_b[l], hp(Gh[l]), hp(Dh[l]), nullptr, l, ACT_NONE, st);
         }
-        if (e == cudaSuccess) e = conv_h(hp(Dh[0]), ch[0], CM_DIRECT, nullptr, 0, out, nullptr, nullptr, Yh.p, 0, ACT_NONE, st);
+        if (e == cudaSuccess && !fused_out())
+            e = conv_h(hp(Dh[0]), ch[0], CM_DIRECT, nullptr, 0, out, nullptr, nullptr, Yh.p, 0, ACT_NONE, st);
         return e;
     }
 

@@ -461,7 +461,7 @@ wc_status fcg_body(wc_solver* s, cudaStream_t st, cudaGraphConditionalHandle h, 
     {
         ProfScope ps(s, 3);
         CK(nhwc ? s->lnet.forward_h(st) : s->lnet.forward(st, false));
-        s->launches += 2 * LPC_LEVELS + 2 * (LPC_LEVELS - 1) + 1;
+        s->launches += nhwc ? s->lnet.forward_h_launches() : 2 * LPC_LEVELS + 2 * (LPC_LEVELS - 1) + 1;
     }
     ProfScope ps(s, 1);
     const float* y = nhwc ? s->lnet.Yh.p : s->lnet.Y.p;
