@@ -321,6 +321,92 @@ __host__ __device__ inline size_t conv_h_smem2(int ci, int co, int kk, bool gate
     return (box + (size_t)ntl * 8 * kk * cp + (gated ? (size_t)th * CM_TX * ntl * 8 : 0)) * 2;
 }
 
+// The convolution's epilogue: bias, activation, gate (from the staged gate tile), and the BF16
+// (or FP32, or fused 1x1 output) store of the warp's RW rows of 16 pixels of the tile at (x0, y0).
+template <int NTL, int RW>
+__device__ __forceinline__ void conv_h_epilogue(const ConvH& p, float (&acc)[RW][NTL][4], const unsigned short* g_s,
+                                                int n, int x0, int y0) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int grp = lane >> 2, tig = lane & 3;
+    // D[pixel][channel]: pixels grp and grp + 8 of the warp's rows, channels t * 8 + tig * 2 + {0, 1}
+    float bias[NTL][2];
+#pragma unroll
+    for (int t = 0; t < NTL; t++) {
+        const int co = t * 8 + tig * 2;
+        bias[t][0] = p.bias && co < p.co ? __ldg(p.bias + co) : 0.f;
+        bias[t][1] = p.bias && co < p.co ? __ldg(p.bias + co + 1) : 0.f;
+    }
+    if constexpr (NTL == 1) {
+        if (p.out_w) {  // the output layer on this layer's 8 gated channels: a dot over the lane quad
+            const int co = tig * 2;
+            const float w00 = __ldg(p.out_w + co), w01 = __ldg(p.out_w + co + 1);
+            const float w10 = __ldg(p.out_w + 8 + co), w11 = __ldg(p.out_w + 8 + co + 1);
+#pragma unroll
+            for (int r = 0; r < RW; r++) {
+                const int y = y0 + warp * RW + r;
+#pragma unroll
+                for (int half = 0; half < 2; half++) {
+                    const int x = x0 + grp + 8 * half;
+                    float v0 = acc[r][0][2 * half] + bias[0][0];
+                    float v1 = acc[r][0][2 * half + 1] + bias[0][1];
+                    if (p.act == ACT_RELU) {
+                        v0 = fmaxf(v0, 0.f);
+                        v1 = fmaxf(v1, 0.f);
+                    }
+                    if (p.gate) {  // the gate tile covers every pixel of the tile (zero outside)
+                        const int lp = (warp * RW + r) * CM_TX + grp + 8 * half;
+                        const unsigned gw = *reinterpret_cast<const unsigned*>(g_s + lp * p.co + co);
+                        v0 *= bf16_lo(gw);
+                        v1 *= bf16_hi(gw);
+                    }
+                    float o0 = w00 * v0 + w01 * v1, o1 = w10 * v0 + w11 * v1;
+                    o0 += __shfl_xor_sync(0xffffffffu, o0, 1);
+                    o1 += __shfl_xor_sync(0xffffffffu, o1, 1);
+                    o0 += __shfl_xor_sync(0xffffffffu, o0, 2);
+                    o1 += __shfl_xor_sync(0xffffffffu, o1, 2);
+                    if (tig == 0 && y < p.H && x < p.W)
+                        *reinterpret_cast<float2*>(p.yf + ((n * p.H + y) * p.W + x) * 2) = make_float2(o0, o1);
+                }
+            }
+            return;
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < RW; r++) {
+        const int y = y0 + warp * RW + r;
+        if (y >= p.H) continue;
+        const int row = (n * p.H + y) * p.W;
+#pragma unroll
+        for (int half = 0; half < 2; half++) {
+            const int x = x0 + grp + 8 * half;
+            if (x >= p.W) continue;
+            const int pix = (row + x) * p.co;
+#pragma unroll
+            for (int t = 0; t < NTL; t++) {
+                const int co = t * 8 + tig * 2;
+                if (co >= p.co) continue;
+                float v0 = acc[r][t][2 * half] + bias[t][0];
+                float v1 = acc[r][t][2 * half + 1] + bias[t][1];
+                if (p.act == ACT_RELU) {
+                    v0 = fmaxf(v0, 0.f);
+                    v1 = fmaxf(v1, 0.f);
+                } else if (p.act == ACT_SIG2) {
+                    v0 = 2.f / (1.f + expf(-v0));
+                    v1 = 2.f / (1.f + expf(-v1));
+                }
+                if (p.gate) {
+                    const int lp = (warp * RW + r) * CM_TX + grp + 8 * half;
+                    const unsigned gw = *reinterpret_cast<const unsigned*>(g_s + lp * p.co + co);
+                    v0 *= bf16_lo(gw);
+                    v1 *= bf16_hi(gw);
+                }
+                if (p.yf) *reinterpret_cast<float2*>(p.yf + pix + co) = make_float2(v0, v1);
+                else *reinterpret_cast<unsigned*>(p.y + pix + co) = bf16_pack(v0, v1);
+            }
+        }
+    }
+}
+
 // KK taps (9 or 1), NTL tiles of 8 output channels, CP input channels padded to 16: all index
 // arithmetic is compile-time and 32-bit (a map of up to 2^31 values). A block computes a tile of
 // 16 x (8 RW) pixels, each warp RW rows of 16; its halo box is staged with cp.async (pooled
@@ -429,83 +515,102 @@ __global__ void __launch_bounds__(CM_NT, 2) conv_h_kernel(ConvH p) {
             }
         }
     }
-    // D[pixel][channel]: pixels grp and grp + 8 of the warp's rows, channels t * 8 + tig * 2 + {0, 1}
-    float bias[NTL][2];
-#pragma unroll
-    for (int t = 0; t < NTL; t++) {
-        const int co = t * 8 + tig * 2;
-        bias[t][0] = p.bias && co < p.co ? __ldg(p.bias + co) : 0.f;
-        bias[t][1] = p.bias && co < p.co ? __ldg(p.bias + co + 1) : 0.f;
+    conv_h_epilogue<NTL, RW>(p, acc, g_s, n, x0, y0);
+}
+
+// A decoder convolution over concat(up(a), b) (3x3; a at half resolution with CPA channels, a
+// multiple of 16; b with the rest of the CP input channels, zero-padded): the a-part is staged
+// once per coarse pixel of the tile (a quarter of the fine halo box) and its A fragments are read
+// by ldmatrix straight from the coarse box, each lane addressing the coarse pixel its fine pixel
+// repeats; the b-part is staged and read as in conv_h_kernel. Same arithmetic and K order as
+// conv_h_kernel on the upsampled map.
+__host__ __device__ inline size_t conv_up_smem(int cpa, int cp, int co, bool gated) {
+    const int ntl = (co + 7) / 8, th = 8 * conv_h_rows(ntl);
+    const size_t abox = (size_t)(th / 2 + 2) * (CM_TX / 2 + 2) * (cpa + 8);
+    const size_t bbox = (size_t)(th + 2) * (CM_TX + 2) * (cp - cpa + 8);
+    return (abox + bbox + (size_t)ntl * 8 * 9 * cp + (gated ? (size_t)th * CM_TX * ntl * 8 : 0)) * 2;
+}
+
+template <int NTL, int CP, int CPA>
+__global__ void __launch_bounds__(CM_NT, 2) conv_up_kernel(ConvH p) {
+    if (p.done && *p.done) return;
+    constexpr int RW = conv_h_rows(NTL), TH = 8 * RW;
+    constexpr int EW = CM_TX + 2, EH = TH + 2, CEW = CM_TX / 2 + 2, CEH = TH / 2 + 2;
+    constexpr int CPB = CP - CPA, PSA = CPA + 8, PSB = CPB + 8, KP = 9 * CP;
+    constexpr int GA = CPA / 8, GB = CPB / 8, UA = CEH * CEW * GA, UB = EH * EW * GB;
+    extern __shared__ __align__(16) unsigned short cm_smem[];
+    unsigned short* a_s = cm_smem;               // [CEH][CEW][PSA]
+    unsigned short* b_s = a_s + CEH * CEW * PSA;  // [EH][EW][PSB]
+    unsigned short* w_s = b_s + EH * EW * PSB;    // [8 NTL][KP]
+    unsigned short* g_s = w_s + 8 * NTL * KP;     // gated layers: [TH][16][co]
+    const int n = blockIdx.z;
+    const int x0 = blockIdx.x * CM_TX, y0 = blockIdx.y * TH;
+    const int Hc = p.H / 2, Wc = p.W / 2;
+    const int cx0 = (x0 >> 1) - 1, cy0 = (y0 >> 1) - 1;
+    {
+        const uint4* src = reinterpret_cast<const uint4*>(p.wre);
+        uint4* dst = reinterpret_cast<uint4*>(w_s);
+        for (int q = threadIdx.x; q < NTL * KP; q += CM_NT) cp_async16(dst + q, src + q, 16);
     }
-    if constexpr (NTL == 1) {
-        if (p.out_w) {  // the output layer on this layer's 8 gated channels: a dot over the lane quad
-            const int co = tig * 2;
-            const float w00 = __ldg(p.out_w + co), w01 = __ldg(p.out_w + co + 1);
-            const float w10 = __ldg(p.out_w + 8 + co), w11 = __ldg(p.out_w + 8 + co + 1);
-#pragma unroll
-            for (int r = 0; r < RW; r++) {
-                const int y = y0 + warp * RW + r;
-#pragma unroll
-                for (int half = 0; half < 2; half++) {
-                    const int x = x0 + grp + 8 * half;
-                    float v0 = acc[r][0][2 * half] + bias[0][0];
-                    float v1 = acc[r][0][2 * half + 1] + bias[0][1];
-                    if (p.act == ACT_RELU) {
-                        v0 = fmaxf(v0, 0.f);
-                        v1 = fmaxf(v1, 0.f);
-                    }
-                    if (p.gate) {  // the gate tile covers every pixel of the tile (zero outside)
-                        const int lp = (warp * RW + r) * CM_TX + grp + 8 * half;
-                        const unsigned gw = *reinterpret_cast<const unsigned*>(g_s + lp * p.co + co);
-                        v0 *= bf16_lo(gw);
-                        v1 *= bf16_hi(gw);
-                    }
-                    float o0 = w00 * v0 + w01 * v1, o1 = w10 * v0 + w11 * v1;
-                    o0 += __shfl_xor_sync(0xffffffffu, o0, 1);
-                    o1 += __shfl_xor_sync(0xffffffffu, o1, 1);
-                    o0 += __shfl_xor_sync(0xffffffffu, o0, 2);
-                    o1 += __shfl_xor_sync(0xffffffffu, o1, 2);
-                    if (tig == 0 && y < p.H && x < p.W)
-                        *reinterpret_cast<float2*>(p.yf + ((n * p.H + y) * p.W + x) * 2) = make_float2(o0, o1);
-                }
-            }
-            return;
+    if (p.gate) {
+        const int gg = p.co / 8;
+        for (int q = threadIdx.x; q < TH * CM_TX * gg; q += CM_NT) {
+            const int pix = q / gg, c0 = (q - pix * gg) * 8;
+            const int y = y0 + pix / CM_TX, x = x0 + pix % CM_TX;
+            const bool in = y < p.H && x < p.W;
+            cp_async16(g_s + pix * p.co + c0, in ? p.gate + ((n * p.H + y) * p.W + x) * p.co + c0 : p.gate, in ? 16 : 0);
         }
     }
+    for (int q = threadIdx.x; q < UA; q += CM_NT) {  // the coarse box of a
+        const int r = q / GA, c0 = (q % GA) * 8;
+        const int cy = cy0 + r / CEW, cx = cx0 + r % CEW;
+        const bool in = (unsigned)cy < (unsigned)Hc && (unsigned)cx < (unsigned)Wc;
+        cp_async16(a_s + r * PSA + c0, in ? p.a + ((n * Hc + cy) * Wc + cx) * p.ca + c0 : p.a, in ? 16 : 0);
+    }
+    for (int q = threadIdx.x; q < UB; q += CM_NT) {  // the fine box of b (channels past cb: zero)
+        const int r = q / GB, c0 = (q % GB) * 8;
+        const int yy = y0 + r / EW - 1, xx = x0 + r % EW - 1;
+        const bool in = (unsigned)yy < (unsigned)p.H && (unsigned)xx < (unsigned)p.W && c0 < p.cb;
+        cp_async16(b_s + r * PSB + c0, in ? p.b + ((n * p.H + yy) * p.W + xx) * p.cb + c0 : p.b, in ? 16 : 0);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int grp = lane >> 2, tig = lane & 3;
+    const int lpix = (lane & 7) + ((lane >> 3) & 1) * 8, lk = (lane >> 4) * 8;
+    float acc[RW][NTL][4];
 #pragma unroll
-    for (int r = 0; r < RW; r++) {
-        const int y = y0 + warp * RW + r;
-        if (y >= p.H) continue;
-        const int row = (n * p.H + y) * p.W;
+    for (int r = 0; r < RW; r++)
 #pragma unroll
-        for (int half = 0; half < 2; half++) {
-            const int x = x0 + grp + 8 * half;
-            if (x >= p.W) continue;
-            const int pix = (row + x) * p.co;
+        for (int t = 0; t < NTL; t++)
+#pragma unroll
+            for (int e = 0; e < 4; e++) acc[r][t][e] = 0.f;
+#pragma unroll 3
+    for (int tap = 0; tap < 9; tap++) {
+        const int dy = tap / 3, dx = tap % 3;
+        const int ccol = (lpix + dx + 1) >> 1;  // the coarse column of this lane's fine pixel (box coordinates)
+#pragma unroll
+        for (int cb = 0; cb < CP; cb += 16) {
+            const int kb = tap * CP + cb;
+            unsigned b[NTL][2];
 #pragma unroll
             for (int t = 0; t < NTL; t++) {
-                const int co = t * 8 + tig * 2;
-                if (co >= p.co) continue;
-                float v0 = acc[r][t][2 * half] + bias[t][0];
-                float v1 = acc[r][t][2 * half + 1] + bias[t][1];
-                if (p.act == ACT_RELU) {
-                    v0 = fmaxf(v0, 0.f);
-                    v1 = fmaxf(v1, 0.f);
-                } else if (p.act == ACT_SIG2) {
-                    v0 = 2.f / (1.f + expf(-v0));
-                    v1 = 2.f / (1.f + expf(-v1));
-                }
-                if (p.gate) {
-                    const int lp = (warp * RW + r) * CM_TX + grp + 8 * half;
-                    const unsigned gw = *reinterpret_cast<const unsigned*>(g_s + lp * p.co + co);
-                    v0 *= bf16_lo(gw);
-                    v1 *= bf16_hi(gw);
-                }
-                if (p.yf) *reinterpret_cast<float2*>(p.yf + pix + co) = make_float2(v0, v1);
-                else *reinterpret_cast<unsigned*>(p.y + pix + co) = bf16_pack(v0, v1);
+                const unsigned* wrow = reinterpret_cast<const unsigned*>(w_s + (t * 8 + grp) * KP + kb + tig * 2);
+                b[t][0] = wrow[0];
+                b[t][1] = wrow[4];
+            }
+#pragma unroll
+            for (int r = 0; r < RW; r++) {
+                const int frow = warp * RW + r + dy;  // fine box row
+                unsigned a[4];
+                if (cb < CPA) ldmatrix_x4(a, a_s + (((frow + 1) >> 1) * CEW + ccol) * PSA + cb + lk);
+                else ldmatrix_x4(a, b_s + (frow * EW + lpix + dx) * PSB + (cb - CPA) + lk);
+#pragma unroll
+                for (int t = 0; t < NTL; t++) mma_bf16_16816(acc[r][t], a, b[t]);
             }
         }
     }
+    conv_h_epilogue<NTL, RW>(p, acc, g_s, n, x0, y0);
 }
 
 // NCHW FP32 maps -> NHWC BF16 (c channels, 2 or a multiple of 2).

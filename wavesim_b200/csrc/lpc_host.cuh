@@ -39,6 +39,9 @@ constexpr size_t CONV_MMA_SMEM_MAX = 160 * 1024;
     X(1, 1, 16) X(1, 1, 32) X(1, 1, 48) X(1, 1, 64) X(1, 2, 16) X(1, 2, 32) X(1, 2, 48) X(1, 2, 64) \
     X(1, 4, 16) X(1, 4, 32) X(1, 4, 48) X(1, 4, 64) X(1, 8, 16) X(1, 8, 32) X(1, 8, 48) X(1, 8, 64)
 constexpr int CONV_H_CP_MAX = 64;
+// The decoder convolutions over concat(up(a), b) with the coarse-box staging: output tiles x
+// padded inputs x channels of a.
+#define CONV_UP_FOR_ALL(X) X(1, 32, 16) X(2, 32, 16) X(2, 48, 32) X(4, 48, 32) X(4, 64, 32) X(8, 64, 32)
 
 inline cudaError_t conv_mma_configure() {
     static cudaError_t st = cudaErrorNotReady;
@@ -50,6 +53,9 @@ inline cudaError_t conv_mma_configure() {
 #define CONV_H_PTR(KK_, NT_, CP_) (const void*)conv_h_kernel<KK_, NT_, CP_>,
                             CONV_H_FOR_ALL(CONV_H_PTR)
 #undef CONV_H_PTR
+#define CONV_UP_PTR(NT_, CP_, CPA_) (const void*)conv_up_kernel<NT_, CP_, CPA_>,
+                            CONV_UP_FOR_ALL(CONV_UP_PTR)
+#undef CONV_UP_PTR
         };
         st = cudaSuccess;
         for (const void* k : ks)
@@ -351,11 +357,22 @@ struct LpcNet {
         p.N = N;
         p.act = act;
         const int nt = mma_tiles(L.co);
-        const size_t smem = conv_h_smem2(L.ci, 8 * nt, L.k * L.k, gate != nullptr);
         const int th = 8 * conv_h_rows(nt);
         dim3 grid((p.W + CM_TX - 1) / CM_TX, (p.H + th - 1) / th, N);
         const int kk = L.k * L.k, cp = conv_mma_cp(L.ci);
         bool launched = false;
+        if (amode == CM_UP && kk == 9 && ca % 16 == 0 && b) {  // the coarse-box decoder kernel
+            const size_t smem = conv_up_smem(ca, cp, 8 * nt, gate != nullptr);
+#define CONV_UP_LAUNCH(NT_, CP_, CPA_)                                          \
+            if (!launched && nt == NT_ && cp == CP_ && ca == CPA_ && smem <= CONV_MMA_SMEM_MAX) { \
+                conv_up_kernel<NT_, CP_, CPA_><<<grid, CM_NT, smem, st>>>(p);    \
+                launched = true;                                                 \
+            }
+            CONV_UP_FOR_ALL(CONV_UP_LAUNCH)
+#undef CONV_UP_LAUNCH
+            if (launched) return cudaGetLastError();
+        }
+        const size_t smem = conv_h_smem2(L.ci, 8 * nt, L.k * L.k, gate != nullptr);
 #define CONV_H_LAUNCH(KK_, NT_, CP_)                                          \
         if (!launched && kk == KK_ && nt == NT_ && cp == CP_) {                 \
             conv_h_kernel<KK_, NT_, CP_><<<grid, CM_NT, smem, st>>>(p);        \
