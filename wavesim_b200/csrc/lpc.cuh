@@ -613,6 +613,108 @@ __global__ void __launch_bounds__(CM_NT, 2) conv_up_kernel(ConvH p) {
     conv_h_epilogue<NTL, RW>(p, acc, g_s, n, x0, y0);
 }
 
+// ---- 3x3 convolutions of an 8-channel input: two taps per K step ---------------------------
+//
+// With 8 input channels a K step of 16 holds two taps (k = tap * 8 + c; the ninth tap's partner
+// has zero weights), so the halo box needs no channel padding (16 bytes a pixel) and a layer
+// takes 5 K steps instead of 9: ldmatrix lanes 0-15 address the pixels of the first tap, lanes
+// 16-31 those of the second. Same products and FP32 accumulation as conv_h_kernel, in another
+// order of the sum.
+constexpr int P8_KP = 80;  // 9 taps x 8 channels, padded to a multiple of 16
+
+__global__ void conv_p8_weights_kernel(const float* __restrict__ w, int co_n, int ntl, unsigned short* __restrict__ out) {
+    const int total = ntl * 8 * P8_KP;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < total; q += gridDim.x * blockDim.x) {
+        const int co = q / P8_KP, k = q % P8_KP, tap = k / 8, c = k % 8;
+        out[q] = (co < co_n && tap < 9) ? (unsigned short)(__float_as_uint(w[((size_t)co * 8 + c) * 9 + tap]) >> 16)
+                                        : (unsigned short)0;
+    }
+}
+
+__host__ __device__ inline size_t conv_p8_smem(int co, bool gated) {
+    const int ntl = (co + 7) / 8, th = 8 * conv_h_rows(ntl);
+    return ((size_t)(th + 2) * (CM_TX + 2) * 8 + (size_t)ntl * 8 * P8_KP + (gated ? (size_t)th * CM_TX * ntl * 8 : 0)) * 2;
+}
+
+template <int NTL>
+__global__ void __launch_bounds__(CM_NT, 2) conv_p8_kernel(ConvH p) {
+    if (p.done && *p.done) return;
+    constexpr int RW = conv_h_rows(NTL), TH = 8 * RW, EW = CM_TX + 2, EH = TH + 2, UNITS = EH * EW;
+    extern __shared__ __align__(16) unsigned short cm_smem[];
+    unsigned short* in_s = cm_smem;           // [EH][EW][8]
+    unsigned short* w_s = in_s + UNITS * 8;   // [8 NTL][P8_KP]
+    unsigned short* g_s = w_s + 8 * NTL * P8_KP;
+    const int n = blockIdx.z;
+    const int x0 = blockIdx.x * CM_TX, y0 = blockIdx.y * TH;
+    {
+        const uint4* src = reinterpret_cast<const uint4*>(p.wre);
+        uint4* dst = reinterpret_cast<uint4*>(w_s);
+        for (int q = threadIdx.x; q < NTL * P8_KP; q += CM_NT) cp_async16(dst + q, src + q, 16);
+    }
+    if (p.gate) {
+        const int gg = p.co / 8;
+        for (int q = threadIdx.x; q < TH * CM_TX * gg; q += CM_NT) {
+            const int pix = q / gg, c0 = (q - pix * gg) * 8;
+            const int y = y0 + pix / CM_TX, x = x0 + pix % CM_TX;
+            const bool in = y < p.H && x < p.W;
+            cp_async16(g_s + pix * p.co + c0, in ? p.gate + ((n * p.H + y) * p.W + x) * p.co + c0 : p.gate, in ? 16 : 0);
+        }
+    }
+    const bool pool = p.amode == CM_POOL;
+    const int Ws = pool ? 2 * p.W : p.W;
+    const int abase = n * (pool ? 2 * p.H : p.H) * Ws;
+    for (int q = threadIdx.x; q < UNITS; q += CM_NT) {
+        const int yy = y0 + q / EW - 1, xx = x0 + q % EW - 1;
+        const bool in = (unsigned)yy < (unsigned)p.H && (unsigned)xx < (unsigned)p.W;
+        uint4* dst = reinterpret_cast<uint4*>(in_s + q * 8);
+        if (pool) {
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (in) {
+                const uint4* w = reinterpret_cast<const uint4*>(p.a);
+                const int at = abase + (2 * yy) * Ws + 2 * xx;
+                const uint4 a0 = __ldg(w + at), a1 = __ldg(w + at + 1), a2 = __ldg(w + at + Ws), a3 = __ldg(w + at + Ws + 1);
+                v = make_uint4(pool_word(a0.x, a1.x, a2.x, a3.x), pool_word(a0.y, a1.y, a2.y, a3.y),
+                               pool_word(a0.z, a1.z, a2.z, a3.z), pool_word(a0.w, a1.w, a2.w, a3.w));
+            }
+            *dst = v;
+        } else {
+            cp_async16(dst, in ? p.a + (abase + yy * Ws + xx) * 8 : p.a, in ? 16 : 0);
+        }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int grp = lane >> 2, tig = lane & 3;
+    const int lpix = (lane & 7) + ((lane >> 3) & 1) * 8, second = lane >> 4;  // ldmatrix row: pixel, which tap
+    float acc[RW][NTL][4];
+#pragma unroll
+    for (int r = 0; r < RW; r++)
+#pragma unroll
+        for (int t = 0; t < NTL; t++)
+#pragma unroll
+            for (int e = 0; e < 4; e++) acc[r][t][e] = 0.f;
+#pragma unroll
+    for (int j = 0; j < 5; j++) {
+        const int tap = min(2 * j + second, 8);  // the ninth tap's partner: zero weights
+        const int dy = tap / 3, dx = tap - 3 * (tap / 3);
+        unsigned b[NTL][2];
+#pragma unroll
+        for (int t = 0; t < NTL; t++) {
+            const unsigned* wrow = reinterpret_cast<const unsigned*>(w_s + (t * 8 + grp) * P8_KP + j * 16 + tig * 2);
+            b[t][0] = wrow[0];
+            b[t][1] = wrow[4];
+        }
+#pragma unroll
+        for (int r = 0; r < RW; r++) {
+            unsigned a[4];
+            ldmatrix_x4(a, in_s + ((warp * RW + r + dy) * EW + lpix + dx) * 8);
+#pragma unroll
+            for (int t = 0; t < NTL; t++) mma_bf16_16816(acc[r][t], a, b[t]);
+        }
+    }
+    conv_h_epilogue<NTL, RW>(p, acc, g_s, n, x0, y0);
+}
+
 // NCHW FP32 maps -> NHWC BF16 (c channels, 2 or a multiple of 2).
 __global__ void to_h_kernel(const float* __restrict__ x, int N, int C, int H, int W, unsigned short* __restrict__ y) {
     const size_t plane = (size_t)H * W, total = (size_t)N * plane * (C / 2);

@@ -42,6 +42,8 @@ constexpr int CONV_H_CP_MAX = 64;
 // The decoder convolutions over concat(up(a), b) with the coarse-box staging: output tiles x
 // padded inputs x channels of a.
 #define CONV_UP_FOR_ALL(X) X(1, 32, 16) X(2, 32, 16) X(2, 48, 32) X(4, 48, 32) X(4, 64, 32) X(8, 64, 32)
+// The 8-channel-input convolutions with two taps per K step: output tiles.
+#define CONV_P8_FOR_ALL(X) X(1) X(2) X(4)
 
 inline cudaError_t conv_mma_configure() {
     static cudaError_t st = cudaErrorNotReady;
@@ -56,6 +58,9 @@ inline cudaError_t conv_mma_configure() {
 #define CONV_UP_PTR(NT_, CP_, CPA_) (const void*)conv_up_kernel<NT_, CP_, CPA_>,
                             CONV_UP_FOR_ALL(CONV_UP_PTR)
 #undef CONV_UP_PTR
+#define CONV_P8_PTR(NT_) (const void*)conv_p8_kernel<NT_>,
+                            CONV_P8_FOR_ALL(CONV_P8_PTR)
+#undef CONV_P8_PTR
         };
         st = cudaSuccess;
         for (const void* k : ks)
@@ -105,6 +110,8 @@ struct LpcNet {
     DBuf wre;                   // tensor-core weights of every layer (BF16 pairs in floats)
     std::vector<size_t> wre_off;  // per layer, in BF16 elements, keyed by the layer's weight offset
     std::vector<int> wre_key;
+    std::vector<size_t> wp8_off;  // 3x3 layers of 8 input channels: the two-taps-per-step order
+    std::vector<int> wp8_key;
 
     // Inference on NHWC BF16 activations (conv_h_kernel): every channel count a multiple of 8
     // and every layer's tile within the shared-memory limit; set by configure_nhwc.
@@ -176,6 +183,14 @@ struct LpcNet {
             wre_off.push_back(total);
             total += (size_t)mma_tiles(l->co) * 8 * l->k * l->k * conv_mma_cp(l->ci);
         }
+        wp8_off.clear();
+        wp8_key.clear();
+        for (auto* l : all)
+            if (l->ci == 8 && l->k == 3) {
+                wp8_key.push_back(l->w);
+                wp8_off.push_back(total);
+                total += (size_t)mma_tiles(l->co) * 8 * P8_KP;
+            }
         cudaError_t e = wre.alloc((total + 1) / 2 + 8);
         if (e != cudaSuccess) return e;
         auto* base = reinterpret_cast<unsigned short*>(wre.p);
@@ -185,12 +200,24 @@ struct LpcNet {
             conv_mma_weights_kernel<<<ew_grid(cnt), 256, 0, st>>>(wq + l->w, l->co, l->ci, l->k * l->k, mma_tiles(l->co),
                                                                   base + wre_off[n]);
         }
+        for (size_t n = 0; n < wp8_key.size(); n++) {
+            const LpcLayer* l = nullptr;
+            for (auto* c : all)
+                if (c->w == wp8_key[n]) l = c;
+            conv_p8_weights_kernel<<<ew_grid(mma_tiles(l->co) * 8 * P8_KP), 256, 0, st>>>(wq + l->w, l->co,
+                                                                                          mma_tiles(l->co), base + wp8_off[n]);
+        }
         return cudaGetLastError();
     }
 
     const unsigned short* wre_of(const LpcLayer& L) const {
         for (size_t n = 0; n < wre_key.size(); n++)
             if (wre_key[n] == L.w) return reinterpret_cast<const unsigned short*>(wre.p) + wre_off[n];
+        return nullptr;
+    }
+    const unsigned short* wp8_of(const LpcLayer& L) const {
+        for (size_t n = 0; n < wp8_key.size(); n++)
+            if (wp8_key[n] == L.w) return reinterpret_cast<const unsigned short*>(wre.p) + wp8_off[n];
         return nullptr;
     }
 
@@ -361,6 +388,19 @@ struct LpcNet {
         dim3 grid((p.W + CM_TX - 1) / CM_TX, (p.H + th - 1) / th, N);
         const int kk = L.k * L.k, cp = conv_mma_cp(L.ci);
         bool launched = false;
+        if (kk == 9 && ca == 8 && cb == 0 && amode != CM_UP && wp8_of(L)) {  // two taps per K step
+            const size_t smem = conv_p8_smem(8 * nt, gate != nullptr);
+            p.wre = wp8_of(L);
+#define CONV_P8_LAUNCH(NT_)                                               \
+            if (!launched && nt == NT_) {                                  \
+                conv_p8_kernel<NT_><<<grid, CM_NT, smem, st>>>(p);         \
+                launched = true;                                           \
+            }
+            CONV_P8_FOR_ALL(CONV_P8_LAUNCH)
+#undef CONV_P8_LAUNCH
+            if (launched) return cudaGetLastError();
+            p.wre = wre_of(L);
+        }
         if (amode == CM_UP && kk == 9 && ca % 16 == 0 && b) {  // the coarse-box decoder kernel
             const size_t smem = conv_up_smem(ca, cp, 8 * nt, gate != nullptr);
 #define CONV_UP_LAUNCH(NT_, CP_, CPA_)                                          \
