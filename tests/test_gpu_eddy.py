@@ -167,3 +167,31 @@ def test_an_ensemble_does_not_take_followed_fronts():
     m = Solver(grid, bed).with_dispersion(eddy_dispersion())
     with pytest.raises(WavecoreError):
         Ensemble([m])
+
+
+def test_frames_and_the_recorder_read_the_memory():
+    """With followed fronts the driver's frame and its per-step breaking statistics read a cell
+    whose memory holds a front as breaking (dispersion.rs:149-152 through breaking_into)."""
+    from wavesim_b200 import Recorder
+
+    grid = Grid(128, 32, 0.25, 0.25)
+    bed, s0 = dam_break(grid)
+    bed.b[:] = bed.b.astype(np.float32).astype(np.float64)
+    sol, _ = pair(grid, bed)
+    sol.upload(s0)
+    rec = Recorder(sol, 0.0, 1.0)
+    for _ in range(40):
+        sol.step_device(0.004)
+    sol.synchronize()
+    _, brk, _ = sol.frame(0.0)
+    s = s0.clone()
+    sol.download(s)
+    mem, h = grid.inner(s.breaking), grid.inner(s.h)
+    held = (mem != 0.0) & (h >= 0.05)
+    assert held.sum() >= 10
+    assert np.all(brk[held] == 1.0)
+    frac = rec.read()["breaking_fraction"]
+    # cells holding a front since the first step have been breaking every recorded second
+    old = (mem >= 40 * 0.004 - 1e-9) & (h >= 0.05)
+    assert old.any() and np.all(frac[old] > 0.99)
+    rec.close()
