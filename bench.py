@@ -48,7 +48,7 @@ STAGE_BYTES_SWE = (36 + 52) / 2                 # stage 1 / stage 2 (RK average 
 
 # DRAM bytes per cell measured by ncu (one capture each; scaled to a launch by cells, and by
 # iterations for the solve): profiles/network_conv_2048x1024.md, profiles/pcg_kernel_sgn_2048x1024.md.
-NETWORK_DRAM_BYTES_PER_CELL = 448.2e6 / (2048 * 1024)    # one application of the U-net
+NETWORK_DRAM_BYTES_PER_CELL = 409.5e6 / (2048 * 1024)    # one application of the U-net
 PCG_DRAM_BYTES_PER_CELL_ITER = 10.53e9 / (2048 * 1024 * 57)  # one iteration of the solve
 STAGE_DRAM_BYTES_PER_CELL_SWE = 573.1e6 / (4096 * 4096)      # one second-order stage
 # (profiles/stage_kernel_swe_4096x4096.md)
