@@ -171,27 +171,32 @@ def test_an_ensemble_does_not_take_followed_fronts():
 
 def test_frames_and_the_recorder_read_the_memory():
     """With followed fronts the driver's frame and its per-step breaking statistics read a cell
-    whose memory holds a front as breaking (dispersion.rs:149-152 through breaking_into)."""
+    whose memory holds a front as breaking (dispersion.rs:149-152 through breaking_into): the
+    device recorder against the FP64 restatement of Stage::record fed with the oracle's states and
+    breaking indicators (memory included), same inputs and dt."""
+    from oracle.record_oracle import Recorder as OracleRecorder
     from wavesim_b200 import Recorder
 
     grid = Grid(128, 32, 0.25, 0.25)
     bed, s0 = dam_break(grid)
-    bed.b[:] = bed.b.astype(np.float32).astype(np.float64)
-    sol, _ = pair(grid, bed)
-    sol.upload(s0)
-    rec = Recorder(sol, 0.0, 1.0)
+    gpu, orc = pair(grid, bed)
+    rec = Recorder(gpu, 0.0, 1.0)
+    ref = OracleRecorder(grid.nx * grid.ny, 0.0, 0.0, 1.0)
+    sg, so = s0.clone(), s0.clone()
+    b = grid.inner(bed.b)
     for _ in range(40):
-        sol.step_device(0.004)
-    sol.synchronize()
-    _, brk, _ = sol.frame(0.0)
-    s = s0.clone()
-    sol.download(s)
-    mem, h = grid.inner(s.breaking), grid.inner(s.h)
+        dt = orc.stable_dt(so)
+        orc.step(so, dt)
+        gpu.step(sg, dt)
+        ref.record(so.time, dt, (grid.inner(so.h) + b).ravel(), orc.breaking_indicator(so).ravel())
+    frac, frac_o = rec.read()["breaking_fraction"].ravel(), ref.breaking_fraction()
+    assert frac_o.max() > 0.9, "nothing broke"
+    assert np.mean(np.abs(frac - frac_o) < 0.05) > 0.99
+    # the frame of the resident state: breaking wherever the memory holds a front
+    gpu.upload(sg)
+    gpu_state = sg.clone()
+    _, brk, _ = gpu.frame(0.0)
+    mem, h = grid.inner(gpu_state.breaking), grid.inner(gpu_state.h)
     held = (mem != 0.0) & (h >= 0.05)
-    assert held.sum() >= 10
-    assert np.all(brk[held] == 1.0)
-    frac = rec.read()["breaking_fraction"]
-    # cells holding a front since the first step have been breaking every recorded second
-    old = (mem >= 40 * 0.004 - 1e-9) & (h >= 0.05)
-    assert old.any() and np.all(frac[old] > 0.99)
+    assert held.sum() >= 10 and np.all(brk[held] == 1.0)
     rec.close()

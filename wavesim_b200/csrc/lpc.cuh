@@ -308,9 +308,13 @@ __device__ __forceinline__ void ldmatrix_x4(unsigned* r, const void* row) {
                  : "r"(sa));
 }
 
-// Rows of 16 pixels per warp: taller tiles for the thin layers (fewer halo cells and less fixed
-// work per pixel), two rows where the output has four or more tiles of 8 channels.
-__host__ __device__ constexpr int conv_h_rows(int ntl) { return ntl <= 2 ? 4 : 2; }
+// Rows of 16 pixels per warp: tall tiles for the 8-channel layers (fewer halo cells and less
+// fixed work per pixel); shorter ones as the output widens, so that the accumulators leave room
+// for more resident blocks and the coarse levels still give every SM several tiles.
+__host__ __device__ constexpr int conv_h_rows(int ntl) { return ntl == 1 ? 4 : 2; }
+// The decoder's concat(up(a), b) kernel stages a quarter-size coarse box, so taller tiles pay
+// there up to two output tiles (measured).
+__host__ __device__ constexpr int conv_up_rows(int ntl) { return ntl <= 2 ? 4 : 2; }
 
 // Shared memory of the channels-innermost convolution (bytes): the input box, the weights and,
 // for a gated layer, the gate tile ([pixel][co]).
@@ -525,7 +529,7 @@ __global__ void __launch_bounds__(CM_NT, 2) conv_h_kernel(ConvH p) {
 // repeats; the b-part is staged and read as in conv_h_kernel. Same arithmetic and K order as
 // conv_h_kernel on the upsampled map.
 __host__ __device__ inline size_t conv_up_smem(int cpa, int cp, int co, bool gated) {
-    const int ntl = (co + 7) / 8, th = 8 * conv_h_rows(ntl);
+    const int ntl = (co + 7) / 8, th = 8 * conv_up_rows(ntl);
     const size_t abox = (size_t)(th / 2 + 2) * (CM_TX / 2 + 2) * (cpa + 8);
     const size_t bbox = (size_t)(th + 2) * (CM_TX + 2) * (cp - cpa + 8);
     return (abox + bbox + (size_t)ntl * 8 * 9 * cp + (gated ? (size_t)th * CM_TX * ntl * 8 : 0)) * 2;
@@ -534,7 +538,7 @@ __host__ __device__ inline size_t conv_up_smem(int cpa, int cp, int co, bool gat
 template <int NTL, int CP, int CPA>
 __global__ void __launch_bounds__(CM_NT, 2) conv_up_kernel(ConvH p) {
     if (p.done && *p.done) return;
-    constexpr int RW = conv_h_rows(NTL), TH = 8 * RW;
+    constexpr int RW = conv_up_rows(NTL), TH = 8 * RW;
     constexpr int EW = CM_TX + 2, EH = TH + 2, CEW = CM_TX / 2 + 2, CEH = TH / 2 + 2;
     constexpr int CPB = CP - CPA, PSA = CPA + 8, PSB = CPB + 8, KP = 9 * CP;
     constexpr int GA = CPA / 8, GB = CPB / 8, UA = CEH * CEW * GA, UB = EH * EW * GB;

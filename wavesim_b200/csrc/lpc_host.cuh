@@ -403,9 +403,11 @@ struct LpcNet {
         }
         if (amode == CM_UP && kk == 9 && ca % 16 == 0 && b) {  // the coarse-box decoder kernel
             const size_t smem = conv_up_smem(ca, cp, 8 * nt, gate != nullptr);
+            const int thu = 8 * conv_up_rows(nt);
+            const dim3 grid_up((p.W + CM_TX - 1) / CM_TX, (p.H + thu - 1) / thu, N);
 #define CONV_UP_LAUNCH(NT_, CP_, CPA_)                                          \
             if (!launched && nt == NT_ && cp == CP_ && ca == CPA_ && smem <= CONV_MMA_SMEM_MAX) { \
-                conv_up_kernel<NT_, CP_, CPA_><<<grid, CM_NT, smem, st>>>(p);    \
+                conv_up_kernel<NT_, CP_, CPA_><<<grid_up, CM_NT, smem, st>>>(p); \
                 launched = true;                                                 \
             }
             CONV_UP_FOR_ALL(CONV_UP_LAUNCH)
