@@ -719,6 +719,120 @@ __global__ void __launch_bounds__(CM_NT, 2) conv_p8_kernel(ConvH p) {
     conv_h_epilogue<NTL, RW>(p, acc, g_s, n, x0, y0);
 }
 
+// conv_up_kernel for an 8-channel skip map b: the b-part takes two taps per K step as in
+// conv_p8_kernel (its box unpadded, 16 bytes a pixel), after the coarse a-part. Weights in the
+// order [co][9 CPA + P8_KP]: the a-part by tap and channel, then the b-part's tap pairs.
+__global__ void conv_up8_weights_kernel(const float* __restrict__ w, int co_n, int cpa, int ntl,
+                                        unsigned short* __restrict__ out) {
+    const int kp = 9 * cpa + P8_KP, ci = cpa + 8;
+    const int total = ntl * 8 * kp;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < total; q += gridDim.x * blockDim.x) {
+        const int co = q / kp, k = q % kp;
+        int tap, c;
+        if (k < 9 * cpa) {
+            tap = k / cpa;
+            c = k % cpa;
+        } else {
+            tap = (k - 9 * cpa) / 8;
+            c = cpa + (k - 9 * cpa) % 8;
+        }
+        out[q] = (co < co_n && tap < 9) ? (unsigned short)(__float_as_uint(w[((size_t)co * ci + c) * 9 + tap]) >> 16)
+                                        : (unsigned short)0;
+    }
+}
+
+__host__ __device__ inline size_t conv_up8_smem(int cpa, int co, bool gated) {
+    const int ntl = (co + 7) / 8, th = 8 * conv_up_rows(ntl);
+    const size_t abox = (size_t)(th / 2 + 2) * (CM_TX / 2 + 2) * (cpa + 8);
+    const size_t bbox = (size_t)(th + 2) * (CM_TX + 2) * 8;
+    return (abox + bbox + (size_t)ntl * 8 * (9 * cpa + P8_KP) + (gated ? (size_t)th * CM_TX * ntl * 8 : 0)) * 2;
+}
+
+template <int NTL, int CPA>
+__global__ void __launch_bounds__(CM_NT, 2) conv_up8_kernel(ConvH p) {
+    if (p.done && *p.done) return;
+    constexpr int RW = conv_up_rows(NTL), TH = 8 * RW;
+    constexpr int EW = CM_TX + 2, EH = TH + 2, CEW = CM_TX / 2 + 2, CEH = TH / 2 + 2;
+    constexpr int PSA = CPA + 8, KP = 9 * CPA + P8_KP, GA = CPA / 8, UA = CEH * CEW * GA, UB = EH * EW;
+    extern __shared__ __align__(16) unsigned short cm_smem[];
+    unsigned short* a_s = cm_smem;                // [CEH][CEW][PSA]
+    unsigned short* b_s = a_s + CEH * CEW * PSA;   // [EH][EW][8]
+    unsigned short* w_s = b_s + EH * EW * 8;       // [8 NTL][KP]
+    unsigned short* g_s = w_s + 8 * NTL * KP;      // gated layers: [TH][16][co]
+    const int n = blockIdx.z;
+    const int x0 = blockIdx.x * CM_TX, y0 = blockIdx.y * TH;
+    const int Hc = p.H / 2, Wc = p.W / 2;
+    const int cx0 = (x0 >> 1) - 1, cy0 = (y0 >> 1) - 1;
+    {
+        const uint4* src = reinterpret_cast<const uint4*>(p.wre);
+        uint4* dst = reinterpret_cast<uint4*>(w_s);
+        for (int q = threadIdx.x; q < NTL * KP; q += CM_NT) cp_async16(dst + q, src + q, 16);
+    }
+    if (p.gate) {
+        const int gg = p.co / 8;
+        for (int q = threadIdx.x; q < TH * CM_TX * gg; q += CM_NT) {
+            const int pix = q / gg, c0 = (q - pix * gg) * 8;
+            const int y = y0 + pix / CM_TX, x = x0 + pix % CM_TX;
+            const bool in = y < p.H && x < p.W;
+            cp_async16(g_s + pix * p.co + c0, in ? p.gate + ((n * p.H + y) * p.W + x) * p.co + c0 : p.gate, in ? 16 : 0);
+        }
+    }
+    for (int q = threadIdx.x; q < UA; q += CM_NT) {  // the coarse box of a
+        const int r = q / GA, c0 = (q % GA) * 8;
+        const int cy = cy0 + r / CEW, cx = cx0 + r % CEW;
+        const bool in = (unsigned)cy < (unsigned)Hc && (unsigned)cx < (unsigned)Wc;
+        cp_async16(a_s + r * PSA + c0, in ? p.a + ((n * Hc + cy) * Wc + cx) * p.ca + c0 : p.a, in ? 16 : 0);
+    }
+    for (int q = threadIdx.x; q < UB; q += CM_NT) {  // the fine box of b, 8 channels
+        const int yy = y0 + q / EW - 1, xx = x0 + q % EW - 1;
+        const bool in = (unsigned)yy < (unsigned)p.H && (unsigned)xx < (unsigned)p.W;
+        cp_async16(b_s + q * 8, in ? p.b + ((n * p.H + yy) * p.W + xx) * 8 : p.b, in ? 16 : 0);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int grp = lane >> 2, tig = lane & 3;
+    const int lpix = (lane & 7) + ((lane >> 3) & 1) * 8, lk = (lane >> 4) * 8, second = lane >> 4;
+    float acc[RW][NTL][4];
+#pragma unroll
+    for (int r = 0; r < RW; r++)
+#pragma unroll
+        for (int t = 0; t < NTL; t++)
+#pragma unroll
+            for (int e = 0; e < 4; e++) acc[r][t][e] = 0.f;
+    auto step = [&](int kb, auto addr) {
+        unsigned b[NTL][2];
+#pragma unroll
+        for (int t = 0; t < NTL; t++) {
+            const unsigned* wrow = reinterpret_cast<const unsigned*>(w_s + (t * 8 + grp) * KP + kb + tig * 2);
+            b[t][0] = wrow[0];
+            b[t][1] = wrow[4];
+        }
+#pragma unroll
+        for (int r = 0; r < RW; r++) {
+            unsigned a[4];
+            ldmatrix_x4(a, addr(r));
+#pragma unroll
+            for (int t = 0; t < NTL; t++) mma_bf16_16816(acc[r][t], a, b[t]);
+        }
+    };
+#pragma unroll 3
+    for (int tap = 0; tap < 9; tap++) {  // a: the upsampled coarse map
+        const int dy = tap / 3, dx = tap % 3;
+        const int ccol = (lpix + dx + 1) >> 1;
+#pragma unroll
+        for (int cb = 0; cb < CPA; cb += 16)
+            step(tap * CPA + cb, [&](int r) { return a_s + (((warp * RW + r + dy + 1) >> 1) * CEW + ccol) * PSA + cb + lk; });
+    }
+#pragma unroll
+    for (int j = 0; j < 5; j++) {  // b: two taps per K step
+        const int tap = min(2 * j + second, 8);
+        const int dy = tap / 3, dx = tap - 3 * (tap / 3);
+        step(9 * CPA + j * 16, [&](int r) { return b_s + ((warp * RW + r + dy) * EW + lpix + dx) * 8; });
+    }
+    conv_h_epilogue<NTL, RW>(p, acc, g_s, n, x0, y0);
+}
+
 // NCHW FP32 maps -> NHWC BF16 (c channels, 2 or a multiple of 2).
 __global__ void to_h_kernel(const float* __restrict__ x, int N, int C, int H, int W, unsigned short* __restrict__ y) {
     const size_t plane = (size_t)H * W, total = (size_t)N * plane * (C / 2);

@@ -44,6 +44,8 @@ constexpr int CONV_H_CP_MAX = 64;
 #define CONV_UP_FOR_ALL(X) X(1, 32, 16) X(2, 32, 16) X(2, 48, 32) X(4, 48, 32) X(4, 64, 32) X(8, 64, 32)
 // The 8-channel-input convolutions with two taps per K step: output tiles.
 #define CONV_P8_FOR_ALL(X) X(1) X(2) X(4)
+// The decoder kernels over concat(up(a), an 8-channel b): output tiles x channels of a.
+#define CONV_UP8_FOR_ALL(X) X(1, 16) X(1, 32) X(2, 16)
 
 inline cudaError_t conv_mma_configure() {
     static cudaError_t st = cudaErrorNotReady;
@@ -61,6 +63,9 @@ inline cudaError_t conv_mma_configure() {
 #define CONV_P8_PTR(NT_) (const void*)conv_p8_kernel<NT_>,
                             CONV_P8_FOR_ALL(CONV_P8_PTR)
 #undef CONV_P8_PTR
+#define CONV_UP8_PTR(NT_, CPA_) (const void*)conv_up8_kernel<NT_, CPA_>,
+                            CONV_UP8_FOR_ALL(CONV_UP8_PTR)
+#undef CONV_UP8_PTR
         };
         st = cudaSuccess;
         for (const void* k : ks)
@@ -112,6 +117,8 @@ struct LpcNet {
     std::vector<int> wre_key;
     std::vector<size_t> wp8_off;  // 3x3 layers of 8 input channels: the two-taps-per-step order
     std::vector<int> wp8_key;
+    std::vector<size_t> wu8_off;  // decoder layers over concat(up(a), 8-channel b): the up8 order
+    std::vector<int> wu8_key, wu8_cpa;
 
     // Inference on NHWC BF16 activations (conv_h_kernel): every channel count a multiple of 8
     // and every layer's tile within the shared-memory limit; set by configure_nhwc.
@@ -191,9 +198,29 @@ struct LpcNet {
                 wp8_off.push_back(total);
                 total += (size_t)mma_tiles(l->co) * 8 * P8_KP;
             }
+        wu8_off.clear();
+        wu8_key.clear();
+        wu8_cpa.clear();
+        for (int l = 0; l + 1 < LPC_LEVELS; l++) {  // dec_a[l]: ch[l + 1] upsampled channels, then ch[l]
+            const LpcLayer& d = dec_a[l];
+            if (d.co > 0 && ch[l] == 8 && ch[l + 1] % 16 == 0) {
+                wu8_key.push_back(d.w);
+                wu8_cpa.push_back(ch[l + 1]);
+                wu8_off.push_back(total);
+                total += (size_t)mma_tiles(d.co) * 8 * (9 * ch[l + 1] + P8_KP);
+            }
+        }
         cudaError_t e = wre.alloc((total + 1) / 2 + 8);
         if (e != cudaSuccess) return e;
         auto* base = reinterpret_cast<unsigned short*>(wre.p);
+        for (size_t n = 0; n < wu8_key.size(); n++) {
+            const LpcLayer* l = nullptr;
+            for (auto* c : all)
+                if (c->w == wu8_key[n]) l = c;
+            const int cnt = mma_tiles(l->co) * 8 * (9 * wu8_cpa[n] + P8_KP);
+            conv_up8_weights_kernel<<<ew_grid(cnt), 256, 0, st>>>(wq + l->w, l->co, wu8_cpa[n], mma_tiles(l->co),
+                                                                  base + wu8_off[n]);
+        }
         for (size_t n = 0; n < all.size(); n++) {
             const LpcLayer* l = all[n];
             const int cnt = mma_tiles(l->co) * 8 * l->k * l->k * conv_mma_cp(l->ci);
@@ -213,6 +240,11 @@ struct LpcNet {
     const unsigned short* wre_of(const LpcLayer& L) const {
         for (size_t n = 0; n < wre_key.size(); n++)
             if (wre_key[n] == L.w) return reinterpret_cast<const unsigned short*>(wre.p) + wre_off[n];
+        return nullptr;
+    }
+    const unsigned short* wu8_of(const LpcLayer& L) const {
+        for (size_t n = 0; n < wu8_key.size(); n++)
+            if (wu8_key[n] == L.w) return reinterpret_cast<const unsigned short*>(wre.p) + wu8_off[n];
         return nullptr;
     }
     const unsigned short* wp8_of(const LpcLayer& L) const {
@@ -398,6 +430,21 @@ struct LpcNet {
             }
             CONV_P8_FOR_ALL(CONV_P8_LAUNCH)
 #undef CONV_P8_LAUNCH
+            if (launched) return cudaGetLastError();
+            p.wre = wre_of(L);
+        }
+        if (amode == CM_UP && kk == 9 && ca % 16 == 0 && cb == 8 && b && wu8_of(L)) {  // 8-channel skip
+            const size_t smem = conv_up8_smem(ca, 8 * nt, gate != nullptr);
+            const int thu = 8 * conv_up_rows(nt);
+            const dim3 grid_up((p.W + CM_TX - 1) / CM_TX, (p.H + thu - 1) / thu, N);
+            p.wre = wu8_of(L);
+#define CONV_UP8_LAUNCH(NT_, CPA_)                                              \
+            if (!launched && nt == NT_ && ca == CPA_ && smem <= CONV_MMA_SMEM_MAX) {  \
+                conv_up8_kernel<NT_, CPA_><<<grid_up, CM_NT, smem, st>>>(p);     \
+                launched = true;                                                 \
+            }
+            CONV_UP8_FOR_ALL(CONV_UP8_LAUNCH)
+#undef CONV_UP8_LAUNCH
             if (launched) return cudaGetLastError();
             p.wre = wre_of(L);
         }
