@@ -85,6 +85,14 @@ def run_ensemble(args, world, rank, local):
     from wavesim_b200 import Ensemble, Solver
 
     torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
     ws = W.config4(seed=4 + 1000 * rank)
     cells = sum(w.interior_cells() for w in ws)
     ens = Ensemble([w.solver(Solver) for w in ws])
@@ -99,6 +107,8 @@ def run_ensemble(args, world, rank, local):
     torch.cuda.synchronize()
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
     times = []
+    if dist:
+        dist.barrier()
     with ClockSampler(local) as clocks:
         for _ in range(args.steps):
             flush.zero_()
@@ -109,8 +119,8 @@ def run_ensemble(args, world, rank, local):
             times.append(time.perf_counter() - t0)
     it1 = [ens.member_stats(m)[0] for m in range(len(ws))]
     iters = sum(b.iterations - a.iterations for a, b in zip(it0, it1)) / max(1, sum(b.solves - a.solves for a, b in zip(it0, it1)))
-    total = sum(times)
-    value = cells * args.steps * world / total
+    total = rank_max(sum(times), dist)  # the slowest rank's time
+    value = rank_sum(float(cells), dist) * args.steps / total  # every rank's members
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -126,6 +136,9 @@ def run_ensemble(args, world, rank, local):
             "clocks": clocks.summary(),
         }
         print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 def measured_peaks():
@@ -198,6 +211,29 @@ class ClockSampler:
                     reasons.add(name)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
                 "samples": len(sm)}
+
+
+def rank_max(value: float, dist=None, device: str = "cuda") -> float:
+    """The largest of one value per rank (timings: the slowest rank's), or the value itself on
+    one rank. `device` is where the collective's tensor lives (cuda for NCCL, cpu for gloo)."""
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def rank_sum(value: float, dist=None, device: str = "cuda") -> float:
+    """The sum of one value per rank (work done by all ranks), or the value itself on one rank."""
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
 
 
 def dist_setup():
@@ -326,11 +362,9 @@ def measure_arm(w, args, world, stream, flush, net=None):
     prof = sol.profile_read()
     sol.profile(False)
     st2 = sol.dispersion_stats()
-    t = torch.tensor([sum(step_ms)], dtype=torch.float64, device="cuda")
+    total_ms_max = rank_max(sum(step_ms), dist)
     if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dist.barrier()
-    total_ms_max = float(t.item())
     cells = w.interior_cells()
 
     # end to end through the reference-facing call, pinned host FP64 arrays
@@ -349,9 +383,7 @@ def measure_arm(w, args, world, stream, flush, net=None):
     for _ in range(n_e2e):
         e2e_sol.step(hs, dt)
     e2e_s = time.perf_counter() - t0
-    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_max = rank_max(e2e_s, dist)
     per_solve = lambda a, b: (b.iterations - a.iterations) / max(1, b.solves - a.solves) if b else 0.0  # noqa: E731
     return {
         "value": cells * args.steps * world / (total_ms_max / 1e3),
@@ -362,7 +394,7 @@ def measure_arm(w, args, world, stream, flush, net=None):
         "prof": prof,
         "launches": int(launches),
         "clocks": clocks.summary(),
-        "e2e": {"value": cells * n_e2e * world / float(te.item()), "unit": UNIT,
+        "e2e": {"value": cells * n_e2e * world / e2e_max, "unit": UNIT,
                 "h2d_bytes_per_step": 3 * w.grid.cells() * 8, "d2h_bytes_per_step": 3 * w.grid.cells() * 8,
                 "steps": n_e2e, "path": "wc_step on pinned host FP64 arrays (upload, step, download per call)"},
     }
