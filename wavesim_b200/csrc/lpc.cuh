@@ -307,6 +307,43 @@ __device__ __forceinline__ void ldmatrix_x4(unsigned* r, const void* row) {
                  : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
                  : "r"(sa));
 }
+__device__ __forceinline__ void ldmatrix_x2(unsigned* r, const void* row) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(row);
+    asm volatile("ldmatrix.sync.aligned.m8n8.x2.shared.b16 {%0,%1}, [%2];\n" : "=r"(r[0]), "=r"(r[1]) : "r"(sa));
+}
+
+// The layer's weights ([8 NTL rows][KP], BF16) into shared memory with rows padded to KP + 8
+// halves: row starts then fall 4 banks apart, so the B-fragment reads are conflict-free.
+template <int NTL, int KP>
+__device__ __forceinline__ void stage_weights(unsigned short* w_s, const unsigned short* wre) {
+    constexpr int G = KP / 8;  // 16-byte groups a row
+    const uint4* src = reinterpret_cast<const uint4*>(wre);
+    for (int q = threadIdx.x; q < 8 * NTL * G; q += CM_NT) {
+        const int row = q / G, c = q - row * G;
+        cp_async16(w_s + row * (KP + 8) + c * 8, src + q, 16);
+    }
+}
+
+// B fragments of the NTL output tiles at K offset kb: ldmatrix on the [n][k] weight rows gives
+// (k = 2 tig, 2 tig + 1; n = grp) and its k + 8 partner directly; one x4 covers two tiles.
+template <int NTL, int KP>
+__device__ __forceinline__ void load_b(unsigned (&b)[NTL][2], const unsigned short* w_s, int kb, int lane) {
+    constexpr int WS = KP + 8;
+    const int koff = ((lane >> 3) & 1) * 8;
+    if constexpr (NTL == 1) {
+        ldmatrix_x2(b[0], w_s + (lane & 7) * WS + kb + koff);
+    } else {
+#pragma unroll
+        for (int t = 0; t < NTL; t += 2) {
+            unsigned r[4];
+            ldmatrix_x4(r, w_s + (t * 8 + ((lane >> 4) & 1) * 8 + (lane & 7)) * WS + kb + koff);
+            b[t][0] = r[0];
+            b[t][1] = r[1];
+            b[t + 1][0] = r[2];
+            b[t + 1][1] = r[3];
+        }
+    }
+}
 
 // Rows of 16 pixels per warp: tall tiles for the 8-channel layers (fewer halo cells and less
 // fixed work per pixel); shorter ones as the output widens, so that the accumulators leave room
@@ -322,7 +359,7 @@ __host__ __device__ inline size_t conv_h_smem2(int ci, int co, int kk, bool gate
     const int r = kk == 9 ? 1 : 0, cp = conv_mma_cp(ci), ntl = (co + 7) / 8;
     const int th = 8 * conv_h_rows(ntl);
     const size_t box = (size_t)(th + 2 * r) * (CM_TX + 2 * r) * conv_h_ps(cp);
-    return (box + (size_t)ntl * 8 * kk * cp + (gated ? (size_t)th * CM_TX * ntl * 8 : 0)) * 2;
+    return (box + (size_t)ntl * 8 * (kk * cp + 8) + (gated ? (size_t)th * CM_TX * ntl * 8 : 0)) * 2;
 }
 
 // The convolution's epilogue: bias, activation, gate (from the staged gate tile), and the BF16
@@ -426,16 +463,12 @@ __global__ void __launch_bounds__(CM_NT, 2) conv_h_kernel(ConvH p) {
     extern __shared__ __align__(16) unsigned short cm_smem[];
     unsigned short* in_s = cm_smem;             // [EH][EW][PS]
     unsigned short* w_s = cm_smem + EH * EW * PS;  // [8 NTL][KP]
-    unsigned short* g_s = w_s + 8 * NTL * KP;      // gated layers: [TH][16][co]
+    unsigned short* g_s = w_s + 8 * NTL * (KP + 8);      // gated layers: [TH][16][co]
     const int ci_total = p.ca + p.cb;
     const int n = blockIdx.z;
     const int x0 = blockIdx.x * CM_TX, y0 = blockIdx.y * TH;
     const bool two = p.ca == 2;
-    {
-        const uint4* src = reinterpret_cast<const uint4*>(p.wre);
-        uint4* dst = reinterpret_cast<uint4*>(w_s);
-        for (int q = threadIdx.x; q < NTL * KP; q += CM_NT) cp_async16(dst + q, src + q, 16);
-    }
+    stage_weights<NTL, KP>(w_s, p.wre);
     if (p.gate) {  // the tile's gate, in flight with the input box
         const int gg = p.co / 8;
         for (int q = threadIdx.x; q < TH * CM_TX * gg; q += CM_NT) {
@@ -488,7 +521,6 @@ __global__ void __launch_bounds__(CM_NT, 2) conv_h_kernel(ConvH p) {
     cp_async_wait_all();
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int grp = lane >> 2, tig = lane & 3;
     const int lpix = (lane & 7) + ((lane >> 3) & 1) * 8, lk = (lane >> 4) * 8;  // ldmatrix row of this lane
     float acc[RW][NTL][4];
 #pragma unroll
@@ -504,12 +536,7 @@ __global__ void __launch_bounds__(CM_NT, 2) conv_h_kernel(ConvH p) {
         for (int cb = 0; cb < CP; cb += 16) {
             const int kb = tap * CP + cb;
             unsigned b[NTL][2];
-#pragma unroll
-            for (int t = 0; t < NTL; t++) {
-                const unsigned* wrow = reinterpret_cast<const unsigned*>(w_s + (t * 8 + grp) * KP + kb + tig * 2);
-                b[t][0] = wrow[0];
-                b[t][1] = wrow[4];
-            }
+            load_b<NTL, KP>(b, w_s, kb, lane);
 #pragma unroll
             for (int r = 0; r < RW; r++) {
                 unsigned a[4];
@@ -532,7 +559,7 @@ __host__ __device__ inline size_t conv_up_smem(int cpa, int cp, int co, bool gat
     const int ntl = (co + 7) / 8, th = 8 * conv_up_rows(ntl);
     const size_t abox = (size_t)(th / 2 + 2) * (CM_TX / 2 + 2) * (cpa + 8);
     const size_t bbox = (size_t)(th + 2) * (CM_TX + 2) * (cp - cpa + 8);
-    return (abox + bbox + (size_t)ntl * 8 * 9 * cp + (gated ? (size_t)th * CM_TX * ntl * 8 : 0)) * 2;
+    return (abox + bbox + (size_t)ntl * 8 * (9 * cp + 8) + (gated ? (size_t)th * CM_TX * ntl * 8 : 0)) * 2;
 }
 
 template <int NTL, int CP, int CPA>
@@ -546,16 +573,12 @@ __global__ void __launch_bounds__(CM_NT, 2) conv_up_kernel(ConvH p) {
     unsigned short* a_s = cm_smem;               // [CEH][CEW][PSA]
     unsigned short* b_s = a_s + CEH * CEW * PSA;  // [EH][EW][PSB]
     unsigned short* w_s = b_s + EH * EW * PSB;    // [8 NTL][KP]
-    unsigned short* g_s = w_s + 8 * NTL * KP;     // gated layers: [TH][16][co]
+    unsigned short* g_s = w_s + 8 * NTL * (KP + 8);     // gated layers: [TH][16][co]
     const int n = blockIdx.z;
     const int x0 = blockIdx.x * CM_TX, y0 = blockIdx.y * TH;
     const int Hc = p.H / 2, Wc = p.W / 2;
     const int cx0 = (x0 >> 1) - 1, cy0 = (y0 >> 1) - 1;
-    {
-        const uint4* src = reinterpret_cast<const uint4*>(p.wre);
-        uint4* dst = reinterpret_cast<uint4*>(w_s);
-        for (int q = threadIdx.x; q < NTL * KP; q += CM_NT) cp_async16(dst + q, src + q, 16);
-    }
+    stage_weights<NTL, KP>(w_s, p.wre);
     if (p.gate) {
         const int gg = p.co / 8;
         for (int q = threadIdx.x; q < TH * CM_TX * gg; q += CM_NT) {
@@ -580,7 +603,6 @@ __global__ void __launch_bounds__(CM_NT, 2) conv_up_kernel(ConvH p) {
     cp_async_wait_all();
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int grp = lane >> 2, tig = lane & 3;
     const int lpix = (lane & 7) + ((lane >> 3) & 1) * 8, lk = (lane >> 4) * 8;
     float acc[RW][NTL][4];
 #pragma unroll
@@ -597,12 +619,7 @@ __global__ void __launch_bounds__(CM_NT, 2) conv_up_kernel(ConvH p) {
         for (int cb = 0; cb < CP; cb += 16) {
             const int kb = tap * CP + cb;
             unsigned b[NTL][2];
-#pragma unroll
-            for (int t = 0; t < NTL; t++) {
-                const unsigned* wrow = reinterpret_cast<const unsigned*>(w_s + (t * 8 + grp) * KP + kb + tig * 2);
-                b[t][0] = wrow[0];
-                b[t][1] = wrow[4];
-            }
+            load_b<NTL, KP>(b, w_s, kb, lane);
 #pragma unroll
             for (int r = 0; r < RW; r++) {
                 const int frow = warp * RW + r + dy;  // fine box row
@@ -637,7 +654,7 @@ __global__ void conv_p8_weights_kernel(const float* __restrict__ w, int co_n, in
 
 __host__ __device__ inline size_t conv_p8_smem(int co, bool gated) {
     const int ntl = (co + 7) / 8, th = 8 * conv_h_rows(ntl);
-    return ((size_t)(th + 2) * (CM_TX + 2) * 8 + (size_t)ntl * 8 * P8_KP + (gated ? (size_t)th * CM_TX * ntl * 8 : 0)) * 2;
+    return ((size_t)(th + 2) * (CM_TX + 2) * 8 + (size_t)ntl * 8 * (P8_KP + 8) + (gated ? (size_t)th * CM_TX * ntl * 8 : 0)) * 2;
 }
 
 template <int NTL>
@@ -647,14 +664,10 @@ __global__ void __launch_bounds__(CM_NT, 2) conv_p8_kernel(ConvH p) {
     extern __shared__ __align__(16) unsigned short cm_smem[];
     unsigned short* in_s = cm_smem;           // [EH][EW][8]
     unsigned short* w_s = in_s + UNITS * 8;   // [8 NTL][P8_KP]
-    unsigned short* g_s = w_s + 8 * NTL * P8_KP;
+    unsigned short* g_s = w_s + 8 * NTL * (P8_KP + 8);
     const int n = blockIdx.z;
     const int x0 = blockIdx.x * CM_TX, y0 = blockIdx.y * TH;
-    {
-        const uint4* src = reinterpret_cast<const uint4*>(p.wre);
-        uint4* dst = reinterpret_cast<uint4*>(w_s);
-        for (int q = threadIdx.x; q < NTL * P8_KP; q += CM_NT) cp_async16(dst + q, src + q, 16);
-    }
+    stage_weights<NTL, P8_KP>(w_s, p.wre);
     if (p.gate) {
         const int gg = p.co / 8;
         for (int q = threadIdx.x; q < TH * CM_TX * gg; q += CM_NT) {
@@ -688,7 +701,6 @@ __global__ void __launch_bounds__(CM_NT, 2) conv_p8_kernel(ConvH p) {
     cp_async_wait_all();
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int grp = lane >> 2, tig = lane & 3;
     const int lpix = (lane & 7) + ((lane >> 3) & 1) * 8, second = lane >> 4;  // ldmatrix row: pixel, which tap
     float acc[RW][NTL][4];
 #pragma unroll
@@ -702,12 +714,7 @@ __global__ void __launch_bounds__(CM_NT, 2) conv_p8_kernel(ConvH p) {
         const int tap = min(2 * j + second, 8);  // the ninth tap's partner: zero weights
         const int dy = tap / 3, dx = tap - 3 * (tap / 3);
         unsigned b[NTL][2];
-#pragma unroll
-        for (int t = 0; t < NTL; t++) {
-            const unsigned* wrow = reinterpret_cast<const unsigned*>(w_s + (t * 8 + grp) * P8_KP + j * 16 + tig * 2);
-            b[t][0] = wrow[0];
-            b[t][1] = wrow[4];
-        }
+        load_b<NTL, P8_KP>(b, w_s, j * 16, lane);
 #pragma unroll
         for (int r = 0; r < RW; r++) {
             unsigned a[4];
@@ -745,7 +752,7 @@ __host__ __device__ inline size_t conv_up8_smem(int cpa, int co, bool gated) {
     const int ntl = (co + 7) / 8, th = 8 * conv_up_rows(ntl);
     const size_t abox = (size_t)(th / 2 + 2) * (CM_TX / 2 + 2) * (cpa + 8);
     const size_t bbox = (size_t)(th + 2) * (CM_TX + 2) * 8;
-    return (abox + bbox + (size_t)ntl * 8 * (9 * cpa + P8_KP) + (gated ? (size_t)th * CM_TX * ntl * 8 : 0)) * 2;
+    return (abox + bbox + (size_t)ntl * 8 * (9 * cpa + P8_KP + 8) + (gated ? (size_t)th * CM_TX * ntl * 8 : 0)) * 2;
 }
 
 template <int NTL, int CPA>
@@ -758,16 +765,12 @@ __global__ void __launch_bounds__(CM_NT, 2) conv_up8_kernel(ConvH p) {
     unsigned short* a_s = cm_smem;                // [CEH][CEW][PSA]
     unsigned short* b_s = a_s + CEH * CEW * PSA;   // [EH][EW][8]
     unsigned short* w_s = b_s + EH * EW * 8;       // [8 NTL][KP]
-    unsigned short* g_s = w_s + 8 * NTL * KP;      // gated layers: [TH][16][co]
+    unsigned short* g_s = w_s + 8 * NTL * (KP + 8);      // gated layers: [TH][16][co]
     const int n = blockIdx.z;
     const int x0 = blockIdx.x * CM_TX, y0 = blockIdx.y * TH;
     const int Hc = p.H / 2, Wc = p.W / 2;
     const int cx0 = (x0 >> 1) - 1, cy0 = (y0 >> 1) - 1;
-    {
-        const uint4* src = reinterpret_cast<const uint4*>(p.wre);
-        uint4* dst = reinterpret_cast<uint4*>(w_s);
-        for (int q = threadIdx.x; q < NTL * KP; q += CM_NT) cp_async16(dst + q, src + q, 16);
-    }
+    stage_weights<NTL, KP>(w_s, p.wre);
     if (p.gate) {
         const int gg = p.co / 8;
         for (int q = threadIdx.x; q < TH * CM_TX * gg; q += CM_NT) {
@@ -791,7 +794,6 @@ __global__ void __launch_bounds__(CM_NT, 2) conv_up8_kernel(ConvH p) {
     cp_async_wait_all();
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int grp = lane >> 2, tig = lane & 3;
     const int lpix = (lane & 7) + ((lane >> 3) & 1) * 8, lk = (lane >> 4) * 8, second = lane >> 4;
     float acc[RW][NTL][4];
 #pragma unroll
@@ -802,12 +804,7 @@ __global__ void __launch_bounds__(CM_NT, 2) conv_up8_kernel(ConvH p) {
             for (int e = 0; e < 4; e++) acc[r][t][e] = 0.f;
     auto step = [&](int kb, auto addr) {
         unsigned b[NTL][2];
-#pragma unroll
-        for (int t = 0; t < NTL; t++) {
-            const unsigned* wrow = reinterpret_cast<const unsigned*>(w_s + (t * 8 + grp) * KP + kb + tig * 2);
-            b[t][0] = wrow[0];
-            b[t][1] = wrow[4];
-        }
+        load_b<NTL, KP>(b, w_s, kb, lane);
 #pragma unroll
         for (int r = 0; r < RW; r++) {
             unsigned a[4];
