@@ -636,6 +636,9 @@ __global__ void __launch_bounds__(CM_NT, 2) conv_up_kernel(ConvH p) {
 
 // ---- 3x3 convolutions of an 8-channel input: two taps per K step ---------------------------
 //
+// (A two-channel input, the network's own and the gates' features, takes the same kernel with
+// its channels zero-padded to 8 in the box: 5 K steps instead of 9 channel-padded ones.)
+//
 // With 8 input channels a K step of 16 holds two taps (k = tap * 8 + c; the ninth tap's partner
 // has zero weights), so the halo box needs no channel padding (16 bytes a pixel) and a layer
 // takes 5 K steps instead of 9: ldmatrix lanes 0-15 address the pixels of the first tap, lanes
@@ -643,12 +646,14 @@ __global__ void __launch_bounds__(CM_NT, 2) conv_up_kernel(ConvH p) {
 // order of the sum.
 constexpr int P8_KP = 80;  // 9 taps x 8 channels, padded to a multiple of 16
 
-__global__ void conv_p8_weights_kernel(const float* __restrict__ w, int co_n, int ntl, unsigned short* __restrict__ out) {
+__global__ void conv_p8_weights_kernel(const float* __restrict__ w, int co_n, int ci_n, int ntl,
+                                       unsigned short* __restrict__ out) {  // ci_n: 8, or 2 (zero-padded)
     const int total = ntl * 8 * P8_KP;
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < total; q += gridDim.x * blockDim.x) {
         const int co = q / P8_KP, k = q % P8_KP, tap = k / 8, c = k % 8;
-        out[q] = (co < co_n && tap < 9) ? (unsigned short)(__float_as_uint(w[((size_t)co * 8 + c) * 9 + tap]) >> 16)
-                                        : (unsigned short)0;
+        out[q] = (co < co_n && tap < 9 && c < ci_n)
+                     ? (unsigned short)(__float_as_uint(w[((size_t)co * ci_n + c) * 9 + tap]) >> 16)
+                     : (unsigned short)0;
     }
 }
 
@@ -684,7 +689,9 @@ __global__ void __launch_bounds__(CM_NT, 2) conv_p8_kernel(ConvH p) {
         const int yy = y0 + q / EW - 1, xx = x0 + q % EW - 1;
         const bool in = (unsigned)yy < (unsigned)p.H && (unsigned)xx < (unsigned)p.W;
         uint4* dst = reinterpret_cast<uint4*>(in_s + q * 8);
-        if (pool) {
+        if (p.ca == 2) {  // a two-channel input, zero-padded to 8 in the box
+            *dst = make_uint4(in ? __ldg(reinterpret_cast<const unsigned*>(p.a) + abase + yy * Ws + xx) : 0u, 0u, 0u, 0u);
+        } else if (pool) {
             uint4 v = make_uint4(0u, 0u, 0u, 0u);
             if (in) {
                 const uint4* w = reinterpret_cast<const uint4*>(p.a);

@@ -193,7 +193,7 @@ struct LpcNet {
         wp8_off.clear();
         wp8_key.clear();
         for (auto* l : all)
-            if (l->ci == 8 && l->k == 3) {
+            if ((l->ci == 8 || l->ci == 2) && l->k == 3) {
                 wp8_key.push_back(l->w);
                 wp8_off.push_back(total);
                 total += (size_t)mma_tiles(l->co) * 8 * P8_KP;
@@ -231,7 +231,7 @@ struct LpcNet {
             const LpcLayer* l = nullptr;
             for (auto* c : all)
                 if (c->w == wp8_key[n]) l = c;
-            conv_p8_weights_kernel<<<ew_grid(mma_tiles(l->co) * 8 * P8_KP), 256, 0, st>>>(wq + l->w, l->co,
+            conv_p8_weights_kernel<<<ew_grid(mma_tiles(l->co) * 8 * P8_KP), 256, 0, st>>>(wq + l->w, l->co, l->ci,
                                                                                           mma_tiles(l->co), base + wp8_off[n]);
         }
         return cudaGetLastError();
@@ -420,7 +420,8 @@ struct LpcNet {
         dim3 grid((p.W + CM_TX - 1) / CM_TX, (p.H + th - 1) / th, N);
         const int kk = L.k * L.k, cp = conv_mma_cp(L.ci);
         bool launched = false;
-        if (kk == 9 && ca == 8 && cb == 0 && amode != CM_UP && wp8_of(L)) {  // two taps per K step
+        if (kk == 9 && (ca == 8 || (ca == 2 && amode == CM_DIRECT)) && cb == 0 && amode != CM_UP &&
+            wp8_of(L)) {  // two taps per K step
             const size_t smem = conv_p8_smem(8 * nt, gate != nullptr);
             p.wre = wp8_of(L);
 #define CONV_P8_LAUNCH(NT_)                                               \
