@@ -487,8 +487,9 @@ def run_b200(args, world, rank, local):
             tflops = spec.flops_per_cell() * ncell / (avg_ms / 1e3) / 1e12
             gbs = spec.bytes_per_cell() * ncell / (avg_ms / 1e3) / 1e9
             bf16 = peak_tensor()
-            roof = {"bound": "hbm", "kernel": "conv_h_kernel chain (one network application: channels-innermost BF16 "
-                                              "mma.sync implicit-GEMM convolutions, FP32 accumulation)",
+            roof = {"bound": "hbm", "kernel": "network convolution chain (one application: conv_p8 / conv_h / conv_up / "
+                                              "conv_up8 kernels, channels-innermost BF16 mma.sync implicit GEMM, FP32 "
+                                              "accumulation)",
                     "achieved": gbs, "unit": "GB/s", "peak": peak, "frac": gbs / peak, "peak_source": peak_kind,
                     "algorithmic_bytes_per_cell": spec.bytes_per_cell(), "flops_per_cell": spec.flops_per_cell(),
                     "avg_ms": avg_ms, "tensor_tflops": tflops, "tensor_frac": tflops / bf16[0],
