@@ -294,7 +294,7 @@ uint64_t wc_ensemble_launch_count(const wc_ensemble* e);
  *     z1 = w r / D,  z2 = z1 + mask N(D^-1 (r - A z1)),  z = z2 + w (r - A z2) / D   (w = 0.5)
  * as the preconditioner of flexible CG, with the Jacobi solve's stopping rule; a solve that does
  * not converge (or breaks down) is finished by Jacobi PCG from where it stopped, so the plain
- * method stays the fallback and the judge of convergence. Training runs on
+ * method stays the fallback and the arbiter of convergence. Training runs on
  * the GPU by the library's own forward and backward kernels, on patches of SGN systems harvested
  * from solver runs, minimising the energy norm of the cycle's error on random error fields. */
 typedef struct wc_lpc wc_lpc;
