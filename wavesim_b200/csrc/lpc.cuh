@@ -274,6 +274,7 @@ struct ConvH {
     const int* done;            // or null: the solve this application serves has ended, skip it
     const float* out_w;         // or null: an 8-channel layer followed by the 2 x 8 1x1 output layer,
                                 // applied in the epilogue; yf then gets its FP32 output
+    const unsigned short* wre2; // conv_enc0_kernel: the second layer's weights (wre: the first's)
     int co, H, W, N, act;
 };
 
@@ -731,6 +732,99 @@ __global__ void __launch_bounds__(CM_NT, 2) conv_p8_kernel(ConvH p) {
         }
     }
     conv_h_epilogue<NTL, RW>(p, acc, g_s, n, x0, y0);
+}
+
+// The network's first two layers in one launch: a = conv3x3(x) over the 2-channel input (no bias,
+// no activation, 8 channels out) and y = conv3x3(a) * gate (8 -> 8). A block stages x over its
+// tile plus a halo of 2, computes a over the tile plus a halo of 1 into shared memory (rounded to
+// BF16, zero outside the map, exactly what the two-launch path stores and re-reads), then the
+// second layer from there: the 8-channel map a never goes through HBM. Both layers take two taps
+// per K step in conv_p8_kernel's order, so the result is bit-identical to the two launches.
+__host__ __device__ inline size_t conv_enc0_smem() {
+    constexpr int th = 8 * conv_h_rows(1);
+    return ((size_t)(th + 4) * (CM_TX + 4) * 8 + (size_t)(th + 2) * (CM_TX + 2) * 8 + 2 * (size_t)8 * (P8_KP + 8) +
+            (size_t)th * CM_TX * 8) * 2;
+}
+
+__global__ void __launch_bounds__(CM_NT, 2) conv_enc0_kernel(ConvH p) {
+    if (p.done && *p.done) return;
+    constexpr int RW = conv_h_rows(1), TH = 8 * RW;
+    constexpr int XW = CM_TX + 4, XH = TH + 4;  // x: tile + halo 2
+    constexpr int AW = CM_TX + 2, AH = TH + 2;  // a: tile + halo 1
+    constexpr int NA = AW * AH, MB = (NA + 15) / 16;
+    extern __shared__ __align__(16) unsigned short cm_smem[];
+    unsigned short* x_s = cm_smem;                  // [XH][XW][8], channels 2-7 zero
+    unsigned short* a_s = x_s + XH * XW * 8;        // [AH][AW][8]
+    unsigned short* w1_s = a_s + AH * AW * 8;       // [8][P8_KP + 8]
+    unsigned short* w2_s = w1_s + 8 * (P8_KP + 8);  // [8][P8_KP + 8]
+    unsigned short* g_s = w2_s + 8 * (P8_KP + 8);   // [TH CM_TX][8]
+    const int n = blockIdx.z;
+    const int x0 = blockIdx.x * CM_TX, y0 = blockIdx.y * TH;
+    stage_weights<1, P8_KP>(w1_s, p.wre);
+    stage_weights<1, P8_KP>(w2_s, p.wre2);
+    for (int q = threadIdx.x; q < TH * CM_TX; q += CM_NT) {
+        const int y = y0 + q / CM_TX, x = x0 + q % CM_TX;
+        const bool in = y < p.H && x < p.W;
+        cp_async16(g_s + q * 8, in ? p.gate + ((n * p.H + y) * p.W + x) * 8 : p.gate, in ? 16 : 0);
+    }
+    const unsigned* xa = reinterpret_cast<const unsigned*>(p.a);  // a pixel's two BF16 channels
+    for (int q = threadIdx.x; q < XH * XW; q += CM_NT) {
+        const int yy = y0 + q / XW - 2, xx = x0 + q % XW - 2;
+        const bool in = (unsigned)yy < (unsigned)p.H && (unsigned)xx < (unsigned)p.W;
+        *reinterpret_cast<uint4*>(x_s + q * 8) = make_uint4(in ? __ldg(xa + (n * p.H + yy) * p.W + xx) : 0u, 0u, 0u, 0u);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, grp = lane >> 2, tig = lane & 3;
+    const int lpix = (lane & 7) + ((lane >> 3) & 1) * 8, second = lane >> 4;  // ldmatrix row: pixel, which tap
+    {  // the first layer over the a box, 16 box pixels (row-major, across box rows) an MMA row block
+        unsigned b1[5][1][2];
+#pragma unroll
+        for (int j = 0; j < 5; j++) load_b<1, P8_KP>(b1[j], w1_s, j * 16, lane);
+        for (int mb = warp; mb < MB; mb += CM_NT / 32) {
+            const int m = min(mb * 16 + lpix, NA - 1);  // rows past the box repeat its last pixel
+            const int py = m / AW, px = m - py * AW;
+            float acc[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+            for (int j = 0; j < 5; j++) {
+                const int tap = min(2 * j + second, 8);
+                const int dy = tap / 3, dx = tap - 3 * (tap / 3);
+                unsigned fa[4];
+                ldmatrix_x4(fa, x_s + ((py + dy) * XW + px + dx) * 8);
+                mma_bf16_16816(acc, fa, b1[j][0]);
+            }
+#pragma unroll
+            for (int half = 0; half < 2; half++) {
+                const int mo = mb * 16 + grp + 8 * half;
+                if (mo >= NA) continue;
+                const int oy = y0 - 1 + mo / AW, ox = x0 - 1 + mo % AW;
+                const bool in = (unsigned)oy < (unsigned)p.H && (unsigned)ox < (unsigned)p.W;
+                // + 0: the epilogue's bias-free sum (a -0 sum stored as +0, as the two launches do)
+                reinterpret_cast<unsigned*>(a_s + mo * 8)[tig] =
+                    in ? bf16_pack(acc[2 * half] + 0.f, acc[2 * half + 1] + 0.f) : 0u;
+            }
+        }
+    }
+    __syncthreads();
+    float acc[RW][1][4];
+#pragma unroll
+    for (int r = 0; r < RW; r++)
+#pragma unroll
+        for (int e = 0; e < 4; e++) acc[r][0][e] = 0.f;
+#pragma unroll
+    for (int j = 0; j < 5; j++) {
+        const int tap = min(2 * j + second, 8);
+        const int dy = tap / 3, dx = tap - 3 * (tap / 3);
+        unsigned b[1][2];
+        load_b<1, P8_KP>(b, w2_s, j * 16, lane);
+#pragma unroll
+        for (int r = 0; r < RW; r++) {
+            unsigned fa[4];
+            ldmatrix_x4(fa, a_s + ((warp * RW + r + dy) * AW + lpix + dx) * 8);
+            mma_bf16_16816(acc[r][0], fa, b[0]);
+        }
+    }
+    conv_h_epilogue<1, RW>(p, acc, g_s, n, x0, y0);
 }
 
 // conv_up_kernel for an 8-channel skip map b: the b-part takes two taps per K step as in

@@ -66,6 +66,7 @@ inline cudaError_t conv_mma_configure() {
 #define CONV_UP8_PTR(NT_, CPA_) (const void*)conv_up8_kernel<NT_, CPA_>,
                             CONV_UP8_FOR_ALL(CONV_UP8_PTR)
 #undef CONV_UP8_PTR
+                            (const void*)conv_enc0_kernel,
         };
         st = cudaSuccess;
         for (const void* k : ks)
@@ -488,14 +489,49 @@ struct LpcNet {
 
     // The output layer rides in dec_b[0]'s epilogue when that layer has one tile of 8 channels.
     bool fused_out() const { return ch[0] == 8 && out.co == 2 && out.k == 1; }
+    // The first level's two encoder layers in one launch (conv_enc0_kernel) when both are 8-channel
+    // 3x3 layers in the two-taps order and the first has no bias (the network's form: linear, the
+    // second gated).
+    bool fused_enc0() const {
+        return ch[0] == 8 && enc_a[0].k == 3 && enc_a[0].ci == 2 && enc_a[0].b < 0 && enc_b[0].k == 3 && enc_b[0].ci == 8 &&
+               wp8_of(enc_a[0]) && wp8_of(enc_b[0]);
+    }
     // launches of forward_h()
-    int forward_h_launches() const { return 2 * LPC_LEVELS + 2 * (LPC_LEVELS - 1) + (fused_out() ? 0 : 1); }
+    int forward_h_launches() const {
+        return 2 * LPC_LEVELS + 2 * (LPC_LEVELS - 1) + (fused_out() ? 0 : 1) - (fused_enc0() ? 1 : 0);
+    }
+
+    // The first level's encoder through conv_enc0_kernel: Eh[0] = conv(conv(Xh)) * Gh[0].
+    cudaError_t enc0_h(cudaStream_t st) {
+        ConvH p{};
+        p.a = hp(Xh);
+        p.ca = 2;
+        p.amode = CM_DIRECT;
+        p.wre = wp8_of(enc_a[0]);
+        p.wre2 = wp8_of(enc_b[0]);
+        p.bias = enc_b[0].b >= 0 ? wq + enc_b[0].b : nullptr;
+        p.gate = hp(Gh[0]);
+        p.y = hp(Eh[0]);
+        p.done = done;
+        p.co = 8;
+        p.H = H;
+        p.W = W;
+        p.N = N;
+        p.act = ACT_NONE;
+        const dim3 grid((W + CM_TX - 1) / CM_TX, (H + 8 * conv_h_rows(1) - 1) / (8 * conv_h_rows(1)), N);
+        conv_enc0_kernel<<<grid, CM_NT, conv_enc0_smem(), st>>>(p);
+        return cudaGetLastError();
+    }
 
     // Yh = N(Xh) on NHWC BF16 activations with the gates already in Gh: the launches of forward()
     // (the output layer fused into the last when fused_out()).
     cudaError_t forward_h(cudaStream_t st) {
         cudaError_t e = cudaSuccess;
         for (int l = 0; l < LPC_LEVELS && e == cudaSuccess; l++) {
+            if (l == 0 && fused_enc0()) {
+                e = enc0_h(st);
+                continue;
+            }
             const int cin = l == 0 ? 2 : ch[l - 1];
             const unsigned short* in = l == 0 ? hp(Xh) : hp(Eh[l - 1]);
             e = conv_h(in, cin, l == 0 ? CM_DIRECT : CM_POOL, nullptr, 0, enc_a[l], nullptr, hp(Ah[l]), nullptr, l,
