@@ -92,23 +92,35 @@ class UNetSpec:
             f += 2.0 * co * ci * k * k / (4.0 ** level)
         return f
 
+    def fused_first_level(self) -> bool:
+        """The device computes the first level's two encoder layers in one launch (the map A
+        between them stays in shared memory) and the 1x1 output layer in the last decoder
+        layer's epilogue (D stays in registers) when the first level has 8 channels."""
+        return self.channels[0] == 8 and self.in_ch == 2 and self.out_ch == 2
+
     def bytes_per_cell(self) -> float:
         """Algorithmic DRAM bytes of one application per cell of the finest level, for the
         device's channels-innermost BF16 activations: every convolution reads each of its inputs
         and its gate once and writes its output once (a pooled input is read at the finer level,
-        an upsampled one at the coarser); the input is 2 BF16 channels, the output 2 FP32."""
+        an upsampled one at the coarser); the input is 2 BF16 channels, the output 2 FP32. Maps
+        that the device keeps on chip (`fused_first_level`) are not counted."""
         c, L, b = self.channels, self.levels, 2.0
+        fused = self.fused_first_level()
         per = [0.0] * L  # bytes per pixel of level l
         for l in range(L):
             cin = self.in_ch if l == 0 else c[l - 1]
             src = b * cin * (4.0 if l > 0 else 1.0)  # enc_a reads its input (pooled: 4 finer pixels)
-            per[l] += src + b * c[l]                 # ... and writes A
-            per[l] += 3 * b * c[l]                   # enc_b: A and the gate in, E out
+            a_io = 0.0 if (l == 0 and fused) else 2 * b * c[l]  # A written by enc_a, read by enc_b
+            per[l] += src + a_io + 2 * b * c[l]      # enc_b: the gate in, E out
         for l in range(L - 2, -1, -1):
             below = b * c[l + 1] / 4.0               # the upsampled map, read once at its level
             per[l] += below + b * c[l] + b * c[l]    # dec_a: up(below), E in, DA out
-            per[l] += 3 * b * c[l]                   # dec_b: DA and the gate in, D out
-        per[0] += b * c[0] + 4.0 * self.out_ch       # out: D in, FP32 output
+            per[l] += 2 * b * c[l]                   # dec_b: DA and the gate in ...
+            if l > 0:
+                per[l] += b * c[l]                   # ... D out
+            elif not fused:
+                per[l] += 2 * b * c[l]               # ... D out, and the output layer reads it
+        per[0] += 4.0 * self.out_ch                  # the FP32 output
         return sum(v / 4.0 ** l for l, v in enumerate(per))
 
 
