@@ -931,6 +931,124 @@ __global__ void __launch_bounds__(CM_NT, 2) conv_up8_kernel(ConvH p) {
     conv_h_epilogue<NTL, RW>(p, acc, g_s, n, x0, y0);
 }
 
+// The network's last two layers at the first level in one launch: DA = conv3x3(concat(up(a), b))
+// (a: CPA channels at the coarse level, b: the 8-channel skip; no bias, no activation) and
+// y = out(conv3x3(DA) * gate), the 1x1 output layer in the epilogue. A block stages the coarse box
+// of a (as conv_up8_kernel does: the tile plus a halo of 2 at the fine level needs the same
+// TH/2 + 2 coarse rows), the skip box with a halo of 2, computes DA over the tile plus a halo of 1
+// into shared memory (rounded to BF16, zero outside the map, what the two launches store and
+// re-read) and the second layer from there. Same K order as conv_up8_kernel and conv_p8_kernel:
+// bit-identical to the two launches, and DA never reaches HBM.
+template <int CPA>
+__host__ __device__ inline size_t conv_dec0_smem() {
+    constexpr int th = 8 * conv_h_rows(1);
+    return ((size_t)(th / 2 + 2) * (CM_TX / 2 + 2) * (CPA + 8) + (size_t)(th + 4) * (CM_TX + 4) * 8 +
+            (size_t)(th + 2) * (CM_TX + 2) * 8 + (size_t)8 * (9 * CPA + P8_KP + 8) + (size_t)8 * (P8_KP + 8) +
+            (size_t)th * CM_TX * 8) * 2;
+}
+
+template <int CPA>
+__global__ void __launch_bounds__(CM_NT, 2) conv_dec0_kernel(ConvH p) {
+    if (p.done && *p.done) return;
+    constexpr int RW = conv_h_rows(1), TH = 8 * RW;
+    constexpr int CEW = CM_TX / 2 + 2, CEH = TH / 2 + 2, PSA = CPA + 8, GA = CPA / 8, UA = CEH * CEW * GA;
+    constexpr int BW = CM_TX + 4, BH = TH + 4;  // skip: tile + halo 2
+    constexpr int DW = CM_TX + 2, DH = TH + 2;  // DA: tile + halo 1
+    constexpr int ND = DW * DH, MB = (ND + 15) / 16;
+    constexpr int KP1 = 9 * CPA + P8_KP, KS1 = KP1 / 16;  // the first layer's K steps
+    extern __shared__ __align__(16) unsigned short cm_smem[];
+    unsigned short* a_s = cm_smem;                   // [CEH][CEW][PSA]
+    unsigned short* b_s = a_s + CEH * CEW * PSA;     // [BH][BW][8]
+    unsigned short* d_s = b_s + BH * BW * 8;         // [DH][DW][8]
+    unsigned short* w1_s = d_s + DH * DW * 8;        // [8][KP1 + 8]
+    unsigned short* w2_s = w1_s + 8 * (KP1 + 8);     // [8][P8_KP + 8]
+    unsigned short* g_s = w2_s + 8 * (P8_KP + 8);    // [TH CM_TX][8]
+    const int n = blockIdx.z;
+    const int x0 = blockIdx.x * CM_TX, y0 = blockIdx.y * TH;
+    const int Hc = p.H / 2, Wc = p.W / 2;
+    const int cx0 = (x0 >> 1) - 1, cy0 = (y0 >> 1) - 1;
+    stage_weights<1, KP1>(w1_s, p.wre);
+    stage_weights<1, P8_KP>(w2_s, p.wre2);
+    for (int q = threadIdx.x; q < TH * CM_TX; q += CM_NT) {
+        const int y = y0 + q / CM_TX, x = x0 + q % CM_TX;
+        const bool in = y < p.H && x < p.W;
+        cp_async16(g_s + q * 8, in ? p.gate + ((n * p.H + y) * p.W + x) * 8 : p.gate, in ? 16 : 0);
+    }
+    for (int q = threadIdx.x; q < UA; q += CM_NT) {  // the coarse box of a
+        const int r = q / GA, c0 = (q % GA) * 8;
+        const int cy = cy0 + r / CEW, cx = cx0 + r % CEW;
+        const bool in = (unsigned)cy < (unsigned)Hc && (unsigned)cx < (unsigned)Wc;
+        cp_async16(a_s + r * PSA + c0, in ? p.a + ((n * Hc + cy) * Wc + cx) * CPA + c0 : p.a, in ? 16 : 0);
+    }
+    for (int q = threadIdx.x; q < BH * BW; q += CM_NT) {  // the skip box
+        const int yy = y0 + q / BW - 2, xx = x0 + q % BW - 2;
+        const bool in = (unsigned)yy < (unsigned)p.H && (unsigned)xx < (unsigned)p.W;
+        cp_async16(b_s + q * 8, in ? p.b + ((n * p.H + yy) * p.W + xx) * 8 : p.b, in ? 16 : 0);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, grp = lane >> 2, tig = lane & 3;
+    const int lpix = (lane & 7) + ((lane >> 3) & 1) * 8, lk = (lane >> 4) * 8, second = lane >> 4;
+    {  // the first layer over the DA box, 16 box pixels (row-major, across box rows) an MMA row block
+        unsigned b1[KS1][1][2];
+#pragma unroll
+        for (int k = 0; k < KS1; k++) load_b<1, KP1>(b1[k], w1_s, k * 16, lane);
+        for (int mb = warp; mb < MB; mb += CM_NT / 32) {
+            const int m = min(mb * 16 + lpix, ND - 1);  // rows past the box repeat its last pixel
+            const int py = m / DW, px = m - py * DW;
+            float acc[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+            for (int tap = 0; tap < 9; tap++) {  // up(a): the fine pixel (py + dy, px + dx) - 2 repeats
+                const int dy = tap / 3, dx = tap % 3;  // coarse box pixel ((py + dy) / 2, (px + dx) / 2)
+#pragma unroll
+                for (int cb = 0; cb < CPA; cb += 16) {
+                    unsigned fa[4];
+                    ldmatrix_x4(fa, a_s + (((py + dy) >> 1) * CEW + ((px + dx) >> 1)) * PSA + cb + lk);
+                    mma_bf16_16816(acc, fa, b1[(tap * CPA + cb) / 16][0]);
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < 5; j++) {  // b: two taps per K step
+                const int tap = min(2 * j + second, 8);
+                const int dy = tap / 3, dx = tap - 3 * (tap / 3);
+                unsigned fa[4];
+                ldmatrix_x4(fa, b_s + ((py + dy) * BW + px + dx) * 8);
+                mma_bf16_16816(acc, fa, b1[9 * CPA / 16 + j][0]);
+            }
+#pragma unroll
+            for (int half = 0; half < 2; half++) {
+                const int mo = mb * 16 + grp + 8 * half;
+                if (mo >= ND) continue;
+                const int oy = y0 - 1 + mo / DW, ox = x0 - 1 + mo % DW;
+                const bool in = (unsigned)oy < (unsigned)p.H && (unsigned)ox < (unsigned)p.W;
+                // + 0: the epilogue's bias-free sum (a -0 sum stored as +0, as the two launches do)
+                reinterpret_cast<unsigned*>(d_s + mo * 8)[tig] =
+                    in ? bf16_pack(acc[2 * half] + 0.f, acc[2 * half + 1] + 0.f) : 0u;
+            }
+        }
+    }
+    __syncthreads();
+    float acc[RW][1][4];
+#pragma unroll
+    for (int r = 0; r < RW; r++)
+#pragma unroll
+        for (int e = 0; e < 4; e++) acc[r][0][e] = 0.f;
+#pragma unroll
+    for (int j = 0; j < 5; j++) {
+        const int tap = min(2 * j + second, 8);
+        const int dy = tap / 3, dx = tap - 3 * (tap / 3);
+        unsigned b[1][2];
+        load_b<1, P8_KP>(b, w2_s, j * 16, lane);
+#pragma unroll
+        for (int r = 0; r < RW; r++) {
+            unsigned fa[4];
+            ldmatrix_x4(fa, d_s + ((warp * RW + r + dy) * DW + lpix + dx) * 8);
+            mma_bf16_16816(acc[r][0], fa, b[0]);
+        }
+    }
+    conv_h_epilogue<1, RW>(p, acc, g_s, n, x0, y0);
+}
+
 // NCHW FP32 maps -> NHWC BF16 (c channels, 2 or a multiple of 2).
 __global__ void to_h_kernel(const float* __restrict__ x, int N, int C, int H, int W, unsigned short* __restrict__ y) {
     const size_t plane = (size_t)H * W, total = (size_t)N * plane * (C / 2);

@@ -66,7 +66,7 @@ inline cudaError_t conv_mma_configure() {
 #define CONV_UP8_PTR(NT_, CPA_) (const void*)conv_up8_kernel<NT_, CPA_>,
                             CONV_UP8_FOR_ALL(CONV_UP8_PTR)
 #undef CONV_UP8_PTR
-                            (const void*)conv_enc0_kernel,
+                            (const void*)conv_enc0_kernel, (const void*)conv_dec0_kernel<16>,
         };
         st = cudaSuccess;
         for (const void* k : ks)
@@ -496,9 +496,42 @@ struct LpcNet {
         return ch[0] == 8 && enc_a[0].k == 3 && enc_a[0].ci == 2 && enc_a[0].b < 0 && enc_b[0].k == 3 && enc_b[0].ci == 8 &&
                wp8_of(enc_a[0]) && wp8_of(enc_b[0]);
     }
+    // The first level's two decoder layers and the output layer in one launch (conv_dec0_kernel)
+    // when the output layer is fused, the first decoder layer has no bias and takes 16 coarse
+    // channels in the up8 order, and the second is an 8-channel 3x3 layer in the two-taps order.
+    bool fused_dec0() const {
+        return LPC_LEVELS > 2 && fused_out() && ch[1] == 16 && dec_a[0].k == 3 && dec_a[0].b < 0 && dec_b[0].k == 3 &&
+               dec_b[0].ci == 8 && wu8_of(dec_a[0]) && wp8_of(dec_b[0]);
+    }
     // launches of forward_h()
     int forward_h_launches() const {
-        return 2 * LPC_LEVELS + 2 * (LPC_LEVELS - 1) + (fused_out() ? 0 : 1) - (fused_enc0() ? 1 : 0);
+        return 2 * LPC_LEVELS + 2 * (LPC_LEVELS - 1) + (fused_out() ? 0 : 1) - (fused_enc0() ? 1 : 0) -
+               (fused_dec0() ? 1 : 0);
+    }
+
+    // The first level's decoder through conv_dec0_kernel: Yh = out(conv(conv(concat(up(Dh[1]), Eh[0]))) * Gh[0]).
+    cudaError_t dec0_h(cudaStream_t st) {
+        ConvH p{};
+        p.a = hp(Dh[1]);
+        p.ca = 16;
+        p.amode = CM_UP;
+        p.b = hp(Eh[0]);
+        p.cb = 8;
+        p.wre = wu8_of(dec_a[0]);
+        p.wre2 = wp8_of(dec_b[0]);
+        p.bias = dec_b[0].b >= 0 ? wq + dec_b[0].b : nullptr;
+        p.gate = hp(Gh[0]);
+        p.yf = Yh.p;
+        p.out_w = wq + out.w;
+        p.done = done;
+        p.co = 8;
+        p.H = H;
+        p.W = W;
+        p.N = N;
+        p.act = ACT_NONE;
+        const dim3 grid((W + CM_TX - 1) / CM_TX, (H + 8 * conv_h_rows(1) - 1) / (8 * conv_h_rows(1)), N);
+        conv_dec0_kernel<16><<<grid, CM_NT, conv_dec0_smem<16>(), st>>>(p);
+        return cudaGetLastError();
     }
 
     // The first level's encoder through conv_enc0_kernel: Eh[0] = conv(conv(Xh)) * Gh[0].
@@ -540,6 +573,10 @@ struct LpcNet {
                 e = conv_h(hp(Ah[l]), ch[l], CM_DIRECT, nullptr, 0, enc_b[l], hp(Gh[l]), hp(Eh[l]), nullptr, l, ACT_NONE, st);
         }
         for (int l = LPC_LEVELS - 2; l >= 0 && e == cudaSuccess; l--) {
+            if (l == 0 && fused_dec0()) {
+                e = dec0_h(st);
+                break;
+            }
             const unsigned short* below = (l == LPC_LEVELS - 2) ? hp(Eh[l + 1]) : hp(Dh[l + 1]);
             e = conv_h(below, ch[l + 1], CM_UP, hp(Eh[l]), ch[l], dec_a[l], nullptr, hp(DAh[l]), nullptr, l, ACT_NONE, st);
             if (e != cudaSuccess) break;
