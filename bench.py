@@ -48,7 +48,7 @@ STAGE_BYTES_SWE = (36 + 52) / 2                 # stage 1 / stage 2 (RK average 
 
 # DRAM bytes per cell measured by ncu (one capture each; scaled to a launch by cells, and by
 # iterations for the solve): profiles/network_conv_2048x1024.md, profiles/pcg_kernel_sgn_2048x1024.md.
-NETWORK_DRAM_BYTES_PER_CELL = 369.8e6 / (2048 * 1024)    # one application of the U-net
+NETWORK_DRAM_BYTES_PER_CELL = 334.1e6 / (2048 * 1024)    # one application of the U-net
 PCG_DRAM_BYTES_PER_CELL_ITER = 10.53e9 / (2048 * 1024 * 57)  # one iteration of the solve
 STAGE_DRAM_BYTES_PER_CELL_SWE = 573.1e6 / (4096 * 4096)      # one second-order stage
 # (profiles/stage_kernel_swe_4096x4096.md)
@@ -479,7 +479,7 @@ def run_b200(args, world, rank, local):
         peak, peak_kind = measured_peaks()
         iters_prof = arm["iterations_per_solve_profiled"]
         if learned and net_ms >= max(solve_ms, stage_ms):
-            # One network application: 18 kFLOP and 261 B per cell of its finest level, 70 FLOP/B,
+            # One network application: 18 kFLOP and 229 B per cell of its finest level, 79 FLOP/B,
             # below the B200's ridge point (about 220 FLOP/B), so its roof is HBM bandwidth.
             spec = net.spec
             ncell = w.grid.nx * w.grid.ny / spec.stride**2
@@ -488,7 +488,7 @@ def run_b200(args, world, rank, local):
             gbs = spec.bytes_per_cell() * ncell / (avg_ms / 1e3) / 1e9
             bf16 = peak_tensor()
             roof = {"bound": "hbm", "kernel": "network convolution chain (one application: conv_enc0 / conv_p8 / "
-                                              "conv_h / conv_up / conv_up8 kernels, channels-innermost BF16 mma.sync "
+                                              "conv_h / conv_up / conv_dec0 kernels, channels-innermost BF16 mma.sync "
                                               "implicit GEMM, FP32 accumulation)",
                     "achieved": gbs, "unit": "GB/s", "peak": peak, "frac": gbs / peak, "peak_source": peak_kind,
                     "algorithmic_bytes_per_cell": spec.bytes_per_cell(), "flops_per_cell": spec.flops_per_cell(),

@@ -92,33 +92,38 @@ class UNetSpec:
             f += 2.0 * co * ci * k * k / (4.0 ** level)
         return f
 
-    def fused_first_level(self) -> bool:
-        """The device computes the first level's two encoder layers in one launch (the map A
-        between them stays in shared memory) and the 1x1 output layer in the last decoder
-        layer's epilogue (D stays in registers) when the first level has 8 channels."""
-        return self.channels[0] == 8 and self.in_ch == 2 and self.out_ch == 2
+    def fused_maps(self) -> tuple:
+        """Which of the first level's maps the device keeps on chip: (A, DA, D). A: the two
+        encoder layers run as one launch, their intermediate map in shared memory; D: the 1x1
+        output layer runs in the last decoder layer's epilogue; DA: the two decoder layers and the
+        output layer run as one launch (16 channels at the second level)."""
+        a = self.channels[0] == 8 and self.in_ch == 2
+        d = self.channels[0] == 8 and self.out_ch == 2
+        da = d and self.levels > 2 and self.channels[1] == 16
+        return a, da, d
 
     def bytes_per_cell(self) -> float:
         """Algorithmic DRAM bytes of one application per cell of the finest level, for the
         device's channels-innermost BF16 activations: every convolution reads each of its inputs
         and its gate once and writes its output once (a pooled input is read at the finer level,
         an upsampled one at the coarser); the input is 2 BF16 channels, the output 2 FP32. Maps
-        that the device keeps on chip (`fused_first_level`) are not counted."""
+        that the device keeps on chip (`fused_maps`) are not counted."""
         c, L, b = self.channels, self.levels, 2.0
-        fused = self.fused_first_level()
+        on_chip_a, on_chip_da, on_chip_d = self.fused_maps()
         per = [0.0] * L  # bytes per pixel of level l
         for l in range(L):
             cin = self.in_ch if l == 0 else c[l - 1]
             src = b * cin * (4.0 if l > 0 else 1.0)  # enc_a reads its input (pooled: 4 finer pixels)
-            a_io = 0.0 if (l == 0 and fused) else 2 * b * c[l]  # A written by enc_a, read by enc_b
+            a_io = 0.0 if (l == 0 and on_chip_a) else 2 * b * c[l]  # A written by enc_a, read by enc_b
             per[l] += src + a_io + 2 * b * c[l]      # enc_b: the gate in, E out
         for l in range(L - 2, -1, -1):
             below = b * c[l + 1] / 4.0               # the upsampled map, read once at its level
-            per[l] += below + b * c[l] + b * c[l]    # dec_a: up(below), E in, DA out
-            per[l] += 2 * b * c[l]                   # dec_b: DA and the gate in ...
+            da_io = 0.0 if (l == 0 and on_chip_da) else 2 * b * c[l]  # DA written by dec_a, read by dec_b
+            per[l] += below + b * c[l] + da_io       # dec_a: up(below) and E in
+            per[l] += b * c[l]                       # dec_b: the gate in ...
             if l > 0:
                 per[l] += b * c[l]                   # ... D out
-            elif not fused:
+            elif not on_chip_d:
                 per[l] += 2 * b * c[l]               # ... D out, and the output layer reads it
         per[0] += 4.0 * self.out_ch                  # the FP32 output
         return sum(v / 4.0 ** l for l, v in enumerate(per))
