@@ -94,3 +94,40 @@ def test_strided_cycle_loss_gradient_matches_finite_differences():
         l1 = U.cycle_loss_grad(spec, q1, c, heff, bed, e, 2.0, 2.0, OMEGA)[0]
         l2 = U.cycle_loss_grad(spec, q2, c, heff, bed, e, 2.0, 2.0, OMEGA)[0]
         assert abs((l1 - l2) / 2e-6 - g[idx]) < 1e-6 + 1e-5 * abs(g[idx]), idx
+
+
+def _map_inventory(spec):
+    """Bytes per finest-level cell of one network application, counted map by map: every map
+    that reaches HBM is written once and read once per reader; maps the device keeps on chip
+    (the first level's A, DA and D when `fused_maps` says so) cost nothing."""
+    c, L, b = spec.channels, spec.levels, 2.0
+    on_a, on_da, on_d = spec.fused_maps()
+    scale = [1.0 / 4.0**l for l in range(L)]
+    total = b * spec.in_ch  # the input, read by enc_a[0]
+    for l in range(L):
+        m = b * c[l] * scale[l]
+        total += m * (2 if l < L - 1 else 1)  # the gate: read by enc_b, and by dec_b below the top
+        total += 0.0 if (l == 0 and on_a) else 2 * m  # A
+        total += m * (3 if l < L - 1 else 2)  # E: written; read pooled by enc_a[l + 1] and by dec_a[l] / as up(E)
+    for l in range(L - 1):
+        m = b * c[l] * scale[l]
+        total += 0.0 if (l == 0 and on_da) else 2 * m  # DA
+        if l > 0:
+            total += 2 * m  # D: written, read upsampled by dec_a[l - 1]
+        elif not on_d:
+            total += 2 * m  # D_0: written, read by the output layer
+    return total + 4.0 * spec.out_ch  # the FP32 output
+
+
+def test_the_bytes_model_counts_each_map_that_reaches_hbm_once():
+    from dataclasses import replace
+
+    spec = UNetSpec()  # the device's network: 8, 16, 32, 32 channels
+    assert spec.fused_maps() == (True, True, True)
+    assert spec.bytes_per_cell() == 229.0 == _map_inventory(spec)
+    wide = replace(spec, channels=(8, 32, 32, 32))  # the decoder's first level runs as two launches
+    assert wide.fused_maps() == (True, False, True)
+    assert wide.bytes_per_cell() == _map_inventory(wide)
+    plain = replace(spec, channels=(16, 16, 32, 32))  # nothing of the first level on chip
+    assert plain.fused_maps() == (False, False, False)
+    assert plain.bytes_per_cell() == 501.0 == _map_inventory(plain)
