@@ -215,8 +215,24 @@ wc_status wc_step_n(wc_solver* s, uint64_t n_steps, double t_end);
 wc_status wc_stable_dt_device(wc_solver* s, double* dt_out);
 /* FP64 reductions over the device-resident state (state.rs:78-102), synchronising. */
 wc_status wc_diagnostics_device(wc_solver* s, wc_diagnostics* out);
+/* The dispersive system of the solver's last solve and its solution, as the device holds them
+ * (FP32 values widened to FP64). The reference keeps the same arrays in Dispersion's private
+ * scratch (crates/wavecore/src/dispersion.rs:203-266, :380-490) and exposes none; this is for
+ * checking a solve, e.g. its true residual ||b - A w|| / ||b|| in FP64. Each output holds the
+ * nx*ny interior values, row-major with y outer: c = phi h^3 / 3, heff = max(h, 1e-8) (a cell
+ * takes part in the system where heff >= 0.05), the right-hand side (bx, by) and the solution
+ * (wx, wy). Any output may be null. WC_EINVAL if the solver has no dispersion. Synchronising. */
+wc_status wc_dispersion_system(wc_solver* s, double* c, double* heff, double* bx, double* by,
+                               double* wx, double* wy);
 /* Device time of the device-resident state, synchronising. */
 wc_status wc_time_device(wc_solver* s, double* time_out);
+/* No counterpart in the reference (which has no device waits): the limit, in nanoseconds, of each
+ * bounded wait of this solver's persistent kernels (a grid barrier of the dispersive solve or of
+ * the followed fronts); 0 restores the default of 2 s. A wait that runs out sets an error bit,
+ * every CTA of the kernel returns, and the call that reports the step's status returns
+ * WC_ETIMEOUT with the context still usable (the next state upload clears the error). A tiny
+ * limit forces that path without any fault, which is how the failure handling is tested. */
+wc_status wc_set_wait_limit(wc_solver* s, uint64_t ns);
 /* Wait for all queued device work of this solver and report its status: WC_ETIMEOUT if a
  * bounded device wait ran out, WC_ENAN if a step met a NaN. */
 wc_status wc_synchronize(wc_solver* s);
@@ -241,18 +257,20 @@ typedef struct wc_kernel_time {
 wc_status wc_profile_enable(wc_solver* s, int32_t on);
 wc_status wc_profile_read(wc_solver* s, wc_kernel_time out[WC_KERNEL_KINDS]);
 
-/* No counterpart in the reference: wc_stable_dt for callers that cannot allocate device memory
- * when they need the time step, such as code running while a CUDA stream capture is open (where
- * cudaMalloc is not allowed) or an application that hands all device memory to its own pool
- * allocator and runs under a fixed budget. The state belongs to the caller: padded FP64 device
- * arrays h, hu, hv of (nx+6)*(ny+6) values each, read on `stream` (a cudaStream_t; NULL is the
- * legacy default stream). The call allocates nothing: its scratch is a fixed 64 KiB array inside
- * the library, which every GPU that loads the library holds until the process exits, and grids
- * of more than 16,777,216 interior cells (4096 x 4096) are refused with WC_EINVAL. The first call
- * on a device looks up that array's device address, so make it before any stream capture begins.
- * All calls share the one array, which keeps the last call's contents (each call rewrites every
- * slot it reads): calls that overlap on the GPU race, so do not run two at once. Returns in
- * *dt_out, with the same status, what wc_stable_dt returns for the same state. */
+/* No counterpart in the reference: wc_stable_dt for callers that cannot have the library allocate
+ * device memory, such as an application that hands all of the GPU's memory to its own pool
+ * allocator at start-up and runs under a fixed budget, or a simulation loop that must not allocate
+ * or free per step (cudaFree synchronises the whole device). The state belongs to the caller:
+ * padded FP64 device arrays h, hu, hv of (nx+6)*(ny+6) values each, read on `stream` (a
+ * cudaStream_t; NULL is the legacy default stream). The call is synchronous: it waits on `stream`
+ * for its result and returns it on the host. It allocates nothing: its scratch is a fixed 64 KiB
+ * array inside the library, which every GPU that loads the library holds until the process exits,
+ * and grids of more than 16,777,216 interior cells (4096 x 4096) are refused with WC_EINVAL. The
+ * first call on a device (and the first after a device reset) looks up that array's device
+ * address, so make that first call before any stream capture begins. All calls share the one
+ * array, which keeps the last call's contents (each call rewrites every slot it reads): calls
+ * that overlap on the GPU race, so do not run two at once. Returns in *dt_out, with the same
+ * status, what wc_stable_dt returns for the same state. */
 wc_status wc_stable_dt_noalloc(const wc_grid* grid, double cfl, const double* d_h,
                                const double* d_hu, const double* d_hv, void* stream,
                                double* dt_out);
@@ -322,8 +340,9 @@ wc_status wc_lpc_forward_backward(wc_lpc* l, int32_t n, int32_t h, int32_t w, co
                                   const float* feat, const float* dy, float* y, float* grad,
                                   float* dx);
 /* The network's output (inference: no training state kept) on host arrays x and feat,
- * [n][2][h][w] (h, w multiples of 8). tensor != 0: BF16 activations on the tensor cores, as the
- * solver applies it; 0: FP32 FMA, as training does. */
+ * [n][2][h][w] (h, w multiples of 8). tensor = 1: BF16 activations on the tensor cores, as the
+ * solver applies it; 2: the same with the first level's layers run one launch per layer instead
+ * of its fused launches (a check that both give the same bits); 0: FP32 FMA, as training does. */
 wc_status wc_lpc_forward(wc_lpc* l, int32_t n, int32_t h, int32_t w, const float* x,
                          const float* feat, int32_t tensor, float* y);
 /* The training objective on given patches, for checking its gradient: c, heff and bed are

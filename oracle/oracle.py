@@ -10,6 +10,7 @@ runs against either.
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 import subprocess
 
@@ -205,6 +206,97 @@ def matvec(grid, periodic, heff, mask, c, px, py):
         abi.dptr(np.ascontiguousarray(c)), abi.dptr(px), abi.dptr(py), abi.dptr(ax), abi.dptr(ay),
     )
     return ax, ay
+
+
+def true_relative_residual(grid, periodic, system) -> float:
+    """||b - A w||_2 / ||b||_2 in FP64 (dispersion.rs:269-317 for A) of a system given as (ny, nx)
+    arrays c, heff, bx, by, wx, wy, e.g. a device solve's (`Solver.dispersion_system`). The ring
+    of c outside the interior follows the boundaries (mirrored at walls, wrapped when periodic),
+    as the reference's c, computed from ghost-filled depths, does; a cell takes part where its
+    FP32 heff is at least 0.05, as on the device. Compared with the recursively updated residual
+    the stopping rule reads, this is the residual of the stored solution itself."""
+    def padded(a):
+        out = np.zeros(grid.cells())
+        grid.inner(out)[:] = a
+        return out
+
+    c = padded(system["c"])
+    mirror_ghosts(grid, c)
+    if periodic:
+        wrap_ghosts_y(grid, c)
+    heff = padded(system["heff"])
+    mask = padded((np.asarray(system["heff"], dtype=np.float32) >= np.float32(0.05)).astype(np.float64))
+    ax, ay = matvec(grid, periodic, heff, mask, c, padded(system["wx"]), padded(system["wy"]))
+    rx = np.asarray(system["bx"]) - grid.inner(ax)
+    ry = np.asarray(system["by"]) - grid.inner(ay)
+    nb = math.sqrt(float(np.sum(np.square(system["bx"])) + np.sum(np.square(system["by"]))))
+    return math.sqrt(float(np.sum(rx * rx) + np.sum(ry * ry))) / nb if nb > 0 else 0.0
+
+
+def pcg_solve(grid, periodic, system, tolerance, max_iterations, w0=None):
+    """The reference's Jacobi PCG (dispersion.rs:440-545) in FP64 on a given system (the (ny, nx)
+    arrays c, heff, bx, by of `true_relative_residual`), from w0 (zero if None) with its stopping
+    rule ||r|| <= tol ||b|| + 1e-10. Returns (wx, wy, iterations, converged)."""
+    def padded(a):
+        out = np.zeros(grid.cells())
+        grid.inner(out)[:] = a
+        return out
+
+    c = padded(system["c"])
+    mirror_ghosts(grid, c)
+    if periodic:
+        wrap_ghosts_y(grid, c)
+    heff_i = np.asarray(system["heff"], dtype=np.float64)
+    m_i = (np.asarray(system["heff"], dtype=np.float32) >= np.float32(0.05)).astype(np.float64)
+    heff, mask = padded(heff_i), padded(m_i)
+    cv = grid.view(c)
+    g3 = 3
+    ci = cv[g3:g3 + grid.ny, g3:g3 + grid.nx]
+    q = 0.25 / (grid.dx * grid.dx)
+    dgx = np.where(m_i > 0, heff_i + (cv[g3:g3 + grid.ny, g3 + 1:g3 + grid.nx + 1] + cv[g3:g3 + grid.ny, g3 - 1:g3 + grid.nx - 1]) * q, 1.0)
+    q = 0.25 / (grid.dy * grid.dy)
+    dgy = np.where(m_i > 0, heff_i + (cv[g3 + 1:g3 + grid.ny + 1, g3:g3 + grid.nx] + cv[g3 - 1:g3 + grid.ny - 1, g3:g3 + grid.nx]) * q, 1.0)
+    del ci
+    bx, by = np.asarray(system["bx"], dtype=np.float64), np.asarray(system["by"], dtype=np.float64)
+    wx = np.zeros_like(bx) if w0 is None else np.array(w0[0], dtype=np.float64) * m_i
+    wy = np.zeros_like(by) if w0 is None else np.array(w0[1], dtype=np.float64) * m_i
+
+    def A(px, py):
+        ax, ay = matvec(grid, periodic, heff, mask, c, padded(px), padded(py))
+        return grid.inner(ax).copy(), grid.inner(ay).copy()
+
+    ax, ay = A(wx, wy)
+    rx, ry = bx - ax, by - ay
+    zx, zy = rx / dgx, ry / dgy
+    px, py = zx.copy(), zy.copy()
+    target = math.sqrt(float(np.sum(bx * bx) + np.sum(by * by))) * tolerance + 1e-10
+    rz = float(np.sum(rx * zx) + np.sum(ry * zy))
+    it = 0
+    converged = math.sqrt(float(np.sum(rx * rx) + np.sum(ry * ry))) <= target
+    while not converged and it < max_iterations:
+        ax, ay = A(px, py)
+        alpha = rz / float(np.sum(px * ax) + np.sum(py * ay))
+        wx += alpha * px
+        wy += alpha * py
+        rx -= alpha * ax
+        ry -= alpha * ay
+        zx, zy = rx / dgx, ry / dgy
+        it += 1
+        converged = math.sqrt(float(np.sum(rx * rx) + np.sum(ry * ry))) <= target
+        rz_next = float(np.sum(rx * zx) + np.sum(ry * zy))
+        beta = rz_next / rz
+        rz = rz_next
+        px, py = zx + beta * px, zy + beta * py
+    return wx, wy, it, converged
+
+
+def diagnostics(grid, s: State):
+    """(volume, max |momentum|, min depth) of a state: state.rs:78-102 (or_volume,
+    or_max_abs_momentum, or_min_depth)."""
+    g = grid.to_c()
+    L = lib()
+    return (L.or_volume(C.byref(g), abi.dptr(s.h)), L.or_max_abs_momentum(C.byref(g), abi.dptr(s.hu), abi.dptr(s.hv)),
+            L.or_min_depth(C.byref(g), abi.dptr(s.h)))
 
 
 def dot(grid, ax, ay, bx, by):

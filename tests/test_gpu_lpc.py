@@ -92,6 +92,21 @@ def test_tensor_core_inference_matches_the_oracle_to_bf16():
     assert rel(yt, yo) > 1e-5  # the tensor path does round to BF16
 
 
+def test_fused_first_level_launches_give_the_bits_of_the_per_layer_launches():
+    # conv_enc0_kernel and conv_dec0_kernel keep the first level's 8-channel maps in shared memory
+    # (rounded to BF16 there, as the per-layer launches round them in HBM); on a map whose sides
+    # are not whole 32x16 tiles (40 x 56), so partial tiles and the zero-filled halos of their
+    # boxes are exercised, the output must be the same bits either way.
+    spec = UNetSpec()
+    net = LearnedPreconditioner(spec)
+    net.set_params(random_params(spec, 17))
+    x, feat, _ = batch(18, n=2, h=40, w=56)
+    fused = net.forward(x, feat, tensor=True, fused=True)
+    per_layer = net.forward(x, feat, tensor=True, fused=False)
+    assert np.abs(fused).max() > 0
+    assert np.array_equal(fused, per_layer)
+
+
 def test_training_loss_and_gradient_match_the_fp64_oracle():
     # The whole training objective (the cycle on patches, the energy-norm loss) and its gradient
     # through the cycle and the network, against the FP64 oracle (FP32 weights on both sides).

@@ -5,9 +5,7 @@ stable_dt), so differences are the device's FP32 arithmetic alone. Tolerances (F
 FP64, stated per test): the free surface eta over cells wet in both, the wet/dry mask (h > 1e-3),
 and the breaking mask (indicator >= 0.8, the driver's threshold, crates/wavesim/src/lib.rs:1222).
 """
-import json
 import math
-import os
 
 import numpy as np
 import pytest
@@ -18,56 +16,14 @@ from wavesim_b200 import workloads as W
 
 pytestmark = pytest.mark.gpu
 
-OUT = os.environ.get("WC_PARITY_OUT")
-
-
-def record(name, metrics):
-    print(name, json.dumps(metrics))
-    if OUT:
-        path = os.path.join(OUT, "parity_metrics.jsonl")
-        with open(path, "a") as f:
-            f.write(json.dumps({"case": name, **metrics}) + "\n")
-
-
-def compare(w, state, steps, every=None):
-    gpu = w.solver(Solver)
-    orc = w.solver(OracleSolver)
-    sg, so = state.clone(), state.clone()
-    g = w.grid
-    for _ in range(steps):
-        dt = orc.stable_dt(so)
-        assert math.isfinite(dt) and dt > 0
-        orc.step(so, dt)
-        gpu.step(sg, dt)
-    hg, ho = g.inner(sg.h), g.inner(so.h)
-    eg, eo = hg + g.inner(w.bed.b), ho + g.inner(w.bed.b)
-    wet_both = (hg > 1e-3) & (ho > 1e-3)
-    d = np.abs(eg - eo)[wet_both]
-    wet_agree = float(np.mean((hg > 1e-3) == (ho > 1e-3)))
-    bg = gpu.breaking_indicator(sg) >= 0.8
-    bo = orc.breaking_indicator(so) >= 0.8
-    m = {
-        "steps": steps,
-        "time_s": so.time,
-        "eta_max_abs_diff_m": float(d.max()),
-        "eta_rms_diff_m": float(np.sqrt(np.mean(d * d))),
-        "eta_range_m": float(eo[ho > 1e-3].max() - eo[ho > 1e-3].min()),
-        "wet_mask_agreement": wet_agree,
-        "breaking_mask_agreement": float(np.mean(bg == bo)),
-        "breaking_cells_oracle": int(bo.sum()),
-        "volume_rel_diff": abs(sg.volume(g) - so.volume(g)) / so.volume(g),
-    }
-    if w.dispersion is not None:
-        m["oracle_iterations_per_solve"] = orc.dispersion_stats().iterations / max(1, orc.dispersion_stats().solves)
-        m["device_iterations_per_solve"] = gpu.dispersion_stats().iterations / max(1, gpu.dispersion_stats().solves)
-    return m, sg, so
+from parity import compare, record
 
 
 def test_swe_plane_beach_config1_matches_the_oracle():
     """256x64 plane beach, second order, maker + sponges + Manning, 1000 steps (48 s)."""
     w = W.config1()
     s0 = State.lake_at_rest(w.grid, w.bed, 0.0)
-    m, _, _ = compare(w, s0, 1000)
+    m, _, _, _ = compare(w, s0, 1000)
     record("swe_plane_beach_256x64_1000steps", m)
     # FP32 against FP64 after 1000 steps of a 1 m wave: measured 2.6e-6 m max, 6.5e-7 m rms.
     assert m["eta_max_abs_diff_m"] < 2e-5
@@ -81,7 +37,7 @@ def test_fifth_order_sgn_periodic_beach_matches_the_oracle():
     """Fifth order + SGN (Jacobi PCG to 1e-8), periodic y, oblique maker: 192x96 at 2 m."""
     w = W.sgn_beach(192, 96, 2.0, seed=11, name="sgn_small")
     s0 = W.wave_train_state(w)
-    m, sg, _ = compare(w, s0, 150)
+    m, sg, _, _ = compare(w, s0, 150)
     record("sgn_beach_192x96_150steps", m)
     # Measured 4.1e-6 m max, 4.5e-7 m rms on a 3.4 m surface range.
     assert m["eta_max_abs_diff_m"] < 3e-5
@@ -166,3 +122,29 @@ def test_adaptive_device_stepping_stops_at_t_end():
     assert mn >= 0.0
     dt = sol.stable_dt_device()
     assert math.isfinite(dt) and dt > 0
+
+
+def test_device_diagnostics_match_the_oracle():
+    """wc_diagnostics_device (FP64 reductions over the resident state) against the reference's
+    State::volume / max_abs_momentum / min_depth (state.rs:78-102) restated in the oracle: on the
+    device state itself (downloaded: the same values), max momentum and min depth are exact and
+    the volume agrees to FP64 rounding (the sums run in another order); against the oracle's own
+    run from the same start, to FP32 level."""
+    from oracle.oracle import diagnostics
+
+    w = W.sgn_beach(192, 96, 2.0, seed=11, name="sgn_small")
+    s0 = W.wave_train_state(w)
+    m, sg, so, gpu = compare(w, s0, 40)
+    gpu.upload(sg)
+    vol, mom, mn = gpu.diagnostics_device()
+    s_dev = sg.clone()
+    gpu.download(s_dev)
+    ovol, omom, omn = diagnostics(w.grid, s_dev)
+    record("diagnostics_192x96_40steps", {"volume": vol, "max_abs_momentum": mom, "min_depth": mn,
+                                          "oracle_run": list(diagnostics(w.grid, so))})
+    assert mom == omom and mn == omn
+    assert abs(vol - ovol) <= 1e-13 * ovol
+    rvol, rmom, rmn = diagnostics(w.grid, so)
+    assert abs(vol - rvol) <= 1e-6 * rvol
+    assert abs(mom - rmom) <= 1e-4 * rmom
+    assert abs(mn - rmn) <= 1e-5

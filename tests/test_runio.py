@@ -72,3 +72,37 @@ def test_run_writer_checks_and_replaces_an_old_run(tmp_path):
     assert not os.path.exists(os.path.join(d, "run.json")) and os.path.exists(os.path.join(d, "keep.txt"))
     remove_run(d)
     assert sorted(os.listdir(d)) == ["keep.txt"]
+
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "run_tiny")
+
+
+def test_writer_reproduces_the_reference_golden_run_byte_for_byte(tmp_path):
+    """The run the reference's `write_tiny` writes (crates/waveio/tests/golden.rs:18-78), built
+    the same way here: a 6 x 4 bed rising 0.75 m per cell from -2 m and four frames of eta and
+    breaking, every value a multiple of 1/16 (exact in FP32). The reference compares its writer's
+    output with the committed fixture byte for byte (golden.rs:80-104); so does this test."""
+    nx, ny = 6, 4
+    n = np.arange(nx * ny)
+    elev = (np.float32(-2.0) + np.float32(0.75) * (n % nx).astype(np.float32)).astype(np.float32)
+    w = RunWriter(str(tmp_path), "tiny", elev.reshape(ny, nx), 3.0, 2.0, fields=("eta", "breaking"),
+                  frame={"crs": "EPSG:32604", "origin_easting": 1000.0, "origin_northing": 2000.0,
+                         "x_bearing_deg": 130.0, "note": "fixture"},
+                  waves={"wave_height_m": 1.0, "wave_period_s": 14.0, "tide_m": 0.0, "maker_x_m": 6.0,
+                         "sponge_offshore_cells": 2, "sponge_side_cells": 1},
+                  source={"name": "Synthetic fixture", "attribution": "none"})
+    for k in range(4):
+        wave = (np.float32(0.125) * np.float32(k) + np.float32(0.0625) * (n % nx).astype(np.float32)
+                - np.float32(0.25)).astype(np.float32)
+        eta = np.where(elev < 0, np.maximum(wave, elev), elev).astype(np.float32)
+        breaking = np.where(elev < 0, np.float32(0.25) * ((n + k) % 4).astype(np.float32), 0.0).astype(np.float32)
+        w.write_frame(2.0 * k, [eta, breaking])
+    w.finish()
+    for name in ("run.json", "bed.f32", "frames.f32"):
+        with open(os.path.join(GOLDEN, name), "rb") as f:
+            want = f.read()
+        with open(tmp_path / name, "rb") as f:
+            got = f.read()
+        assert got == want, name
+    r = Run(GOLDEN)
+    assert r.header["frame_count"] == 4 and np.array_equal(r.field("breaking", 3).ravel()[:3], [0.75, 0.0, 0.25])

@@ -124,6 +124,7 @@ struct LpcNet {
     // Inference on NHWC BF16 activations (conv_h_kernel): every channel count a multiple of 8
     // and every layer's tile within the shared-memory limit; set by configure_nhwc.
     bool nhwc = false;
+    bool fuse_level0 = true;    // the first level's fused launches (conv_enc0_kernel, conv_dec0_kernel)
     const int* done = nullptr;  // the flexible CG's end flag: applications after it are skipped
     DBuf Xh, Yh, Fh[LPC_LEVELS], HIDh[LPC_LEVELS], Gh[LPC_LEVELS], Ah[LPC_LEVELS], Eh[LPC_LEVELS],
         DAh[LPC_LEVELS], Dh[LPC_LEVELS];
@@ -491,16 +492,18 @@ struct LpcNet {
     bool fused_out() const { return ch[0] == 8 && out.co == 2 && out.k == 1; }
     // The first level's two encoder layers in one launch (conv_enc0_kernel) when both are 8-channel
     // 3x3 layers in the two-taps order and the first has no bias (the network's form: linear, the
-    // second gated).
+    // second gated). The fused kernel applies no activation to the first layer's map: forward_h
+    // runs every layer with ACT_NONE, and a network with activations would need the per-layer path.
     bool fused_enc0() const {
-        return ch[0] == 8 && enc_a[0].k == 3 && enc_a[0].ci == 2 && enc_a[0].b < 0 && enc_b[0].k == 3 && enc_b[0].ci == 8 &&
+        return fuse_level0 && ch[0] == 8 && enc_a[0].k == 3 && enc_a[0].ci == 2 && enc_a[0].b < 0 && enc_b[0].k == 3 && enc_b[0].ci == 8 &&
                wp8_of(enc_a[0]) && wp8_of(enc_b[0]);
     }
     // The first level's two decoder layers and the output layer in one launch (conv_dec0_kernel)
     // when the output layer is fused, the first decoder layer has no bias and takes 16 coarse
     // channels in the up8 order, and the second is an 8-channel 3x3 layer in the two-taps order.
+    // As for fused_enc0, the first layer's map gets no activation, matching forward_h's ACT_NONE.
     bool fused_dec0() const {
-        return LPC_LEVELS > 2 && fused_out() && ch[1] == 16 && dec_a[0].k == 3 && dec_a[0].b < 0 && dec_b[0].k == 3 &&
+        return fuse_level0 && LPC_LEVELS > 2 && fused_out() && ch[1] == 16 && dec_a[0].k == 3 && dec_a[0].b < 0 && dec_b[0].k == 3 &&
                dec_b[0].ci == 8 && wu8_of(dec_a[0]) && wp8_of(dec_b[0]);
     }
     // launches of forward_h()

@@ -1,15 +1,17 @@
 // noalloc.cu — the CFL time-step limit on caller-owned device arrays, allocating nothing.
 //
-// Some callers cannot allocate device memory at the moment they need the time step: code that
-// runs while a CUDA stream capture is open (cudaMalloc is not permitted during capture), and host
-// applications that hand all of the GPU's memory to their own pool allocator up front and run
-// under a fixed device-memory budget. wc_stable_dt allocates its scratch inside its solver; this
-// entry point instead takes the state as device pointers from the caller and keeps its own
-// scratch — one partial result per CTA plus the final result — in a file-scope __device__ array
-// of fixed size, which every GPU that loads the library holds until the process exits.
+// Some callers cannot have a library allocate device memory when they need the time step: host
+// applications that hand all of the GPU's memory to their own pool allocator at start-up and run
+// under a fixed device-memory budget (a cudaMalloc from the library would fail or break that
+// budget), and simulation loops that must not allocate or free per step because cudaFree
+// synchronises the whole device. wc_stable_dt allocates its scratch inside its solver; this entry
+// point instead takes the state as device pointers from the caller and keeps its own scratch —
+// one partial result per CTA plus the final result — in a file-scope __device__ array of fixed
+// size, which every GPU that loads the library holds until the process exits.
 //
 // The computation is the same FP64 rate, cell for cell, as wc_stable_dt's
 // (crates/wavecore/src/solver.rs:94-100 and :431-450), so both return the same bits.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -31,21 +33,53 @@ constexpr int NA_SLOTS = 2 * (NA_MAX_BLOCKS + 1);          // (max rate bits, fi
 static __device__ __align__(256) unsigned long long g_noalloc_scratch[NA_SLOTS];
 
 std::mutex g_na_mutex;
-void* g_na_ptr[64] = {nullptr};  // the scratch's device address, per device
+void* g_na_ptr[64] = {nullptr};             // the scratch's device address, per device
+unsigned long long g_na_ctx[64] = {0};      // the context that address belongs to, per device
+
+// The id of the calling thread's current context (0 if none is current), through the driver
+// entry points the runtime hands out, so the library needs no link-time libcuda. A context id is
+// unique for the life of the process: a device reset gives the device a new one.
+unsigned long long current_context_id() {
+    using GetCurrent = CUresult (*)(CUcontext*);
+    using GetId = CUresult (*)(CUcontext, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static bool looked_up = false;
+    if (!looked_up) {
+        void* f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault) == cudaSuccess)
+            get_current = reinterpret_cast<GetCurrent>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault) == cudaSuccess)
+            get_id = reinterpret_cast<GetId>(f);
+        looked_up = true;
+    }
+    if (!get_current || !get_id) return 0;
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (get_current(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+    if (get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
 
 // The device address of the scratch on the current device. Host code must not pass the symbol
-// itself to a kernel: on the host it names a stand-in, not device memory.
+// itself to a kernel: on the host it names a stand-in, not device memory. The address is looked
+// up (cudaGetSymbolAddress, which also makes the device's primary context current) on the first
+// call on a device, and again whenever the current context is not the one it was looked up in,
+// as after cudaDeviceReset, which unloads the module the old address belonged to.
 cudaError_t scratch_on_current_device(unsigned long long** out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
     std::lock_guard<std::mutex> lock(g_na_mutex);
-    if (!g_na_ptr[dev]) {
+    const unsigned long long ctx = current_context_id();
+    if (!g_na_ptr[dev] || ctx == 0 || ctx != g_na_ctx[dev]) {
         void* p = nullptr;
         e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess) return e;
         g_na_ptr[dev] = p;
+        g_na_ctx[dev] = current_context_id();
     }
     *out = static_cast<unsigned long long*>(g_na_ptr[dev]);
     return cudaSuccess;

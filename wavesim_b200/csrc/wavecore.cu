@@ -149,6 +149,8 @@ struct wc_solver {
     // the sub-steps' momentum banks and the cooperative kernel's barrier state.
     int eddy_on = 0;
     EddyParams eddy{};
+    // The limit of every bounded device wait (grid barriers of the persistent kernels).
+    unsigned long long wait_ns = BARRIER_TIMEOUT_NS;
     double *mem = nullptr, *mem_new = nullptr;
     float* nu = nullptr;
     float2 *mb0 = nullptr, *mb1 = nullptr;
@@ -343,7 +345,7 @@ PcgArgs pcg_args(const wc_solver* s, int mode, const float4* qold, float4* qout,
     a.tiles_x = s->pcg_tiles_x;
     a.tiles_y = s->pcg_tiles_y;
     a.damp = s->damp;
-    a.timeout_ns = BARRIER_TIMEOUT_NS;
+    a.timeout_ns = s->wait_ns;
     return a;
 }
 
@@ -569,7 +571,7 @@ wc_status launch_eddy(wc_solver* s, int finish, int* sub_out) {
     a.sub_out = sub_out;
     a.e = s->eddy;
     a.finish = finish;
-    a.timeout_ns = BARRIER_TIMEOUT_NS;
+    a.timeout_ns = s->wait_ns;
     CK(cudaMemsetAsync(s->ed_bar, 0, 2 * sizeof(unsigned), s->stream));
     ProfScope ps(s, 4);
     cudaLaunchConfig_t lc{};
@@ -997,6 +999,18 @@ wc_status wc_profile_read(wc_solver* s, wc_kernel_time out[WC_KERNEL_KINDS]) {
     return WC_OK;
 }
 
+wc_status wc_set_wait_limit(wc_solver* s, uint64_t ns) {
+    if (!s) return set_err(WC_EINVAL, "null argument");
+    s->wait_ns = ns ? (unsigned long long)ns : BARRIER_TIMEOUT_NS;
+    // A captured step holds the old limit in its kernels' arguments: capture again.
+    if (s->step_graph) {
+        CK(cudaStreamSynchronize(s->stream));
+        CK(cudaGraphExecDestroy(s->step_graph));
+        s->step_graph = nullptr;
+    }
+    return WC_OK;
+}
+
 wc_status wc_set_stream(wc_solver* s, void* stream) {
     if (!s) return set_err(WC_EINVAL, "null solver");
     CK(cudaStreamSynchronize(s->stream));
@@ -1249,6 +1263,32 @@ wc_status wc_diagnostics_device(wc_solver* s, wc_diagnostics* out) {
     out->volume = v[0];
     out->max_abs_momentum = v[1];
     out->min_depth = v[2];
+    return WC_OK;
+}
+
+wc_status wc_dispersion_system(wc_solver* s, double* c, double* heff, double* bx, double* by, double* wx,
+                               double* wy) {
+    if (!s) return set_err(WC_EINVAL, "null argument");
+    if (!s->sgn) return set_err(WC_EINVAL, "the solver has no dispersion");
+    const size_t n = s->ncell;
+    std::vector<float> hc(n), hh(n);
+    std::vector<float2> hb(n), hw(n);
+    CK(cudaMemcpyAsync(hc.data(), s->cc, n * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaMemcpyAsync(hh.data(), s->heff, n * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaMemcpyAsync(hb.data(), s->bv, n * sizeof(float2), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaMemcpyAsync(hw.data(), s->w, n * sizeof(float2), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    const int nx = s->g.nx, ny = s->g.ny, pitch = s->g.pitch;
+    for (int j = 0; j < ny; j++)
+        for (int i = 0; i < nx; i++) {
+            const size_t k = (size_t)j * pitch + i, o = (size_t)j * nx + i;
+            if (c) c[o] = hc[k];
+            if (heff) heff[o] = hh[k];
+            if (bx) bx[o] = hb[k].x;
+            if (by) by[o] = hb[k].y;
+            if (wx) wx[o] = hw[k].x;
+            if (wy) wy[o] = hw[k].y;
+        }
     return WC_OK;
 }
 
@@ -1764,6 +1804,7 @@ wc_status wc_lpc_forward(wc_lpc* l, int32_t n, int32_t h, int32_t w, const float
     net.layout(m.net.ch, m.net.hidden);
     net.wq = m.wq.p;
     net.tensor = tensor != 0;
+    net.fuse_level0 = tensor != 2;
     net.configure_nhwc();
     cudaStream_t st = m.st;
     if (net.tensor) {

@@ -24,8 +24,20 @@ LAYOUT_RUN = ("per frame: one block per field, in `fields` order; each block row
               "(increasing), x inner (increasing)")
 
 
+FRAME_KEYS = ("crs", "origin_easting", "origin_northing", "x_bearing_deg", "note")  # bed.rs:16-24
+
+
 class FormatError(ValueError):
     pass
+
+
+def _sorted_json(v):
+    """A JSON value with every object's keys sorted, recursively."""
+    if isinstance(v, dict):
+        return {k: _sorted_json(v[k]) for k in sorted(v)}
+    if isinstance(v, list):
+        return [_sorted_json(x) for x in v]
+    return v
 
 
 def default_frame() -> dict:
@@ -127,10 +139,18 @@ class RunWriter:
         self.header["stats"] = {"file": "stats.f32", "fields": list(fields), "from_s": float(start), "to_s": float(end)}
 
     def finish(self) -> str:
+        """Close the frames and write run.json (run.rs:200-212) as the reference's serializer
+        does: two-space pretty JSON and a newline, the header's and the frame's keys in their
+        declaration order (run.rs:14-43, bed.rs:16-24), the free-form `waves` and `source`
+        objects with their keys sorted at every depth, as serde_json's maps keep them."""
         self._frames.close()
         path = os.path.join(self.dir, "run.json")
+        h = dict(self.header)
+        h["frame"] = {k: h["frame"][k] for k in FRAME_KEYS if k in h["frame"]}
+        h["waves"] = _sorted_json(h["waves"])
+        h["source"] = _sorted_json(h["source"])
         with open(path, "w") as f:
-            f.write(json.dumps(self.header, indent=2) + "\n")
+            f.write(json.dumps(h, indent=2) + "\n")
         return path
 
 

@@ -45,9 +45,11 @@ EXPORTS = [
     "wc_step_n",
     "wc_stable_dt_device",
     "wc_diagnostics_device",
+    "wc_dispersion_system",
     "wc_time_device",
     "wc_synchronize",
     "wc_set_stream",
+    "wc_set_wait_limit",
     "wc_profile_enable",
     "wc_profile_read",
     "wc_launch_count",
@@ -125,9 +127,11 @@ def load(path: str = LIB_PATH):
     L.wc_step_n.argtypes = [V, C.c_uint64, C.c_double]
     L.wc_stable_dt_device.argtypes = [V, D]
     L.wc_diagnostics_device.argtypes = [V, C.POINTER(abi.wc_diagnostics)]
+    L.wc_dispersion_system.argtypes = [V, D, D, D, D, D, D]
     L.wc_time_device.argtypes = [V, D]
     L.wc_synchronize.argtypes = [V]
     L.wc_set_stream.argtypes = [V, V]
+    L.wc_set_wait_limit.argtypes = [V, C.c_uint64]
     L.wc_profile_enable.argtypes = [V, C.c_int32]
     L.wc_profile_read.argtypes = [V, C.POINTER(abi.wc_kernel_time)]
     L.wc_ensemble_create.argtypes = [C.c_uint64, C.POINTER(abi.wc_grid), C.POINTER(D), C.POINTER(abi.wc_config), C.POINTER(V)]
@@ -189,8 +193,8 @@ def load(path: str = LIB_PATH):
     for name in (
         "wc_solver_create", "wc_step", "wc_stable_dt", "wc_limiting_cell", "wc_breaking_indicator",
         "wc_dispersion_stats", "wc_state_upload", "wc_state_download", "wc_step_device", "wc_step_n",
-        "wc_stable_dt_device", "wc_diagnostics_device", "wc_time_device", "wc_synchronize",
-        "wc_set_stream", "wc_profile_enable", "wc_profile_read", "wc_breaking_upload", "wc_breaking_download",
+        "wc_stable_dt_device", "wc_diagnostics_device", "wc_dispersion_system", "wc_time_device", "wc_synchronize",
+        "wc_set_stream", "wc_set_wait_limit", "wc_profile_enable", "wc_profile_read", "wc_breaking_upload", "wc_breaking_download",
         "wc_follow_breaking",
     ):
         getattr(L, name).restype = C.c_int
@@ -213,7 +217,8 @@ def _check(status: int, allow=(abi.WC_OK,)):
 def stable_dt_noalloc(grid, cfl: float, d_h: int, d_hu: int, d_hv: int, stream: int = 0) -> float:
     """`wc_stable_dt_noalloc`: the time-step limit of a state held in the caller's device memory
     (padded FP64 arrays given as device addresses), computed without allocating anything. For
-    callers that cannot allocate device memory at that point, e.g. inside a stream capture."""
+    callers whose device memory all belongs to their own allocator, or that must not allocate per
+    step. The call waits on `stream` and returns the result on the host."""
     g = grid.to_c()
     out = C.c_double()
     _check(
@@ -358,6 +363,18 @@ class Solver(SolverConfig):
         _check(load().wc_diagnostics_device(self._h(), C.byref(d)))
         return d.volume, d.max_abs_momentum, d.min_depth
 
+    def set_wait_limit(self, ns: int) -> None:
+        """`wc_set_wait_limit`: the limit of the persistent kernels' bounded waits (0: 2 s)."""
+        _check(load().wc_set_wait_limit(self._h(), int(ns)))
+
+    def dispersion_system(self) -> dict:
+        """The last dispersive solve's system and solution as the device holds them
+        (`wc_dispersion_system`): (ny, nx) FP64 arrays c, heff, bx, by, wx, wy."""
+        g = self.grid
+        out = {k: np.zeros((g.ny, g.nx)) for k in ("c", "heff", "bx", "by", "wx", "wy")}
+        _check(load().wc_dispersion_system(self._h(), *(abi.dptr(out[k]) for k in ("c", "heff", "bx", "by", "wx", "wy"))))
+        return out
+
     def time_device(self) -> float:
         t = C.c_double()
         _check(load().wc_time_device(self._h(), C.byref(t)))
@@ -445,14 +462,16 @@ class LearnedPreconditioner:
                                               _fptr(g), _fptr(dx)))
         return y, g, dx
 
-    def forward(self, x, feat, tensor: bool = True):
+    def forward(self, x, feat, tensor: bool = True, fused: bool = True):
         """The network's output on [n][2][h][w] arrays: BF16 tensor-core inference (as the solver
-        applies it) or the FP32 path training uses."""
+        applies it; `fused=False` runs the first level one launch per layer) or the FP32 path
+        training uses."""
         x = np.ascontiguousarray(x, dtype=np.float32)
         feat = np.ascontiguousarray(feat, dtype=np.float32)
         n, c, h, w = x.shape
         y = np.zeros_like(x)
-        _check(load().wc_lpc_forward(self._handle, n, h, w, _fptr(x), _fptr(feat), 1 if tensor else 0, _fptr(y)))
+        mode = (1 if fused else 2) if tensor else 0
+        _check(load().wc_lpc_forward(self._handle, n, h, w, _fptr(x), _fptr(feat), mode, _fptr(y)))
         return y
 
     def loss_grad(self, c, heff, bed, e, dx: float, dy: float):
