@@ -46,12 +46,12 @@ SOLVE_ITER_BYTES = (8 * 4 + 8 * 2 + 4 * 2) + 8 * 5  # read r, q, s, diag, p, w, 
 SOLVE_FINISH_BYTES = (44 + 60) / 2              # stage 1 / stage 2 epilogue, averaged
 STAGE_BYTES_SWE = (36 + 52) / 2                 # stage 1 / stage 2 (RK average + damping)
 
-# DRAM bytes per cell measured by ncu (one capture each; scaled to a launch by cells, and by
-# iterations for the solve): profiles/network_conv_2048x1024.md, profiles/pcg_kernel_sgn_2048x1024.md.
+# DRAM bytes per cell measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum of one capture
+# each, on the network at 2048x1024, the solve at 2048x1024 over 57 iterations and the stage at
+# 4096x4096; scaled to a launch by cells, and by iterations for the solve).
 NETWORK_DRAM_BYTES_PER_CELL = 334.1e6 / (2048 * 1024)    # one application of the U-net
 PCG_DRAM_BYTES_PER_CELL_ITER = 10.53e9 / (2048 * 1024 * 57)  # one iteration of the solve
 STAGE_DRAM_BYTES_PER_CELL_SWE = 573.1e6 / (4096 * 4096)      # one second-order stage
-# (profiles/stage_kernel_swe_4096x4096.md)
 
 
 def workload(name: str, eddy: bool = False):

@@ -3,8 +3,8 @@
  *
  * The reference (mlaegn/wavesim, crate `wavecore`) is a Rust library with no FFI. Each entry
  * point below replaces one method or builder of its `Solver` / `State` API, cited as
- * `crates/wavecore/src/<file>.rs:<line>`; a Rust `extern "C"` block can bind this header as is
- * (INTEGRATION.md shows the binding).
+ * `crates/wavecore/src/<file>.rs:<line>`; a Rust `extern "C"` block binds this header as is
+ * (crates/wavecore-b200-sys/src/lib.rs).
  *
  * Conventions shared with the reference:
  *   - every array is "padded": (nx + 2*WC_GHOST) * (ny + 2*WC_GHOST) values, row-major with y
