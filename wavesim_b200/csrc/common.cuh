@@ -108,6 +108,15 @@ __device__ __forceinline__ Mapped map_cell(const DevGrid& g, int i, int j) {
     return m;
 }
 
+// The hardware square root (PTX sqrt.approx.f32: a couple of ulps, exact at 0). The wave speeds
+// and the CFL rate take it: their FP32 values are already further from the FP64 reference than
+// that, and the correctly rounded sqrtf costs several instructions more per call.
+__device__ __forceinline__ float sqrt_approx(float x) {
+    float r;
+    asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 // solver.rs:90-92, with the fast single-precision division (two ulps; the FP32 state is already
 // further from the FP64 reference than that).
 __device__ __forceinline__ float velocity(float h, float hm) { return h > H_DRY ? __fdividef(hm, h) : 0.f; }
@@ -260,9 +269,13 @@ __device__ __forceinline__ void damp_cell(const DampParams& dp, const DevGrid& g
     if (dp.manning > 0.f) {
         const float h32 = (float)h;
         if (h32 > H_FRICTION_MIN) {
-            const float speed = hypotf(hu, hv) / h32;
-            const float k = G * dp.manning * dp.manning / (h32 * cbrtf(h32));
-            const float f = 1.f / (1.f + (float)dt * k * speed);
+            // speed = |hu| / h and k = g n^2 h^(-4/3), from the hardware reciprocal, square root,
+            // log2 and exp2 (a few ulps; the reference's hypot only guards overflow, which physical
+            // momenta cannot reach in FP32)
+            const float inv_h = __fdividef(1.f, h32);
+            const float speed = sqrt_approx(hu * hu + hv * hv) * inv_h;
+            const float k = G * dp.manning * dp.manning * exp2f(-1.3333333f * __log2f(h32));
+            const float f = __fdividef(1.f, 1.f + (float)dt * k * speed);
             hu *= f;
             hv *= f;
         }
@@ -272,7 +285,7 @@ __device__ __forceinline__ void damp_cell(const DampParams& dp, const DevGrid& g
 
 // CFL rate of one cell: solver.rs:94-100.
 __device__ __forceinline__ float cfl_rate(const DevGrid& g, float h, float hu, float hv) {
-    const float c = sqrtf(G * h);
+    const float c = sqrt_approx(G * h);
     const float u = fabsf(velocity(h, hu));
     const float v = fabsf(velocity(h, hv));
     return (u + c) * g.inv_dx + (v + c) * g.inv_dy;

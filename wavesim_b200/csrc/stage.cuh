@@ -104,11 +104,11 @@ struct Side {
     float eta, un, ut, z, h;
 };
 
-// solver.rs:102-116
+// solver.rs:102-116, without branches: the smallest of three positive slopes, the largest of
+// three negative ones, else zero (a zero or mixed-sign triple has min <= 0 <= max).
 __device__ __forceinline__ float minmod3(float a, float b, float c) {
-    if (a > 0.f && b > 0.f && c > 0.f) return fminf(fminf(a, b), c);
-    if (a < 0.f && b < 0.f && c < 0.f) return fmaxf(fmaxf(a, b), c);
-    return 0.f;
+    const float mn = fminf(fminf(a, b), c), mx = fmaxf(fmaxf(a, b), c);
+    return mn > 0.f ? mn : (mx < 0.f ? mx : 0.f);
 }
 
 // solver.rs:118-138, as offsets from the centre value: the reference's
@@ -200,7 +200,7 @@ __device__ __forceinline__ void hll_face(const Side& l, const Side& r, float& F0
         RR = -0.5f * G * hr * hr;
         return;
     }
-    const float cl = sqrtf(G * hl), cr = sqrtf(G * hr);
+    const float cl = sqrt_approx(G * hl), cr = sqrt_approx(G * hr);
     const float sl = fminf(l.un - cl, r.un - cr);
     const float sr = fmaxf(l.un + cl, r.un + cr);
     const float ql = hl * l.un, qr = hr * r.un;   // mass flux = normal momentum

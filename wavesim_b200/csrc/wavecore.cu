@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -24,6 +25,7 @@
 #include "pcg.cuh"
 #include "record.cuh"
 #include "stage.cuh"
+#include "stream.cuh"
 
 using namespace wcb;
 
@@ -151,6 +153,10 @@ struct wc_solver {
     EddyParams eddy{};
     // The limit of every bounded device wait (grid barriers of the persistent kernels).
     unsigned long long wait_ns = BARRIER_TIMEOUT_NS;
+    // Shallow-water stages of first and second order: the register-streaming kernel (stream.cuh),
+    // or, with WAVECORE_B200_STAGE=tiled in the environment at creation, the shared-memory tiled
+    // kernel (stage.cuh) that dispersive and fifth-order stages use; both give the same bits.
+    bool swe_streaming = true;
     double *mem = nullptr, *mem_new = nullptr;
     float* nu = nullptr;
     float2 *mb0 = nullptr, *mb1 = nullptr;
@@ -293,6 +299,16 @@ wc_status launch_stage(wc_solver* s, int mode, const float4* qin, const float4* 
     cudaStream_t st = s->stream;
     ProfScope ps(s, 0);
     const int o = s->order;
+    if (!s->sgn && o <= 1 && s->swe_streaming) {
+        const int strips_x = (s->g.nx + SW_OUT - 1) / SW_OUT;
+        const dim3 sgrid((strips_x + SW_WARPS - 1) / SW_WARPS, (s->g.ny + SW_ROWS - 1) / SW_ROWS);
+        if (mode == MODE_FIRST) swe_stream_kernel<MODE_FIRST, 0, SW_CPL><<<sgrid, SW_NT, 0, st>>>(a, strips_x);
+        else if (mode == MODE_STAGE1) swe_stream_kernel<MODE_STAGE1, 1, SW_CPL><<<sgrid, SW_NT, 0, st>>>(a, strips_x);
+        else swe_stream_kernel<MODE_STAGE2, 1, SW_CPL><<<sgrid, SW_NT, 0, st>>>(a, strips_x);
+        s->launches++;
+        CK(cudaGetLastError());
+        return WC_OK;
+    }
     if (s->sgn) {
         if (o == 0) stage_kernel<MODE_STAGE1, 0, true><<<grid, block, SMEM_SGN, st>>>(a);
         else if (o == 1) stage_kernel<MODE_STAGE1, 1, true><<<grid, block, SMEM_SGN, st>>>(a);
@@ -763,6 +779,10 @@ wc_status wc_solver_create(const wc_grid* grid, const double* bed_padded, const 
         return st;
     };
     s->grid = *grid;
+    {
+        const char* v = std::getenv("WAVECORE_B200_STAGE");
+        s->swe_streaming = !(v && std::strcmp(v, "tiled") == 0);
+    }
     const int nx = (int)grid->nx, ny = (int)grid->ny;
     s->W = nx + 6;
     s->R = ny + 6;
