@@ -374,14 +374,15 @@ def measure_arm(w, args, world, stream, flush, net=None):
     e2e_sol.set_stream(stream.cuda_stream)
     if net is not None:
         e2e_sol.set_preconditioner(net)
-    dt = 0.5 * sol.stable_dt_device()
+    # The reference driver's loop (crates/wavesim/src/lib.rs:1385-1426): the step size from the
+    # state's stable_dt, then the step, both through the C ABI on the host arrays.
     for _ in range(2):
-        e2e_sol.step(hs, dt)
+        e2e_sol.step(hs, e2e_sol.stable_dt(hs))
     n_e2e = max(3, min(args.steps, 50))
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(n_e2e):
-        e2e_sol.step(hs, dt)
+        e2e_sol.step(hs, e2e_sol.stable_dt(hs))
     e2e_s = time.perf_counter() - t0
     e2e_max = rank_max(e2e_s, dist)
     per_solve = lambda a, b: (b.iterations - a.iterations) / max(1, b.solves - a.solves) if b else 0.0  # noqa: E731
@@ -395,9 +396,30 @@ def measure_arm(w, args, world, stream, flush, net=None):
         "launches": int(launches),
         "clocks": clocks.summary(),
         "e2e": {"value": cells * n_e2e * world / e2e_max, "unit": UNIT,
-                "h2d_bytes_per_step": 3 * w.grid.cells() * 8, "d2h_bytes_per_step": 3 * w.grid.cells() * 8,
-                "steps": n_e2e, "path": "wc_step on pinned host FP64 arrays (upload, step, download per call)"},
+                "h2d_bytes_per_step": 6 * w.grid.cells() * 8 + 24, "d2h_bytes_per_step": 3 * w.grid.cells() * 8 + 24,
+                "steps": n_e2e,
+                "path": "per step wc_stable_dt then wc_step on pinned host FP64 arrays (each uploads the state; "
+                        "the step downloads it), as the reference's driver loop calls stable_dt and step"},
     }
+
+
+def true_residuals(w, arms):
+    """The true FP64 relative residual ||b - A w|| / ||b|| of each arm's last dispersive solve (the
+    device stops on its recursively updated FP32 residual at the tolerance), the oracle's FP64
+    Jacobi PCG on the same system from zero, and that FP64 solution rounded to FP32 (the floor any
+    FP32-stored solution has)."""
+    from oracle.oracle import pcg_solve, true_relative_residual
+
+    out = {"tolerance": w.dispersion.tolerance}
+    f32 = lambda a: np.asarray(a, dtype=np.float32).astype(np.float64)  # noqa: E731
+    for k, sol in arms.items():
+        sysd = sol.dispersion_system()
+        wx, wy, it, conv = pcg_solve(w.grid, w.periodic_y, sysd, w.dispersion.tolerance, 2000)
+        out[k] = {"device": true_relative_residual(w.grid, w.periodic_y, sysd),
+                  "oracle_fp64_same_system": true_relative_residual(w.grid, w.periodic_y, {**sysd, "wx": wx, "wy": wy}),
+                  "oracle_iterations_from_zero": it,
+                  "fp32_solution_floor": true_relative_residual(w.grid, w.periodic_y, {**sysd, "wx": f32(wx), "wy": f32(wy)})}
+    return out
 
 
 def eta_errors(w, net, steps: int):
@@ -421,7 +443,7 @@ def eta_errors(w, net, steps: int):
             sol.step(ss[k], dt)
     g = w.grid
     ho = g.inner(so.h)
-    out = {}
+    out = {"true_rel_residual": true_residuals(w, arms)}
     for k, s in ss.items():
         hg = g.inner(s.h)
         wet = (hg > 1e-3) & (ho > 1e-3)

@@ -1,7 +1,10 @@
 """Training of the learned preconditioner on the GPU, on SGN systems the solver itself generates.
 
 Runs of the seeded beach workload draw a swell height H ~ U(0.5, 4) m, a period T ~ U(8, 18) s
-and an angle ~ U(-20, 20) degrees (and their own random bed); each run starts from its linear
+and an angle ~ U(-20, 20) degrees (and their own random bed); the harvest runs have walls at
+their y ends, so the maker takes the drawn angle exactly (a periodic width would snap it to the
+nearest angle that fits, which on a 512 m harvest grid leaves most draws at 0 degrees or outside
+the range); each run starts from its linear
 wave train and, every few steps, hands the system of its last dispersive solve (c, h, bed) to
 the network (`LearnedPreconditioner.harvest`). Training then takes Adam steps on batches of
 random patches of those systems with random error fields (`LearnedPreconditioner.train`): every
@@ -23,8 +26,10 @@ from .solver import LearnedPreconditioner, Solver
 
 
 def harvest_runs(net: LearnedPreconditioner, runs: int = 8, nx: int = 512, ny: int = 256, dx: float = 2.0,
-                 steps: int = 120, every: int = 20, seed: int = 0) -> dict:
-    """`runs` solver runs of `steps` steps each, harvested every `every` steps."""
+                 steps: int = 120, every: int = 20, seed: int = 0, validation: list | None = None) -> dict:
+    """`runs` solver runs of `steps` steps each, harvested every `every` steps. With `validation`
+    (a list), each run's last system is also appended to it whole, with its right-hand side and
+    converged solution: (c, heff, bed, bx, by, wx, wy) as (ny, nx) FP32 arrays."""
     rng = np.random.default_rng(seed)
     draws = []
     t0 = time.perf_counter()
@@ -33,13 +38,17 @@ def harvest_runs(net: LearnedPreconditioner, runs: int = 8, nx: int = 512, ny: i
         period = float(rng.uniform(8.0, 18.0))
         angle = float(rng.uniform(-20.0, 20.0))
         w = W.sgn_beach(nx, ny, dx, seed=int(rng.integers(1 << 30)), height=height, period=period, angle_deg=angle,
-                        name=f"harvest_{r}")
+                        name=f"harvest_{r}", periodic=False)
         sol = w.solver(Solver)
         sol.upload(W.wave_train_state(w))
         for _ in range(steps // every):
             sol.step_n(every)
             sol.synchronize()
             net.harvest(sol)
+        if validation is not None:
+            sysd = sol.dispersion_system()
+            sysd["bed"] = w.grid.inner(w.bed.b).copy()
+            validation.append({k: np.asarray(v, dtype=np.float32) for k, v in sysd.items()})
         draws.append({"H_m": round(height, 3), "T_s": round(period, 3), "angle_deg": round(w.meta["angle_deg"], 3)})
     return {"runs": runs, "grid": f"{nx}x{ny} at {dx:g} m", "systems": net.n_systems, "draws": draws,
             "seconds": time.perf_counter() - t0}
@@ -60,12 +69,43 @@ def train(net: LearnedPreconditioner, steps: int = 20000, batch: int = 16, patch
             "seconds": time.perf_counter() - t0}
 
 
+def validation_loss(net: LearnedPreconditioner, systems: list, dx: float, patch: int = 64, per_system: int = 8,
+                    seed: int = 1) -> float:
+    """The training objective on SGN systems harvested whole from solver runs (depth, bed, right-hand
+    side, converged solution), with the converged solution itself as the error field: on random
+    patches (zero outside, as in training), the mean of <d, A d> / <e, A e> with d = e - M A e is
+    the share of a real solution's energy that one application of the preconditioner leaves."""
+    rng = np.random.default_rng(seed)
+    cs, hs, bs, es = [], [], [], []
+    for sy in systems:
+        ny, nx = sy["c"].shape
+        for _ in range(per_system):
+            y0 = int(rng.integers(0, ny - patch + 1))
+            x0 = int(rng.integers(0, nx - patch + 1))
+            sl = (slice(y0, y0 + patch), slice(x0, x0 + patch))
+            wet = sy["heff"][sl] >= np.float32(0.05)
+            cs.append(sy["c"][sl])
+            hs.append(sy["heff"][sl])
+            bs.append(sy["bed"][sl])
+            es.append(np.stack([sy["wx"][sl] * wet, sy["wy"][sl] * wet]))
+    loss, _ = net.loss_grad(np.stack(cs), np.stack(hs), np.stack(bs), np.stack(es), dx, dx)
+    return float(loss)
+
+
 def trained_network(dx: float = 2.0, steps: int = 20000, seed: int = 0, spec: UNetSpec | None = None):
-    """A network harvested and trained from scratch on this GPU; returns (network, record)."""
-    net = LearnedPreconditioner(spec or UNetSpec(), seed=seed)
-    h = harvest_runs(net, dx=dx, seed=seed)
+    """A network harvested and trained from scratch on this GPU; returns (network, record). The
+    record holds the validation loss on the harvest runs' whole systems (their right-hand sides and
+    converged solutions) for the trained network and for the same cycle without a network (an
+    untrained network's output layer is zero: the two Jacobi sweeps alone)."""
+    spec = spec or UNetSpec()
+    net = LearnedPreconditioner(spec, seed=seed)
+    val = []
+    h = harvest_runs(net, dx=dx, seed=seed, validation=val)
     t = train(net, steps=steps, seed=seed)
-    return net, {"harvest": h, "training": t, "params": net.n_params}
+    v = {"systems": len(val), "patches": 8 * len(val), "error_field": "the converged solution of the system",
+         "loss_trained": validation_loss(net, val, dx),
+         "loss_without_network": validation_loss(LearnedPreconditioner(spec, seed=seed), val, dx)}
+    return net, {"harvest": h, "training": t, "validation": v, "params": net.n_params}
 
 
 def main():

@@ -118,12 +118,13 @@ def config1() -> Workload:
 
 def sgn_beach(nx: int, ny: int, dx: float, seed: int, tolerance: float = 1e-8, height: float = 2.0,
               period: float = 14.0, angle_deg: float = 15.0, sigma_bed: float = 0.5, corr: float = 20.0,
-              name: str | None = None, steps: int = 5000, preconditioner: int = 0) -> Workload:
+              name: str | None = None, steps: int = 5000, preconditioner: int = 0, periodic: bool = True) -> Workload:
     """Fifth order + SGN by PCG, periodic in y: a 20 m shelf, then a 1:30 beach whose still-water
     shoreline is at 0.85 Lx, plus a Gaussian random field; maker H, T at x = 160 m (0.15 Lx on
     small grids) in ~20 m,
     oblique at the angle nearest `angle_deg` that fits the periodic width; a 100 m sponge at the
-    offshore edge; Manning 0.02; CFL 0.4."""
+    offshore edge; Manning 0.02; CFL 0.4. With `periodic=False` the y ends are walls and the maker
+    takes `angle_deg` itself (an oblique maker needs no fit between walls)."""
     grid = Grid(nx, ny, dx, dx)
     lx, ly = nx * dx, ny * dx
     base = shelf_and_beach(grid, 20.0, 1.0 / 30.0, 0.85 * lx)
@@ -133,7 +134,10 @@ def sgn_beach(nx: int, ny: int, dx: float, seed: int, tolerance: float = 1e-8, h
     i_m = min(max(int(round(maker_x / dx - 0.5)), 0), nx - 1)
     depth = -b[ny // 2, i_m]
     omega = 2.0 * math.pi / period
-    angle, turns = snapped_angle(omega, depth, ly, math.radians(angle_deg), True)
+    if periodic:
+        angle, turns = snapped_angle(omega, depth, ly, math.radians(angle_deg), True)
+    else:
+        angle, turns = math.radians(angle_deg), None
     maker = WaveMaker(x=maker_x, amplitude=height / 2.0, period=period, angle=angle, sigma=2.0 * dx, ramp_periods=4.0)
     return Workload(
         name=name or f"sgn_beach_{nx}x{ny}_dx{dx:g}",
@@ -142,7 +146,7 @@ def sgn_beach(nx: int, ny: int, dx: float, seed: int, tolerance: float = 1e-8, h
         order=Order.Fifth,
         cfl=0.4,
         manning=0.02,
-        periodic_y=True,
+        periodic_y=periodic,
         sponges=[Sponge(int(round(100.0 / dx)), 1.5).edges(True, False, False, False)],
         maker=maker,
         dispersion=Dispersion(tolerance=tolerance, max_iterations=1000, preconditioner=preconditioner),
