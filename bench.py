@@ -78,8 +78,67 @@ REF_BUDGET_S = 120.0  # the reference arm's timed CPU sample
 EDDY_SUBSTEP_BYTES = 28
 
 
+def time_ensemble(ens, n_members, steps, warmup, flush, clocks_gpu, dist=None):
+    """Warm-up steps, then `steps` timed steps of every member (host wall clock around each
+    synchronised step; L2 flushed between steps): (seconds, PCG iterations per solve, launches, clocks)."""
+    import torch
+
+    ens.step_n(warmup)
+    ens.synchronize()
+    l0 = ens.launch_count()
+    it0 = [ens.member_stats(m)[0] for m in range(n_members)]
+    torch.cuda.synchronize()
+    times = []
+    if dist:
+        dist.barrier()
+    with ClockSampler(clocks_gpu) as clocks:
+        for _ in range(steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            ens.step_n(1)
+            ens.synchronize()
+            times.append(time.perf_counter() - t0)
+    it1 = [ens.member_stats(m)[0] for m in range(n_members)]
+    solves = sum(b.solves - a.solves for a, b in zip(it0, it1))
+    iters = sum(b.iterations - a.iterations for a, b in zip(it0, it1)) / max(1, solves)
+    return sum(times), iters, int(ens.launch_count() - l0), clocks.summary()
+
+
+def members_alone(ws, net, steps: int, flush):
+    """The same members run one at a time by standalone solvers (the network attached to the
+    dispersive ones when given): the sum of their device-timed steps, per ensemble step."""
+    import torch
+
+    from wavesim_b200 import Solver
+
+    total_ms = 0.0
+    for w in ws:
+        sol = w.solver(Solver)
+        if net is not None and w.dispersion is not None:
+            sol.set_preconditioner(net)
+        sol.upload(W.wave_train_state(w))
+        sol.step_n(2)
+        sol.synchronize()
+        st = torch.cuda.current_stream()
+        sol.set_stream(st.cuda_stream)
+        for _ in range(steps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(st)
+            sol.step_n(1)
+            b.record(st)
+            b.synchronize()
+            total_ms += a.elapsed_time(b)
+        del sol
+    return total_ms / steps
+
+
 def run_ensemble(args, world, rank, local):
-    """The 64-member ensemble (config 4): every timed step advances every member one step."""
+    """The 64-member ensemble (config 4): every timed step advances every member one step. With the
+    learned preconditioner (the default --pc), the network is trained first and the learned
+    ensemble is the reported value, beside the same ensemble by plain PCG in one persistent launch
+    per step and the learned members run one at a time."""
     import torch
 
     from wavesim_b200 import Ensemble, Solver
@@ -95,46 +154,58 @@ def run_ensemble(args, world, rank, local):
                                 device_id=torch.device("cuda", local))
     ws = W.config4(seed=4 + 1000 * rank)
     cells = sum(w.interior_cells() for w in ws)
-    ens = Ensemble([w.solver(Solver) for w in ws])
-    starts = [W.wave_train_state(w) for w in ws]
-    for m, s0 in enumerate(starts):
-        ens.upload(m, s0)
-    choice, tune_ms = ens.autotune(2)
-    ens.step_n(args.warmup)
-    ens.synchronize()
-    l0 = ens.launch_count()
-    it0 = [ens.member_stats(m)[0] for m in range(len(ws))]
-    torch.cuda.synchronize()
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
-    times = []
-    if dist:
-        dist.barrier()
-    with ClockSampler(local) as clocks:
-        for _ in range(args.steps):
-            flush.zero_()
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            ens.step_n(1)
-            ens.synchronize()
-            times.append(time.perf_counter() - t0)
-    it1 = [ens.member_stats(m)[0] for m in range(len(ws))]
-    iters = sum(b.iterations - a.iterations for a, b in zip(it0, it1)) / max(1, sum(b.solves - a.solves for a, b in zip(it0, it1)))
-    total = rank_max(sum(times), dist)  # the slowest rank's time
-    value = rank_sum(float(cells), dist) * args.steps / total  # every rank's members
+    learned = args.pc == "learned"
+    net, train_rec = None, None
+    if learned:
+        from wavesim_b200.lpc import UNetSpec
+        from wavesim_b200.train_lpc import trained_network
+
+        chans = tuple(int(c) for c in args.lpc_channels.split(","))
+        net, train_rec = trained_network(dx=2.5, steps=args.train_steps, spec=UNetSpec(channels=chans))
+
+    def arm(with_net):
+        ens = Ensemble([w.solver(Solver) for w in ws])
+        if with_net is not None:
+            ens.set_preconditioner(with_net)
+        for m, w in enumerate(ws):
+            ens.upload(m, W.wave_train_state(w))
+        choice, tune_ms = ens.autotune(2)
+        sec, iters, launches, clocks = time_ensemble(ens, len(ws), args.steps, args.warmup, flush, local, dist)
+        total = rank_max(sec, dist)  # the slowest rank's time
+        return {"value": rank_sum(float(cells), dist) * args.steps / total, "ms_per_step": 1e3 * total / args.steps,
+                "iterations_per_solve": iters, "launches": launches, "clocks": clocks,
+                "variant": Ensemble.VARIANTS[choice] if choice >= 0 else "members' own step graphs on their own streams",
+                "autotune_ms_per_step": tune_ms}
+
+    main = arm(net)
+    plain = arm(None) if learned else None
+    alone_ms = members_alone(ws, net, max(2, min(args.steps, 5)), flush) if rank == 0 else None
     if rank == 0:
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
+            "metric": METRIC, "value": main["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": main["ms_per_step"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "ensemble_64_uneven_beaches", "members": len(ws), "cells": cells,
-                       "scheme": "fifth order + SGN", "preconditioner": "jacobi (plain PCG)", "tolerance": 1e-8,
-                       "pcg_iterations_per_solve": iters,
-                       "autotuned_variant": Ensemble.VARIANTS[choice], "autotune_ms_per_step": tune_ms,
+                       "scheme": "fifth order + SGN",
+                       "preconditioner": "learned (flexible CG)" if learned else "jacobi (plain PCG)", "tolerance": 1e-8,
+                       "pcg_iterations_per_solve": main["iterations_per_solve"], "variant": main["variant"],
+                       "autotune_ms_per_step": main["autotune_ms_per_step"],
                        "timing": "host wall clock around each synchronised ensemble step",
                        "l2": "flushed between timed steps (256 MiB write outside the timed region)"},
-            "gpu_launches": int(ens.launch_count() - l0),
-            "clocks": clocks.summary(),
+            "gpu_launches": main["launches"],
+            "clocks": main["clocks"],
+            "members_alone": {"ms_per_step": alone_ms, "value": cells / (alone_ms / 1e3),
+                              "ensemble_speedup": alone_ms / main["ms_per_step"],
+                              "how": "each member by a standalone solver, device-timed steps summed"},
         }
+        if plain is not None:
+            line["plain_pcg"] = {"value": plain["value"], "ms_per_step": plain["ms_per_step"],
+                                 "iterations_per_solve": plain["iterations_per_solve"], "variant": plain["variant"],
+                                 "autotune_ms_per_step": plain["autotune_ms_per_step"],
+                                 "gpu_launches": plain["launches"], "clocks": plain["clocks"]}
+            line["learned_vs_plain"] = main["value"] / plain["value"]
+            line["training"] = train_rec
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

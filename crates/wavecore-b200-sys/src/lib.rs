@@ -232,6 +232,7 @@ extern "C" {
     pub fn wc_ensemble_step_n(e: *mut wc_ensemble, n_steps: u64, t_end: f64) -> wc_status;
     pub fn wc_ensemble_autotune(e: *mut wc_ensemble, trial_steps: u32, choice: *mut i32,
                                 ms_per_step: *mut f64) -> wc_status;
+    pub fn wc_ensemble_set_lpc(e: *mut wc_ensemble, l: *mut wc_lpc) -> wc_status;
     pub fn wc_ensemble_synchronize(e: *mut wc_ensemble) -> wc_status;
     pub fn wc_ensemble_member_stats(e: *mut wc_ensemble, member: u64, stats: *mut wc_stats,
                                     time: *mut f64) -> wc_status;

@@ -280,10 +280,13 @@ wc_status wc_stable_dt_noalloc(const wc_grid* grid, double cfl, const double* d_
  * n independent runs, each with its own grid, bed (padded FP64) and configuration (second or
  * fifth order), advanced together: every step of every member is one persistent cooperative
  * launch, replayed from a CUDA graph, in which each member's own group of CTAs runs its whole
- * SSP-RK2 step with its own adaptive time step, clock and PCG state. The stage tile shape and
- * the CTAs per SM are chosen by an autotuner that times each compiled variant on the live state
- * (then restores it); wc_ensemble_step_n runs it on first use. */
+ * SSP-RK2 step with its own adaptive time step, clock and PCG state. The CTAs are split over the
+ * members by their work per step (cells, and the PCG iterations per solve the autotuner measures
+ * on its first call). The stage tile shape and the CTAs per SM are chosen by an autotuner that
+ * times each compiled variant on the live state (then restores it); wc_ensemble_step_n runs it on
+ * first use. */
 typedef struct wc_ensemble wc_ensemble;
+typedef struct wc_lpc wc_lpc;  /* the learned preconditioner, below */
 wc_status wc_ensemble_create(uint64_t n, const wc_grid* grids, const double* const* beds,
                              const wc_config* cfgs, wc_ensemble** out);
 void wc_ensemble_destroy(wc_ensemble* e);
@@ -296,9 +299,17 @@ wc_status wc_ensemble_download(wc_ensemble* e, uint64_t member, double* h, doubl
 wc_status wc_ensemble_step_n(wc_ensemble* e, uint64_t n_steps, double t_end);
 /* Time every variant over trial_steps steps and keep the fastest; *choice is its index (stage
  * tile height 8 or 16 by CTAs per SM 1 or 2: 0 = 8/1, 1 = 8/2, 2 = 16/1, 3 = 16/2) and
- * ms_per_step[4] the measured times (-1 for a variant that cannot run). */
+ * ms_per_step[4] the measured times (-1 for a variant that cannot run). A learned ensemble
+ * (wc_ensemble_set_lpc) has no variants: *choice is -1 and ms_per_step[0] its time per step. */
 wc_status wc_ensemble_autotune(wc_ensemble* e, uint32_t trial_steps, int32_t* choice,
                                double* ms_per_step);
+/* The learned preconditioner for every dispersive member (config 4's method). The network's
+ * solve is a chain of kernels with a data-dependent loop, which a persistent launch cannot hold,
+ * so a learned ensemble steps each member through its own captured step (the flexible CG's
+ * while-node included) on its own stream, forked from the ensemble's stream and joined back every
+ * step, so the members' kernels overlap on the GPU. Call once, before stepping; the network must
+ * outlive the ensemble. */
+wc_status wc_ensemble_set_lpc(wc_ensemble* e, wc_lpc* l);
 wc_status wc_ensemble_synchronize(wc_ensemble* e);
 wc_status wc_ensemble_member_stats(wc_ensemble* e, uint64_t member, wc_stats* stats,
                                    double* time);
@@ -315,7 +326,6 @@ uint64_t wc_ensemble_launch_count(const wc_ensemble* e);
  * method stays the fallback and the arbiter of convergence. Training runs on
  * the GPU by the library's own forward and backward kernels, on patches of SGN systems harvested
  * from solver runs, minimising the energy norm of the cycle's error on random error fields. */
-typedef struct wc_lpc wc_lpc;
 
 /* channels[4]: feature maps per level, finest first (null: 8, 16, 32, 32); gate_hidden: width of
  * the gate networks' hidden layer (8); stride 1, 2 or 4: the network runs on a grid that many

@@ -56,3 +56,39 @@ def test_ensemble_members_stop_at_their_end_time():
     for m in range(len(ws)):
         _, t = ens.member_stats(m)
         assert abs(t - 57.0) < 1e-9
+
+
+def test_learned_ensemble_members_match_standalone_learned_runs():
+    """With the learned preconditioner attached, every member steps through its own captured step
+    on its own stream: the same kernels as a standalone solver with the same network, so the same
+    bits."""
+    from wavesim_b200 import LearnedPreconditioner
+    from wavesim_b200.lpc import UNetSpec
+
+    net = LearnedPreconditioner(UNetSpec(), seed=3)
+    ws = _members()
+    ens = Ensemble([w.solver(Solver) for w in ws])
+    ens.set_preconditioner(net)
+    starts = [W.wave_train_state(w) if w.dispersion else State.lake_at_rest(w.grid, w.bed, 0.0) for w in ws]
+    for m, s0 in enumerate(starts):
+        ens.upload(m, s0)
+    choice, ms = ens.autotune(2)
+    assert choice == -1 and ms[0] > 0
+    ens.step_n(20)
+    ens.synchronize()
+    for m, (w, s0) in enumerate(zip(ws, starts)):
+        ref = w.solver(Solver)
+        if w.dispersion:
+            ref.set_preconditioner(net)
+        ref.upload(s0)
+        ref.step_n(20)
+        ref.synchronize()
+        a, b = s0.clone(), s0.clone()
+        ens.download(m, a)
+        ref.download(b)
+        assert a.time == b.time, m
+        assert np.array_equal(a.h, b.h) and np.array_equal(a.hu, b.hu) and np.array_equal(a.hv, b.hv), m
+        st, _ = ens.member_stats(m)
+        if w.dispersion:
+            assert st.solves == 40 and st.unconverged == 0
+    assert ens.launch_count() > 0

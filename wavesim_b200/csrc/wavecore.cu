@@ -1329,7 +1329,8 @@ constexpr int EN_VARIANTS = 4;  // stage tile height {8, 16} x CTAs per SM {1, 2
 
 struct EnVariant {
     int ty, minb;
-    int ctas = 0;
+    int ctas = 0;    // CTAs of the launch
+    int budget = 0;  // CTAs the split may hand out (co-resident ones, at least one per member)
     std::vector<EnsembleMember> table;
     EnsembleMember* d_table = nullptr;
     int* d_cta_member = nullptr;
@@ -1384,6 +1385,18 @@ struct wc_ensemble {
     std::vector<float4*> snap_q;
     std::vector<float2*> snap_w;
     unsigned long long launches = 0;
+    // Work per member and step, the persistent launch's CTA split: algorithmic bytes per cell of
+    // a step times cells (shallow water 88; dispersive 368 + 192 I with I the member's measured
+    // PCG iterations per solve, 55 until the autotuner has measured it).
+    std::vector<double> work;
+    bool work_measured = false;
+    // With a learned preconditioner attached (wc_ensemble_set_lpc), every member steps through its
+    // own captured step (the flexible CG's while-node included) on its own stream; a step forks
+    // from the ensemble's stream to the members' and joins back.
+    bool learned = false;
+    std::vector<cudaStream_t> member_streams;
+    std::vector<cudaEvent_t> member_done;
+    cudaEvent_t fork = nullptr;
 
     ~wc_ensemble() {
         if (stream) cudaStreamSynchronize(stream);
@@ -1397,21 +1410,24 @@ struct wc_ensemble {
         if (counters) cudaFree(counters);
         if (partials) cudaFree(partials);
         for (auto m : members) wc_solver_destroy(m);
+        for (auto ev : member_done) cudaEventDestroy(ev);
+        if (fork) cudaEventDestroy(fork);
+        for (auto st : member_streams) cudaStreamDestroy(st);
         if (stream) cudaStreamDestroy(stream);
     }
 };
 
 namespace {
 
-// Split `ctas` CTAs over the members in proportion to their cells (at least one each, at most
-// one per PCG tile), and fill the member table of one variant.
+// Split `ctas` CTAs over the members in proportion to their work per step (at least one each, at
+// most one per PCG or stage tile), and fill the member table of one variant.
 wc_status build_variant(wc_ensemble* e, EnVariant& v, int ctas) {
     const size_t n = e->members.size();
-    std::vector<double> cells(n);
+    std::vector<double> cells(n);  // the member's work, in the units of e->work
     double total = 0;
     std::vector<int> cap(n);
     for (size_t m = 0; m < n; m++) {
-        cells[m] = (double)e->members[m]->g.nx * e->members[m]->g.ny;
+        cells[m] = e->work[m];
         total += cells[m];
         const int tiles_pcg = e->members[m]->pcg_tiles_x * e->members[m]->pcg_tiles_y;
         const int tiles_st = ((e->members[m]->g.nx + ST_TX - 1) / ST_TX) * ((e->members[m]->g.ny + v.ty - 1) / v.ty);
@@ -1462,6 +1478,10 @@ wc_status build_variant(wc_ensemble* e, EnVariant& v, int ctas) {
             M.pcg[k].cnt = e->counters + 2 * m;
             M.pcg[k].part = e->partials + 8 * (size_t)m * e->max_ctas;
         }
+    }
+    if (v.graph) {  // the captured launch holds the previous grid size
+        CK(cudaGraphExecDestroy(v.graph));
+        v.graph = nullptr;
     }
     if (!v.d_table) CK(cudaMalloc(&v.d_table, n * sizeof(EnsembleMember)));
     if (!v.d_cta_member) CK(cudaMalloc(&v.d_cta_member, (size_t)e->max_ctas * EN_VARIANTS * sizeof(int)));
@@ -1514,9 +1534,33 @@ wc_status ensemble_finish(wc_ensemble* e) {
     return WC_OK;
 }
 
+// Work per member and step from the cells and the PCG iterations per solve (see wc_ensemble).
+double member_work(const wc_solver* s, double iterations) {
+    const double cells = (double)s->g.nx * s->g.ny;
+    return s->sgn ? cells * (368.0 + 192.0 * iterations) : cells * 88.0;
+}
+
+// One step of a learned ensemble: every member's own step graph on its own stream, forked from
+// and joined back to the ensemble's stream.
+wc_status ensemble_step_members(wc_ensemble* e) {
+    CK(cudaEventRecord(e->fork, e->stream));
+    for (size_t m = 0; m < e->members.size(); m++) {
+        wc_solver* s = e->members[m];
+        CK(cudaStreamWaitEvent(s->stream, e->fork, 0));
+        TRY(enqueue_step(s));
+        CK(cudaEventRecord(e->member_done[m], s->stream));
+        CK(cudaStreamWaitEvent(e->stream, e->member_done[m], 0));
+    }
+    e->launches++;
+    return WC_OK;
+}
+
 // The autotuner: every compiled variant runs `trial` steps on a snapshot of the live state
 // (timed with events on the ensemble's stream), the state and clocks are restored after each,
-// and the fastest variant is kept.
+// and the fastest variant is kept. Before that, on its first call, one trial of the cell-split
+// launch measures each member's PCG iterations per solve, and the CTAs of every variant are
+// split again by the work that gives. A learned ensemble has no variants: its trial times the
+// members' own steps.
 wc_status ensemble_tune(wc_ensemble* e, int trial) {
     const size_t n = e->members.size();
     if (e->snap_q.empty()) {
@@ -1537,9 +1581,59 @@ wc_status ensemble_tune(wc_ensemble* e, int trial) {
         CK(cudaMemcpyAsync(&ctl[m], s->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, e->stream));
     }
     CK(cudaStreamSynchronize(e->stream));
+    auto restore = [&]() -> wc_status {
+        for (size_t m = 0; m < n; m++) {  // the state, the warm start and the clock
+            wc_solver* s = e->members[m];
+            CK(cudaMemcpyAsync(s->q0, e->snap_q[m], s->ncell * sizeof(float4), cudaMemcpyDeviceToDevice, e->stream));
+            if (s->sgn) CK(cudaMemcpyAsync(s->w, e->snap_w[m], s->ncell * sizeof(float2), cudaMemcpyDeviceToDevice, e->stream));
+            CK(cudaMemcpyAsync(s->ctl, &ctl[m], sizeof(Ctl), cudaMemcpyHostToDevice, e->stream));
+            s->rate_current = false;
+        }
+        CK(cudaStreamSynchronize(e->stream));
+        return WC_OK;
+    };
     cudaEvent_t a, b;
     CK(cudaEventCreate(&a));
     CK(cudaEventCreate(&b));
+    if (e->learned) {
+        TRY(ensemble_prepare(e, INFINITY));
+        TRY(ensemble_step_members(e));  // capture and warm
+        CK(cudaEventRecord(a, e->stream));
+        for (int t = 0; t < trial; t++) TRY(ensemble_step_members(e));
+        CK(cudaEventRecord(b, e->stream));
+        CK(cudaEventSynchronize(b));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, a, b));
+        for (int k = 0; k < EN_VARIANTS; k++) e->tune_ms[k] = -1.0;
+        e->tune_ms[0] = ms / trial;
+        e->chosen = -1;
+        TRY(restore());
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        TRY(ensemble_finish(e));
+        return WC_OK;
+    }
+    if (!e->work_measured) {
+        int k0 = 0;
+        while (k0 < EN_VARIANTS && e->var[k0].ctas <= 0) k0++;
+        if (k0 < EN_VARIANTS) {
+            TRY(ensemble_prepare(e, INFINITY));
+            for (int t = 0; t < std::max(1, trial); t++) TRY(ensemble_step(e, e->var[k0]));
+            CK(cudaStreamSynchronize(e->stream));
+            for (size_t m = 0; m < n; m++) {
+                wc_solver* s = e->members[m];
+                Ctl c{};
+                CK(cudaMemcpy(&c, s->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost));
+                const unsigned long long solves = c.solves - ctl[m].solves;
+                const double it = solves ? (double)(c.iterations - ctl[m].iterations) / (double)solves : 55.0;
+                e->work[m] = member_work(s, it);
+            }
+            TRY(restore());
+            for (int k = 0; k < EN_VARIANTS; k++)
+                if (e->var[k].ctas > 0) TRY(build_variant(e, e->var[k], e->var[k].budget));
+        }
+        e->work_measured = true;
+    }
     double best = 1e300;
     for (int k = 0; k < EN_VARIANTS; k++) {
         if (e->var[k].ctas <= 0) {
@@ -1559,14 +1653,7 @@ wc_status ensemble_tune(wc_ensemble* e, int trial) {
             best = ms;
             e->chosen = k;
         }
-        for (size_t m = 0; m < n; m++) {  // restore the state, the warm start and the clock
-            wc_solver* s = e->members[m];
-            CK(cudaMemcpyAsync(s->q0, e->snap_q[m], s->ncell * sizeof(float4), cudaMemcpyDeviceToDevice, e->stream));
-            if (s->sgn) CK(cudaMemcpyAsync(s->w, e->snap_w[m], s->ncell * sizeof(float2), cudaMemcpyDeviceToDevice, e->stream));
-            CK(cudaMemcpyAsync(s->ctl, &ctl[m], sizeof(Ctl), cudaMemcpyHostToDevice, e->stream));
-            s->rate_current = false;
-        }
-        CK(cudaStreamSynchronize(e->stream));
+        TRY(restore());
     }
     cudaEventDestroy(a);
     cudaEventDestroy(b);
@@ -1622,11 +1709,38 @@ wc_status wc_ensemble_create(uint64_t n, const wc_grid* grids, const double* con
     wc_status st;
     if ((st = dalloc(&e->counters, 2 * n)) != WC_OK) return fail(st);
     if ((st = dalloc(&e->partials, 8 * n * (size_t)max_ctas)) != WC_OK) return fail(st);
+    e->work.resize(n);
+    for (uint64_t m = 0; m < n; m++) e->work[m] = member_work(e->members[m], 55.0);
     for (int k = 0; k < EN_VARIANTS; k++) {
         if (e->var[k].ctas <= 0) continue;
-        if ((st = build_variant(e, e->var[k], std::max((int)n, e->var[k].ctas))) != WC_OK) return fail(st);
+        e->var[k].budget = std::max((int)n, e->var[k].ctas);
+        if ((st = build_variant(e, e->var[k], e->var[k].budget)) != WC_OK) return fail(st);
     }
     *out = e;
+    return WC_OK;
+}
+
+wc_status wc_ensemble_set_lpc(wc_ensemble* e, wc_lpc* l) {
+    if (!e || !l) return set_err(WC_EINVAL, "null argument");
+    if (e->learned) return set_err(WC_EINVAL, "the ensemble already has a learned preconditioner");
+    CK(cudaStreamSynchronize(e->stream));
+    const size_t n = e->members.size();
+    for (size_t m = 0; m < n; m++) {
+        cudaStream_t st = nullptr;
+        cudaEvent_t ev = nullptr;
+        CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        e->member_streams.push_back(st);
+        CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        e->member_done.push_back(ev);
+    }
+    CK(cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming));
+    for (size_t m = 0; m < n; m++) {
+        wc_solver* s = e->members[m];
+        s->stream = e->member_streams[m];
+        if (s->sgn) TRY(wc_solver_set_lpc(s, l));
+    }
+    e->learned = true;
+    e->chosen = -1;
     return WC_OK;
 }
 
@@ -1654,9 +1768,12 @@ wc_status wc_ensemble_autotune(wc_ensemble* e, uint32_t trial_steps, int32_t* ch
 
 wc_status wc_ensemble_step_n(wc_ensemble* e, uint64_t n_steps, double t_end) {
     if (!e) return set_err(WC_EINVAL, "null ensemble");
-    if (e->chosen < 0) TRY(ensemble_tune(e, 2));
+    if (!e->learned && e->chosen < 0) TRY(ensemble_tune(e, 2));
     TRY(ensemble_prepare(e, t_end));
-    for (uint64_t k = 0; k < n_steps; k++) TRY(ensemble_step(e, e->var[e->chosen]));
+    for (uint64_t k = 0; k < n_steps; k++) {
+        if (e->learned) TRY(ensemble_step_members(e));
+        else TRY(ensemble_step(e, e->var[e->chosen]));
+    }
     TRY(ensemble_finish(e));
     return WC_OK;
 }
@@ -1681,7 +1798,13 @@ wc_status wc_ensemble_member_stats(wc_ensemble* e, uint64_t m, wc_stats* stats, 
     return WC_OK;
 }
 
-uint64_t wc_ensemble_launch_count(const wc_ensemble* e) { return e ? e->launches : 0; }
+uint64_t wc_ensemble_launch_count(const wc_ensemble* e) {
+    if (!e) return 0;
+    uint64_t n = e->launches;
+    if (e->learned)  // the members' own steps: their kernels, the flexible CG's iterations included
+        for (const wc_solver* s : e->members) n += wc_launch_count(s);
+    return n;
+}
 
 }  // extern "C"
 

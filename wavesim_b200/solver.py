@@ -61,6 +61,7 @@ EXPORTS = [
     "wc_ensemble_download",
     "wc_ensemble_step_n",
     "wc_ensemble_autotune",
+    "wc_ensemble_set_lpc",
     "wc_ensemble_synchronize",
     "wc_ensemble_member_stats",
     "wc_ensemble_launch_count",
@@ -142,11 +143,13 @@ def load(path: str = LIB_PATH):
     L.wc_ensemble_step_n.argtypes = [V, C.c_uint64, C.c_double]
     L.wc_ensemble_autotune.argtypes = [V, C.c_uint32, C.POINTER(C.c_int32), D]
     L.wc_ensemble_synchronize.argtypes = [V]
+    L.wc_ensemble_set_lpc.argtypes = [V, V]
     L.wc_ensemble_member_stats.argtypes = [V, C.c_uint64, C.POINTER(abi.wc_stats), D]
     L.wc_ensemble_launch_count.argtypes = [V]
     L.wc_ensemble_launch_count.restype = C.c_uint64
     for name in ("wc_ensemble_create", "wc_ensemble_upload", "wc_ensemble_download", "wc_ensemble_step_n",
-                 "wc_ensemble_autotune", "wc_ensemble_synchronize", "wc_ensemble_member_stats"):
+                 "wc_ensemble_autotune", "wc_ensemble_synchronize", "wc_ensemble_member_stats",
+                 "wc_ensemble_set_lpc"):
         getattr(L, name).restype = C.c_int
     L.wc_stable_dt_noalloc.argtypes = [C.POINTER(abi.wc_grid), C.c_double, V, V, V, V, D]
     L.wc_stable_dt_noalloc.restype = C.c_int
@@ -653,6 +656,13 @@ class Ensemble:
 
     def step_n(self, n: int, t_end: float = math.inf) -> None:
         _check(load().wc_ensemble_step_n(self._h, int(n), float(t_end)))
+
+    def set_preconditioner(self, net) -> None:
+        """`wc_ensemble_set_lpc`: the learned preconditioner for every dispersive member; each member
+        then steps through its own captured step on its own stream (forked and joined every step).
+        The network must outlive the ensemble."""
+        _check(load().wc_ensemble_set_lpc(self._h, net._handle))
+        self._net = net
 
     def autotune(self, trial_steps: int = 2):
         choice = C.c_int32()
