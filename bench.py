@@ -113,15 +113,15 @@ def members_alone(ws, net, steps: int, flush):
     from wavesim_b200 import Solver
 
     total_ms = 0.0
+    st = torch.cuda.Stream()  # a real stream handle: the solver and the events share it
     for w in ws:
         sol = w.solver(Solver)
+        sol.set_stream(st.cuda_stream)
         if net is not None and w.dispersion is not None:
             sol.set_preconditioner(net)
         sol.upload(W.wave_train_state(w))
         sol.step_n(2)
         sol.synchronize()
-        st = torch.cuda.current_stream()
-        sol.set_stream(st.cuda_stream)
         for _ in range(steps):
             flush.zero_()
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

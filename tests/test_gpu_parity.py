@@ -186,3 +186,33 @@ def test_streaming_and_tiled_shallow_water_stages_give_the_same_bits(case, monke
     a, b = outs
     assert a.time == b.time
     assert np.array_equal(a.h, b.h) and np.array_equal(a.hu, b.hu) and np.array_equal(a.hv, b.hv)
+
+
+def test_streaming_and_tiled_jacobi_solves_agree(monkeypatch):
+    """The Jacobi solve runs with register-streaming sweeps by default; the tiled sweeps
+    (WAVECORE_B200_SOLVE=tiled) do the same arithmetic per cell but add the dot products' partial
+    sums over other sets of cells, so the FP64 dots round differently: the two agree to the solve's
+    tolerance, and their iteration counts within one per solve. Walls and periodic, sides that are
+    not whole strips."""
+    for w in (W.sgn_beach(200, 90, 2.0, seed=5, name="periodic"),
+              W.sgn_beach(150, 70, 2.0, seed=6, name="walls", periodic=False)):
+        s0 = W.wave_train_state(w)
+        monkeypatch.setenv("WAVECORE_B200_SOLVE", "tiled")
+        tiled = w.solver(Solver)
+        monkeypatch.delenv("WAVECORE_B200_SOLVE")
+        stream = w.solver(Solver)
+        outs = []
+        for sol in (tiled, stream):
+            sol.upload(s0)
+            sol.step_n(30)
+            sol.synchronize()
+            s = s0.clone()
+            sol.download(s)
+            outs.append((s, sol.dispersion_stats()))
+        (a, sa), (b, sb) = outs
+        g = w.grid
+        assert abs(a.time - b.time) < 1e-9 * a.time
+        assert np.max(np.abs(g.inner(a.h) - g.inner(b.h))) < 2e-6, w.name
+        assert np.max(np.abs(g.inner(a.hu) - g.inner(b.hu))) < 2e-5, w.name
+        assert sa.solves == sb.solves and sb.unconverged == 0
+        assert abs(sa.iterations - sb.iterations) <= sa.solves, (sa, sb)

@@ -58,6 +58,7 @@ struct PcgArgs {
     int mode;         // StageMode
     int defer_finish; // the step's last kernel comes later (followed fronts): do not close the step
     int tiles_x, tiles_y;
+    int strip_rows;   // rows per strip of the streaming sweeps (pcg_stream.cuh)
     DampParams damp;
     unsigned long long timeout_ns;
 };
@@ -68,10 +69,11 @@ struct PcgArgs {
 // banks by epoch parity: a CTA that has left barrier e can reach barrier e+1 while a slower CTA
 // still reads the partials of e, but it cannot reach e+2 before every CTA has arrived at e+1,
 // i.e. finished reading e. Returns false if the wait timed out.
+template <int NT = PG_NT>
 __device__ bool reduce_barrier(const PcgArgs& a, unsigned& epoch, double v0, double v1, double v2,
                                double* out, double* red, int cta, int ncta) {
     __shared__ int s_ok;
-    block_sum3<PG_NT>(v0, v1, v2, red);
+    block_sum3<NT>(v0, v1, v2, red);
     epoch += 1;  // every thread keeps the count: it selects the bank below
     if (threadIdx.x == 0) {
         double* pp = a.part + 4 * ((size_t)cta + (epoch & 1u) * (size_t)ncta);
@@ -104,13 +106,13 @@ __device__ bool reduce_barrier(const PcgArgs& a, unsigned& epoch, double v0, dou
     if (!s_ok) return false;
     double x = 0.0, y = 0.0, z = 0.0;
     const double* bank = a.part + 4 * (size_t)(epoch & 1u) * (size_t)ncta;
-    for (int b = threadIdx.x; b < ncta; b += PG_NT) {
+    for (int b = threadIdx.x; b < ncta; b += NT) {
         const double* pp = bank + 4 * (size_t)b;
         x += __ldcg(pp);
         y += __ldcg(pp + 1);
         z += __ldcg(pp + 2);
     }
-    block_sum3<PG_NT>(x, y, z, red);
+    block_sum3<NT>(x, y, z, red);
     out[0] = x;
     out[1] = y;
     out[2] = z;

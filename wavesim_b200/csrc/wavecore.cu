@@ -23,6 +23,7 @@
 #include "lpc_host.cuh"
 #include "nest.cuh"
 #include "pcg.cuh"
+#include "pcg_stream.cuh"
 #include "record.cuh"
 #include "stage.cuh"
 #include "stream.cuh"
@@ -114,6 +115,11 @@ struct wc_solver {
     unsigned* diag_done = nullptr;
     double* diag_out = nullptr;
     int pcg_blocks = 0, pcg_tiles_x = 0, pcg_tiles_y = 0;
+    // The Jacobi solve: register-streaming sweeps (pcg_stream.cuh) in pcg_stream_blocks CTAs, or,
+    // with WAVECORE_B200_SOLVE=tiled in the environment at creation, the shared-memory tiled
+    // sweeps of pcg.cuh (which the ensemble's persistent launch uses).
+    bool solve_streaming = true;
+    int pcg_stream_blocks = 0, pcg_strip_rows = 16;
     unsigned long long launches = 0;
     unsigned long long seen_unconverged = 0;
     // Opt-in per-kernel timing: event pairs per launch, read back by wc_profile_read.
@@ -359,6 +365,7 @@ PcgArgs pcg_args(const wc_solver* s, int mode, const float4* qold, float4* qout,
     a.mode = mode;
     a.defer_finish = s->eddy_on;
     a.tiles_x = s->pcg_tiles_x;
+    a.strip_rows = s->pcg_strip_rows;
     a.tiles_y = s->pcg_tiles_y;
     a.damp = s->damp;
     a.timeout_ns = s->wait_ns;
@@ -380,7 +387,13 @@ wc_status launch_pcg(wc_solver* s, int mode, const float4* qold, float4* qout, c
     attr[0].val.cooperative = 1;
     lc.attrs = attr;
     lc.numAttrs = 1;
-    CK(cudaLaunchKernelEx(&lc, pcg_kernel, a));
+    if (s->solve_streaming) {
+        lc.gridDim = dim3(s->pcg_stream_blocks);
+        lc.blockDim = dim3(PS_NT);
+        CK(cudaLaunchKernelEx(&lc, pcg_stream_kernel, a));
+    } else {
+        CK(cudaLaunchKernelEx(&lc, pcg_kernel, a));
+    }
     s->launches++;
     return WC_OK;
 }
@@ -947,7 +960,17 @@ wc_status wc_solver_create(const wc_grid* grid, const double* bed_padded, const 
         s->pcg_tiles_y = (ny + PG_TY - 1) / PG_TY;
         const int tiles = s->pcg_tiles_x * s->pcg_tiles_y;
         s->pcg_blocks = std::max(1, std::min(tiles, sms * std::min(occ, 4)));
-        ALLOC(s->part, 8 * (size_t)s->pcg_blocks);
+        int occ_s = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s, pcg_stream_kernel, PS_NT, 0) != cudaSuccess || occ_s < 1)
+            return fail(set_err(WC_ECUDA, "occupancy query for the streaming solve kernel failed"));
+        s->pcg_strip_rows = ps_rows_for(nx, ny, sms * occ_s * PS_WARPS);
+        const int strip_ctas = (ps_strips(nx, ny, s->pcg_strip_rows) + PS_WARPS - 1) / PS_WARPS;
+        s->pcg_stream_blocks = std::max(1, std::min(strip_ctas, sms * occ_s));
+        {
+            const char* v = std::getenv("WAVECORE_B200_SOLVE");
+            s->solve_streaming = !(v && std::strcmp(v, "tiled") == 0);
+        }
+        ALLOC(s->part, 8 * (size_t)std::max(s->pcg_blocks, s->pcg_stream_blocks));
         ALLOC(s->bar, 2);
     }
     if (s->eddy_on) {
