@@ -190,6 +190,37 @@ def test_untrained_network_solve_matches_the_oracle():
     assert st.solves == 120 and st.unconverged == 0
 
 
+def test_streaming_and_tiled_flexible_cg_passes_agree(monkeypatch):
+    # The learned solve's pre, post and dir passes run with register-streaming sweeps by default;
+    # the tiled passes (WAVECORE_B200_FCG=tiled) do the same per-cell arithmetic but partition the
+    # dot products differently, so the two agree to the solve's tolerance and their iteration
+    # counts within one per solve. Walls and periodic; sides that are not whole strips.
+    net = LearnedPreconditioner(UNetSpec(), seed=1)
+    for w in (W.sgn_beach(200, 90, 2.0, seed=5, name="periodic"),
+              W.sgn_beach(150, 70, 2.0, seed=6, name="walls", periodic=False)):
+        s0 = W.wave_train_state(w)
+        monkeypatch.setenv("WAVECORE_B200_FCG", "tiled")
+        tiled = w.solver(Solver)
+        monkeypatch.delenv("WAVECORE_B200_FCG")
+        stream = w.solver(Solver)
+        outs = []
+        for sol in (tiled, stream):
+            sol.set_preconditioner(net)
+            sol.upload(s0)
+            sol.step_n(30)
+            sol.synchronize()
+            s = s0.clone()
+            sol.download(s)
+            outs.append((s, sol.dispersion_stats()))
+        (a, sa), (b, sb) = outs
+        g = w.grid
+        assert abs(a.time - b.time) < 1e-9 * a.time
+        assert np.max(np.abs(g.inner(a.h) - g.inner(b.h))) < 2e-6, w.name
+        assert np.max(np.abs(g.inner(a.hu) - g.inner(b.hu))) < 2e-5, w.name
+        assert sa.solves == sb.solves and sb.unconverged == 0
+        assert abs(sa.iterations - sb.iterations) <= sa.solves, (sa, sb)
+
+
 def harvest(net, seeds=(21, 22, 23), steps=40, every=10, nx=256, ny=128):
     for k, seed in enumerate(seeds):
         w = W.sgn_beach(nx, ny, 2.0, seed=seed, height=1.0 + k, period=10.0 + 3 * k, angle_deg=-15.0 + 15 * k)

@@ -52,8 +52,9 @@ inline int ps_rows_for(int nx, int ny, int warps) {
     return rows > PS_ROWS_MAX ? PS_ROWS_MAX : rows;
 }
 
-// One strip: rows j0-2 .. j0+rows+1 of the lane's column are fetched (`fetch(k, sy, j)`: the
-// loads at stored index k of padded row j, sy the sign of the y-normal component there) and turned
+// One strip: rows j0-2 .. j0+rows+1 of the lane's column are fetched (`fetch(k, sy, j, own, mi, mj)`:
+// the loads at stored index k = mj pitch + mi of padded row j, sy the sign of the y-normal
+// component there, own whether the cell is one the strip updates) and turned
 // into window rows (`make(raw)`: a Row with the signed vector v, c and heff); for every own cell
 // `out(k, i, j, row, Av, c_left, c_right, c_below, c_above)` gets the row, the product and the
 // four neighbouring c.
@@ -75,7 +76,7 @@ __device__ __forceinline__ void ps_strip(const DevGrid& g, int strip, int rows, 
             mj = reflect_idx(j, g.ny);
             sy = ((unsigned)j < (unsigned)g.ny) ? 1.f : -1.f;
         }
-        return fetch(mj * g.pitch + mi, sy, j, own_col && j >= j0 && j < j0 + rows && j < g.ny);
+        return fetch(mj * g.pitch + mi, sy, j, own_col && j >= j0 && j < j0 + rows && j < g.ny, mi, mj);
     };
     // f = c div v of the window's middle row
     auto fval = [&](const Row& m, const Row& c, const Row& p) -> float {
@@ -172,7 +173,7 @@ __device__ __forceinline__ bool pcg_solve_stream(const PcgArgs& a, int cta, int 
             const float sx = ((unsigned)i_lane < (unsigned)g.nx) ? 1.f : -1.f;
             ps_strip<PsInitRaw, PsInitRow>(
                 g, st, rows,
-                [&](int k, float sy, int, bool own) {
+                [&](int k, float sy, int, bool own, int, int) {
                     PsInitRaw r;
                     r.w = __ldcg(a.w + k);
                     r.cc = __ldg(a.cc + k);
@@ -223,7 +224,7 @@ __device__ __forceinline__ bool pcg_solve_stream(const PcgArgs& a, int cta, int 
                 const float sx = ((unsigned)i_lane < (unsigned)g.nx) ? 1.f : -1.f;
                 ps_strip<PsCgRaw, PsCgRow>(
                     g, st, rows,
-                    [&](int k, float sy, int, bool own) {
+                    [&](int k, float sy, int, bool own, int, int) {
                         PsCgRaw r;
                         r.r = __ldcg(a.rb[rb] + k);
                         r.d = __ldcg(a.diag + k);

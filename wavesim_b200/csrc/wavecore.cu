@@ -24,6 +24,7 @@
 #include "nest.cuh"
 #include "pcg.cuh"
 #include "pcg_stream.cuh"
+#include "fcg_stream.cuh"
 #include "record.cuh"
 #include "stage.cuh"
 #include "stream.cuh"
@@ -120,6 +121,10 @@ struct wc_solver {
     // sweeps of pcg.cuh (which the ensemble's persistent launch uses).
     bool solve_streaming = true;
     int pcg_stream_blocks = 0, pcg_strip_rows = 16;
+    // The learned path's passes with a network on the solver's own grid: streaming (fcg_stream.cuh)
+    // or, with WAVECORE_B200_FCG=tiled at creation, the tiled passes of lpc.cuh.
+    bool fcg_streaming = true;
+    int fcg_stream_blocks = 0, fcg_strip_rows = 16;
     unsigned long long launches = 0;
     unsigned long long seen_unconverged = 0;
     // Opt-in per-kernel timing: event pairs per launch, read back by wc_profile_read.
@@ -482,7 +487,10 @@ wc_status fcg_body(wc_solver* s, cudaStream_t st, cudaGraphConditionalHandle h, 
     {
         ProfScope ps(s, 1);
         unsigned* xh = nhwc ? reinterpret_cast<unsigned*>(s->lnet.Xh.p) : nullptr;
-        if (S == 1)
+        if (S == 1 && s->fcg_streaming)
+            FCG_LAUNCH(fcg_pre_stream_kernel<<<s->fcg_stream_blocks, FS_NT, 0, st>>>(
+                g, s->fcg_strip_rows, s->r, s->diag, s->cc, s->heff, z1, LPC_OMEGA, s->lnet.X[0].p, xh, hp, wp, sc));
+        else if (S == 1)
             FCG_LAUNCH(fcg_pre_tile_kernel<<<nt, FT_NT, 0, st>>>(g, s->r, s->diag, s->cc, s->heff, z1, LPC_OMEGA,
                                                                  s->lnet.X[0].p, xh, hp, wp, sc));
         else
@@ -497,11 +505,21 @@ wc_status fcg_body(wc_solver* s, cudaStream_t st, cudaGraphConditionalHandle h, 
     ProfScope ps(s, 1);
     const float* y = nhwc ? s->lnet.Yh.p : s->lnet.Y.p;
     const int lgS = S == 1 ? 0 : S == 2 ? 1 : S == 4 ? 2 : 3;
-    FCG_LAUNCH(fcg_post_tile_kernel<<<nt, FT_NT, 0, st>>>(g, z1, y, nhwc ? 1 : 0, s->r, s->diag, s->cc, s->heff, z, q,
-                                                          LPC_OMEGA, hp, wp, lgS, s->fpart, sc));
-    TRY(fcg_scalars(s, st, FCG_BETA, nt, h, 0));
-    FCG_LAUNCH(fcg_dir_tile_kernel<<<nt, FT_NT, 0, st>>>(g, z, p_old, p_new, s->cc, s->heff, q, s->r, s->fpart, sc));
-    TRY(fcg_scalars(s, st, FCG_ALPHA, nt, h, 0));
+    if (S == 1 && s->fcg_streaming) {
+        const int nf = s->fcg_stream_blocks, rows = s->fcg_strip_rows;
+        FCG_LAUNCH(fcg_post_stream_kernel<<<nf, FS_NT, 0, st>>>(g, rows, z1, y, nhwc ? 1 : 0, s->r, s->diag, s->cc,
+                                                                s->heff, z, q, LPC_OMEGA, hp, wp, s->fpart, sc));
+        TRY(fcg_scalars(s, st, FCG_BETA, nf, h, 0));
+        FCG_LAUNCH(fcg_dir_stream_kernel<<<nf, FS_NT, 0, st>>>(g, rows, z, p_old, p_new, s->cc, s->heff, q, s->r,
+                                                               s->fpart, sc));
+        TRY(fcg_scalars(s, st, FCG_ALPHA, nf, h, 0));
+    } else {
+        FCG_LAUNCH(fcg_post_tile_kernel<<<nt, FT_NT, 0, st>>>(g, z1, y, nhwc ? 1 : 0, s->r, s->diag, s->cc, s->heff, z,
+                                                              q, LPC_OMEGA, hp, wp, lgS, s->fpart, sc));
+        TRY(fcg_scalars(s, st, FCG_BETA, nt, h, 0));
+        FCG_LAUNCH(fcg_dir_tile_kernel<<<nt, FT_NT, 0, st>>>(g, z, p_old, p_new, s->cc, s->heff, q, s->r, s->fpart, sc));
+        TRY(fcg_scalars(s, st, FCG_ALPHA, nt, h, 0));
+    }
     FCG_LAUNCH(fcg_upd_kernel<<<nb, 256, 0, st>>>(g, s->w, s->r, p_new, q, s->fpart, sc));
     TRY(fcg_scalars(s, st, FCG_RESID, nb, h, cond));
     return WC_OK;
@@ -969,6 +987,17 @@ wc_status wc_solver_create(const wc_grid* grid, const double* bed_padded, const 
         {
             const char* v = std::getenv("WAVECORE_B200_SOLVE");
             s->solve_streaming = !(v && std::strcmp(v, "tiled") == 0);
+        }
+        {
+            const char* v = std::getenv("WAVECORE_B200_FCG");
+            s->fcg_streaming = !(v && std::strcmp(v, "tiled") == 0);
+            int occ_f = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_f, fcg_dir_stream_kernel, FS_NT, 0) != cudaSuccess || occ_f < 1)
+                return fail(set_err(WC_ECUDA, "occupancy query for the flexible-CG passes failed"));
+            occ_f = std::min(occ_f, FS_MINB);
+            s->fcg_strip_rows = ps_rows_for(nx, ny, sms * occ_f * FS_WARPS);
+            const int strip_ctas = (ps_strips(nx, ny, s->fcg_strip_rows) + FS_WARPS - 1) / FS_WARPS;
+            s->fcg_stream_blocks = std::max(1, std::min(strip_ctas, sms * occ_f));
         }
         ALLOC(s->part, 8 * (size_t)std::max(s->pcg_blocks, s->pcg_stream_blocks));
         ALLOC(s->bar, 2);
