@@ -455,17 +455,19 @@ __device__ __forceinline__ void conv_h_epilogue(const ConvH& p, float (&acc)[RW]
 // inputs through registers), A fragments are read with ldmatrix, and values are rounded to BF16
 // by the hardware conversion (round to nearest even, as bf16_bits).
 template <int KK, int NTL, int CP>
-__device__ __forceinline__ void conv_h_tile(const ConvH& p, int bx, int by, int bz, unsigned short* cm_smem) {
+__global__ void __launch_bounds__(CM_NT, 2) conv_h_kernel(ConvH p) {
+    if (p.done && *p.done) return;
     constexpr int RW = conv_h_rows(NTL), TH = 8 * RW;
     constexpr int R = KK == 9 ? 1 : 0, EW = CM_TX + 2 * R, EH = TH + 2 * R;
     constexpr int PS = CP + 8, KP = KK * CP, GROUPS = CP / 8, UNITS = EH * EW * GROUPS;
     constexpr int PER = (UNITS + CM_NT - 1) / CM_NT;
+    extern __shared__ __align__(16) unsigned short cm_smem[];
     unsigned short* in_s = cm_smem;             // [EH][EW][PS]
     unsigned short* w_s = cm_smem + EH * EW * PS;  // [8 NTL][KP]
     unsigned short* g_s = w_s + 8 * NTL * (KP + 8);      // gated layers: [TH][16][co]
     const int ci_total = p.ca + p.cb;
-    const int n = bz;
-    const int x0 = bx * CM_TX, y0 = by * TH;
+    const int n = blockIdx.z;
+    const int x0 = blockIdx.x * CM_TX, y0 = blockIdx.y * TH;
     const bool two = p.ca == 2;
     stage_weights<NTL, KP>(w_s, p.wre);
     if (p.gate) {  // the tile's gate, in flight with the input box
@@ -548,13 +550,6 @@ __device__ __forceinline__ void conv_h_tile(const ConvH& p, int bx, int by, int 
     conv_h_epilogue<NTL, RW>(p, acc, g_s, n, x0, y0);
 }
 
-template <int KK, int NTL, int CP>
-__global__ void __launch_bounds__(CM_NT, 2) conv_h_kernel(ConvH p) {
-    if (p.done && *p.done) return;
-    extern __shared__ __align__(16) unsigned short cm_smem[];
-    conv_h_tile<KK, NTL, CP>(p, blockIdx.x, blockIdx.y, blockIdx.z, cm_smem);
-}
-
 // A decoder convolution over concat(up(a), b) (3x3; a at half resolution with CPA channels, a
 // multiple of 16; b with the rest of the CP input channels, zero-padded): the a-part is staged
 // once per coarse pixel of the tile (a quarter of the fine halo box) and its A fragments are read
@@ -569,17 +564,19 @@ __host__ __device__ inline size_t conv_up_smem(int cpa, int cp, int co, bool gat
 }
 
 template <int NTL, int CP, int CPA>
-__device__ __forceinline__ void conv_up_tile(const ConvH& p, int bx, int by, int bz, unsigned short* cm_smem) {
+__global__ void __launch_bounds__(CM_NT, 2) conv_up_kernel(ConvH p) {
+    if (p.done && *p.done) return;
     constexpr int RW = conv_up_rows(NTL), TH = 8 * RW;
     constexpr int EW = CM_TX + 2, EH = TH + 2, CEW = CM_TX / 2 + 2, CEH = TH / 2 + 2;
     constexpr int CPB = CP - CPA, PSA = CPA + 8, PSB = CPB + 8, KP = 9 * CP;
     constexpr int GA = CPA / 8, GB = CPB / 8, UA = CEH * CEW * GA, UB = EH * EW * GB;
+    extern __shared__ __align__(16) unsigned short cm_smem[];
     unsigned short* a_s = cm_smem;               // [CEH][CEW][PSA]
     unsigned short* b_s = a_s + CEH * CEW * PSA;  // [EH][EW][PSB]
     unsigned short* w_s = b_s + EH * EW * PSB;    // [8 NTL][KP]
     unsigned short* g_s = w_s + 8 * NTL * (KP + 8);     // gated layers: [TH][16][co]
-    const int n = bz;
-    const int x0 = bx * CM_TX, y0 = by * TH;
+    const int n = blockIdx.z;
+    const int x0 = blockIdx.x * CM_TX, y0 = blockIdx.y * TH;
     const int Hc = p.H / 2, Wc = p.W / 2;
     const int cx0 = (x0 >> 1) - 1, cy0 = (y0 >> 1) - 1;
     stage_weights<NTL, KP>(w_s, p.wre);
@@ -638,13 +635,6 @@ __device__ __forceinline__ void conv_up_tile(const ConvH& p, int bx, int by, int
     conv_h_epilogue<NTL, RW>(p, acc, g_s, n, x0, y0);
 }
 
-template <int NTL, int CP, int CPA>
-__global__ void __launch_bounds__(CM_NT, 2) conv_up_kernel(ConvH p) {
-    if (p.done && *p.done) return;
-    extern __shared__ __align__(16) unsigned short cm_smem[];
-    conv_up_tile<NTL, CP, CPA>(p, blockIdx.x, blockIdx.y, blockIdx.z, cm_smem);
-}
-
 // ---- 3x3 convolutions of an 8-channel input: two taps per K step ---------------------------
 //
 // (A two-channel input, the network's own and the gates' features, takes the same kernel with
@@ -674,13 +664,15 @@ __host__ __device__ inline size_t conv_p8_smem(int co, bool gated) {
 }
 
 template <int NTL>
-__device__ __forceinline__ void conv_p8_tile(const ConvH& p, int bx, int by, int bz, unsigned short* cm_smem) {
+__global__ void __launch_bounds__(CM_NT, 2) conv_p8_kernel(ConvH p) {
+    if (p.done && *p.done) return;
     constexpr int RW = conv_h_rows(NTL), TH = 8 * RW, EW = CM_TX + 2, EH = TH + 2, UNITS = EH * EW;
+    extern __shared__ __align__(16) unsigned short cm_smem[];
     unsigned short* in_s = cm_smem;           // [EH][EW][8]
     unsigned short* w_s = in_s + UNITS * 8;   // [8 NTL][P8_KP]
     unsigned short* g_s = w_s + 8 * NTL * (P8_KP + 8);
-    const int n = bz;
-    const int x0 = bx * CM_TX, y0 = by * TH;
+    const int n = blockIdx.z;
+    const int x0 = blockIdx.x * CM_TX, y0 = blockIdx.y * TH;
     stage_weights<NTL, P8_KP>(w_s, p.wre);
     if (p.gate) {
         const int gg = p.co / 8;
@@ -740,13 +732,6 @@ __device__ __forceinline__ void conv_p8_tile(const ConvH& p, int bx, int by, int
         }
     }
     conv_h_epilogue<NTL, RW>(p, acc, g_s, n, x0, y0);
-}
-
-template <int NTL>
-__global__ void __launch_bounds__(CM_NT, 2) conv_p8_kernel(ConvH p) {
-    if (p.done && *p.done) return;
-    extern __shared__ __align__(16) unsigned short cm_smem[];
-    conv_p8_tile<NTL>(p, blockIdx.x, blockIdx.y, blockIdx.z, cm_smem);
 }
 
 // The network's first two layers in one launch: a = conv3x3(x) over the 2-channel input (no bias,
@@ -1065,81 +1050,6 @@ __global__ void __launch_bounds__(CM_NT, 2) conv_dec0_kernel(ConvH p) {
 }
 
 // NCHW FP32 maps -> NHWC BF16 (c channels, 2 or a multiple of 2).
-// ---- the coarse levels in one launch -----------------------------------------------------------
-//
-// Below the first level the network's maps are small (a quarter of the grid's pixels and less),
-// and each of its ten layers as its own launch is mostly latency: a partial wave, the launch, the
-// drain. conv_chain_kernel runs those layers in one cooperative launch: layer by layer every CTA
-// takes tiles b, b + nb, ... and computes them with the same tile function the layer's own kernel
-// would run (so the same bits), then all CTAs meet at a grid barrier before the next layer reads
-// what this one wrote. The barrier's wait is bounded in time: on expiry the kernel sets
-// ERR_TIMEOUT in the error word and every CTA returns.
-enum ChainKind { CK_P8_2 = 0, CK_H_9_2_16, CK_H_9_4_16, CK_H_9_4_32, CK_UP_4_64_32, CK_UP_2_48_32 };
-constexpr int CHAIN_MAX = 12;
-
-struct ChainLayer {
-    ConvH p;
-    int kind, gx, gy, gz;
-};
-
-__device__ __forceinline__ bool chain_barrier(unsigned* bar, int* err, unsigned long long timeout_ns, unsigned& epoch,
-                                              int& s_ok) {
-    __syncthreads();
-    epoch += 1;
-    if (threadIdx.x == 0) {
-        __threadfence();
-        int ok = 1;
-        const unsigned arrived = atomicAdd(bar, 1u) + 1u;
-        if (arrived == epoch * gridDim.x) {
-            st_release_u32(bar + 1, epoch);
-        } else {
-            const unsigned long long t0 = globaltimer_ns();
-            while (ld_acquire_u32(bar + 1) < epoch) {
-                if (ld_volatile_int(err) & ERR_TIMEOUT) {
-                    ok = 0;
-                    break;
-                }
-                if (globaltimer_ns() - t0 > timeout_ns) {
-                    atomicOr(err, ERR_TIMEOUT);
-                    ok = 0;
-                    break;
-                }
-            }
-        }
-        __threadfence();
-        s_ok = ok;
-    }
-    __syncthreads();
-    return s_ok != 0;
-}
-
-__global__ void __launch_bounds__(CM_NT, 2) conv_chain_kernel(const ChainLayer* __restrict__ layers, int n,
-                                                              const int* done, unsigned* bar, int* err,
-                                                              unsigned long long timeout_ns) {
-    if (done && *done) return;
-    extern __shared__ __align__(16) unsigned short cm_smem[];
-    __shared__ int s_ok;
-    unsigned epoch = 0;
-    for (int L = 0; L < n; L++) {
-        const ConvH& p = layers[L].p;
-        const int kind = layers[L].kind, gx = layers[L].gx, gy = layers[L].gy;
-        const int tiles = gx * gy * layers[L].gz;
-        for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
-            const int bx = t % gx, rest = t / gx, by = rest % gy, bz = rest / gy;
-            __syncthreads();  // the previous tile's shared memory is free
-            switch (kind) {
-                case CK_P8_2: conv_p8_tile<2>(p, bx, by, bz, cm_smem); break;
-                case CK_H_9_2_16: conv_h_tile<9, 2, 16>(p, bx, by, bz, cm_smem); break;
-                case CK_H_9_4_16: conv_h_tile<9, 4, 16>(p, bx, by, bz, cm_smem); break;
-                case CK_H_9_4_32: conv_h_tile<9, 4, 32>(p, bx, by, bz, cm_smem); break;
-                case CK_UP_4_64_32: conv_up_tile<4, 64, 32>(p, bx, by, bz, cm_smem); break;
-                default: conv_up_tile<2, 48, 32>(p, bx, by, bz, cm_smem); break;
-            }
-        }
-        if (L + 1 < n && !chain_barrier(bar, err, timeout_ns, epoch, s_ok)) return;
-    }
-}
-
 __global__ void to_h_kernel(const float* __restrict__ x, int N, int C, int H, int W, unsigned short* __restrict__ y) {
     const size_t plane = (size_t)H * W, total = (size_t)N * plane * (C / 2);
     for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {

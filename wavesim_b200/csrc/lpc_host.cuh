@@ -67,7 +67,6 @@ inline cudaError_t conv_mma_configure() {
                             CONV_UP8_FOR_ALL(CONV_UP8_PTR)
 #undef CONV_UP8_PTR
                             (const void*)conv_enc0_kernel, (const void*)conv_dec0_kernel<16>,
-                            (const void*)conv_chain_kernel,
         };
         st = cudaSuccess;
         for (const void* k : ks)
@@ -126,16 +125,6 @@ struct LpcNet {
     // and every layer's tile within the shared-memory limit; set by configure_nhwc.
     bool nhwc = false;
     bool fuse_level0 = true;    // the first level's fused launches (conv_enc0_kernel, conv_dec0_kernel)
-    // The coarse levels in one cooperative launch (conv_chain_kernel), when the first level's
-    // launches are fused and every coarse layer maps to a tile function the chain holds:
-    // chain_dev holds the layer table, then the barrier words; err_word gets ERR_TIMEOUT if a
-    // barrier wait runs out (the solver's error word, else chain_dev's own).
-    DBuf chain_dev;
-    bool chain_ok = false;
-    int chain_n = 0, chain_grid = 0;
-    size_t chain_smem = 0;
-    int* err_word = nullptr;
-    unsigned long long wait_ns = 2000000000ull;
     const int* done = nullptr;  // the flexible CG's end flag: applications after it are skipped
     DBuf Xh, Yh, Fh[LPC_LEVELS], HIDh[LPC_LEVELS], Gh[LPC_LEVELS], Ah[LPC_LEVELS], Eh[LPC_LEVELS],
         DAh[LPC_LEVELS], Dh[LPC_LEVELS];
@@ -324,7 +313,6 @@ struct LpcNet {
         A_(Y, sz(0, 2));
         if (nhwc && !training) {  // BF16 halves, two per float of the buffer
             auto H_ = [&](DBuf& b, size_t halves) { A_(b, (halves + 1) / 2); };
-            A_(chain_dev, (sizeof(ChainLayer) * CHAIN_MAX + 16) / sizeof(float));
             H_(Xh, sz(0, 2));
             A_(Yh, sz(0, 2));
             for (int l = 0; l < LPC_LEVELS; l++) {
@@ -520,7 +508,6 @@ struct LpcNet {
     }
     // launches of forward_h()
     int forward_h_launches() const {
-        if (chain_ok) return 3;
         return 2 * LPC_LEVELS + 2 * (LPC_LEVELS - 1) + (fused_out() ? 0 : 1) - (fused_enc0() ? 1 : 0) -
                (fused_dec0() ? 1 : 0);
     }
@@ -572,139 +559,10 @@ struct LpcNet {
         return cudaGetLastError();
     }
 
-    // The chain's entry for one layer, mirroring conv_h's choice of kernel; false if conv_h would run
-    // a kernel the chain does not hold.
-    bool describe(const unsigned short* a, int ca, int amode, const unsigned short* b, int cb, const LpcLayer& L,
-                  const unsigned short* gate, unsigned short* y, int level, ChainLayer& out, size_t& smem) const {
-        ConvH p{};
-        p.a = a;
-        p.ca = ca;
-        p.amode = amode;
-        p.b = b;
-        p.cb = cb;
-        p.wre = wre_of(L);
-        p.bias = L.b >= 0 ? wq + L.b : nullptr;
-        p.gate = gate;
-        p.y = y;
-        p.yf = nullptr;
-        p.done = done;
-        p.out_w = nullptr;
-        p.co = L.co;
-        p.H = h_of(level);
-        p.W = w_of(level);
-        p.N = N;
-        p.act = ACT_NONE;
-        const int nt = mma_tiles(L.co), kk = L.k * L.k, cp = conv_mma_cp(L.ci);
-        const bool gated = gate != nullptr;
-        int th = 0;
-        if (kk == 9 && (ca == 8 || (ca == 2 && amode == CM_DIRECT)) && cb == 0 && amode != CM_UP && wp8_of(L)) {
-            if (nt != 2) return false;
-            p.wre = wp8_of(L);
-            out.kind = CK_P8_2;
-            th = 8 * conv_h_rows(nt);
-            smem = conv_p8_smem(8 * nt, gated);
-        } else if (amode == CM_UP && kk == 9 && ca % 16 == 0 && cb == 8 && b && wu8_of(L)) {
-            return false;  // the 8-channel-skip decoder kernel
-        } else if (amode == CM_UP && kk == 9 && ca % 16 == 0 && b &&
-                   conv_up_smem(ca, cp, 8 * nt, gated) <= CONV_MMA_SMEM_MAX) {
-            if (nt == 4 && cp == 64 && ca == 32) out.kind = CK_UP_4_64_32;
-            else if (nt == 2 && cp == 48 && ca == 32) out.kind = CK_UP_2_48_32;
-            else return false;
-            th = 8 * conv_up_rows(nt);
-            smem = conv_up_smem(ca, cp, 8 * nt, gated);
-        } else {
-            if (kk != 9) return false;
-            if (nt == 2 && cp == 16) out.kind = CK_H_9_2_16;
-            else if (nt == 4 && cp == 16) out.kind = CK_H_9_4_16;
-            else if (nt == 4 && cp == 32) out.kind = CK_H_9_4_32;
-            else return false;
-            th = 8 * conv_h_rows(nt);
-            smem = conv_h_smem2(L.ci, 8 * nt, 9, gated);
-        }
-        out.p = p;
-        out.gx = (p.W + CM_TX - 1) / CM_TX;
-        out.gy = (p.H + th - 1) / th;
-        out.gz = N;
-        return true;
-    }
-
-    // The table of the coarse layers (levels 1 .. LPC_LEVELS-1, encoder then decoder, in
-    // forward_h's order) and the chain's launch shape. Call after shape(), prepare_tensor() and
-    // once `done` is set, outside any stream capture.
-    cudaError_t build_chain() {
-        chain_ok = false;
-        if (!nhwc || !fused_enc0() || !fused_dec0() || !chain_dev.p) return cudaSuccess;
-        ChainLayer t[CHAIN_MAX];
-        size_t smem = 0, sm = 0;
-        int n = 0;
-        bool ok = true;
-        auto add = [&](const unsigned short* a, int ca, int amode, const unsigned short* b, int cb, const LpcLayer& L,
-                       const unsigned short* gate, unsigned short* y, int level) {
-            if (!ok || n >= CHAIN_MAX || !describe(a, ca, amode, b, cb, L, gate, y, level, t[n], sm)) {
-                ok = false;
-                return;
-            }
-            smem = std::max(smem, sm);
-            n++;
-        };
-        for (int l = 1; l < LPC_LEVELS; l++) {
-            add(hp(Eh[l - 1]), ch[l - 1], CM_POOL, nullptr, 0, enc_a[l], nullptr, hp(Ah[l]), l);
-            add(hp(Ah[l]), ch[l], CM_DIRECT, nullptr, 0, enc_b[l], hp(Gh[l]), hp(Eh[l]), l);
-        }
-        for (int l = LPC_LEVELS - 2; l >= 1; l--) {
-            const unsigned short* below = (l == LPC_LEVELS - 2) ? hp(Eh[l + 1]) : hp(Dh[l + 1]);
-            add(below, ch[l + 1], CM_UP, hp(Eh[l]), ch[l], dec_a[l], nullptr, hp(DAh[l]), l);
-            add(hp(DAh[l]), ch[l], CM_DIRECT, nullptr, 0, dec_b[l], hp(Gh[l]), hp(Dh[l]), l);
-        }
-        if (!ok || smem > CONV_MMA_SMEM_MAX) return cudaSuccess;
-        int dev = 0, sms = 0, occ = 0;
-        cudaError_t e = cudaGetDevice(&dev);
-        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (e == cudaSuccess) e = conv_mma_configure();
-        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, conv_chain_kernel, CM_NT, smem);
-        if (e != cudaSuccess || occ < 1) return e;
-        e = cudaMemcpy(chain_dev.p, t, sizeof(ChainLayer) * n, cudaMemcpyHostToDevice);
-        if (e != cudaSuccess) return e;
-        chain_n = n;
-        chain_smem = smem;
-        chain_grid = sms * std::min(occ, 2);
-        chain_ok = true;
-        return cudaSuccess;
-    }
-
-    unsigned* chain_bar() { return reinterpret_cast<unsigned*>(reinterpret_cast<char*>(chain_dev.p) + sizeof(ChainLayer) * CHAIN_MAX); }
-
-    // the coarse levels: the barrier words cleared, then one cooperative launch
-    cudaError_t launch_chain(cudaStream_t st) {
-        unsigned* bar = chain_bar();
-        int* err = err_word ? err_word : reinterpret_cast<int*>(bar + 2);
-        // the barrier words; the chain's own error word too when it has no solver's to report to
-        cudaError_t e = cudaMemsetAsync(bar, 0, (err_word ? 2 : 3) * sizeof(unsigned), st);
-        if (e != cudaSuccess) return e;
-        cudaLaunchConfig_t lc{};
-        lc.gridDim = dim3(chain_grid);
-        lc.blockDim = dim3(CM_NT);
-        lc.dynamicSmemBytes = chain_smem;
-        lc.stream = st;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeCooperative;
-        attr[0].val.cooperative = 1;
-        lc.attrs = attr;
-        lc.numAttrs = 1;
-        return cudaLaunchKernelEx(&lc, conv_chain_kernel, reinterpret_cast<const ChainLayer*>(chain_dev.p), chain_n,
-                                  done, bar, err, wait_ns);
-    }
-
     // Yh = N(Xh) on NHWC BF16 activations with the gates already in Gh: the launches of forward()
     // (the output layer fused into the last when fused_out()).
     cudaError_t forward_h(cudaStream_t st) {
         cudaError_t e = cudaSuccess;
-        if (chain_ok) {  // the first level's fused encoder, the coarse levels in one launch, the fused decoder
-            e = enc0_h(st);
-            if (e == cudaSuccess) e = launch_chain(st);
-            if (e == cudaSuccess) e = dec0_h(st);
-            return e;
-        }
         for (int l = 0; l < LPC_LEVELS && e == cudaSuccess; l++) {
             if (l == 0 && fused_enc0()) {
                 e = enc0_h(st);

@@ -1074,7 +1074,6 @@ wc_status wc_profile_read(wc_solver* s, wc_kernel_time out[WC_KERNEL_KINDS]) {
 wc_status wc_set_wait_limit(wc_solver* s, uint64_t ns) {
     if (!s) return set_err(WC_EINVAL, "null argument");
     s->wait_ns = ns ? (unsigned long long)ns : BARRIER_TIMEOUT_NS;
-    s->lnet.wait_ns = s->wait_ns;
     // A captured step holds the old limit in its kernels' arguments: capture again.
     if (s->step_graph) {
         CK(cudaStreamSynchronize(s->stream));
@@ -2009,7 +2008,6 @@ wc_status wc_lpc_forward(wc_lpc* l, int32_t n, int32_t h, int32_t w, const float
     }
     const size_t per = (size_t)n * 2 * h * w;
     TRY(lpc_ck(net.shape(n, h, w, false), "activations"));
-    if (net.tensor) TRY(lpc_ck(net.build_chain(), "coarse-level chain"));
     TRY(lpc_ck(cudaMemcpyAsync(net.X[0].p, x, per * sizeof(float), cudaMemcpyHostToDevice, st), "upload"));
     TRY(lpc_ck(cudaMemcpyAsync(net.F[0].p, feat, per * sizeof(float), cudaMemcpyHostToDevice, st), "upload"));
     if (net.nhwc) {  // the solver's path: NHWC BF16 activations
@@ -2165,9 +2163,6 @@ wc_status wc_solver_set_lpc(wc_solver* s, wc_lpc* l) {
         CK(cudaStreamCreateWithFlags(&s->body_stream, cudaStreamNonBlocking));
     }
     s->lnet.done = &s->fsc->done;
-    s->lnet.err_word = &s->ctl->error;
-    s->lnet.wait_ns = s->wait_ns;
-    CK(s->lnet.build_chain());
     // training and inference may run on different streams: the weights are final from here
     CK(cudaStreamSynchronize(l->m.st));
     s->lpc = &l->m;
