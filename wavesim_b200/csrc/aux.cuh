@@ -121,17 +121,44 @@ struct Rate64Out {
     unsigned long long first_max;  // smallest row-major interior index whose rate equals the max
 };
 
-// Pass 1: max rate and first NaN over the interior.
+// Pass 1: max rate and first NaN over the interior. Both are order-independent (a max of
+// non-negative doubles compared as integers, a min of indices), so each thread keeps its own,
+// the warp and the block reduce them, and one thread per block folds them into `out`.
 __global__ void rate64_kernel(int nx, int ny, double dx, double dy, const double* __restrict__ h,
                               const double* __restrict__ hu, const double* __restrict__ hv,
                               Rate64Out* out) {
+    __shared__ unsigned long long s_max[32], s_nan[32];
     const int W = nx + 6;
+    unsigned long long mx = 0ull, first_nan = ~0ull;
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < (long long)nx * ny;
          c += (long long)gridDim.x * blockDim.x) {
         const int i = (int)(c % nx), j = (int)(c / nx);
         const double r = rate64(h, hu, hv, (long long)(j + 3) * W + (i + 3), dx, dy);
-        if (r != r) atomicMin(&out->first_nan, (unsigned long long)c);
-        else atomicMax(&out->max_bits, (unsigned long long)__double_as_longlong(r));
+        if (r != r) {
+            if ((unsigned long long)c < first_nan) first_nan = (unsigned long long)c;
+        } else {
+            const unsigned long long b = (unsigned long long)__double_as_longlong(r);
+            if (b > mx) mx = b;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long om = __shfl_down_sync(0xffffffffu, mx, o);
+        const unsigned long long on = __shfl_down_sync(0xffffffffu, first_nan, o);
+        mx = om > mx ? om : mx;
+        first_nan = on < first_nan ? on : first_nan;
+    }
+    if ((threadIdx.x & 31) == 0) {
+        s_max[threadIdx.x >> 5] = mx;
+        s_nan[threadIdx.x >> 5] = first_nan;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (unsigned w = 1; w < blockDim.x / 32; w++) {
+            mx = s_max[w] > mx ? s_max[w] : mx;
+            first_nan = s_nan[w] < first_nan ? s_nan[w] : first_nan;
+        }
+        if (mx) atomicMax(&out->max_bits, mx);
+        if (first_nan != ~0ull) atomicMin(&out->first_nan, first_nan);
     }
 }
 
