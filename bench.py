@@ -175,7 +175,7 @@ def run_ensemble(args, world, rank, local):
         total = rank_max(sec, dist)  # the slowest rank's time
         return {"value": rank_sum(float(cells), dist) * args.steps / total, "ms_per_step": 1e3 * total / args.steps,
                 "iterations_per_solve": iters, "launches": launches, "clocks": clocks,
-                "variant": Ensemble.VARIANTS[choice] if choice >= 0 else "members' own step graphs on their own streams",
+                "variant": Ensemble.VARIANTS[choice],
                 "autotune_ms_per_step": tune_ms}
 
     main = arm(net)

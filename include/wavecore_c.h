@@ -280,7 +280,8 @@ wc_status wc_stable_dt_noalloc(const wc_grid* grid, double cfl, const double* d_
  * n independent runs, each with its own grid, bed (padded FP64) and configuration (second or
  * fifth order), advanced together: every step of every member is one persistent cooperative
  * launch, replayed from a CUDA graph, in which each member's own group of CTAs runs its whole
- * SSP-RK2 step with its own adaptive time step, clock and PCG state. The CTAs are split over the
+ * SSP-RK2 step with its own adaptive time step, clock and PCG state (or, if the autotuner finds it
+ * faster, every member's own captured step on its own stream). The CTAs are split over the
  * members by their work per step (cells, and the PCG iterations per solve the autotuner measures
  * on its first call). The stage tile shape and the CTAs per SM are chosen by an autotuner that
  * times each compiled variant on the live state (then restores it); wc_ensemble_step_n runs it on
@@ -297,10 +298,11 @@ wc_status wc_ensemble_download(wc_ensemble* e, uint64_t member, double* h, doubl
 /* Up to n_steps steps of every member, each of size min(stable_dt, t_end - time); a member stops
  * once its time reaches t_end. Asynchronous. */
 wc_status wc_ensemble_step_n(wc_ensemble* e, uint64_t n_steps, double t_end);
-/* Time every variant over trial_steps steps and keep the fastest; *choice is its index (stage
- * tile height 8 or 16 by CTAs per SM 1 or 2: 0 = 8/1, 1 = 8/2, 2 = 16/1, 3 = 16/2) and
- * ms_per_step[4] the measured times (-1 for a variant that cannot run). A learned ensemble
- * (wc_ensemble_set_lpc) has no variants: *choice is -1 and ms_per_step[0] its time per step. */
+/* Time every choice over trial_steps steps and keep the fastest; *choice is its index (0-3: the
+ * persistent launch with stage tile height 8 or 16 by CTAs per SM 1 or 2: 0 = 8/1, 1 = 8/2,
+ * 2 = 16/1, 3 = 16/2; 4: no persistent launch, every member's own captured step on its own
+ * stream, forked from the ensemble's stream and joined back) and ms_per_step[5] the measured times
+ * (-1 for a choice that cannot run). A learned ensemble (wc_ensemble_set_lpc) has only choice 4. */
 wc_status wc_ensemble_autotune(wc_ensemble* e, uint32_t trial_steps, int32_t* choice,
                                double* ms_per_step);
 /* The learned preconditioner for every dispersive member (config 4's method). The network's

@@ -25,7 +25,7 @@ def test_ensemble_members_match_standalone_runs():
     for m, s0 in enumerate(starts):
         ens.upload(m, s0)
     choice, ms = ens.autotune(2)
-    assert 0 <= choice < 4 and ms[choice] > 0
+    assert 0 <= choice < 5 and ms[choice] > 0 and ms[4] > 0
     ens.step_n(25)
     ens.synchronize()
     for m, (w, s0) in enumerate(zip(ws, starts)):
@@ -73,7 +73,7 @@ def test_learned_ensemble_members_match_standalone_learned_runs():
     for m, s0 in enumerate(starts):
         ens.upload(m, s0)
     choice, ms = ens.autotune(2)
-    assert choice == -1 and ms[0] > 0
+    assert choice == 4 and ms[4] > 0 and ms[:4] == [-1.0] * 4
     ens.step_n(20)
     ens.synchronize()
     for m, (w, s0) in enumerate(zip(ws, starts)):

@@ -1378,6 +1378,9 @@ wc_status wc_time_device(wc_solver* s, double* time_out) {
 namespace {
 
 constexpr int EN_VARIANTS = 4;  // stage tile height {8, 16} x CTAs per SM {1, 2}
+// The autotuner's fifth choice: no persistent launch, every member's own captured step on its own
+// stream (the only choice of a learned ensemble).
+constexpr int EN_STREAMS = EN_VARIANTS;
 
 struct EnVariant {
     int ty, minb;
@@ -1432,7 +1435,7 @@ struct wc_ensemble {
     int max_ctas = 0;
     EnVariant var[EN_VARIANTS];
     int chosen = -1;
-    double tune_ms[EN_VARIANTS] = {0, 0, 0, 0};
+    double tune_ms[EN_VARIANTS + 1] = {0, 0, 0, 0, 0};
     // snapshot of the resident states for tuning trials
     std::vector<float4*> snap_q;
     std::vector<float2*> snap_w;
@@ -1442,9 +1445,9 @@ struct wc_ensemble {
     // PCG iterations per solve, 55 until the autotuner has measured it).
     std::vector<double> work;
     bool work_measured = false;
-    // With a learned preconditioner attached (wc_ensemble_set_lpc), every member steps through its
-    // own captured step (the flexible CG's while-node included) on its own stream; a step forks
-    // from the ensemble's stream to the members' and joins back.
+    // Every member has its own stream: with the EN_STREAMS choice (and always with a learned
+    // preconditioner, wc_ensemble_set_lpc) every member steps through its own captured step on it;
+    // a step forks from the ensemble's stream to the members' and joins back.
     bool learned = false;
     std::vector<cudaStream_t> member_streams;
     std::vector<cudaEvent_t> member_done;
@@ -1657,8 +1660,8 @@ wc_status ensemble_tune(wc_ensemble* e, int trial) {
         float ms = 0.f;
         CK(cudaEventElapsedTime(&ms, a, b));
         for (int k = 0; k < EN_VARIANTS; k++) e->tune_ms[k] = -1.0;
-        e->tune_ms[0] = ms / trial;
-        e->chosen = -1;
+        e->tune_ms[EN_STREAMS] = ms / trial;
+        e->chosen = EN_STREAMS;
         TRY(restore());
         cudaEventDestroy(a);
         cudaEventDestroy(b);
@@ -1707,6 +1710,22 @@ wc_status ensemble_tune(wc_ensemble* e, int trial) {
         }
         TRY(restore());
     }
+    {  // the members' own steps on their own streams
+        TRY(ensemble_prepare(e, INFINITY));
+        TRY(ensemble_step_members(e));  // capture and warm
+        CK(cudaEventRecord(a, e->stream));
+        for (int t = 0; t < trial; t++) TRY(ensemble_step_members(e));
+        CK(cudaEventRecord(b, e->stream));
+        CK(cudaEventSynchronize(b));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, a, b));
+        e->tune_ms[EN_STREAMS] = ms / trial;
+        if (ms < best) {
+            best = ms;
+            e->chosen = EN_STREAMS;
+        }
+        TRY(restore());
+    }
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     if (e->chosen < 0) return set_err(WC_ECUDA, "no ensemble kernel variant can run on this device");
@@ -1736,12 +1755,21 @@ wc_status wc_ensemble_create(uint64_t n, const wc_grid* grids, const double* con
     };
     if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess)
         return fail(set_err(WC_ECUDA, "cudaStreamCreate failed"));
+    if (cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming) != cudaSuccess)
+        return fail(set_err(WC_ECUDA, "cudaEventCreate failed"));
     for (uint64_t m = 0; m < n; m++) {
         wc_solver* s = nullptr;
         wc_status st = wc_solver_create(&grids[m], beds[m], &cfgs[m], &s);
         if (st != WC_OK) return fail(st);
         e->members.push_back(s);
-        s->stream = e->stream;  // members queue on the ensemble's stream
+        cudaStream_t ms = nullptr;
+        cudaEvent_t ev = nullptr;
+        if (cudaStreamCreateWithFlags(&ms, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess)
+            return fail(set_err(WC_ECUDA, "cudaStreamCreate failed"));
+        e->member_streams.push_back(ms);
+        e->member_done.push_back(ev);
+        s->stream = ms;  // the member's own steps; the persistent launches run on the ensemble's stream
     }
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
@@ -1776,23 +1804,10 @@ wc_status wc_ensemble_set_lpc(wc_ensemble* e, wc_lpc* l) {
     if (!e || !l) return set_err(WC_EINVAL, "null argument");
     if (e->learned) return set_err(WC_EINVAL, "the ensemble already has a learned preconditioner");
     CK(cudaStreamSynchronize(e->stream));
-    const size_t n = e->members.size();
-    for (size_t m = 0; m < n; m++) {
-        cudaStream_t st = nullptr;
-        cudaEvent_t ev = nullptr;
-        CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-        e->member_streams.push_back(st);
-        CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-        e->member_done.push_back(ev);
-    }
-    CK(cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming));
-    for (size_t m = 0; m < n; m++) {
-        wc_solver* s = e->members[m];
-        s->stream = e->member_streams[m];
+    for (wc_solver* s : e->members)
         if (s->sgn) TRY(wc_solver_set_lpc(s, l));
-    }
     e->learned = true;
-    e->chosen = -1;
+    e->chosen = EN_STREAMS;
     return WC_OK;
 }
 
@@ -1814,16 +1829,16 @@ wc_status wc_ensemble_autotune(wc_ensemble* e, uint32_t trial_steps, int32_t* ch
     TRY(ensemble_tune(e, (int)std::max<uint32_t>(1, trial_steps)));
     if (choice) *choice = e->chosen;
     if (ms_per_step)
-        for (int k = 0; k < EN_VARIANTS; k++) ms_per_step[k] = e->tune_ms[k];
+        for (int k = 0; k <= EN_STREAMS; k++) ms_per_step[k] = e->tune_ms[k];
     return WC_OK;
 }
 
 wc_status wc_ensemble_step_n(wc_ensemble* e, uint64_t n_steps, double t_end) {
     if (!e) return set_err(WC_EINVAL, "null ensemble");
-    if (!e->learned && e->chosen < 0) TRY(ensemble_tune(e, 2));
+    if (e->chosen < 0) TRY(ensemble_tune(e, 2));
     TRY(ensemble_prepare(e, t_end));
     for (uint64_t k = 0; k < n_steps; k++) {
-        if (e->learned) TRY(ensemble_step_members(e));
+        if (e->chosen == EN_STREAMS) TRY(ensemble_step_members(e));
         else TRY(ensemble_step(e, e->var[e->chosen]));
     }
     TRY(ensemble_finish(e));
@@ -1853,8 +1868,7 @@ wc_status wc_ensemble_member_stats(wc_ensemble* e, uint64_t m, wc_stats* stats, 
 uint64_t wc_ensemble_launch_count(const wc_ensemble* e) {
     if (!e) return 0;
     uint64_t n = e->launches;
-    if (e->learned)  // the members' own steps: their kernels, the flexible CG's iterations included
-        for (const wc_solver* s : e->members) n += wc_launch_count(s);
+    for (const wc_solver* s : e->members) n += wc_launch_count(s);  // the members' own steps' kernels
     return n;
 }
 

@@ -620,7 +620,8 @@ class Ensemble:
     `Solver` per grid in turn.
     """
 
-    VARIANTS = ("tile 32x8, 1 CTA/SM", "tile 32x8, 2 CTAs/SM", "tile 32x16, 1 CTA/SM", "tile 32x16, 2 CTAs/SM")
+    VARIANTS = ("tile 32x8, 1 CTA/SM", "tile 32x8, 2 CTAs/SM", "tile 32x16, 1 CTA/SM", "tile 32x16, 2 CTAs/SM",
+                "members' own step graphs on their own streams")
 
     def __init__(self, members):
         L = load()
@@ -666,7 +667,7 @@ class Ensemble:
 
     def autotune(self, trial_steps: int = 2):
         choice = C.c_int32()
-        ms = (C.c_double * 4)()
+        ms = (C.c_double * 5)()
         _check(load().wc_ensemble_autotune(self._h, int(trial_steps), C.byref(choice), ms))
         return choice.value, list(ms)
 
