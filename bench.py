@@ -47,11 +47,12 @@ SOLVE_FINISH_BYTES = (44 + 60) / 2              # stage 1 / stage 2 epilogue, av
 STAGE_BYTES_SWE = (36 + 52) / 2                 # stage 1 / stage 2 (RK average + damping)
 
 # DRAM bytes per cell measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum of one capture
-# each, on the network at 2048x1024, the solve at 2048x1024 over 57 iterations and the stage at
-# 4096x4096; scaled to a launch by cells, and by iterations for the solve).
+# each, on the network at 2048x1024, the streaming solve at 2048x1024 over 58 iterations and the
+# two streaming second-order stages at 2048x2048; scaled to a launch by cells, and by iterations
+# for the solve).
 NETWORK_DRAM_BYTES_PER_CELL = 334.1e6 / (2048 * 1024)    # one application of the U-net
-PCG_DRAM_BYTES_PER_CELL_ITER = 10.53e9 / (2048 * 1024 * 57)  # one iteration of the solve
-STAGE_DRAM_BYTES_PER_CELL_SWE = 573.1e6 / (4096 * 4096)      # one second-order stage
+PCG_DRAM_BYTES_PER_CELL_ITER = (6.30e9 + 4.44e9) / (2048 * 1024 * 58)  # one iteration of the solve
+STAGE_DRAM_BYTES_PER_CELL_SWE = ((93.0e6 + 32.1e6) + (161.3e6 + 35.6e6)) / 2 / (2048 * 2048)  # a stage
 
 
 def workload(name: str, eddy: bool = False):
@@ -592,15 +593,15 @@ def run_b200(args, world, rank, local):
         else:
             if solve_n and solve_ms >= stage_ms:
                 per_cell = SOLVE_INIT_BYTES + SOLVE_ITER_BYTES * iters_prof + SOLVE_FINISH_BYTES
-                dom = {"kernel": "pcg_kernel (persistent dispersive solve)", "launches": solve_n,
+                dom = {"kernel": "pcg_stream_kernel (persistent dispersive solve, streaming sweeps)", "launches": solve_n,
                        "avg_ms": solve_ms / solve_n, "bytes_per_cell": per_cell}
             else:
                 per_cell = STAGE_BYTES_SGN if w.dispersion else STAGE_BYTES_SWE
-                dom = {"kernel": "stage_kernel (fused RK stage)", "launches": stage_n,
+                dom = {"kernel": ("swe_stream_kernel (fused RK stage, streaming rows)" if not w.dispersion else "stage_kernel (fused RK stage)"), "launches": stage_n,
                        "avg_ms": stage_ms / max(1, stage_n), "bytes_per_cell": per_cell}
             achieved = per_cell * cells / (dom["avg_ms"] / 1e3) / 1e9
             traffic = None
-            if dom["kernel"].startswith("pcg_kernel"):
+            if dom["kernel"].startswith("pcg_stream_kernel"):
                 traffic = PCG_DRAM_BYTES_PER_CELL_ITER * iters_prof * cells
             elif not w.dispersion and w.order.value == 1:
                 traffic = STAGE_DRAM_BYTES_PER_CELL_SWE * cells
@@ -608,8 +609,8 @@ def run_b200(args, world, rank, local):
                     "frac": achieved / peak, "peak_source": peak_kind, "algorithmic_bytes_per_cell": dom["bytes_per_cell"],
                     "avg_ms": dom["avg_ms"], "traffic": traffic,
                     "traffic_source": ("ncu DRAM bytes per cell and iteration of one solve at 2048x1024, scaled by "
-                                       "cells and iterations" if dom["kernel"].startswith("pcg_kernel") else
-                                       "ncu DRAM bytes of one second-order stage at 4096x4096, scaled by cells")
+                                       "cells and iterations" if dom["kernel"].startswith("pcg_stream_kernel") else
+                                       "ncu DRAM bytes of the two second-order stages at 2048x2048, averaged and scaled by cells")
                     if traffic else None}
         line = {
             "metric": METRIC,
