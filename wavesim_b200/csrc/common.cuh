@@ -151,6 +151,26 @@ __device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
 
 __device__ __forceinline__ int ld_volatile_int(const int* p) { return *(const volatile int*)p; }
 
+// Asynchronous global -> shared copies of 8 and 4 bytes (PTX cp.async): the data in flight holds
+// no registers; a thread's own copies are visible to it after cp_async_wait. Both addresses are
+// aligned to the copy's size.
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(smem)),
+                 "l"(gmem)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((unsigned)__cvta_generic_to_shared(smem)),
+                 "l"(gmem)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// Wait until at most N of this thread's committed groups are still in flight.
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // Sum over the block with a fixed reduction tree; every thread gets the same value.
 template <int NT>
 __device__ __forceinline__ double block_sum(double v, double* red) {

@@ -1,4 +1,4 @@
-// fcg_stream.cuh — the learned path's flexible-CG passes with register-streaming sweeps.
+// fcg_stream.cuh — the learned path's flexible-CG passes with streaming sweeps.
 //
 // The passes of lpc.cuh (pre, post, dir; the update pass is pointwise and stays there) compute
 // one matrix product each of a vector that is formed, cell by cell, from the inputs it is made of:
@@ -17,7 +17,13 @@
 
 namespace wcb {
 
-constexpr int FS_NT = 256, FS_WARPS = FS_NT / 32, FS_MINB = 3;
+#ifndef WCB_FS_MINB
+#define WCB_FS_MINB 3
+#endif
+constexpr int FS_NT = 256, FS_WARPS = FS_NT / 32, FS_MINB = WCB_FS_MINB;
+// Ring fields per row (the post pass's: z1, y as pairs; c, heff, y as two planes).
+constexpr int FS_NF2 = 2, FS_NF1 = 4;
+constexpr int FS_SMEM = FS_WARPS * ps_ring_bytes<FS_NF2, FS_NF1>();  // dynamic shared memory per block
 
 struct FsRaw {
     float2 a, b;   // the pass's inputs at the cell
@@ -45,7 +51,7 @@ __device__ __forceinline__ void fs_sweep(const DevGrid& g, int rows, Fetch fetch
     for (int st = gw; st < nstrips; st += nw) {
         const int i_lane = (st % strips_x) * PS_OUT - PS_HALO + (threadIdx.x & 31);
         const float sx = ((unsigned)i_lane < (unsigned)g.nx) ? 1.f : -1.f;
-        ps_strip<FsRaw, FsRow>(
+        ps_strip<FsRaw, FsRow, FS_NF2, FS_NF1>(
             g, st, rows, fetch, [&](const FsRaw& r) { return make(r, sx); }, out);
     }
 }
@@ -70,12 +76,12 @@ __global__ void __launch_bounds__(FS_NT, FS_MINB) fcg_pre_stream_kernel(
     const size_t plane = (size_t)Hp * Wp;
     fs_sweep(
         g, rows,
-        [&](int k, float sy, int, bool, int, int) {
+        [&](const auto& ld, int k, float sy, int, bool, int, int) {
             FsRaw o;
-            o.a = __ldg(r + k);
-            o.b = __ldg(d + k);
-            o.cc = __ldg(cc + k);
-            o.he = __ldg(heff + k);
+            o.a = ld.ld2(0, r + k, true);
+            o.b = ld.ld2(1, d + k, true);
+            o.cc = ld.ld1(0, cc + k, true);
+            o.he = ld.ld1(1, heff + k, true);
             o.sy = sy;
             return o;
         },
@@ -107,13 +113,15 @@ __global__ void __launch_bounds__(FS_NT, FS_MINB) fcg_post_stream_kernel(
     double s0 = 0.0;
     fs_sweep(
         g, rows,
-        [&](int k, float sy, int, bool, int mi, int mj) {
+        [&](const auto& ld, int k, float sy, int, bool, int mi, int mj) {
             FsRaw o;
             const int q = mj * Wp + mi;
-            o.a = __ldg(z1 + k);
-            o.b = nhwc ? __ldg(reinterpret_cast<const float2*>(y) + q) : make_float2(__ldg(y + q), __ldg(y + plane + q));
-            o.cc = __ldg(cc + k);
-            o.he = __ldg(heff + k);
+            o.a = ld.ld2(0, z1 + k, true);
+            const float2 yp = ld.ld2(1, reinterpret_cast<const float2*>(y) + q, nhwc);
+            const float y0 = ld.ld1(2, y + q, !nhwc), y1 = ld.ld1(3, y + plane + q, !nhwc);
+            o.b = nhwc ? yp : make_float2(y0, y1);
+            o.cc = ld.ld1(0, cc + k, true);
+            o.he = ld.ld1(1, heff + k, true);
             o.sy = sy;
             return o;
         },
@@ -142,12 +150,12 @@ __global__ void __launch_bounds__(FS_NT, FS_MINB) fcg_dir_stream_kernel(
     double s0 = 0.0, s1 = 0.0;
     fs_sweep(
         g, rows,
-        [&](int k, float sy, int, bool, int, int) {
+        [&](const auto& ld, int k, float sy, int, bool, int, int) {
             FsRaw o;
-            o.a = __ldg(zv + k);
-            o.b = first ? make_float2(0.f, 0.f) : __ldg(p_old + k);
-            o.cc = __ldg(cc + k);
-            o.he = __ldg(heff + k);
+            o.a = ld.ld2(0, zv + k, true);
+            o.b = ld.ld2(1, p_old + k, !first);
+            o.cc = ld.ld1(0, cc + k, true);
+            o.he = ld.ld1(1, heff + k, true);
             o.sy = sy;
             return o;
         },

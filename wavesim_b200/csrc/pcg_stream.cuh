@@ -1,4 +1,4 @@
-// pcg_stream.cuh — the dispersive solve with register-streaming sweeps.
+// pcg_stream.cuh — the dispersive solve with streaming sweeps.
 //
 // The same method as pcg.cuh's pcg_solve: the reference's Jacobi-preconditioned CG
 // (crates/wavecore/src/dispersion.rs:493-545) in its single-reduction form, one persistent
@@ -10,8 +10,9 @@
 // new u = r / diag, recomputed at halo cells from the banks, as pcg_solve does) stays in
 // registers, and the x-neighbours of the matrix product
 //   A v = mask (heff v - grad f),  f = c div v   (dispersion.rs:269-317)
-// come from the lanes beside by warp shuffles: no shared memory and no block barrier inside a
-// sweep. Rows are fetched PS_AHEAD rows before they are used.
+// come from the lanes beside by warp shuffles: no block barrier inside a sweep. Each lane copies
+// its column's rows a few rows ahead with cp.async into the warp's ring in shared memory and reads
+// them back as they enter the window, so the loads in flight hold no registers.
 #pragma once
 
 #include "common.cuh"
@@ -19,21 +20,28 @@
 
 namespace wcb {
 
-// Launch shape, the best of eight measured on 2048 x 1024 and 4096 x 4096 (2-4 blocks per SM, 1-3
-// rows in flight, 16 or 32 rows per strip or rows fitted to the grid): 3 blocks of 256 threads per
-// SM, 1 row in flight, rows per strip fitted so that every warp gets one strip (solve 5.17 and
-// 75.2 ms per step against 6.08 and 85.1 for 2 blocks and 2 rows). The macros let a tuning build
-// try others.
+// Launch shape. Rows are fetched PS_DEPTH rows before they are used, by cp.async into a ring in
+// shared memory (the rows in flight hold no registers), or, with PS_DEPTH 0, PS_AHEAD rows ahead
+// into registers. Measured on 2048 x 1024 and 4096 x 4096 (Jacobi, ms per step): the ring with 3
+// rows in flight and 2 blocks of 256 threads per SM (127 registers, no spills) 4.95 and 75.4; 4 or
+// 5 rows 5.00-5.09 and 74.7-77.9; 3 blocks per SM (80 registers, spills) 5.50 and 80.5; registers
+// with 1 or 2 rows ahead 5.83-5.89 and 90.7-92.3 at 2 blocks, 5.49 and 79.5 at 3. Rows per strip
+// are fitted so that every warp gets one strip. The macros let a tuning build try others.
 #ifndef WCB_PS_MINB
-#define WCB_PS_MINB 3
+#define WCB_PS_MINB 2
 #endif
 #ifndef WCB_PS_AHEAD
 #define WCB_PS_AHEAD 1
 #endif
+#ifndef WCB_PS_DEPTH
+#define WCB_PS_DEPTH 3
+#endif
 constexpr int PS_NT = 256, PS_WARPS = PS_NT / 32, PS_MINB = WCB_PS_MINB;
 constexpr int PS_HALO = 2, PS_OUT = 32 - 2 * PS_HALO;  // 28 own columns per strip
 constexpr int PS_ROWS_MIN = 16, PS_ROWS_MAX = 512;      // rows per strip, chosen per grid
-constexpr int PS_AHEAD = WCB_PS_AHEAD;                 // rows in flight beyond the window
+constexpr int PS_AHEAD = WCB_PS_AHEAD;                 // register mode: rows in flight beyond the window
+constexpr int PS_DEPTH = WCB_PS_DEPTH;                 // ring mode: rows in flight
+constexpr int PS_SLOTS = PS_DEPTH + 1;                 // ring slots: a slot is refilled one row after it is read
 
 __device__ __forceinline__ float ps_up(float v) { return __shfl_up_sync(0xffffffffu, v, 1); }
 __device__ __forceinline__ float ps_dn(float v) { return __shfl_down_sync(0xffffffffu, v, 1); }
@@ -52,13 +60,62 @@ inline int ps_rows_for(int nx, int ny, int warps) {
     return rows > PS_ROWS_MAX ? PS_ROWS_MAX : rows;
 }
 
-// One strip: rows j0-2 .. j0+rows+1 of the lane's column are fetched (`fetch(k, sy, j, own, mi, mj)`:
-// the loads at stored index k = mj pitch + mi of padded row j, sy the sign of the y-normal
-// component there, own whether the cell is one the strip updates) and turned
-// into window rows (`make(raw)`: a Row with the signed vector v, c and heff); for every own cell
-// `out(k, i, j, row, Av, c_left, c_right, c_below, c_above)` gets the row, the product and the
-// four neighbouring c.
-template <class Raw, class Row, class Fetch, class Make, class Out>
+// A warp's ring of rows in flight: PS_SLOTS slots of NF2 float2 and NF1 float fields, laid out
+// [slot][field][lane] so that a field of a row is one conflict-free shared access of 32 lanes.
+// Bytes per warp, and per block of `warps` warps (dynamic shared memory).
+template <int NF2, int NF1>
+__host__ __device__ constexpr int ps_ring_bytes() {
+    return PS_DEPTH > 0 ? PS_SLOTS * 32 * (8 * NF2 + 4 * NF1) : 0;
+}
+
+// The loads of one row go through a loader: ld2(n, p, en) / ld1(n, p, en) give field n of the row,
+// the float2 or float at p, or zero where en is false. A fetch names every load of its row in the
+// same order with the same en on every call.
+//   PsDirect  loads into registers now;
+//   PsIssue   starts the copies into the row's ring slot (returns zeros);
+//   PsRead    reads the slot back once its copies have landed.
+struct PsDirect {
+    __device__ __forceinline__ float2 ld2(int, const float2* p, bool en) const {
+        return en ? __ldcg(p) : make_float2(0.f, 0.f);
+    }
+    __device__ __forceinline__ float ld1(int, const float* p, bool en) const { return en ? __ldg(p) : 0.f; }
+};
+struct PsIssue {
+    float2* f2;  // the lane's field 0 in the slot; field n at +32 n
+    float* f1;
+    bool on;     // false: the row is past the strip's end, nothing is copied
+    __device__ __forceinline__ float2 ld2(int n, const float2* p, bool en) const {
+        if (on && en) cp_async8(f2 + 32 * n, p);
+        return make_float2(0.f, 0.f);
+    }
+    __device__ __forceinline__ float ld1(int n, const float* p, bool en) const {
+        if (on && en) cp_async4(f1 + 32 * n, p);
+        return 0.f;
+    }
+};
+struct PsRead {
+    const float2* f2;
+    const float* f1;
+    __device__ __forceinline__ float2 ld2(int n, const float2*, bool en) const {
+        return en ? f2[32 * n] : make_float2(0.f, 0.f);
+    }
+    __device__ __forceinline__ float ld1(int n, const float*, bool en) const { return en ? f1[32 * n] : 0.f; }
+};
+
+// The calling warp's ring in the block's dynamic shared memory.
+template <int NF2, int NF1>
+__device__ __forceinline__ unsigned char* ps_ring() {
+    extern __shared__ __align__(16) unsigned char ps_dyn[];
+    return ps_dyn + (threadIdx.x >> 5) * ps_ring_bytes<NF2, NF1>();
+}
+
+// One strip: rows j0-2 .. j0+rows+1 of the lane's column are fetched
+// (`fetch(loader, k, sy, j, own, mi, mj)`: the loads at stored index k = mj pitch + mi of padded
+// row j, sy the sign of the y-normal component there, own whether the cell is one the strip
+// updates) and turned into window rows (`make(raw)`: a Row with the signed vector v, c and heff);
+// for every own cell `out(k, i, j, row, Av, c_left, c_right, c_below, c_above)` gets the row, the
+// product and the four neighbouring c. NF2 / NF1: the ring's fields per row (at least the fetch's).
+template <class Raw, class Row, int NF2, int NF1, class Fetch, class Make, class Out>
 __device__ __forceinline__ void ps_strip(const DevGrid& g, int strip, int rows, Fetch fetch, Make make, Out out) {
     const int strips_x = (g.nx + PS_OUT - 1) / PS_OUT;
     const int lane = threadIdx.x & 31;
@@ -66,7 +123,7 @@ __device__ __forceinline__ void ps_strip(const DevGrid& g, int strip, int rows, 
     const int j0 = (strip / strips_x) * rows;
     const int mi = reflect_idx(i, g.nx);
     const bool own_col = lane >= PS_HALO && lane < PS_HALO + PS_OUT && i < g.nx;
-    auto get = [&](int j) -> Raw {
+    auto get = [&](const auto& ld, int j) -> Raw {
         int mj;
         float sy;
         if (g.periodic) {
@@ -76,28 +133,60 @@ __device__ __forceinline__ void ps_strip(const DevGrid& g, int strip, int rows, 
             mj = reflect_idx(j, g.ny);
             sy = ((unsigned)j < (unsigned)g.ny) ? 1.f : -1.f;
         }
-        return fetch(mj * g.pitch + mi, sy, j, own_col && j >= j0 && j < j0 + rows && j < g.ny, mi, mj);
+        return fetch(ld, mj * g.pitch + mi, sy, j, own_col && j >= j0 && j < j0 + rows && j < g.ny, mi, mj);
     };
     // f = c div v of the window's middle row
     auto fval = [&](const Row& m, const Row& c, const Row& p) -> float {
         const float vl = ps_up(c.v.x), vr = ps_dn(c.v.x);
         return c.cc * ((vr - vl) * g.ix + (p.v.y - m.v.y) * g.iy);
     };
-    Raw ahead[PS_AHEAD];
+    // The last row the strip reads: the window reaches two rows below its last own row.
+    const int j_last = (j0 + rows < g.ny ? j0 + rows : g.ny) + 1;
+    unsigned char* ring = nullptr;
+    int slot_in = 0, slot_out = 0;
+    auto slot_f2 = [&](int sl) { return reinterpret_cast<float2*>(ring) + sl * NF2 * 32 + lane; };
+    auto slot_f1 = [&](int sl) {
+        return reinterpret_cast<float*>(ring + PS_SLOTS * NF2 * 32 * 8) + sl * NF1 * 32 + lane;
+    };
+    auto issue = [&](int j) {  // start row j's copies into the next free slot
+        PsIssue ld{slot_f2(slot_in), slot_f1(slot_in), j <= j_last};
+        (void)get(ld, j);
+        cp_async_commit();
+        slot_in = slot_in + 1 == PS_SLOTS ? 0 : slot_in + 1;
+    };
+    Raw ahead[PS_DEPTH > 0 ? 1 : PS_AHEAD];
+    // row j, the oldest row in flight: wait for it, read it, and start row j + (rows in flight)
+    auto take = [&](int j) -> Raw {
+        if constexpr (PS_DEPTH > 0) {
+            cp_async_wait<PS_DEPTH - 1>();
+            const Raw raw = get(PsRead{slot_f2(slot_out), slot_f1(slot_out)}, j);
+            slot_out = slot_out + 1 == PS_SLOTS ? 0 : slot_out + 1;
+            issue(j + PS_DEPTH);
+            return raw;
+        } else {
+            const Raw raw = ahead[0];
 #pragma unroll
-    for (int d = 0; d < PS_AHEAD; d++) ahead[d] = get(j0 + 2 + d);
-    Row rm2 = make(get(j0 - 2)), rm1 = make(get(j0 - 1)), r0 = make(get(j0)), r1 = make(get(j0 + 1));
+            for (int d = 0; d < PS_AHEAD - 1; d++) ahead[d] = ahead[d + 1];
+            ahead[PS_AHEAD - 1] = get(PsDirect{}, j + PS_AHEAD);
+            return raw;
+        }
+    };
+    if constexpr (PS_DEPTH > 0) {
+        ring = ps_ring<NF2, NF1>();
+#pragma unroll
+        for (int d = 0; d < PS_DEPTH; d++) issue(j0 - 2 + d);
+    } else {
+#pragma unroll
+        for (int d = 0; d < PS_AHEAD; d++) ahead[d] = get(PsDirect{}, j0 - 2 + d);
+    }
+    Row rm2 = make(take(j0 - 2)), rm1 = make(take(j0 - 1)), r0 = make(take(j0)), r1 = make(take(j0 + 1));
     float f_m = fval(rm2, rm1, r0);  // row j0-1
     float f_0 = fval(rm1, r0, r1);   // row j0
     float c_m = rm1.cc;
     for (int r = 0; r < rows; r++) {
         const int j = j0 + r;
         if (j >= g.ny) break;  // uniform over the warp
-        const Raw nraw = ahead[0];
-#pragma unroll
-        for (int d = 0; d < PS_AHEAD - 1; d++) ahead[d] = ahead[d + 1];
-        ahead[PS_AHEAD - 1] = get(j + 2 + PS_AHEAD);
-        const Row r2 = make(nraw);  // row j+2
+        const Row r2 = make(take(j + 2));  // row j+2
         const float f_1 = fval(r0, r1, r2);
         const float fl = ps_up(f_0), fr = ps_dn(f_0);
         const float cl = ps_up(r0.cc), cr = ps_dn(r0.cc);
@@ -114,6 +203,7 @@ __device__ __forceinline__ void ps_strip(const DevGrid& g, int strip, int rows, 
         f_m = f_0;
         f_0 = f_1;
     }
+    if constexpr (PS_DEPTH > 0) cp_async_wait<0>();  // the rows started past the strip's end copy nothing
 }
 
 // The initial sweep's loads: the warm start, c, heff; the right-hand side on own cells.
@@ -138,6 +228,9 @@ struct PsCgRow {
     float2 v;
     float cc, he;
 };
+// Ring fields per row of the solve's sweeps (the CG sweep's; the initial sweep's fit).
+constexpr int PS_NF2 = 6, PS_NF1 = 2;
+constexpr int PS_SMEM = PS_WARPS * ps_ring_bytes<PS_NF2, PS_NF1>();  // dynamic shared memory per block
 
 // The solve and the stage epilogue by the `ncta` CTAs (this one is number `cta`) of the launch;
 // returns false if a bounded wait expired (every CTA then returns).
@@ -171,14 +264,14 @@ __device__ __forceinline__ bool pcg_solve_stream(const PcgArgs& a, int cta, int 
             const int strips_x = (g.nx + PS_OUT - 1) / PS_OUT;
             const int i_lane = (st % strips_x) * PS_OUT - PS_HALO + lane_i;
             const float sx = ((unsigned)i_lane < (unsigned)g.nx) ? 1.f : -1.f;
-            ps_strip<PsInitRaw, PsInitRow>(
+            ps_strip<PsInitRaw, PsInitRow, PS_NF2, PS_NF1>(
                 g, st, rows,
-                [&](int k, float sy, int, bool own, int, int) {
+                [&](const auto& ld, int k, float sy, int, bool own, int, int) {
                     PsInitRaw r;
-                    r.w = __ldcg(a.w + k);
-                    r.cc = __ldg(a.cc + k);
-                    r.he = __ldg(a.heff + k);
-                    r.b = own ? __ldg(a.bv + k) : make_float2(0.f, 0.f);
+                    r.w = ld.ld2(0, a.w + k, true);
+                    r.b = ld.ld2(1, a.bv + k, own);
+                    r.cc = ld.ld1(0, a.cc + k, true);
+                    r.he = ld.ld1(1, a.heff + k, true);
                     r.sy = sy;
                     return r;
                 },
@@ -222,26 +315,18 @@ __device__ __forceinline__ bool pcg_solve_stream(const PcgArgs& a, int cta, int 
                 const int strips_x = (g.nx + PS_OUT - 1) / PS_OUT;
                 const int i_lane = (st % strips_x) * PS_OUT - PS_HALO + lane_i;
                 const float sx = ((unsigned)i_lane < (unsigned)g.nx) ? 1.f : -1.f;
-                ps_strip<PsCgRaw, PsCgRow>(
+                ps_strip<PsCgRaw, PsCgRow, PS_NF2, PS_NF1>(
                     g, st, rows,
-                    [&](int k, float sy, int, bool own, int, int) {
+                    [&](const auto& ld, int k, float sy, int, bool own, int, int) {
                         PsCgRaw r;
-                        r.r = __ldcg(a.rb[rb] + k);
-                        r.d = __ldcg(a.diag + k);
-                        r.q = make_float2(0.f, 0.f);
-                        r.s = make_float2(0.f, 0.f);
-                        if (!init) {
-                            r.q = __ldcg(a.qb[rb] + k);
-                            if (!first) r.s = __ldcg(a.sb[rb] + k);
-                        }
-                        r.p = make_float2(0.f, 0.f);
-                        r.x = make_float2(0.f, 0.f);
-                        if (!init && own) {
-                            r.x = __ldcg(a.w + k);
-                            if (!first) r.p = __ldcg(a.p0 + k);
-                        }
-                        r.cc = __ldg(a.cc + k);
-                        r.he = __ldg(a.heff + k);
+                        r.r = ld.ld2(0, a.rb[rb] + k, true);
+                        r.d = ld.ld2(1, a.diag + k, true);
+                        r.q = ld.ld2(2, a.qb[rb] + k, !init);
+                        r.s = ld.ld2(3, a.sb[rb] + k, !init && !first);
+                        r.x = ld.ld2(4, a.w + k, !init && own);
+                        r.p = ld.ld2(5, a.p0 + k, !init && !first && own);
+                        r.cc = ld.ld1(0, a.cc + k, true);
+                        r.he = ld.ld1(1, a.heff + k, true);
                         r.sy = sy;
                         r.k = own ? k : -1;
                         return r;

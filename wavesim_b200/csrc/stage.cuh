@@ -114,11 +114,14 @@ __device__ __forceinline__ float minmod3(float a, float b, float c) {
 // solver.rs:118-138, as offsets from the centre value: the reference's
 // (2 v0 - 13 v1 + 47 c + 27 v3 - 3 v4)/60 is c + (2(v0-c) - 13(v1-c) + 27(v3-c) - 3(v4-c))/60
 // because the weights sum to 60; a flat field gives exactly c at both faces.
+// The MC slope s = minmod(2 dl, (dl + dh)/2, 2 dh) enters only as s/2, which is
+// minmod(dl, (dl + dh)/4, dh): scaling by powers of two is exact, so this is the same value
+// unless (dl + dh)/4 falls below the normal range (differences of 1e-42 in momenta near zero).
 __device__ __forceinline__ void face_values(float v0, float v1, float c, float v3, float v4,
                                             float blend, float& lo, float& hi) {
     const float dl = c - v1, dh = v3 - c;
-    const float s = minmod3(2.f * dl, 0.5f * (dl + dh), 2.f * dh);
-    float mlo = -0.5f * s, mhi = 0.5f * s;
+    float mhi = minmod3(dl, 0.25f * (dl + dh), dh);
+    float mlo = -mhi;
     if (blend > 0.f) {
         const float a0 = v0 - c, a1 = -dl, a3 = dh, a4 = v4 - c;
         const float fh = (2.f * a0 - 13.f * a1 + 27.f * a3 - 3.f * a4) * (1.f / 60.f);

@@ -1,13 +1,14 @@
-// stream.cuh — the shallow-water RK stage (first and second order) as a register-streaming kernel.
+// stream.cuh — the shallow-water RK stage (first and second order) as a streaming kernel.
 //
 // Each warp owns a strip of SW_OUT = 32 SW_CPL - 4 interior columns and marches down SW_ROWS rows
 // of it. Its 32 lanes hold the strip's columns plus two halo columns on each side (SW_CPL adjacent
 // columns per lane), so the x-neighbours a reconstruction needs come from the lane itself or from
 // the lanes beside it by warp shuffles. Down the march, a three-row window of (eta, h, u, v, b),
-// the high-side y reconstruction of the current row, the y-face flux just above it and a queue of
-// prefetched rows stay in registers. Per cell and row the kernel reconstructs once per axis
+// the high-side y reconstruction of the current row and the y-face flux just above it stay in
+// registers; the rows below are copied ahead by cp.async into the warp's ring in shared memory,
+// each lane its own columns. Per cell and row the kernel reconstructs once per axis
 // (solver.rs:140-183), computes one x face and one y face (solver.rs:185-226) and updates the cell
-// (solver.rs:481-616): no shared-memory staging, no block barriers, every face once. The
+// (solver.rs:481-616): no tile staging, no block barriers, every face once. The
 // arithmetic is the tiled stage kernel's (stage.cuh), operation for operation: the same
 // reconstruction, the remainder-form HLL, the well-balanced momentum update and the FP64 mass
 // telescoping, so both kernels give the same bits.
@@ -22,10 +23,13 @@
 
 namespace wcb {
 
-// Launch shape, the best of seven measured on 4096 x 4096 (0.396-0.448 ms per stage: one or two
-// columns per lane, 128 or 256 threads, 2-6 blocks per SM, 16-64 rows per strip, 2-5 rows in
-// flight): one column per lane, 128 threads, 6 blocks per SM, 32 rows, 3 rows in flight. The
-// macros let a tuning build try others.
+// Launch shape. Rows are fetched SW_DEPTH rows before they enter the window, by cp.async into a
+// per-warp ring in shared memory (no registers held while in flight); SW_DEPTH 0 keeps SW_AHEAD
+// rows in registers instead. On 4096 x 4096 (ms per stage): the ring with 3 rows in flight, one
+// column per lane, 128 threads, 6 blocks per SM and 32 rows per strip 0.335 (4 or 6 rows the same;
+// 7 or 8 blocks per SM 0.337-0.345); registers with 3 rows ahead 0.386, the best of seven register
+// shapes (one or two columns per lane, 128 or 256 threads, 2-6 blocks per SM, 16-64 rows per
+// strip, 2-5 rows in flight: 0.396-0.448 before the ring). The macros let a tuning build try others.
 #ifndef WCB_SW_CPL
 #define WCB_SW_CPL 1
 #endif
@@ -41,13 +45,32 @@ namespace wcb {
 #ifndef WCB_SW_AHEAD
 #define WCB_SW_AHEAD 3
 #endif
+#ifndef WCB_SW_DEPTH
+#define WCB_SW_DEPTH 3
+#endif
 constexpr int SW_HALO = 2;
 constexpr int SW_CPL = WCB_SW_CPL;      // columns per lane
 constexpr int SW_NT = WCB_SW_NT, SW_WARPS = SW_NT / 32, SW_MINB = WCB_SW_MINB;
 constexpr int SW_ROWS = WCB_SW_ROWS;    // rows per strip
-constexpr int SW_AHEAD = WCB_SW_AHEAD;  // rows in flight beyond the window
+constexpr int SW_AHEAD = WCB_SW_AHEAD;  // register mode: rows in flight beyond the window
+constexpr int SW_DEPTH = WCB_SW_DEPTH;  // ring mode (> 0): rows in flight, by cp.async into shared memory
+constexpr int SW_SLOTS = SW_DEPTH + 1;  // ring slots: a slot is refilled one row after it is read
 constexpr int sw_out(int cpl) { return 32 * cpl - 2 * SW_HALO; }
 constexpr int SW_OUT = sw_out(SW_CPL);
+
+// A ring slot holds one row of the lane's columns: the state and bed of row R and, for a finishing
+// second stage, the own cells' state at the start of the step of row R - 2 (the row that is
+// updated when row R enters the window). Laid out [field][column][lane]: conflict-free accesses.
+template <int CPL>
+__host__ __device__ constexpr int sw_slot_bytes() { return CPL * 32 * (16 + 16 + 4); }
+template <int CPL>
+__host__ __device__ constexpr int sw_smem() { return SW_DEPTH > 0 ? SW_WARPS * SW_SLOTS * sw_slot_bytes<CPL>() : 0; }
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(smem)),
+                 "l"(gmem)
+                 : "memory");
+}
 
 // One loaded cell: the state as stored (h_hi, h_lo, hu, hv with the ghost sign flips applied) and
 // the bed.
@@ -188,10 +211,8 @@ __global__ void __launch_bounds__(SW_NT, SW_MINB) swe_stream_kernel(StageArgs a,
         prof[c] = (a.maker.on && own[c]) ? __ldg(a.maker.prof + col[c]) : 0.f;
     }
 
-    // row j of this lane's columns, ghost rows mirrored or wrapped
-    auto load_row = [&](int j, SwRaw* out) {
-        int mj;
-        float sy;
+    // padded row j: its stored row and the sign of the y-normal momentum there
+    auto map_row = [&](int j, int& mj, float& sy) {
         if (g.periodic) {
             mj = wrap_idx(j, g.ny);
             sy = 1.f;
@@ -199,18 +220,98 @@ __global__ void __launch_bounds__(SW_NT, SW_MINB) swe_stream_kernel(StageArgs a,
             mj = reflect_idx(j, g.ny);
             sy = ((unsigned)j < (unsigned)g.ny) ? 1.f : -1.f;
         }
+    };
+    // row j of this lane's columns, ghost rows mirrored or wrapped
+    auto load_row = [&](int j, SwRaw* out) {
+        int mj;
+        float sy;
+        map_row(j, mj, sy);
 #pragma unroll
         for (int c = 0; c < CPL; c++) out[c] = sw_load(a, mj * g.pitch + mi[c], sx[c], sy);
     };
     auto wall_y = [&](int jf) -> bool { return !g.periodic && (jf == 0 || jf == g.ny); };  // face below row jf
 
+    // Rows enter the window through take(R), in order from j0-2; the row updated when row R
+    // enters is R-2, and its start-of-step state comes with it (q_old, own cells of a finishing
+    // second stage).
+    const int j_end = (j0 + SW_ROWS < g.ny ? j0 + SW_ROWS : g.ny) - 1;  // the strip's last row
+    const int j_last = j_end + 2;                                      // the last row it reads
+    unsigned char* ring = nullptr;
+    int slot_in = 0, slot_out = 0;
+    auto ring_q = [&](int sl, int c) {
+        return reinterpret_cast<float4*>(ring + sl * sw_slot_bytes<CPL>()) + c * 32 + lane;
+    };
+    auto ring_qo = [&](int sl, int c) {
+        return reinterpret_cast<float4*>(ring + sl * sw_slot_bytes<CPL>()) + (CPL + c) * 32 + lane;
+    };
+    auto ring_b = [&](int sl, int c) {
+        return reinterpret_cast<float*>(ring + sl * sw_slot_bytes<CPL>() + CPL * 32 * 32) + c * 32 + lane;
+    };
+    auto issue = [&](int R) {  // start row R's copies (and row R-2's q_old) into the next free slot
+        if (R <= j_last) {
+            int mj;
+            float sy;
+            map_row(R, mj, sy);
+            const bool qo_on = MODE == MODE_STAGE2 && R - 2 >= j0 && R - 2 <= j_end;
+#pragma unroll
+            for (int c = 0; c < CPL; c++) {
+                cp_async16(ring_q(slot_in, c), a.qin + mj * g.pitch + mi[c]);
+                cp_async4(ring_b(slot_in, c), a.bed + mj * g.pitch + mi[c]);
+                if (qo_on && own[c]) cp_async16(ring_qo(slot_in, c), a.qold + (size_t)(R - 2) * g.pitch + col[c]);
+            }
+        }
+        cp_async_commit();
+        slot_in = slot_in + 1 == SW_SLOTS ? 0 : slot_in + 1;
+    };
+    SwRaw ahead[SW_DEPTH > 0 ? 1 : SW_AHEAD][CPL];
+    auto take = [&](int R, SwRaw* out, float4* q_old) {
+        if constexpr (SW_DEPTH > 0) {
+            cp_async_wait<SW_DEPTH - 1>();
+            int mj;
+            float sy;
+            map_row(R, mj, sy);
+            const bool qo_on = MODE == MODE_STAGE2 && R - 2 >= j0 && R - 2 <= j_end;
+#pragma unroll
+            for (int c = 0; c < CPL; c++) {
+                out[c].q = *ring_q(slot_out, c);
+                out[c].q.z *= sx[c];
+                out[c].q.w *= sy;
+                out[c].b = *ring_b(slot_out, c);
+                q_old[c] = (qo_on && own[c]) ? *ring_qo(slot_out, c) : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+            slot_out = slot_out + 1 == SW_SLOTS ? 0 : slot_out + 1;
+            issue(R + SW_DEPTH);
+        } else {
+#pragma unroll
+            for (int c = 0; c < CPL; c++) out[c] = ahead[0][c];
+#pragma unroll
+            for (int d = 0; d < SW_AHEAD - 1; d++)
+#pragma unroll
+                for (int c = 0; c < CPL; c++) ahead[d][c] = ahead[d + 1][c];
+            load_row(R + SW_AHEAD, ahead[SW_AHEAD - 1]);
+#pragma unroll
+            for (int c = 0; c < CPL; c++) {
+                q_old[c] = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (MODE == MODE_STAGE2 && own[c] && R - 2 >= j0 && R - 2 <= j_end)
+                    q_old[c] = __ldg(a.qold + (size_t)(R - 2) * g.pitch + col[c]);
+            }
+        }
+    };
+    if constexpr (SW_DEPTH > 0) {
+        extern __shared__ __align__(16) unsigned char sw_dyn[];
+        ring = sw_dyn + warp * SW_SLOTS * sw_slot_bytes<CPL>();
+#pragma unroll
+        for (int d = 0; d < SW_DEPTH; d++) issue(j0 - 2 + d);
+    } else {
+#pragma unroll
+        for (int d = 0; d < SW_AHEAD; d++) load_row(j0 - 2 + d, ahead[d]);
+    }
+
     // ---- prologue: rows j0-2 .. j0+1, the y faces below j0 ----------------------------------
     SwRaw rw[4][CPL];
+    float4 q_old[CPL];
 #pragma unroll
-    for (int d = 0; d < 4; d++) load_row(j0 - 2 + d, rw[d]);
-    SwRaw ahead[SW_AHEAD][CPL];
-#pragma unroll
-    for (int d = 0; d < SW_AHEAD; d++) load_row(j0 + 2 + d, ahead[d]);
+    for (int d = 0; d < 4; d++) take(j0 - 2 + d, rw[d], q_old);
     SwCell c0[CPL], c1[CPL];
     float4 q_own[CPL], q_nxt[CPL];
     float b_own[CPL], b_nxt[CPL];
@@ -238,21 +339,9 @@ __global__ void __launch_bounds__(SW_NT, SW_MINB) swe_stream_kernel(StageArgs a,
     for (int r = 0; r < SW_ROWS; r++) {
         const int j = j0 + r;
         if (j >= g.ny) break;  // uniform over the warp
-        // the next row enters the window; another row is requested
+        // the next row enters the window (with row j's start-of-step state)
         SwRaw r2[CPL];
-#pragma unroll
-        for (int c = 0; c < CPL; c++) r2[c] = ahead[0][c];
-#pragma unroll
-        for (int d = 0; d < SW_AHEAD - 1; d++)
-#pragma unroll
-            for (int c = 0; c < CPL; c++) ahead[d][c] = ahead[d + 1][c];
-        load_row(j + 2 + SW_AHEAD, ahead[SW_AHEAD - 1]);
-        float4 q_old[CPL];
-#pragma unroll
-        for (int c = 0; c < CPL; c++) {
-            q_old[c] = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (MODE == MODE_STAGE2 && own[c]) q_old[c] = __ldg(a.qold + (size_t)j * g.pitch + col[c]);
-        }
+        take(j + 2, r2, q_old);
 
         // y: reconstruct row j+1, the face above row j
         SwCell c2[CPL];
@@ -359,6 +448,8 @@ __global__ void __launch_bounds__(SW_NT, SW_MINB) swe_stream_kernel(StageArgs a,
             fy_lo[c] = fy_hi[c];
         }
     }
+
+    if constexpr (SW_DEPTH > 0) cp_async_wait<0>();  // rows past the strip's end copy nothing
 
     if (MODE != MODE_STAGE1) {
         rmax = warp_max(rmax);

@@ -313,9 +313,9 @@ wc_status launch_stage(wc_solver* s, int mode, const float4* qin, const float4* 
     if (!s->sgn && o <= 1 && s->swe_streaming) {
         const int strips_x = (s->g.nx + SW_OUT - 1) / SW_OUT;
         const dim3 sgrid((strips_x + SW_WARPS - 1) / SW_WARPS, (s->g.ny + SW_ROWS - 1) / SW_ROWS);
-        if (mode == MODE_FIRST) swe_stream_kernel<MODE_FIRST, 0, SW_CPL><<<sgrid, SW_NT, 0, st>>>(a, strips_x);
-        else if (mode == MODE_STAGE1) swe_stream_kernel<MODE_STAGE1, 1, SW_CPL><<<sgrid, SW_NT, 0, st>>>(a, strips_x);
-        else swe_stream_kernel<MODE_STAGE2, 1, SW_CPL><<<sgrid, SW_NT, 0, st>>>(a, strips_x);
+        if (mode == MODE_FIRST) swe_stream_kernel<MODE_FIRST, 0, SW_CPL><<<sgrid, SW_NT, sw_smem<SW_CPL>(), st>>>(a, strips_x);
+        else if (mode == MODE_STAGE1) swe_stream_kernel<MODE_STAGE1, 1, SW_CPL><<<sgrid, SW_NT, sw_smem<SW_CPL>(), st>>>(a, strips_x);
+        else swe_stream_kernel<MODE_STAGE2, 1, SW_CPL><<<sgrid, SW_NT, sw_smem<SW_CPL>(), st>>>(a, strips_x);
         s->launches++;
         CK(cudaGetLastError());
         return WC_OK;
@@ -395,6 +395,7 @@ wc_status launch_pcg(wc_solver* s, int mode, const float4* qold, float4* qout, c
     if (s->solve_streaming) {
         lc.gridDim = dim3(s->pcg_stream_blocks);
         lc.blockDim = dim3(PS_NT);
+        lc.dynamicSmemBytes = PS_SMEM;
         CK(cudaLaunchKernelEx(&lc, pcg_stream_kernel, a));
     } else {
         CK(cudaLaunchKernelEx(&lc, pcg_kernel, a));
@@ -488,7 +489,7 @@ wc_status fcg_body(wc_solver* s, cudaStream_t st, cudaGraphConditionalHandle h, 
         ProfScope ps(s, 1);
         unsigned* xh = nhwc ? reinterpret_cast<unsigned*>(s->lnet.Xh.p) : nullptr;
         if (S == 1 && s->fcg_streaming)
-            FCG_LAUNCH(fcg_pre_stream_kernel<<<s->fcg_stream_blocks, FS_NT, 0, st>>>(
+            FCG_LAUNCH(fcg_pre_stream_kernel<<<s->fcg_stream_blocks, FS_NT, FS_SMEM, st>>>(
                 g, s->fcg_strip_rows, s->r, s->diag, s->cc, s->heff, z1, LPC_OMEGA, s->lnet.X[0].p, xh, hp, wp, sc));
         else if (S == 1)
             FCG_LAUNCH(fcg_pre_tile_kernel<<<nt, FT_NT, 0, st>>>(g, s->r, s->diag, s->cc, s->heff, z1, LPC_OMEGA,
@@ -507,10 +508,10 @@ wc_status fcg_body(wc_solver* s, cudaStream_t st, cudaGraphConditionalHandle h, 
     const int lgS = S == 1 ? 0 : S == 2 ? 1 : S == 4 ? 2 : 3;
     if (S == 1 && s->fcg_streaming) {
         const int nf = s->fcg_stream_blocks, rows = s->fcg_strip_rows;
-        FCG_LAUNCH(fcg_post_stream_kernel<<<nf, FS_NT, 0, st>>>(g, rows, z1, y, nhwc ? 1 : 0, s->r, s->diag, s->cc,
+        FCG_LAUNCH(fcg_post_stream_kernel<<<nf, FS_NT, FS_SMEM, st>>>(g, rows, z1, y, nhwc ? 1 : 0, s->r, s->diag, s->cc,
                                                                 s->heff, z, q, LPC_OMEGA, hp, wp, s->fpart, sc));
         TRY(fcg_scalars(s, st, FCG_BETA, nf, h, 0));
-        FCG_LAUNCH(fcg_dir_stream_kernel<<<nf, FS_NT, 0, st>>>(g, rows, z, p_old, p_new, s->cc, s->heff, q, s->r,
+        FCG_LAUNCH(fcg_dir_stream_kernel<<<nf, FS_NT, FS_SMEM, st>>>(g, rows, z, p_old, p_new, s->cc, s->heff, q, s->r,
                                                                s->fpart, sc));
         TRY(fcg_scalars(s, st, FCG_ALPHA, nf, h, 0));
     } else {
@@ -979,7 +980,13 @@ wc_status wc_solver_create(const wc_grid* grid, const double* bed_padded, const 
         const int tiles = s->pcg_tiles_x * s->pcg_tiles_y;
         s->pcg_blocks = std::max(1, std::min(tiles, sms * std::min(occ, 4)));
         int occ_s = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s, pcg_stream_kernel, PS_NT, 0) != cudaSuccess || occ_s < 1)
+        // the streaming sweeps' rings of rows in flight are dynamic shared memory
+        if (cudaFuncSetAttribute(pcg_stream_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, PS_SMEM) != cudaSuccess ||
+            cudaFuncSetAttribute(fcg_pre_stream_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, FS_SMEM) != cudaSuccess ||
+            cudaFuncSetAttribute(fcg_post_stream_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, FS_SMEM) != cudaSuccess ||
+            cudaFuncSetAttribute(fcg_dir_stream_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, FS_SMEM) != cudaSuccess)
+            return fail(set_err(WC_ECUDA, "setting the streaming sweeps' shared memory failed"));
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s, pcg_stream_kernel, PS_NT, PS_SMEM) != cudaSuccess || occ_s < 1)
             return fail(set_err(WC_ECUDA, "occupancy query for the streaming solve kernel failed"));
         s->pcg_strip_rows = ps_rows_for(nx, ny, sms * occ_s * PS_WARPS);
         const int strip_ctas = (ps_strips(nx, ny, s->pcg_strip_rows) + PS_WARPS - 1) / PS_WARPS;
@@ -992,7 +999,7 @@ wc_status wc_solver_create(const wc_grid* grid, const double* bed_padded, const 
             const char* v = std::getenv("WAVECORE_B200_FCG");
             s->fcg_streaming = !(v && std::strcmp(v, "tiled") == 0);
             int occ_f = 0;
-            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_f, fcg_dir_stream_kernel, FS_NT, 0) != cudaSuccess || occ_f < 1)
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_f, fcg_dir_stream_kernel, FS_NT, FS_SMEM) != cudaSuccess || occ_f < 1)
                 return fail(set_err(WC_ECUDA, "occupancy query for the flexible-CG passes failed"));
             occ_f = std::min(occ_f, FS_MINB);
             s->fcg_strip_rows = ps_rows_for(nx, ny, sms * occ_f * FS_WARPS);
