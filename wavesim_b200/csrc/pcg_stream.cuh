@@ -255,6 +255,10 @@ __device__ __forceinline__ bool pcg_solve_stream(const PcgArgs& a, int cta, int 
 
     long long it = 0;
     bool converged = false;
+    // w takes the iterations' steps alpha p in pairs (odd sweeps add their own and the even sweep's
+    // before them): after an odd number of iterations the last step is still to be added.
+    bool w_pending = false;
+    float alpha_last = 0.f;
     if (a.fcg && a.fcg->converged) {  // solved by the learned flexible CG: finish only
         converged = true;
     } else {  // the Jacobi solve; after a learned solve that failed, from where that one stopped
@@ -303,12 +307,15 @@ __device__ __forceinline__ bool pcg_solve_stream(const PcgArgs& a, int cta, int 
         const double target = a.tol * sqrt(tot[0]) + 1e-10;
         converged = sqrt(tot[2]) <= target;
         // ---- single-reduction CG (see pcg.cuh): with u = r / diag and q = A u, one sweep per
-        // iteration does p = u + beta p, s = q + beta s, w += alpha p, r -= alpha s, u = r / diag,
-        // q = A u and the three dots <r, u>, <u, q>, <r, r>; sweep k = -1 only forms q0 = A u0.
+        // iteration does p = u + beta p, s = q + beta s, r -= alpha s, u = r / diag, q = A u and the
+        // three dots <r, u>, <u, q>, <r, r>, and every second sweep w += alpha' p' + alpha p (the
+        // steps of the sweep before and its own: w is read and written half as often); sweep
+        // k = -1 only forms q0 = A u0.
         double gamma = 0.0, delta = 0.0, alpha_prev = 1.0, beta = 0.0;
-        auto cg_sweep = [&](int kk, float alpha_f, float beta_f, double* dots) -> bool {
+        auto cg_sweep = [&](int kk, float alpha_f, float beta_f, float alpha_prev_f, double* dots) -> bool {
             const bool init = kk < 0;
             const bool first = kk == 0;
+            const bool w_step = !init && (kk & 1);  // w takes this and the previous iteration's steps
             const int rb = init ? 0 : (kk & 1), wb = init ? 0 : ((kk + 1) & 1);
             double g1 = 0.0, g2 = 0.0, g3 = 0.0;
             for (int st = gw; st < nstrips; st += nw) {
@@ -323,7 +330,7 @@ __device__ __forceinline__ bool pcg_solve_stream(const PcgArgs& a, int cta, int 
                         r.d = ld.ld2(1, a.diag + k, true);
                         r.q = ld.ld2(2, a.qb[rb] + k, !init);
                         r.s = ld.ld2(3, a.sb[rb] + k, !init && !first);
-                        r.x = ld.ld2(4, a.w + k, !init && own);
+                        r.x = ld.ld2(4, a.w + k, w_step && own);
                         r.p = ld.ld2(5, a.p0 + k, !init && !first && own);
                         r.cc = ld.ld1(0, a.cc + k, true);
                         r.he = ld.ld1(1, a.heff + k, true);
@@ -347,7 +354,9 @@ __device__ __forceinline__ bool pcg_solve_stream(const PcgArgs& a, int cta, int 
                                     pk.y += beta_f * r.p.y;
                                 }
                                 a.p0[r.k] = pk;
-                                a.w[r.k] = make_float2(r.x.x + alpha_f * pk.x, r.x.y + alpha_f * pk.y);
+                                if (w_step)
+                                    a.w[r.k] = make_float2(r.x.x + (alpha_prev_f * r.p.x + alpha_f * pk.x),
+                                                           r.x.y + (alpha_prev_f * r.p.y + alpha_f * pk.y));
                                 a.sb[wb][r.k] = sk;
                                 a.rb[wb][r.k] = rn;
                             }
@@ -372,13 +381,13 @@ __device__ __forceinline__ bool pcg_solve_stream(const PcgArgs& a, int cta, int 
             return reduce_barrier<PS_NT>(a, epoch, g1, g2, g3, dots, red, cta, ncta);
         };
         if (!converged) {
-            if (!cg_sweep(-1, 0.f, 0.f, tot)) return false;
+            if (!cg_sweep(-1, 0.f, 0.f, 0.f, tot)) return false;
             gamma = tot[0];
             delta = tot[1];
         }
         while (!converged && it < a.max_iter) {
             const double alpha = it == 0 ? gamma / delta : gamma / (delta - beta * gamma / alpha_prev);
-            if (!cg_sweep((int)it, (float)alpha, (float)beta, tot)) return false;
+            if (!cg_sweep((int)it, (float)alpha, (float)beta, (float)alpha_prev, tot)) return false;
             it += 1;
             converged = sqrt(tot[2]) <= target;
             beta = tot[0] / gamma;
@@ -386,6 +395,8 @@ __device__ __forceinline__ bool pcg_solve_stream(const PcgArgs& a, int cta, int 
             delta = tot[1];
             alpha_prev = alpha;
         }
+        w_pending = (it & 1) != 0;
+        alpha_last = (float)alpha_prev;
     }
     if (a.fcg) it += a.fcg->iterations;
     if (cta == 0 && tid == 0) {
@@ -396,7 +407,8 @@ __device__ __forceinline__ bool pcg_solve_stream(const PcgArgs& a, int cta, int 
         ctl->last_iterations = (int)it;
     }
 
-    // ---- finish the stage from the solution (every w is final: the last reduction was a barrier)
+    // ---- finish the stage from the solution (every w and p is final: the last reduction was a
+    // barrier); a pending step of w is added here and w kept as the next solve's warm start
     float rmax = 0.f;
     int nan_here = 0;
     const long long ncell = (long long)g.nx * g.ny;
@@ -405,7 +417,12 @@ __device__ __forceinline__ bool pcg_solve_stream(const PcgArgs& a, int cta, int 
         const int k = j * g.pitch + i;
         const float2 hn = __ldg(a.hn + k);
         const float2 pr = __ldg(a.pred + k);
-        const float2 w = __ldcg(a.w + k);
+        float2 w = __ldcg(a.w + k);
+        if (w_pending) {
+            const float2 pk = __ldcg(a.p0 + k);
+            w = make_float2(w.x + alpha_last * pk.x, w.y + alpha_last * pk.y);
+            a.w[k] = w;
+        }
         const float he = __ldg(a.heff + k);
         float4 q0 = make_float4(0.f, 0.f, 0.f, 0.f);
         if (a.mode == MODE_STAGE2) q0 = __ldg(a.qold + k);
