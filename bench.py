@@ -53,7 +53,7 @@ STAGE_BYTES_SWE = (36 + 52) / 2                 # stage 1 / stage 2 (RK average 
 # two streaming second-order stages at 2048x2048; scaled to a launch by cells, and by iterations
 # for the solve).
 NETWORK_DRAM_BYTES_PER_CELL = 334.1e6 / (2048 * 1024)    # one application of the U-net
-PCG_DRAM_BYTES_PER_CELL_ITER = (6.30e9 + 4.44e9) / (2048 * 1024 * 58)  # one iteration of the solve
+PCG_DRAM_BYTES_PER_CELL_ITER = (5.57e9 + 3.88e9) / (2048 * 1024 * 58)  # one iteration of the solve
 STAGE_DRAM_BYTES_PER_CELL_SWE = ((93.0e6 + 32.1e6) + (161.3e6 + 35.6e6)) / 2 / (2048 * 2048)  # a stage
 
 

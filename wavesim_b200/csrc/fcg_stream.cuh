@@ -21,8 +21,9 @@ namespace wcb {
 #define WCB_FS_MINB 3
 #endif
 constexpr int FS_NT = 256, FS_WARPS = FS_NT / 32, FS_MINB = WCB_FS_MINB;
-// Ring fields per row (the post pass's: z1, y as pairs; c, heff, y as two planes).
-constexpr int FS_NF2 = 2, FS_NF1 = 4;
+// Ring fields per row (the post pass's: z1, y as pairs and r, D, q of the own cell two rows up;
+// c, heff, y as two planes).
+constexpr int FS_NF2 = 5, FS_NF1 = 4;
 constexpr int FS_SMEM = FS_WARPS * ps_ring_bytes<FS_NF2, FS_NF1>();  // dynamic shared memory per block
 
 struct FsRaw {
@@ -32,6 +33,10 @@ struct FsRaw {
 struct FsRow {
     float2 v;
     float cc, he;
+};
+// What an own cell's output reads besides the product: r, D and q, as the pass needs them.
+struct FsOwn {
+    float2 r, d, q;
 };
 
 __device__ __forceinline__ FsRow fs_row(const FsRaw& r, float2 v, float sx) {
@@ -43,8 +48,9 @@ __device__ __forceinline__ FsRow fs_row(const FsRaw& r, float2 v, float sx) {
 }
 
 // The warp's strips of one pass: strips gw, gw + nw, ... with rows per strip `rows`.
-template <class Fetch, class Make, class Out>
-__device__ __forceinline__ void fs_sweep(const DevGrid& g, int rows, Fetch fetch, Make make, Out out) {
+template <class Fetch, class Make, class Out, class FetchOwn>
+__device__ __forceinline__ void fs_sweep(const DevGrid& g, int rows, Fetch fetch, Make make, Out out,
+                                         FetchOwn fetch_own) {
     const int nstrips = ps_strips(g.nx, g.ny, rows);
     const int strips_x = (g.nx + PS_OUT - 1) / PS_OUT;
     const int gw = blockIdx.x * FS_WARPS + (threadIdx.x >> 5), nw = gridDim.x * FS_WARPS;
@@ -52,7 +58,7 @@ __device__ __forceinline__ void fs_sweep(const DevGrid& g, int rows, Fetch fetch
         const int i_lane = (st % strips_x) * PS_OUT - PS_HALO + (threadIdx.x & 31);
         const float sx = ((unsigned)i_lane < (unsigned)g.nx) ? 1.f : -1.f;
         ps_strip<FsRaw, FsRow, FS_NF2, FS_NF1>(
-            g, st, rows, fetch, [&](const FsRaw& r) { return make(r, sx); }, out);
+            g, st, rows, fetch, [&](const FsRaw& r) { return make(r, sx); }, out, fetch_own);
     }
 }
 
@@ -88,8 +94,8 @@ __global__ void __launch_bounds__(FS_NT, FS_MINB) fcg_pre_stream_kernel(
         [&](const FsRaw& w, float sx) {
             return fs_row(w, make_float2(omega * w.a.x * w.b.x, omega * w.a.y * w.b.y), sx);
         },
-        [&](int k, int i, int j, const FsRow& row, float2 tv, float, float, float, float) {
-            const float2 rr = __ldg(r + k), dd = __ldg(d + k);
+        [&](int k, int i, int j, const FsRow& row, float2 tv, float, float, float, float, const FsOwn& ow) {
+            const float2 rr = ow.r, dd = ow.d;
             z1[k] = row.v;  // own cells: no sign flip
             const float vx = (rr.x - tv.x) * dd.x, vy = (rr.y - tv.y) * dd.y;
             const size_t q = (size_t)j * Wp + i;
@@ -99,6 +105,12 @@ __global__ void __launch_bounds__(FS_NT, FS_MINB) fcg_pre_stream_kernel(
                 x[q] = vx;
                 x[plane + q] = vy;
             }
+        },
+        [&](const auto& ld, int k, bool en) {
+            FsOwn o;
+            o.r = ld.ld2(2, r + k, en);
+            o.d = ld.ld2(3, d + k, en);
+            return o;
         });
 }
 
@@ -129,12 +141,19 @@ __global__ void __launch_bounds__(FS_NT, FS_MINB) fcg_post_stream_kernel(
             const float mk = w.he >= H_DISP_MIN ? 1.f : 0.f;
             return fs_row(w, make_float2(w.a.x + mk * w.b.x, w.a.y + mk * w.b.y), sx);
         },
-        [&](int k, int, int, const FsRow& row, float2 tv, float, float, float, float) {
-            const float2 a2 = row.v, rr = __ldg(r + k), dd = __ldg(d + k);
+        [&](int k, int, int, const FsRow& row, float2 tv, float, float, float, float, const FsOwn& ow) {
+            const float2 a2 = row.v, rr = ow.r, dd = ow.d;
             const float2 zz = make_float2(a2.x + omega * (rr.x - tv.x) * dd.x, a2.y + omega * (rr.y - tv.y) * dd.y);
             z[k] = zz;
-            const float2 qq = __ldg(qv + k);
+            const float2 qq = ow.q;
             s0 += (double)zz.x * qq.x + (double)zz.y * qq.y;
+        },
+        [&](const auto& ld, int k, bool en) {
+            FsOwn o;
+            o.r = ld.ld2(2, r + k, en);
+            o.d = ld.ld2(3, d + k, en);
+            o.q = ld.ld2(4, qv + k, en);
+            return o;
         });
     fs_partials(s0, 0.0, part);
 }
@@ -162,12 +181,17 @@ __global__ void __launch_bounds__(FS_NT, FS_MINB) fcg_dir_stream_kernel(
         [&](const FsRaw& w, float sx) {
             return fs_row(w, make_float2(w.a.x + beta * w.b.x, w.a.y + beta * w.b.y), sx);
         },
-        [&](int k, int, int, const FsRow& row, float2 qq, float, float, float, float) {
-            const float2 pp = row.v, rr = __ldg(r + k);
+        [&](int k, int, int, const FsRow& row, float2 qq, float, float, float, float, const FsOwn& ow) {
+            const float2 pp = row.v, rr = ow.r;
             p_new[k] = pp;
             qv[k] = qq;
             s0 += (double)pp.x * qq.x + (double)pp.y * qq.y;
             s1 += (double)rr.x * pp.x + (double)rr.y * pp.y;
+        },
+        [&](const auto& ld, int k, bool en) {
+            FsOwn o;
+            o.r = ld.ld2(2, r + k, en);
+            return o;
         });
     fs_partials(s0, s1, part);
 }

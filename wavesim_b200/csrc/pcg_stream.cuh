@@ -109,23 +109,34 @@ __device__ __forceinline__ unsigned char* ps_ring() {
     return ps_dyn + (threadIdx.x >> 5) * ps_ring_bytes<NF2, NF1>();
 }
 
+// Loads of an own cell that only its output needs (none by default).
+struct PsNoOwn {};
+struct PsNoFetchOwn {
+    template <class Ld>
+    __device__ __forceinline__ PsNoOwn operator()(const Ld&, int, bool) const { return PsNoOwn{}; }
+};
+
 // One strip: rows j0-2 .. j0+rows+1 of the lane's column are fetched
 // (`fetch(loader, k, sy, j, own, mi, mj)`: the loads at stored index k = mj pitch + mi of padded
 // row j, sy the sign of the y-normal component there, own whether the cell is one the strip
 // updates) and turned into window rows (`make(raw)`: a Row with the signed vector v, c and heff);
-// for every own cell `out(k, i, j, row, Av, c_left, c_right, c_below, c_above)` gets the row, the
-// product and the four neighbouring c. NF2 / NF1: the ring's fields per row (at least the fetch's).
-template <class Raw, class Row, int NF2, int NF1, class Fetch, class Make, class Out>
-__device__ __forceinline__ void ps_strip(const DevGrid& g, int strip, int rows, Fetch fetch, Make make, Out out) {
+// for every own cell `out(k, i, j, row, Av, c_left, c_right, c_below, c_above, own)` gets the
+// row, the product, the four neighbouring c and what `fetch_own(loader, k, en)` loaded for the
+// cell: in ring mode those loads travel with the row two below (they are read as that row enters
+// the window, just before the cell's output), so they do not wait at the output. NF2 / NF1: the
+// ring's fields per row (at least those of fetch and fetch_own together).
+template <class Raw, class Row, int NF2, int NF1, class Fetch, class Make, class Out,
+          class FetchOwn = PsNoFetchOwn>
+__device__ __forceinline__ void ps_strip(const DevGrid& g, int strip, int rows, Fetch fetch, Make make, Out out,
+                                         FetchOwn fetch_own = FetchOwn{}) {
+    using Own = decltype(fetch_own(PsDirect{}, 0, false));
     const int strips_x = (g.nx + PS_OUT - 1) / PS_OUT;
     const int lane = threadIdx.x & 31;
     const int i = (strip % strips_x) * PS_OUT - PS_HALO + lane;
     const int j0 = (strip / strips_x) * rows;
     const int mi = reflect_idx(i, g.nx);
     const bool own_col = lane >= PS_HALO && lane < PS_HALO + PS_OUT && i < g.nx;
-    auto get = [&](const auto& ld, int j) -> Raw {
-        int mj;
-        float sy;
+    auto map_row = [&](int j, int& mj, float& sy) {
         if (g.periodic) {
             mj = wrap_idx(j, g.ny);
             sy = 1.f;
@@ -133,8 +144,16 @@ __device__ __forceinline__ void ps_strip(const DevGrid& g, int strip, int rows, 
             mj = reflect_idx(j, g.ny);
             sy = ((unsigned)j < (unsigned)g.ny) ? 1.f : -1.f;
         }
-        return fetch(ld, mj * g.pitch + mi, sy, j, own_col && j >= j0 && j < j0 + rows && j < g.ny, mi, mj);
     };
+    auto is_own = [&](int j) { return own_col && j >= j0 && j < j0 + rows && j < g.ny; };
+    auto get = [&](const auto& ld, int j) -> Raw {
+        int mj;
+        float sy;
+        map_row(j, mj, sy);
+        return fetch(ld, mj * g.pitch + mi, sy, j, is_own(j), mi, mj);
+    };
+    // the own-cell loads of row j (an interior row where they are enabled)
+    auto get_own = [&](const auto& ld, int j) -> Own { return fetch_own(ld, j * g.pitch + i, is_own(j)); };
     // f = c div v of the window's middle row
     auto fval = [&](const Row& m, const Row& c, const Row& p) -> float {
         const float vl = ps_up(c.v.x), vr = ps_dn(c.v.x);
@@ -148,18 +167,23 @@ __device__ __forceinline__ void ps_strip(const DevGrid& g, int strip, int rows, 
     auto slot_f1 = [&](int sl) {
         return reinterpret_cast<float*>(ring + PS_SLOTS * NF2 * 32 * 8) + sl * NF1 * 32 + lane;
     };
-    auto issue = [&](int j) {  // start row j's copies into the next free slot
+    auto issue = [&](int j) {  // start row j's copies (and row j-2's own-cell loads) into the next free slot
         PsIssue ld{slot_f2(slot_in), slot_f1(slot_in), j <= j_last};
         (void)get(ld, j);
+        (void)get_own(ld, j - 2);
         cp_async_commit();
         slot_in = slot_in + 1 == PS_SLOTS ? 0 : slot_in + 1;
     };
     Raw ahead[PS_DEPTH > 0 ? 1 : PS_AHEAD];
-    // row j, the oldest row in flight: wait for it, read it, and start row j + (rows in flight)
+    Own own_cur{};  // the own-cell loads of the row two above the one taken last
+    // row j, the oldest row in flight: wait for it, read it (and row j-2's own-cell loads), and
+    // start row j + (rows in flight)
     auto take = [&](int j) -> Raw {
         if constexpr (PS_DEPTH > 0) {
             cp_async_wait<PS_DEPTH - 1>();
-            const Raw raw = get(PsRead{slot_f2(slot_out), slot_f1(slot_out)}, j);
+            const PsRead ld{slot_f2(slot_out), slot_f1(slot_out)};
+            const Raw raw = get(ld, j);
+            own_cur = get_own(ld, j - 2);
             slot_out = slot_out + 1 == PS_SLOTS ? 0 : slot_out + 1;
             issue(j + PS_DEPTH);
             return raw;
@@ -168,6 +192,7 @@ __device__ __forceinline__ void ps_strip(const DevGrid& g, int strip, int rows, 
 #pragma unroll
             for (int d = 0; d < PS_AHEAD - 1; d++) ahead[d] = ahead[d + 1];
             ahead[PS_AHEAD - 1] = get(PsDirect{}, j + PS_AHEAD);
+            own_cur = get_own(PsDirect{}, j - 2);
             return raw;
         }
     };
@@ -186,7 +211,7 @@ __device__ __forceinline__ void ps_strip(const DevGrid& g, int strip, int rows, 
     for (int r = 0; r < rows; r++) {
         const int j = j0 + r;
         if (j >= g.ny) break;  // uniform over the warp
-        const Row r2 = make(take(j + 2));  // row j+2
+        const Row r2 = make(take(j + 2));  // row j+2, with row j's own-cell loads
         const float f_1 = fval(r0, r1, r2);
         const float fl = ps_up(f_0), fr = ps_dn(f_0);
         const float cl = ps_up(r0.cc), cr = ps_dn(r0.cc);
@@ -195,7 +220,7 @@ __device__ __forceinline__ void ps_strip(const DevGrid& g, int strip, int rows, 
             float2 av;
             av.x = mask * (r0.he * r0.v.x - (fr - fl) * g.ix);
             av.y = mask * (r0.he * r0.v.y - (f_1 - f_m) * g.iy);
-            out(j * g.pitch + i, i, j, r0, av, cl, cr, c_m, r1.cc);
+            out(j * g.pitch + i, i, j, r0, av, cl, cr, c_m, r1.cc, own_cur);
         }
         c_m = r0.cc;
         r0 = r1;
@@ -288,7 +313,8 @@ __device__ __forceinline__ bool pcg_solve_stream(const PcgArgs& a, int cta, int 
                     o.he = r.he;
                     return o;
                 },
-                [&](int k, int, int, const PsInitRow& row, float2 aw, float cl, float cr, float cb, float ca) {
+                [&](int k, int, int, const PsInitRow& row, float2 aw, float cl, float cr, float cb, float ca,
+                    PsNoOwn) {
                     float2 d = make_float2(1.f, 1.f);
                     if (row.he >= H_DISP_MIN) {
                         d.x = row.he + (cr + cl) * 0.25f / (g.dx * g.dx);
@@ -372,7 +398,7 @@ __device__ __forceinline__ bool pcg_solve_stream(const PcgArgs& a, int cta, int 
                         o.he = r.he;
                         return o;
                     },
-                    [&](int k, int, int, const PsCgRow& row, float2 q, float, float, float, float) {
+                    [&](int k, int, int, const PsCgRow& row, float2 q, float, float, float, float, PsNoOwn) {
                         const float2 u = row.v;  // own cells: no sign flip
                         a.qb[wb][k] = q;
                         g2 += (double)u.x * q.x + (double)u.y * q.y;
