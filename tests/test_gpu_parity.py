@@ -188,6 +188,38 @@ def test_streaming_and_tiled_shallow_water_stages_give_the_same_bits(case, monke
     assert np.array_equal(a.h, b.h) and np.array_equal(a.hu, b.hu) and np.array_equal(a.hv, b.hv)
 
 
+@pytest.mark.parametrize("iters", [3, 4])
+def test_streaming_solve_adds_the_pending_step_of_w(iters, monkeypatch):
+    """The streaming Jacobi solve adds the iterations' steps to w in pairs (every second sweep adds
+    its own and the previous sweep's), and after an odd number of iterations the stage epilogue
+    adds the one still pending. With every solve stopped after 3 or 4 iterations, the streaming and
+    the tiled solve (which adds each step at once) agree to rounding: a step left out would leave
+    w short by a whole CG step."""
+    import dataclasses
+    base = W.sgn_beach(200, 90, 2.0, seed=5, name="periodic")
+    w = dataclasses.replace(base, dispersion=Dispersion(tolerance=1e-14, max_iterations=iters))
+    s0 = W.wave_train_state(w)
+    monkeypatch.setenv("WAVECORE_B200_SOLVE", "tiled")
+    tiled = w.solver(Solver)
+    monkeypatch.delenv("WAVECORE_B200_SOLVE")
+    stream = w.solver(Solver)
+    outs = []
+    for sol in (tiled, stream):
+        sol.upload(s0)
+        sol.step_n(4)
+        sol.synchronize()
+        s = s0.clone()
+        sol.download(s)
+        outs.append((s, sol.dispersion_stats()))
+    (a, sa), (b, sb) = outs
+    g = w.grid
+    assert sa.solves == sb.solves == 8
+    assert sa.unconverged == sb.unconverged == 8 and sa.iterations == sb.iterations == 8 * iters
+    assert np.max(np.abs(g.inner(a.h) - g.inner(b.h))) < 1e-6
+    assert np.max(np.abs(g.inner(a.hu) - g.inner(b.hu))) < 1e-5
+    assert np.max(np.abs(g.inner(a.hv) - g.inner(b.hv))) < 1e-5
+
+
 def test_streaming_and_tiled_jacobi_solves_agree(monkeypatch):
     """The Jacobi solve runs with register-streaming sweeps by default; the tiled sweeps
     (WAVECORE_B200_SOLVE=tiled) do the same arithmetic per cell but add the dot products' partial
