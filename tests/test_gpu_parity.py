@@ -188,6 +188,42 @@ def test_streaming_and_tiled_shallow_water_stages_give_the_same_bits(case, monke
     assert np.array_equal(a.h, b.h) and np.array_equal(a.hu, b.hu) and np.array_equal(a.hv, b.hv)
 
 
+@pytest.mark.parametrize("case", ["sgn_periodic_ragged", "sgn_walls_ragged", "fifth_order_walls"])
+def test_tma_staged_and_gathered_stage_boxes_give_the_same_bits(case, monkeypatch):
+    """Fifth-order and dispersive stages stage every interior tile's box (the tile and its 4-cell
+    halo of state and bed) by TMA box loads; tiles at the grid's edges, whose boxes hold ghost
+    cells, gather with the boundary rule as before. WAVECORE_B200_STAGE_TMA=0 gathers every box.
+    On a periodic and a walled dispersive beach whose sides are not whole tiles (300 x 90, 20 steps
+    with the PCG solve) and on a walled fifth-order shallow-water beach (60 steps), both give the
+    same bits."""
+    import dataclasses
+    if case == "sgn_periodic_ragged":
+        w = W.sgn_beach(300, 90, 2.0, seed=5, name="periodic")
+        steps = 20
+    elif case == "sgn_walls_ragged":
+        w = W.sgn_beach(300, 90, 2.0, seed=6, name="walls", periodic=False)
+        steps = 20
+    else:
+        w = dataclasses.replace(W.swe_beach(300, 77, 2.0, seed=3), order=Order.Fifth)
+        steps = 60
+    s0 = W.wave_train_state(w)
+    monkeypatch.setenv("WAVECORE_B200_STAGE_TMA", "0")
+    gathered = w.solver(Solver)
+    monkeypatch.delenv("WAVECORE_B200_STAGE_TMA")
+    boxed = w.solver(Solver)
+    outs = []
+    for sol in (gathered, boxed):
+        sol.upload(s0)
+        sol.step_n(steps)
+        sol.synchronize()
+        s = s0.clone()
+        sol.download(s)
+        outs.append(s)
+    a, b = outs
+    assert a.time == b.time
+    assert np.array_equal(a.h, b.h) and np.array_equal(a.hu, b.hu) and np.array_equal(a.hv, b.hv)
+
+
 @pytest.mark.parametrize("iters", [3, 4])
 def test_streaming_solve_adds_the_pending_step_of_w(iters, monkeypatch):
     """The streaming Jacobi solve adds the iterations' steps to w in pairs (every second sweep adds

@@ -26,6 +26,7 @@ constexpr int MAX_SPONGES = 8;
 // Error bits in Ctl::error.
 constexpr int ERR_TIMEOUT = 1;
 constexpr int ERR_NAN = 2;
+constexpr int ERR_TMA = 8;  // a stage kernel's TMA box did not arrive within its wait limit
 
 struct DevGrid {
     int nx, ny, pitch, periodic;

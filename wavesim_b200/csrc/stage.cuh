@@ -2,7 +2,8 @@
 //
 // One CTA advances a TX x TY tile of interior cells through one stage of SSP-RK2:
 //   P1  the tile plus a 4-cell halo of (h, hu, hv, b) is staged in shared memory, ghost cells
-//       synthesised by the boundary rule as they are loaded;
+//       synthesised by the boundary rule as they are loaded; in stage_tma_kernel a tile whose
+//       box holds no ghost cell is brought in by two TMA box loads (state and bed) instead;
 //   P2  the breaking switch phi (dispersion.rs:113-160) on the tile plus 3 cells;
 //   P2b (dispersive runs) masked velocities, their divergence, c = phi h^3/3 and c N
 //       (dispersion.rs:380-438) on the tile plus 1-2 cells;
@@ -24,6 +25,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "tma.cuh"
 
 namespace wcb {
 
@@ -228,13 +230,32 @@ __device__ __forceinline__ void hll_face(const Side& l, const Side& r, float& F0
 // Shared scalars of one tile's work.
 struct StageShared {
     float maker[2];
+    unsigned long long bar;  // the TMA box loads' mbarrier
 };
+
+// The TMA boxes of a tile with a 4-cell halo: the state (4 floats per cell) and the bed, both
+// BX x BY cells, landed in the reconstruction arrays' space (unused until P3).
+template <typename Gm>
+struct StageTma {
+    static constexpr int OFF_RQ = Gm::OFF_SX;              // float4 per box cell
+    static constexpr int OFF_RB = Gm::OFF_SX + 4 * Gm::NB; // float per box cell
+    static constexpr unsigned BYTES = 5u * 4u * Gm::NB;
+    static_assert(5 * Gm::NB <= 8 * Gm::SX_N + 8 * Gm::SY_N, "the boxes must fit before OFF_P");
+    static_assert((OFF_RQ * 4) % 128 == 0 && (OFF_RB * 4) % 128 == 0, "TMA destinations are 128-byte aligned");
+    static_assert(Gm::HALO % 4 == 0, "a box starts at a column that is a multiple of 4 (16 bytes of bed)");
+};
+constexpr unsigned long long ST_TMA_WAIT_NS = 100000000ull;  // 0.1 s: a 13 KB box takes microseconds
 
 // One RK stage on the TX x TY tile at (i0, j0), by a block of NT threads, in the dynamic shared
 // memory `sm`. Finishing shallow-water stages fold the tile's CFL rate into rmax / nan_here.
-template <int MODE, int ORDER, bool SGN, int TY, int NT>
+// With TMA (one tile per CTA, 4-cell halo, `sm` 128-byte aligned), a tile whose box lies inside
+// the grid is staged by the copy engine from the tensor maps tq (the state as 4 floats per cell)
+// and tb (the bed); other tiles gather as without.
+template <int MODE, int ORDER, bool SGN, int TY, int NT, bool TMA = false>
 __device__ __forceinline__ void stage_tile(const StageArgs& a, int i0, int j0, float* sm,
-                                           StageShared& ss, float& rmax, int& nan_here) {
+                                           StageShared& ss, float& rmax, int& nan_here,
+                                           const CUtensorMap* tq = nullptr,
+                                           const CUtensorMap* tb = nullptr) {
     using Gm = StageGeom<TY, stage_halo<ORDER, SGN>()>;
     constexpr int ST_BX = Gm::BX, ST_BY = Gm::BY, ST_NB = Gm::NB, ST_HALO = Gm::HALO;
     constexpr int SX_W = Gm::SX_W, SX_N = Gm::SX_N, SY_N = Gm::SY_N, FX_W = Gm::FX_W;
@@ -253,8 +274,23 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int i0, int j0, f
     const float dt_f = (float)dt;
     const float dtdx = (float)(dt / g.dxd), dtdy = (float)(dt / g.dyd);
 
+    bool boxed = false;  // this tile's box comes by TMA
+    if constexpr (TMA) {
+        boxed = i0 >= ST_HALO && i0 + ST_TX + ST_HALO <= g.nx && j0 >= ST_HALO &&
+                j0 + ST_TY_ + ST_HALO <= g.ny && (smem_addr(sm) & 127u) == 0;
+        if (boxed && tid == 0) mbar_init(&ss.bar, 1);
+    }
     __syncthreads();  // the previous tile's shared memory is free
     if (tid == 0) {
+        if constexpr (TMA) {
+            if (boxed) {
+                using Tm = StageTma<Gm>;
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                mbar_expect_tx(&ss.bar, Tm::BYTES);
+                tma_load_2d(sm + Tm::OFF_RQ, tq, 4 * (i0 - ST_HALO), j0 - ST_HALO, &ss.bar);
+                tma_load_2d(sm + Tm::OFF_RB, tb, i0 - ST_HALO, j0 - ST_HALO, &ss.bar);
+            }
+        }
         if (a.maker.on) {
             // forcing.rs:124-138 split as profile(x) * ramp(t) * (sin wt cos k_y y - cos wt sin k_y y)
             const double t = ctl->t + (a.stage_time_plus_dt ? dt : 0.0);
@@ -267,7 +303,28 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int i0, int j0, f
     }
 
     // ---- P1: the box with ghost cells synthesised ------------------------------------------
-    for (int p = tid; p < ST_NB; p += NT) {
+    if constexpr (TMA) {
+        if (boxed) {
+            using Tm = StageTma<Gm>;
+            if (!mbar_wait_bounded(&ss.bar, 0, ST_TMA_WAIT_NS)) {
+                atomicOr(&a.ctl->error, ERR_TMA);
+                mbar_wait_bounded(&ss.bar, 0, ST_TMA_WAIT_NS);  // let a late copy land first
+            }
+            const float4* rq = reinterpret_cast<const float4*>(sm + Tm::OFF_RQ);
+            const float* rb = sm + Tm::OFF_RB;
+            for (int p = tid; p < ST_NB; p += NT) {
+                const float4 q = rq[p];
+                const float b = rb[p];
+                const float h = q.x;
+                sm[OFF_H + p] = h;
+                sm[OFF_B + p] = b;
+                sm[OFF_ETA + p] = h + b;
+                sm[OFF_U + p] = velocity(h, q.z);
+                sm[OFF_V + p] = velocity(h, q.w);
+            }
+        }
+    }
+    for (int p = tid; p < ST_NB && !boxed; p += NT) {
         const int bx = p % ST_BX, by = p / ST_BX;
         const Mapped m = map_cell(g, i0 - ST_HALO + bx, j0 - ST_HALO + by);
         const float4 q = __ldg(a.qin + m.k);
@@ -521,6 +578,24 @@ __global__ void __launch_bounds__(ST_NT) stage_kernel(StageArgs a) {
     float rmax = 0.f;
     int nan_here = 0;
     stage_tile<MODE, ORDER, SGN, ST_TY, ST_NT>(a, blockIdx.x * ST_TX, blockIdx.y * ST_TY, sm, ss, rmax, nan_here);
+    if (!SGN && MODE != MODE_STAGE1) stage_fold<ST_NT>(a.ctl, rmax, nan_here, gridDim.x * gridDim.y);
+}
+
+// The same stage with every interior tile's box staged by TMA (4-cell-halo variants: fifth order
+// or dispersive). tq maps the state as {4 * nx, ny} floats with a row stride of 16 * pitch bytes
+// and a {4 * BX, BY} box; tb maps the bed as {nx, ny} floats, stride 4 * pitch, box {BX, BY}.
+template <int MODE, int ORDER, bool SGN>
+__global__ void __launch_bounds__(ST_NT) stage_tma_kernel(StageArgs a, const __grid_constant__ CUtensorMap tq,
+                                                         const __grid_constant__ CUtensorMap tb) {
+    static_assert(stage_halo<ORDER, SGN>() == ST_HALO, "TMA staging serves the 4-cell halo");
+    extern __shared__ __align__(128) float4 smem_tma[];
+    float* sm = reinterpret_cast<float*>(smem_tma);
+    __shared__ StageShared ss;
+    if (!a.ctl->active) return;
+    float rmax = 0.f;
+    int nan_here = 0;
+    stage_tile<MODE, ORDER, SGN, ST_TY, ST_NT, true>(a, blockIdx.x * ST_TX, blockIdx.y * ST_TY, sm, ss, rmax,
+                                                     nan_here, &tq, &tb);
     if (!SGN && MODE != MODE_STAGE1) stage_fold<ST_NT>(a.ctl, rmax, nan_here, gridDim.x * gridDim.y);
 }
 

@@ -5,6 +5,8 @@
 // `step` runs the whole update on the CPU; here `wc_step` moves the caller's FP64 arrays to the
 // device, runs the step there and moves them back, and the device-resident entry points keep
 // the state in HBM across steps with the clock and the adaptive time step on the device.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -168,6 +170,7 @@ struct wc_solver {
     // or, with WAVECORE_B200_STAGE=tiled in the environment at creation, the shared-memory tiled
     // kernel (stage.cuh) that dispersive and fifth-order stages use; both give the same bits.
     bool swe_streaming = true;
+    bool stage_tma = true;  // 4-cell-halo stages stage interior tiles by TMA
     double *mem = nullptr, *mem_new = nullptr;
     float* nu = nullptr;
     float2 *mb0 = nullptr, *mb1 = nullptr;
@@ -267,6 +270,11 @@ wc_status configure_kernels() {
     ATTR((stage_kernel<MODE_STAGE1, 0, true>), SMEM_SGN);
     ATTR((stage_kernel<MODE_STAGE1, 1, true>), SMEM_SGN);
     ATTR((stage_kernel<MODE_STAGE1, 2, true>), SMEM_SGN);
+    ATTR((stage_tma_kernel<MODE_STAGE1, 2, false>), SMEM_SWE);
+    ATTR((stage_tma_kernel<MODE_STAGE2, 2, false>), SMEM_SWE);
+    ATTR((stage_tma_kernel<MODE_STAGE1, 0, true>), SMEM_SGN);
+    ATTR((stage_tma_kernel<MODE_STAGE1, 1, true>), SMEM_SGN);
+    ATTR((stage_tma_kernel<MODE_STAGE1, 2, true>), SMEM_SGN);
     ATTR((ensemble_step_kernel<8, 1>), StageGeom<8>::SMEM_SGN);
     ATTR((ensemble_step_kernel<8, 2>), StageGeom<8>::SMEM_SGN);
     ATTR((ensemble_step_kernel<16, 1>), StageGeom<16>::SMEM_SGN);
@@ -302,6 +310,39 @@ StageArgs stage_args(const wc_solver* s, const float4* qin, const float4* qold, 
     return a;
 }
 
+// The tensor maps of a 4-cell-halo stage's TMA boxes over the state `qin` (4 floats per cell,
+// {4 nx, ny}, rows 16 pitch bytes apart) and the bed ({nx, ny}, rows 4 pitch bytes apart), with
+// the boxes of StageGeom<ST_TY>. False if the driver's encoder is unavailable or refuses.
+bool stage_tensor_maps(const wc_solver* s, const float4* qin, CUtensorMap& tq, CUtensorMap& tb) {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    static bool looked = false;
+    if (!looked) {
+        looked = true;
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    if (!encode) return false;
+    using Gm = StageGeom<ST_TY>;
+    const DevGrid& g = s->g;
+    const cuuint32_t one[2] = {1, 1};
+    const cuuint64_t dq[2] = {4ull * (cuuint64_t)g.nx, (cuuint64_t)g.ny};
+    const cuuint64_t sq[1] = {16ull * (cuuint64_t)g.pitch};
+    const cuuint32_t bq[2] = {4u * Gm::BX, (cuuint32_t)Gm::BY};
+    if (encode(&tq, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float4*>(qin), dq, sq, bq, one,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return false;
+    const cuuint64_t db[2] = {(cuuint64_t)g.nx, (cuuint64_t)g.ny};
+    const cuuint64_t sb[1] = {4ull * (cuuint64_t)g.pitch};
+    const cuuint32_t bb[2] = {(cuuint32_t)Gm::BX, (cuuint32_t)Gm::BY};
+    return encode(&tb, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(s->bed), db, sb, bb, one,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 wc_status launch_stage(wc_solver* s, int mode, const float4* qin, const float4* qold, float4* qout,
                        bool plus_dt) {
     const StageArgs a = stage_args(s, qin, qold, qout, plus_dt);
@@ -316,6 +357,24 @@ wc_status launch_stage(wc_solver* s, int mode, const float4* qin, const float4* 
         if (mode == MODE_FIRST) swe_stream_kernel<MODE_FIRST, 0, SW_CPL><<<sgrid, SW_NT, sw_smem<SW_CPL>(), st>>>(a, strips_x);
         else if (mode == MODE_STAGE1) swe_stream_kernel<MODE_STAGE1, 1, SW_CPL><<<sgrid, SW_NT, sw_smem<SW_CPL>(), st>>>(a, strips_x);
         else swe_stream_kernel<MODE_STAGE2, 1, SW_CPL><<<sgrid, SW_NT, sw_smem<SW_CPL>(), st>>>(a, strips_x);
+        s->launches++;
+        CK(cudaGetLastError());
+        return WC_OK;
+    }
+    // Fifth-order and dispersive stages (4-cell halo) on grids with interior tiles: TMA boxes.
+    const bool halo4 = s->sgn || (o == 2 && mode != MODE_FIRST);
+    CUtensorMap tq, tb;
+    if (halo4 && s->stage_tma && s->g.nx >= ST_TX + 2 * ST_HALO && s->g.ny >= ST_TY + 2 * ST_HALO &&
+        stage_tensor_maps(s, qin, tq, tb)) {
+        if (s->sgn) {
+            if (o == 0) stage_tma_kernel<MODE_STAGE1, 0, true><<<grid, block, SMEM_SGN, st>>>(a, tq, tb);
+            else if (o == 1) stage_tma_kernel<MODE_STAGE1, 1, true><<<grid, block, SMEM_SGN, st>>>(a, tq, tb);
+            else stage_tma_kernel<MODE_STAGE1, 2, true><<<grid, block, SMEM_SGN, st>>>(a, tq, tb);
+        } else if (mode == MODE_STAGE1) {
+            stage_tma_kernel<MODE_STAGE1, 2, false><<<grid, block, SMEM_SWE, st>>>(a, tq, tb);
+        } else {
+            stage_tma_kernel<MODE_STAGE2, 2, false><<<grid, block, SMEM_SWE, st>>>(a, tq, tb);
+        }
         s->launches++;
         CK(cudaGetLastError());
         return WC_OK;
@@ -702,6 +761,8 @@ wc_status status_of(wc_solver* s) {
     TRY(read_ctl(s));
     if (s->ctl_host->error & ERR_TIMEOUT)
         return set_err(WC_ETIMEOUT, "a grid barrier of the dispersive solve timed out");
+    if (s->ctl_host->error & ERR_TMA)
+        return set_err(WC_ECUDA, "a stage kernel's TMA box load did not complete within its wait limit");
     if (s->ctl_host->error & ERR_NAN) return set_err(WC_ENAN, "the state holds a NaN");
     if (s->ctl_host->error & ERR_EDDY)
         return set_err(WC_EUNSUPPORTED, "the eddy viscosity needed more than 65536 sub-steps; it was not applied");
@@ -814,6 +875,8 @@ wc_status wc_solver_create(const wc_grid* grid, const double* bed_padded, const 
     {
         const char* v = std::getenv("WAVECORE_B200_STAGE");
         s->swe_streaming = !(v && std::strcmp(v, "tiled") == 0);
+        const char* t = std::getenv("WAVECORE_B200_STAGE_TMA");
+        s->stage_tma = !(t && std::strcmp(t, "0") == 0);
     }
     const int nx = (int)grid->nx, ny = (int)grid->ny;
     s->W = nx + 6;
