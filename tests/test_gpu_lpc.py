@@ -76,10 +76,13 @@ def test_forward_uses_bf16_rounded_weights():
     assert np.array_equal(net.get_params(), p)  # the master weights stay FP32
 
 
-def test_tensor_core_inference_matches_the_oracle_to_bf16():
+@pytest.mark.parametrize("channels", [(8, 16, 32, 32), (32, 32, 32, 32)])
+def test_tensor_core_inference_matches_the_oracle_to_bf16(channels):
     # The solver's network: BF16 activations on the tensor cores, FP32 accumulation. Against the
-    # FP64 oracle with the same (BF16-rounded) weights: a few BF16 roundings per layer.
-    spec = UNetSpec()
+    # FP64 oracle with the same (BF16-rounded) weights: a few BF16 roundings per layer. Both the
+    # default widths and 32 channels at every level (the kernels of a wider first level: 2 -> 32
+    # and 32 -> 32 layers, a 64-channel decoder input at full resolution, a separate output layer).
+    spec = UNetSpec(channels=channels)
     net = LearnedPreconditioner(spec)
     p = random_params(spec, 11)
     net.set_params(p)
