@@ -556,7 +556,8 @@ def run_b200(args, world, rank, local):
 
         spec = UNetSpec(channels=tuple(int(c) for c in args.lpc_channels.split(",")), stride=args.lpc_stride)
         if args.train_steps > 0:
-            net, train_rec = trained_network(dx=w.grid.dx, steps=args.train_steps, seed=0, spec=spec)
+            family = args.harvest or ("reef" if args.workload == "config5" else "beach")
+            net, train_rec = trained_network(dx=w.grid.dx, steps=args.train_steps, seed=0, spec=spec, family=family)
         else:  # an untrained network (profiling runs: same kernels, no harvest or training launches)
             from wavesim_b200 import LearnedPreconditioner
 
@@ -691,6 +692,8 @@ def main():
     ap.add_argument("--train-steps", type=int, default=20000)
     ap.add_argument("--lpc-stride", type=int, default=1, choices=[1, 2, 4])
     ap.add_argument("--lpc-channels", default="8,16,32,32")
+    ap.add_argument("--harvest", default=None, choices=["beach", "reef"],
+                    help="workload family the training systems are harvested from (default: the workload's own)")
     ap.add_argument("--eta-steps", type=int, default=10)
     ap.add_argument("--cpu-steps", type=int, default=40)
     ap.add_argument("--no-cpu-baseline", action="store_true")

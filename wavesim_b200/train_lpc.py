@@ -1,6 +1,7 @@
 """Training of the learned preconditioner on the GPU, on SGN systems the solver itself generates.
 
-Runs of the seeded beach workload draw a swell height H ~ U(0.5, 4) m, a period T ~ U(8, 18) s
+Runs of a seeded workload family (the beach of the 2 m configurations, or config 5's reef) draw a
+swell height H ~ U(0.5, 4) m, a period T ~ U(8, 18) s
 and an angle ~ U(-20, 20) degrees (and their own random bed); the harvest runs have walls at
 their y ends, so the maker takes the drawn angle exactly (a periodic width would snap it to the
 nearest angle that fits, which on a 512 m harvest grid leaves most draws at 0 degrees or outside
@@ -25,11 +26,22 @@ from .lpc import UNetSpec
 from .solver import LearnedPreconditioner, Solver
 
 
-def harvest_runs(net: LearnedPreconditioner, runs: int = 8, nx: int = 512, ny: int = 256, dx: float = 2.0,
-                 steps: int = 120, every: int = 20, seed: int = 0, validation: list | None = None) -> dict:
-    """`runs` solver runs of `steps` steps each, harvested every `every` steps. With `validation`
-    (a list), each run's last system is also appended to it whole, with its right-hand side and
-    converged solution: (c, heff, bed, bx, by, wx, wy) as (ny, nx) FP32 arrays."""
+# Harvest grids per workload family: the beach of the 2 m configurations, and config 5's reef
+# (wide enough at 1 m for its 20 m shelf, the shoal and the beach: 1024 m x 256 m).
+HARVEST_GRIDS = {"beach": (512, 256), "reef": (1024, 256)}
+
+
+def harvest_runs(net: LearnedPreconditioner, runs: int = 8, nx: int = 0, ny: int = 0, dx: float = 2.0,
+                 steps: int = 120, every: int = 20, seed: int = 0, validation: list | None = None,
+                 family: str = "beach") -> dict:
+    """`runs` solver runs of `steps` steps each, harvested every `every` steps, on seeded beds of
+    `family` ("beach": `workloads.sgn_beach`; "reef": `workloads.sgn_reef`, config 5's bed) at the
+    family's harvest grid unless nx, ny are given. With `validation` (a list), each run's last
+    system is also appended to it whole, with its right-hand side and converged solution:
+    (c, heff, bed, bx, by, wx, wy) as (ny, nx) FP32 arrays."""
+    if family not in HARVEST_GRIDS:
+        raise ValueError(f"unknown harvest family {family!r}")
+    nx, ny = (nx, ny) if nx and ny else HARVEST_GRIDS[family]
     rng = np.random.default_rng(seed)
     draws = []
     t0 = time.perf_counter()
@@ -37,8 +49,12 @@ def harvest_runs(net: LearnedPreconditioner, runs: int = 8, nx: int = 512, ny: i
         height = float(rng.uniform(0.5, 4.0))
         period = float(rng.uniform(8.0, 18.0))
         angle = float(rng.uniform(-20.0, 20.0))
-        w = W.sgn_beach(nx, ny, dx, seed=int(rng.integers(1 << 30)), height=height, period=period, angle_deg=angle,
-                        name=f"harvest_{r}", periodic=False)
+        if family == "reef":
+            w = W.sgn_reef(nx, ny, dx, seed=int(rng.integers(1 << 30)), height=height, period=period,
+                           angle_deg=angle, name=f"harvest_{r}")
+        else:
+            w = W.sgn_beach(nx, ny, dx, seed=int(rng.integers(1 << 30)), height=height, period=period,
+                            angle_deg=angle, name=f"harvest_{r}", periodic=False)
         sol = w.solver(Solver)
         sol.upload(W.wave_train_state(w))
         for _ in range(steps // every):
@@ -50,7 +66,7 @@ def harvest_runs(net: LearnedPreconditioner, runs: int = 8, nx: int = 512, ny: i
             sysd["bed"] = w.grid.inner(w.bed.b).copy()
             validation.append({k: np.asarray(v, dtype=np.float32) for k, v in sysd.items()})
         draws.append({"H_m": round(height, 3), "T_s": round(period, 3), "angle_deg": round(w.meta["angle_deg"], 3)})
-    return {"runs": runs, "grid": f"{nx}x{ny} at {dx:g} m", "systems": net.n_systems, "draws": draws,
+    return {"runs": runs, "family": family, "grid": f"{nx}x{ny} at {dx:g} m", "systems": net.n_systems, "draws": draws,
             "seconds": time.perf_counter() - t0}
 
 
@@ -92,15 +108,17 @@ def validation_loss(net: LearnedPreconditioner, systems: list, dx: float, patch:
     return float(loss)
 
 
-def trained_network(dx: float = 2.0, steps: int = 20000, seed: int = 0, spec: UNetSpec | None = None):
-    """A network harvested and trained from scratch on this GPU; returns (network, record). The
+def trained_network(dx: float = 2.0, steps: int = 20000, seed: int = 0, spec: UNetSpec | None = None,
+                    family: str = "beach"):
+    """A network harvested (from runs of `family`) and trained from scratch on this GPU; returns
+    (network, record). The
     record holds the validation loss on the harvest runs' whole systems (their right-hand sides and
     converged solutions) for the trained network and for the same cycle without a network (an
     untrained network's output layer is zero: the two Jacobi sweeps alone)."""
     spec = spec or UNetSpec()
     net = LearnedPreconditioner(spec, seed=seed)
     val = []
-    h = harvest_runs(net, dx=dx, seed=seed, validation=val)
+    h = harvest_runs(net, dx=dx, seed=seed, validation=val, family=family)
     t = train(net, steps=steps, seed=seed)
     v = {"systems": len(val), "patches": 8 * len(val), "error_field": "the converged solution of the system",
          "loss_trained": validation_loss(net, val, dx),
@@ -114,8 +132,9 @@ def main():
     ap.add_argument("--steps", type=int, default=20000)
     ap.add_argument("--dx", type=float, default=2.0)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--family", default="beach", choices=sorted(HARVEST_GRIDS))
     a = ap.parse_args()
-    net, rec = trained_network(a.dx, a.steps, a.seed)
+    net, rec = trained_network(a.dx, a.steps, a.seed, family=a.family)
     net.save(a.out)
     print(rec)
 

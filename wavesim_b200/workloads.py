@@ -182,6 +182,19 @@ def swe_large(seed: int = 7) -> Workload:
     return swe_beach(4096, 4096, 2.0, seed, name="swe_beach_4096x4096_dx2")
 
 
+def reef_bed(grid: Grid, seed: int, shore_x: float, shoal_x: float, shoal_y: float, shoal_radius: float = 150.0,
+             sigma: float = 1.0, corr: float = 10.0) -> np.ndarray:
+    """(ny, nx) reef-like bed: a 20 m shelf and a 1:30 beach with its still-water shoreline at
+    shore_x, a Gaussian shoal centred at (shoal_x, shoal_y) whose crest is 1 m deep (the beach is
+    kept where it is shallower), plus a ridged random field (sigma, correlation length)."""
+    X, Y = grid.centres()
+    base = shelf_and_beach(grid, 20.0, 1.0 / 30.0, shore_x)
+    base_at_shoal = float(np.maximum(-20.0, (shoal_x - shore_x) / 30.0))
+    shoal = (-1.0 - base_at_shoal) * np.exp(-((X - shoal_x) ** 2 + (Y - shoal_y) ** 2) / (shoal_radius**2))
+    return np.maximum(base + shoal, np.minimum(base, -1.0)) + ridged_field(grid.nx, grid.ny, grid.dx, grid.dy,
+                                                                          sigma, corr, seed)
+
+
 def config5(seed: int = 2026, preconditioner: int = 0) -> Workload:
     """4096 x 4096 at 1 m: a 1:30 plane beach behind a 20 m shelf plus a ridged random field
     (sigma 1 m, correlation 10 m) and a Gaussian shoal (radius 150 m) whose crest is 1 m deep;
@@ -191,12 +204,7 @@ def config5(seed: int = 2026, preconditioner: int = 0) -> Workload:
     dx = 1.0
     grid = Grid(nx, ny, dx, dx)
     lx, ly = nx * dx, ny * dx
-    X, Y = grid.centres()
-    base = shelf_and_beach(grid, 20.0, 1.0 / 30.0, 0.85 * lx)
-    shoal_x = 0.5 * lx
-    base_at_shoal = float(np.maximum(-20.0, (shoal_x - 0.85 * lx) / 30.0))
-    shoal = (-1.0 - base_at_shoal) * np.exp(-((X - shoal_x) ** 2 + (Y - 0.5 * ly) ** 2) / (150.0**2))
-    b = np.maximum(base + shoal, np.minimum(base, -1.0)) + ridged_field(nx, ny, dx, dx, 1.0, 10.0, seed)
+    b = reef_bed(grid, seed, 0.85 * lx, 0.5 * lx, 0.5 * ly)
     bed = Bathymetry.from_interior(grid, b)
     maker_x = 160.0
     i_m = int(round(maker_x / dx - 0.5))
@@ -209,6 +217,29 @@ def config5(seed: int = 2026, preconditioner: int = 0) -> Workload:
         periodic_y=True, sponges=[Sponge(100, 1.5).edges(True, False, False, False)], maker=maker,
         dispersion=Dispersion(tolerance=1e-8, max_iterations=1000, preconditioner=preconditioner), steps=10000,
         meta={"seed": seed, "maker_depth_m": depth, "angle_deg": math.degrees(angle), "alongshore_turns": turns,
+              "bed": "20 m shelf + 1:30 beach + ridged field sigma 1 m / 10 m + shoal to 1 m depth"},
+    )
+
+
+def sgn_reef(nx: int, ny: int, dx: float, seed: int, height: float = 3.0, period: float = 16.0,
+             angle_deg: float = 10.0, name: str | None = None, steps: int = 1000) -> Workload:
+    """A smaller run of config 5's family between walls: the reef bed (20 m shelf, 1:30 beach with
+    its shoreline at 0.85 Lx, a shoal to 1 m depth at mid-width, a ridged field sigma 1 m /
+    10 m), fifth order + SGN to 1e-8, a maker of height H and period T at x = 160 m taking
+    `angle_deg` itself, a 100 m offshore sponge, Manning 0.02, CFL 0.4."""
+    grid = Grid(nx, ny, dx, dx)
+    lx, ly = nx * dx, ny * dx
+    b = reef_bed(grid, seed, 0.85 * lx, 0.5 * lx, 0.5 * ly)
+    bed = Bathymetry.from_interior(grid, b)
+    maker_x = min(160.0, 0.15 * lx)
+    i_m = min(max(int(round(maker_x / dx - 0.5)), 0), nx - 1)
+    maker = WaveMaker(x=maker_x, amplitude=height / 2.0, period=period, angle=math.radians(angle_deg),
+                      sigma=2.0 * dx, ramp_periods=4.0)
+    return Workload(
+        name=name or f"sgn_reef_{nx}x{ny}_dx{dx:g}", grid=grid, bed=bed, order=Order.Fifth, cfl=0.4, manning=0.02,
+        periodic_y=False, sponges=[Sponge(int(round(100.0 / dx)), 1.5).edges(True, False, False, False)],
+        maker=maker, dispersion=Dispersion(tolerance=1e-8, max_iterations=1000), steps=steps,
+        meta={"seed": seed, "maker_depth_m": -b[ny // 2, i_m], "angle_deg": angle_deg,
               "bed": "20 m shelf + 1:30 beach + ridged field sigma 1 m / 10 m + shoal to 1 m depth"},
     )
 
