@@ -354,7 +354,9 @@ wc_status wc_lpc_forward_backward(wc_lpc* l, int32_t n, int32_t h, int32_t w, co
 /* The network's output (inference: no training state kept) on host arrays x and feat,
  * [n][2][h][w] (h, w multiples of 8). tensor = 1: BF16 activations on the tensor cores, as the
  * solver applies it; 2: the same with the first level's layers run one launch per layer instead
- * of its fused launches (a check that both give the same bits); 0: FP32 FMA, as training does. */
+ * of its fused launches; 3: the same with every layer on tiles of its usual height (no 16 x 8
+ * tiles for the coarse levels' 32-channel layers); 2 and 3 check that each variant gives the same
+ * bits; 0: FP32 FMA, as training does. */
 wc_status wc_lpc_forward(wc_lpc* l, int32_t n, int32_t h, int32_t w, const float* x,
                          const float* feat, int32_t tensor, float* y);
 /* The training objective on given patches, for checking its gradient: c, heff and bed are

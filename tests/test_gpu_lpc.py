@@ -110,6 +110,22 @@ def test_fused_first_level_launches_give_the_bits_of_the_per_layer_launches():
     assert np.array_equal(fused, per_layer)
 
 
+@pytest.mark.parametrize("h,w", [(40, 56), (136, 264)])
+def test_coarse_layers_on_16x8_tiles_give_the_bits_of_the_usual_tiles(h, w):
+    # The 32-channel layers of maps too small to give every SM two blocks of 16 x 16 pixels (the
+    # coarse levels) run on 16 x 8 tiles; each pixel's accumulation is the same sequence of MMAs,
+    # so the output must be the same bits as with the usual tiles. Sides that are not whole tiles
+    # at any level exercise the partial tiles and their zero-filled halos.
+    spec = UNetSpec()
+    net = LearnedPreconditioner(spec)
+    net.set_params(random_params(spec, 19))
+    x, feat, _ = batch(20, n=1, h=h, w=w)
+    small = net.forward(x, feat, tensor=True)
+    usual = net.forward(x, feat, tensor=True, small_tiles=False)
+    assert np.abs(small).max() > 0
+    assert np.array_equal(small, usual)
+
+
 def test_training_loss_and_gradient_match_the_fp64_oracle():
     # The whole training objective (the cycle on patches, the energy-norm loss) and its gradient
     # through the cycle and the network, against the FP64 oracle (FP32 weights on both sides).

@@ -356,9 +356,9 @@ __host__ __device__ constexpr int conv_up_rows(int ntl) { return ntl <= 2 ? 4 : 
 
 // Shared memory of the channels-innermost convolution (bytes): the input box, the weights and,
 // for a gated layer, the gate tile ([pixel][co]).
-__host__ __device__ inline size_t conv_h_smem2(int ci, int co, int kk, bool gated) {
+__host__ __device__ inline size_t conv_h_smem2(int ci, int co, int kk, bool gated, int rw = 0) {
     const int r = kk == 9 ? 1 : 0, cp = conv_mma_cp(ci), ntl = (co + 7) / 8;
-    const int th = 8 * conv_h_rows(ntl);
+    const int th = 8 * (rw ? rw : conv_h_rows(ntl));
     const size_t box = (size_t)(th + 2 * r) * (CM_TX + 2 * r) * conv_h_ps(cp);
     return (box + (size_t)ntl * 8 * (kk * cp + 8) + (gated ? (size_t)th * CM_TX * ntl * 8 : 0)) * 2;
 }
@@ -451,13 +451,14 @@ __device__ __forceinline__ void conv_h_epilogue(const ConvH& p, float (&acc)[RW]
 
 // KK taps (9 or 1), NTL tiles of 8 output channels, CP input channels padded to 16: all index
 // arithmetic is compile-time and 32-bit (a map of up to 2^31 values). A block computes a tile of
-// 16 x (8 RW) pixels, each warp RW rows of 16; its halo box is staged with cp.async (pooled
-// inputs through registers), A fragments are read with ldmatrix, and values are rounded to BF16
-// by the hardware conversion (round to nearest even, as bf16_bits).
-template <int KK, int NTL, int CP>
+// 16 x (8 RW) pixels, each warp RW rows of 16 (RW = 1 for maps too small to give every SM two
+// blocks of the usual height); its halo box is staged with cp.async (pooled inputs through
+// registers), A fragments are read with ldmatrix, and values are rounded to BF16 by the hardware
+// conversion (round to nearest even, as bf16_bits).
+template <int KK, int NTL, int CP, int RW = conv_h_rows(NTL)>
 __global__ void __launch_bounds__(CM_NT, 2) conv_h_kernel(ConvH p) {
     if (p.done && *p.done) return;
-    constexpr int RW = conv_h_rows(NTL), TH = 8 * RW;
+    constexpr int TH = 8 * RW;
     constexpr int R = KK == 9 ? 1 : 0, EW = CM_TX + 2 * R, EH = TH + 2 * R;
     constexpr int PS = CP + 8, KP = KK * CP, GROUPS = CP / 8, UNITS = EH * EW * GROUPS;
     constexpr int PER = (UNITS + CM_NT - 1) / CM_NT;

@@ -39,6 +39,10 @@ constexpr size_t CONV_MMA_SMEM_MAX = 160 * 1024;
     X(1, 1, 16) X(1, 1, 32) X(1, 1, 48) X(1, 1, 64) X(1, 2, 16) X(1, 2, 32) X(1, 2, 48) X(1, 2, 64) \
     X(1, 4, 16) X(1, 4, 32) X(1, 4, 48) X(1, 4, 64) X(1, 8, 16) X(1, 8, 32) X(1, 8, 48) X(1, 8, 64)
 constexpr int CONV_H_CP_MAX = 64;
+// Instantiations with one row of 16 pixels per warp (16 x 8 tiles), for 32-channel outputs on maps
+// whose usual tiles would give fewer than two blocks per SM (the coarse levels): taps x padded inputs.
+#define CONV_H1_FOR_ALL(X) X(9, 16) X(9, 32)
+constexpr int CONV_H1_MIN_BLOCKS = 2 * 148;
 // The decoder convolutions over concat(up(a), b) with the coarse-box staging: output tiles x
 // padded inputs x channels of a.
 #define CONV_UP_FOR_ALL(X) X(1, 32, 16) X(2, 32, 16) X(2, 48, 32) X(4, 48, 32) X(4, 64, 32) X(8, 64, 32)
@@ -57,6 +61,9 @@ inline cudaError_t conv_mma_configure() {
 #define CONV_H_PTR(KK_, NT_, CP_) (const void*)conv_h_kernel<KK_, NT_, CP_>,
                             CONV_H_FOR_ALL(CONV_H_PTR)
 #undef CONV_H_PTR
+#define CONV_H1_PTR(KK_, CP_) (const void*)conv_h_kernel<KK_, 4, CP_, 1>,
+                            CONV_H1_FOR_ALL(CONV_H1_PTR)
+#undef CONV_H1_PTR
 #define CONV_UP_PTR(NT_, CP_, CPA_) (const void*)conv_up_kernel<NT_, CP_, CPA_>,
                             CONV_UP_FOR_ALL(CONV_UP_PTR)
 #undef CONV_UP_PTR
@@ -125,6 +132,7 @@ struct LpcNet {
     // and every layer's tile within the shared-memory limit; set by configure_nhwc.
     bool nhwc = false;
     bool fuse_level0 = true;    // the first level's fused launches (conv_enc0_kernel, conv_dec0_kernel)
+    bool small_tiles = true;    // 16 x 8 tiles for 32-channel layers on maps too small for two blocks per SM
     const int* done = nullptr;  // the flexible CG's end flag: applications after it are skipped
     DBuf Xh, Yh, Fh[LPC_LEVELS], HIDh[LPC_LEVELS], Gh[LPC_LEVELS], Ah[LPC_LEVELS], Eh[LPC_LEVELS],
         DAh[LPC_LEVELS], Dh[LPC_LEVELS];
@@ -462,6 +470,18 @@ struct LpcNet {
             }
             CONV_UP_FOR_ALL(CONV_UP_LAUNCH)
 #undef CONV_UP_LAUNCH
+            if (launched) return cudaGetLastError();
+        }
+        if (nt == 4 && (size_t)grid.x * grid.y * grid.z < CONV_H1_MIN_BLOCKS && small_tiles) {
+            const size_t smem1 = conv_h_smem2(L.ci, 8 * nt, L.k * L.k, gate != nullptr, 1);
+            const dim3 grid1(grid.x, (p.H + 7) / 8, N);
+#define CONV_H1_LAUNCH(KK_, CP_)                                                   \
+            if (!launched && kk == KK_ && cp == CP_) {                              \
+                conv_h_kernel<KK_, 4, CP_, 1><<<grid1, CM_NT, smem1, st>>>(p);     \
+                launched = true;                                                    \
+            }
+            CONV_H1_FOR_ALL(CONV_H1_LAUNCH)
+#undef CONV_H1_LAUNCH
             if (launched) return cudaGetLastError();
         }
         const size_t smem = conv_h_smem2(L.ci, 8 * nt, L.k * L.k, gate != nullptr);

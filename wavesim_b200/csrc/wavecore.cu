@@ -2084,6 +2084,7 @@ wc_status wc_lpc_forward(wc_lpc* l, int32_t n, int32_t h, int32_t w, const float
     net.wq = m.wq.p;
     net.tensor = tensor != 0;
     net.fuse_level0 = tensor != 2;
+    net.small_tiles = tensor != 3;
     net.configure_nhwc();
     cudaStream_t st = m.st;
     if (net.tensor) {
@@ -2231,6 +2232,10 @@ wc_status wc_solver_set_lpc(wc_solver* s, wc_lpc* l) {
     s->lnet.wq = l->m.wq.p;
     s->lnet.gw = nullptr;
     s->lnet.tensor = true;  // the solve applies the network on the tensor cores
+    {
+        const char* v = std::getenv("WAVECORE_B200_LPC_SMALL_TILES");  // 0: usual tiles everywhere
+        s->lnet.small_tiles = !(v && std::strcmp(v, "0") == 0);
+    }
     s->lnet.configure_nhwc();
     CK(conv_mma_configure());
     CK(s->lnet.prepare_tensor(s->stream));

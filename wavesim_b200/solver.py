@@ -465,15 +465,17 @@ class LearnedPreconditioner:
                                               _fptr(g), _fptr(dx)))
         return y, g, dx
 
-    def forward(self, x, feat, tensor: bool = True, fused: bool = True):
+    def forward(self, x, feat, tensor: bool = True, fused: bool = True, small_tiles: bool = True):
         """The network's output on [n][2][h][w] arrays: BF16 tensor-core inference (as the solver
-        applies it; `fused=False` runs the first level one launch per layer) or the FP32 path
-        training uses."""
+        applies it; `fused=False` runs the first level one launch per layer, `small_tiles=False`
+        keeps the coarse levels' 32-channel layers on tiles of their usual height) or the FP32
+        path training uses."""
         x = np.ascontiguousarray(x, dtype=np.float32)
         feat = np.ascontiguousarray(feat, dtype=np.float32)
         n, c, h, w = x.shape
         y = np.zeros_like(x)
-        mode = (1 if fused else 2) if tensor else 0
+        mode = (1 if small_tiles else 3) if fused else 2
+        mode = mode if tensor else 0
         _check(load().wc_lpc_forward(self._handle, n, h, w, _fptr(x), _fptr(feat), mode, _fptr(y)))
         return y
 
