@@ -51,9 +51,11 @@ constexpr int CONV_H1_MIN_BLOCKS = 2 * 148;
 // The decoder kernels over concat(up(a), an 8-channel b): output tiles x channels of a.
 #define CONV_UP8_FOR_ALL(X) X(1, 16) X(1, 32) X(2, 16)
 
+// Once per process (a function-local static is initialised once, also when several host threads
+// reach it together); every call returns the first status.
 inline cudaError_t conv_mma_configure() {
-    static cudaError_t st = cudaErrorNotReady;
-    if (st == cudaErrorNotReady) {
+    static const cudaError_t status = [] {
+        cudaError_t st = cudaSuccess;
         const void* ks[] = {(const void*)conv_mma_kernel<9, 1>, (const void*)conv_mma_kernel<9, 2>,
                             (const void*)conv_mma_kernel<9, 4>, (const void*)conv_mma_kernel<9, 8>,
                             (const void*)conv_mma_kernel<1, 1>, (const void*)conv_mma_kernel<1, 2>,
@@ -75,12 +77,12 @@ inline cudaError_t conv_mma_configure() {
 #undef CONV_UP8_PTR
                             (const void*)conv_enc0_kernel, (const void*)conv_dec0_kernel<16>,
         };
-        st = cudaSuccess;
         for (const void* k : ks)
             if (st == cudaSuccess)
                 st = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CONV_MMA_SMEM_MAX);
-    }
-    return st;
+        return st;
+    }();
+    return status;
 }
 
 inline dim3 ew_grid(size_t n) {

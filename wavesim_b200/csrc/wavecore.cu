@@ -255,12 +255,8 @@ dim3 aux_grid(size_t n) {
     return dim3((unsigned)std::min<size_t>(std::max<size_t>(b, 1), 148 * 16));
 }
 
-// Configure every stage-kernel instantiation for its dynamic shared memory once per process.
-wc_status configure_kernels() {
-    static bool done = false;
-    static wc_status st = WC_OK;
-    if (done) return st;
-    done = true;
+// Configure every stage-kernel instantiation for its dynamic shared memory.
+wc_status configure_kernels_once() {
 #define ATTR(K, B) CK(cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, B))
     ATTR((stage_kernel<MODE_STAGE1, 1, false>), SMEM_SWE2);
     ATTR((stage_kernel<MODE_STAGE1, 2, false>), SMEM_SWE);
@@ -281,6 +277,14 @@ wc_status configure_kernels() {
     ATTR((ensemble_step_kernel<16, 2>), StageGeom<16>::SMEM_SGN);
 #undef ATTR
     return WC_OK;
+}
+
+// Once per process: a function-local static is initialised once, also when several host threads
+// (each with its own solver) reach it together, and every later call returns the first status.
+wc_status configure_kernels() {
+    static const wc_status st = configure_kernels_once();
+    if (st != WC_OK) return set_err(st, "setting the stage kernels' shared-memory limits failed");
+    return st;
 }
 
 StageArgs stage_args(const wc_solver* s, const float4* qin, const float4* qold, float4* qout, bool plus_dt) {
@@ -314,16 +318,16 @@ StageArgs stage_args(const wc_solver* s, const float4* qin, const float4* qold, 
 // {4 nx, ny}, rows 16 pitch bytes apart) and the bed ({nx, ny}, rows 4 pitch bytes apart), with
 // the boxes of StageGeom<ST_TY>. False if the driver's encoder is unavailable or refuses.
 bool stage_tensor_maps(const wc_solver* s, const float4* qin, CUtensorMap& tq, CUtensorMap& tb) {
-    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
-    static bool looked = false;
-    if (!looked) {
-        looked = true;
+    // looked up once per process (a function-local static is initialised once, even when several
+    // host threads, each with its own solver, reach it together)
+    static const PFN_cuTensorMapEncodeTiled_v12000 encode = [] {
         void* fn = nullptr;
         cudaDriverEntryPointQueryResult q{};
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
-    }
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            fn = nullptr;
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }();
     if (!encode) return false;
     using Gm = StageGeom<ST_TY>;
     const DevGrid& g = s->g;
