@@ -66,3 +66,43 @@ def test_invalid_grid_is_refused_without_a_gpu():
     bed = np.zeros(10)
     st = L.wc_solver_create(ctypes.byref(g), abi.dptr(bed), ctypes.byref(cfg), ctypes.byref(out))
     assert st == abi.WC_EINVAL
+
+
+def test_solver_creation_from_many_threads_reports_the_setup_error_in_each_thread():
+    """Solvers may be created from several host threads at once (one handle per thread). On a
+    host without a usable GPU the once-per-process kernel set-up fails: every thread gets that
+    status, on its first call and on later ones, each with its own error text."""
+    import threading
+
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("checks the set-up failure path of a host without a usable GPU")
+    from wavesim_b200 import Bathymetry, Grid, Solver, WavecoreError, abi
+
+    grid = Grid(64, 32, 2.0, 2.0)
+    bed = Bathymetry.flat(grid, 5.0)
+    results = [None] * 8
+    start = threading.Barrier(len(results))
+
+    def create(k):
+        start.wait()
+        out = []
+        for _ in range(2):
+            try:
+                Solver(grid, bed).check()
+                out.append(("created", ""))
+            except WavecoreError as e:
+                out.append((e.status, str(e)))
+        results[k] = out
+
+    threads = [threading.Thread(target=create, args=(k,)) for k in range(len(results))]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join(timeout=60)
+    for out in results:
+        assert out is not None and len(out) == 2
+        for status, text in out:
+            assert status == abi.WC_ECUDA
+            assert "shared-memory limits" in text
