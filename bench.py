@@ -1,13 +1,17 @@
 """Benchmark of wavecore's time step on B200: cell-steps/s with SGN on.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload config2|config3|config1]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload config3|config2|config4|config5|swe4096|config1]
+                    [--pc learned|jacobi] [--harvest beach|reef] [--lpc-channels 8,16,32,32]
     python bench.py --impl reference ...   # the reference algorithm on the host cores
 
 A step is one SSP-RK2 step of the whole grid (both stages, both dispersive solves); one
-cell-step is one interior cell advanced one step. The default workload is a 1024x512 grid at
-2 m: fifth order + SGN by Jacobi PCG to a relative residual of 1e-8, periodic in y, a seeded
-rough 1:30 beach, H = 2 m, T = 14 s (see wavesim_b200/workloads.py). The state starts as a
-linear wave train over the shelf, so every timed step carries the swell.
+cell-step is one interior cell advanced one step. The default workload is config 3: a 2048x1024
+grid at 2 m, fifth order + SGN to a relative residual of 1e-8, periodic in y, a seeded rough 1:30
+beach behind a 20 m shelf, H = 2 m, T = 14 s (see wavesim_b200/workloads.py). The state starts as
+a linear wave train over the shelf, so every timed step carries the swell. With the learned
+preconditioner (the default) the run first harvests systems from seeded runs of the workload's
+own family and trains the network on the GPU, then times the learned arm (`value`) and plain
+Jacobi PCG on the same workload (`plain_pcg`, `learned_vs_plain`).
 
 `value` is device-timed (CUDA events on the solver's stream, one step at a time, L2 flushed
 between steps by writing a 256 MiB buffer outside the timed events). `e2e` is the same metric
