@@ -6,7 +6,9 @@ to the FP64 oracle. Every random draw takes an explicit seed.
 
 Beds: a 1:30 plane beach behind a flat 20 m shelf plus a Gaussian random field
 (white noise filtered by exp(-|k|^2 l^2 / 4), i.e. convolved with exp(-r^2/l^2), scaled to the
-requested standard deviation; periodic in both directions, so it suits a periodic-y domain).
+requested standard deviation; periodic in both directions, so it suits a periodic-y domain);
+config 5's reef adds a Gaussian shoal whose crest is 1 m deep and takes a ridged field instead
+(`reef_bed`, also the bed of the smaller reef runs the learned preconditioner's training harvests).
 """
 from __future__ import annotations
 
